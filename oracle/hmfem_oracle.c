@@ -1,0 +1,715 @@
+/*
+ * hmfem_oracle.c -- CPU restatement of hmfem's pressure-solve path.
+ *
+ * TEST INFRASTRUCTURE ONLY (the correctness oracle and the CPU "port"
+ * baseline).  Never linked into, loaded by or called from the GPU product
+ * library.  Every function restates a reference routine; the citation is the
+ * file:line in the hmfem tree (toolbox paths relative to the tree root).
+ *
+ * Floating-point expressions keep the reference's evaluation order so that
+ * assembly, setup and transfer results are bit-identical to the reference
+ * compiled with the same flags (no FMA contraction: -ffp-contract=off).
+ */
+#include "hmfem_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define IDX(i, j, k) ((i) + (j) * nx + (k) * nxy)
+
+double or_hm(double a, double b) { return 2 * a * b / (a + b); }
+
+/* permeabilities.c:196-492 */
+void or_assemble(int nx, int ny, int nz, double hx, double hy, double hz,
+                 double visc, const double *KX, const double *KY,
+                 const double *KZ, const int bc_type[6], const double *KI,
+                 const double *WI, or_ele *perm, or_ind *indcol)
+{
+    const int nxy = nx * ny;
+    int i, j, k, s;
+    /* interior faces (permeabilities.c:214-293) */
+    for (k = 0; k < nz; k++)
+        for (j = 0; j < ny; j++)
+            for (i = 0; i < nx; i++) {
+                s = IDX(i, j, k);
+                if (j < ny - 1) {
+                    perm[s].u = or_hm(KY[s], KY[s + nx]);
+                    perm[s].u = perm[s].u / (hy * hy * visc);
+                    indcol[s].u = s + nx;
+                }
+                if (i < nx - 1) {
+                    perm[s].r = or_hm(KX[s], KX[s + 1]);
+                    perm[s].r = perm[s].r / (hx * hx * visc);
+                    indcol[s].r = s + 1;
+                }
+                if (j > 0) {
+                    perm[s].d = or_hm(KY[s], KY[s - nx]);
+                    perm[s].d = perm[s].d / (hy * hy * visc);
+                    indcol[s].d = s - nx;
+                }
+                if (i > 0) {
+                    perm[s].l = or_hm(KX[s], KX[s - 1]);
+                    perm[s].l = perm[s].l / (hx * hx * visc);
+                    indcol[s].l = s - 1;
+                }
+                if (k < nz - 1) {
+                    perm[s].t = or_hm(KZ[s], KZ[s + nxy]);
+                    perm[s].t = perm[s].t / (hz * hz * visc);
+                    indcol[s].t = s + nxy;
+                }
+                if (k > 0) {
+                    perm[s].b = or_hm(KZ[s], KZ[s - nxy]);
+                    perm[s].b = perm[s].b / (hz * hz * visc);
+                    indcol[s].b = s - nxy;
+                }
+            }
+    /* boundary faces (permeabilities.c:297-477): Dirichlet 2K/(h^2 mu),
+     * Neumann 0; both go to the right-hand side (indcol = -1). */
+    for (k = 0; k < nz; k++)
+        for (j = 0; j < ny; j++) {
+            s = IDX(0, j, k);
+            perm[s].l = bc_type[0] == 0 ? 2.0 * KX[s] / (hx * hx * visc) : 0;
+            indcol[s].l = -1;
+            s = IDX(nx - 1, j, k);
+            perm[s].r = bc_type[1] == 0 ? 2.0 * KX[s] / (hx * hx * visc) : 0;
+            indcol[s].r = -1;
+        }
+    if (bc_type[0] == 1 && bc_type[1] == 1 && bc_type[2] == 1 &&
+        bc_type[3] == 1 && bc_type[4] == 1 && bc_type[5] == 1) {
+        /* all-Neumann: one Dirichlet face pins the pressure
+         * (permeabilities.c:327-333) */
+        s = IDX(0, ny - 1, nz / 2);
+        perm[s].l = 2.0 * KX[s] / (hx * hx * visc);
+        indcol[s].l = -1;
+    }
+    for (k = 0; k < nz; k++)
+        for (i = 0; i < nx; i++) {
+            s = IDX(i, 0, k);
+            perm[s].d = bc_type[3] == 0 ? 2.0 * KY[s] / (hy * hy * visc) : 0;
+            indcol[s].d = -1;
+            s = IDX(i, ny - 1, k);
+            perm[s].u = bc_type[2] == 0 ? 2.0 * KY[s] / (hy * hy * visc) : 0;
+            indcol[s].u = -1;
+        }
+    for (j = 0; j < ny; j++)
+        for (i = 0; i < nx; i++) {
+            s = IDX(i, j, nz - 1);
+            perm[s].t = bc_type[4] == 0 ? 2.0 * KZ[s] / (hz * hz * visc) : 0;
+            indcol[s].t = -1;
+            s = IDX(i, j, 0);
+            perm[s].b = bc_type[5] == 0 ? 2.0 * KZ[s] / (hz * hz * visc) : 0;
+            indcol[s].b = -1;
+        }
+    /* centre (permeabilities.c:480-489) */
+    for (s = 0; s < nx * ny * nz; s++) {
+        double ki = KI ? KI[s] : 0.0, wi = WI ? WI[s] : 0.0;
+        perm[s].c = perm[s].l + perm[s].r + perm[s].u + perm[s].d +
+                    perm[s].t + perm[s].b + ki / (visc * hx * hy * hz) +
+                    wi / (visc * hx * hy * hz);
+        indcol[s].c = s;
+    }
+}
+
+/* set_source_term.c:9-223; faces in the reference's interface order
+ * L, R, D, U, T, B. */
+void or_source_term(int nx, int ny, int nz, double hx, double hy, double hz,
+                    double visc, const or_bound *B, const int bc_type[6],
+                    const or_ele *perm, const double *KI, const double *WI,
+                    const double *pc, const double *pw, double *b)
+{
+    const int nxy = nx * ny;
+    int i, j, k, s;
+    for (j = 0; j < ny; j++)
+        for (k = 0; k < nz; k++) {
+            s = IDX(0, j, k);
+            int l = k * ny + j;
+            if (bc_type[0] == 0) b[s] = b[s] + (perm[s].l) * B->l[l];
+            if (bc_type[0] == 1) b[s] = b[s] + B->l[l] / hx;
+        }
+    if (bc_type[0] == 1 && bc_type[1] == 1 && bc_type[2] == 1 &&
+        bc_type[3] == 1 && bc_type[4] == 1 && bc_type[5] == 1) {
+        s = IDX(0, ny - 1, nz / 2);
+        b[s] = b[s] + (perm[s].l) * 1.0;
+    }
+    for (j = 0; j < ny; j++)
+        for (k = 0; k < nz; k++) {
+            s = IDX(nx - 1, j, k);
+            int l = k * ny + j;
+            if (bc_type[1] == 0) b[s] = b[s] + perm[s].r * B->r[l];
+            if (bc_type[1] == 1) b[s] = b[s] - B->r[l] / hx;
+        }
+    for (i = 0; i < nx; i++)
+        for (k = 0; k < nz; k++) {
+            s = IDX(i, 0, k);
+            int l = k * nx + i;
+            if (bc_type[3] == 0) b[s] = b[s] + perm[s].d * B->d[l];
+            if (bc_type[3] == 1) b[s] = b[s] + B->d[l] / hy;
+        }
+    for (i = 0; i < nx; i++)
+        for (k = 0; k < nz; k++) {
+            s = IDX(i, ny - 1, k);
+            int l = k * nx + i;
+            if (bc_type[2] == 0) b[s] = b[s] + perm[s].u * B->u[l];
+            if (bc_type[2] == 1) b[s] = b[s] - B->u[l] / hy;
+        }
+    for (i = 0; i < nx; i++)
+        for (j = 0; j < ny; j++) {
+            s = IDX(i, j, nz - 1);
+            int l = j * nx + i;
+            if (bc_type[4] == 0) b[s] = b[s] + perm[s].t * B->t[l];
+            if (bc_type[4] == 1) b[s] = b[s] - B->t[l] / hz;
+        }
+    for (i = 0; i < nx; i++)
+        for (j = 0; j < ny; j++) {
+            s = IDX(i, j, 0);
+            int l = j * nx + i;
+            if (bc_type[5] == 0) b[s] = b[s] + perm[s].b * B->b[l];
+            if (bc_type[5] == 1) b[s] = b[s] + B->b[l] / hz;
+        }
+    /* sources (set_source_term.c:206-220) */
+    double Ve = hx * hy * hz;
+    for (s = 0; s < nx * ny * nz; s++) {
+        double ki = KI ? KI[s] : 0.0, wi = WI ? WI[s] : 0.0;
+        double pcs = pc ? pc[s] : 0.0, pws = pw ? pw[s] : 0.0;
+        b[s] = b[s] + (ki * pcs) / (visc * Ve) + (wi * pws) / (visc * Ve);
+    }
+}
+
+/* solve_linearsystem_AMG.c:55-141 */
+long or_pack_csr(int n, const or_ele *perm, const or_ind *indcol, int *cnt,
+                 int *col, double *ele)
+{
+    long l = 0;
+    for (int s = 0; s < n; s++) {
+        int c = 0;
+#define PUT(f, v)                                                            \
+    if (indcol[s].f != -1) {                                                 \
+        if (col) { col[l] = indcol[s].f; ele[l] = (v); }                     \
+        l++; c++;                                                            \
+    }
+        PUT(d, -perm[s].d)
+        PUT(l, -perm[s].l)
+        PUT(c, perm[s].c)
+        PUT(r, -perm[s].r)
+        PUT(u, -perm[s].u)
+        PUT(t, -perm[s].t)
+        PUT(b, -perm[s].b)
+#undef PUT
+        if (cnt) cnt[s] = c;
+    }
+    return l;
+}
+
+/* ---------------------------------------------------------------- AMG -- */
+
+static long *offsets(int n, const int *cnt)
+{
+    long *dsp = (long *)malloc(sizeof(long) * (n + 1));
+    dsp[0] = 0;
+    for (int i = 0; i < n; i++) dsp[i + 1] = dsp[i] + cnt[i];
+    return dsp;
+}
+
+/* node_selection (toolbox.h / amg.h:1-32) for one rank: bou = true. */
+static void node_select(char sel, int n, const int *cnt, const long *dsp,
+                        const int *col, const char *cox, char *asel)
+{
+    for (int i = 0; i < n; i++) {
+        if (asel[i] != sel) continue;
+        if (sel == 0) asel[i] = 1; /* master (C) node */
+        for (long j = dsp[i]; j < dsp[i] + cnt[i]; j++) {
+            int c = col[j];
+            if (asel[c] != 0) continue;
+            for (long k = dsp[c]; k < dsp[c] + cnt[c]; k++)
+                if (col[k] == i && cox[k] != 0) { asel[c] = 2; break; }
+        }
+    }
+}
+
+/* sparse_multiply_transpose (amg.h:408-563, the active #else branch):
+ * C = (A B)^T with B having `bcols` columns.  Columns of each C row come out
+ * ascending (A's row index). */
+static void spmt(int arows, const int *acnt, const int *acol,
+                 const double *aele, int brows, const int *bcnt,
+                 const int *bcol, const double *bele, int bcols, int **ccnt_o,
+                 int **ccol_o, double **cele_o, long *csize_o)
+{
+    long *bdsp = offsets(brows, bcnt);
+    int *ccnt = (int *)calloc(bcols > 0 ? bcols : 1, sizeof(int));
+    int *clst = (int *)malloc(sizeof(int) * (bcols > 0 ? bcols : 1));
+    for (int i = 0; i < bcols; i++) clst[i] = -1;
+    long csize = 0, m = 0;
+    for (int i = 0; i < arows; i++)
+        for (int j = 0; j < acnt[i]; j++) {
+            int c = acol[m++];
+            for (long k = bdsp[c]; k < bdsp[c] + bcnt[c]; k++) {
+                int d = bcol[k];
+                if (clst[d] != i) { clst[d] = i; ccnt[d]++; csize++; }
+            }
+        }
+    for (int i = 0; i < bcols; i++) clst[i] = -1;
+    long *cdsp = (long *)malloc(sizeof(long) * (bcols > 0 ? bcols : 1));
+    for (long t = 0, i = 0; i < bcols; i++) { cdsp[i] = t; t += ccnt[i]; }
+    int *ccol = (int *)malloc(sizeof(int) * (csize > 0 ? csize : 1));
+    double *cele = (double *)malloc(sizeof(double) * (csize > 0 ? csize : 1));
+    m = 0;
+    for (int i = 0; i < arows; i++)
+        for (int j = 0; j < acnt[i]; j++) {
+            int c = acol[m];
+            double s = aele[m];
+            m++;
+            for (long k = bdsp[c]; k < bdsp[c] + bcnt[c]; k++) {
+                int d = bcol[k];
+                long e = cdsp[d];
+                double t = s * bele[k];
+                if (clst[d] != i) {
+                    clst[d] = i;
+                    ccol[e] = i;
+                    cele[e] = t;
+                    cdsp[d] = e + 1;
+                } else {
+                    cele[e - 1] += t;
+                }
+            }
+        }
+    free(bdsp); free(clst); free(cdsp);
+    *ccnt_o = ccnt; *ccol_o = ccol; *cele_o = cele; *csize_o = csize;
+}
+
+/* One coarsening step: parallel_coarsening (amg.h:37-223), then
+ * parallel_interpolation (amg.h:228-406), then new_triple_product
+ * (amg.h:567-582), for a single rank (no interface nodes). */
+static void coarsen_level(double eps, or_level *A, or_level *Cn)
+{
+    int n = A->n;
+    long *dsp = offsets(n, A->cnt);
+    /* diagonal: last stored diagonal entry (amg.h:159-166) */
+    double *dia = (double *)calloc(n, sizeof(double));
+    for (int i = 0; i < n; i++)
+        for (long j = dsp[i]; j < dsp[i] + A->cnt[i]; j++)
+            if (A->col[j] == i) dia[i] = A->ele[j];
+    /* strength (amg.h:167-193): |a_ij| >= |eps a_ii| */
+    char *cox = (char *)malloc(A->nnz > 0 ? A->nnz : 1);
+    for (int i = 0; i < n; i++) {
+        double sda = fabs(eps * dia[i]);
+        for (long j = dsp[i]; j < dsp[i] + A->cnt[i]; j++)
+            cox[j] = fabs(A->ele[j]) >= sda ? 1 : 0;
+    }
+    /* phases (b) and (c) (amg.h:219-223) */
+    char *sel = (char *)calloc(n, 1);
+    node_select(1, n, A->cnt, dsp, A->col, cox, sel);
+    node_select(0, n, A->cnt, dsp, A->col, cox, sel);
+    A->sel = sel;
+    /* interpolation (amg.h:326-387) */
+    int *pcnt = (int *)calloc(n, sizeof(int));
+    for (int i = 0; i < n; i++) {
+        if (sel[i] == 1) { pcnt[i] = 1; continue; }
+        for (long j = dsp[i]; j < dsp[i] + A->cnt[i]; j++)
+            if (sel[A->col[j]] == 1 && cox[j] != 0) pcnt[i]++;
+    }
+    long pnnz = 0;
+    for (int i = 0; i < n; i++) pnnz += pcnt[i];
+    int *pcol = (int *)malloc(sizeof(int) * (pnnz > 0 ? pnnz : 1));
+    double *pele = (double *)malloc(sizeof(double) * (pnnz > 0 ? pnnz : 1));
+    long m = 0;
+    for (int i = 0; i < n; i++) {
+        if (sel[i] == 1) { pcol[m] = i; pele[m] = 1.0; m++; continue; }
+        for (long j = dsp[i]; j < dsp[i] + A->cnt[i]; j++)
+            if (sel[A->col[j]] == 1 && cox[j] != 0) {
+                pcol[m] = A->col[j];
+                pele[m] = 1.0 / pcnt[i];
+                m++;
+            }
+    }
+    /* coarse numbering: ascending order of the fine ids that appear in P
+     * (amg.h:394-403, binary_sort_copy + unique_resize) */
+    int *cid = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+    for (int i = 0; i < n; i++) cid[i] = 0;
+    for (long q = 0; q < pnnz; q++) cid[pcol[q]] = 1;
+    int nc = 0;
+    for (int i = 0; i < n; i++) { int a = cid[i]; cid[i] = a ? nc : -1; nc += a; }
+    for (long q = 0; q < pnnz; q++) pcol[q] = cid[pcol[q]];
+    A->pcnt = pcnt; A->pcol = pcol; A->pele = pele; A->pnnz = pnnz;
+    /* Galerkin product P^T A P as two (X P)^T passes (amg.h:567-582) */
+    int *tcnt, *tcol; double *tele; long tsize;
+    spmt(n, A->cnt, A->col, A->ele, n, pcnt, pcol, pele, nc, &tcnt, &tcol,
+         &tele, &tsize);
+    int *ccnt, *ccol; double *cele; long csize;
+    spmt(nc, tcnt, tcol, tele, n, pcnt, pcol, pele, nc, &ccnt, &ccol, &cele,
+         &csize);
+    free(tcnt); free(tcol); free(tele);
+    Cn->n = nc; Cn->nnz = csize; Cn->cnt = ccnt; Cn->col = ccol; Cn->ele = cele;
+    /* 1/diag on this level (amg.h:1195) */
+    A->dinv = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+    for (int i = 0; i < n; i++) A->dinv[i] = 1.0 / dia[i];
+    free(dia); free(cox); free(cid); free(dsp);
+}
+
+int or_amg_setup(int n, const int *cnt, const int *col, const double *ele,
+                 int max_level, int max_size, double eps, or_hierarchy *H)
+{
+    memset(H, 0, sizeof(*H));
+    if (max_level > OR_MAX_LEVELS) max_level = OR_MAX_LEVELS;
+    or_level *L0 = &H->lv[0];
+    long nnz = 0;
+    for (int i = 0; i < n; i++) nnz += cnt[i];
+    L0->n = n; L0->nnz = nnz;
+    L0->cnt = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+    L0->col = (int *)malloc(sizeof(int) * (nnz > 0 ? nnz : 1));
+    L0->ele = (double *)malloc(sizeof(double) * (nnz > 0 ? nnz : 1));
+    memcpy(L0->cnt, cnt, sizeof(int) * n);
+    memcpy(L0->col, col, sizeof(int) * nnz);
+    memcpy(L0->ele, ele, sizeof(double) * nnz);
+    /* level loop (amg.h:1188-1213) */
+    int l = 0, gcnt = n;
+    double rel = 0.0;
+    while (l < max_level - 1 && gcnt > max_size && rel < 1.0) {
+        coarsen_level(eps, &H->lv[l], &H->lv[l + 1]);
+        l++;
+        int gold = gcnt;
+        gcnt = H->lv[l].n;
+        rel = (double)gcnt / (double)gold;
+    }
+    /* coarsest level: 1/diag (amg.h:1214-1226) */
+    or_level *C = &H->lv[l];
+    C->dinv = (double *)malloc(sizeof(double) * (C->n > 0 ? C->n : 1));
+    for (long t = 0, i = 0; i < C->n; i++) {
+        double d = 0.0;
+        int have = 0;
+        for (int j = 0; j < C->cnt[i]; j++, t++)
+            if (C->col[t] == i) { d = C->ele[t]; have = 1; }
+        C->dinv[i] = have ? 1.0 / d : 1.0 / 0.0;
+    }
+    H->nlevels = l + 1;
+    return H->nlevels;
+}
+
+void or_amg_free(or_hierarchy *H)
+{
+    for (int l = 0; l < H->nlevels; l++) {
+        or_level *A = &H->lv[l];
+        free(A->cnt); free(A->col); free(A->ele); free(A->dinv);
+        free(A->sel); free(A->pcnt); free(A->pcol); free(A->pele);
+    }
+    memset(H, 0, sizeof(*H));
+}
+
+int or_level_info(const or_hierarchy *H, int l, int *n, long *nnz, long *pnnz)
+{
+    if (l < 0 || l >= H->nlevels) return -1;
+    *n = H->lv[l].n;
+    *nnz = H->lv[l].nnz;
+    *pnnz = l < H->nlevels - 1 ? H->lv[l].pnnz : 0;
+    return 0;
+}
+
+or_hierarchy *or_amg_create(int n, const int *cnt, const int *col,
+                            const double *ele, int max_level, int max_size,
+                            double eps)
+{
+    or_hierarchy *H = (or_hierarchy *)malloc(sizeof(or_hierarchy));
+    or_amg_setup(n, cnt, col, ele, max_level, max_size, eps, H);
+    return H;
+}
+
+void or_amg_destroy(or_hierarchy *H)
+{
+    if (!H) return;
+    or_amg_free(H);
+    free(H);
+}
+
+int or_amg_nlevels(const or_hierarchy *H) { return H->nlevels; }
+
+int or_level_copy(const or_hierarchy *H, int l, int *cnt, int *col,
+                  double *ele, double *dinv, char *sel, int *pcnt, int *pcol,
+                  double *pele)
+{
+    if (l < 0 || l >= H->nlevels) return -1;
+    const or_level *A = &H->lv[l];
+    memcpy(cnt, A->cnt, sizeof(int) * A->n);
+    memcpy(col, A->col, sizeof(int) * A->nnz);
+    memcpy(ele, A->ele, sizeof(double) * A->nnz);
+    memcpy(dinv, A->dinv, sizeof(double) * A->n);
+    if (l < H->nlevels - 1) {
+        memcpy(sel, A->sel, A->n);
+        memcpy(pcnt, A->pcnt, sizeof(int) * A->n);
+        memcpy(pcol, A->pcol, sizeof(int) * A->pnnz);
+        memcpy(pele, A->pele, sizeof(double) * A->pnnz);
+    }
+    return 0;
+}
+
+/* generic_operator.h:212-247 */
+void or_spmv(int n, const int *cnt, const int *col, const double *ele,
+             const double *x, double *y)
+{
+    long m = 0;
+    for (int i = 0; i < n; i++) {
+        double s = 0.0;
+        for (int j = 0; j < cnt[i]; j++, m++) s += ele[m] * x[col[m]];
+        y[i] = s;
+    }
+}
+
+/* simple_restriction (generic_operator.h:68-129): s = P^T u with 1/c */
+static void restrict_simple(const or_level *A, int nc, const double *u,
+                            double *s)
+{
+    for (int i = 0; i < nc; i++) s[i] = 0.0;
+    long m = 0;
+    for (int i = 0; i < A->n; i++) {
+        int c = A->pcnt[i];
+        if (c == 0) continue;
+        double t = c == 1 ? u[i] : u[i] / (double)c;
+        for (int j = 0; j < c; j++) s[A->pcol[m++]] += t;
+    }
+}
+
+/* simple_prolongation (generic_operator.h:7-66): s = P u (average) */
+static void prolong_simple(const or_level *A, const double *u, double *s)
+{
+    long m = 0;
+    for (int i = 0; i < A->n; i++) {
+        int c = A->pcnt[i];
+        if (c == 0) continue;
+        if (c == 1) { s[i] = u[A->pcol[m++]]; continue; }
+        double t = u[A->pcol[m++]];
+        for (int j = 1; j < c; j++) t += u[A->pcol[m++]];
+        s[i] = t / (double)c;
+    }
+}
+
+typedef struct { double *u, *f, *s, *r; } or_work;
+
+static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
+               double omega)
+{
+    const or_level *A = &H->lv[l];
+    int n = A->n;
+    double *u = W[l].u, *f = W[l].f, *s = W[l].s, *r = W[l].r;
+    if (l == H->nlevels - 1) {
+        /* diagonal_solver (amg.h:1074-1097) */
+        for (int i = 0; i < n; i++) u[i] = A->dinv[i] * f[i];
+        return;
+    }
+    if (smoother == 0) {
+        /* gauss_seidel_f 3-arg (amg.h:759-784) */
+        for (int i = 0; i < n; i++) r[i] = f[i];
+        long m = 0;
+        for (int i = 0; i < n; i++) {
+            double t = A->dinv[i] * r[i];
+            u[i] = t;
+            for (int j = 0; j < A->cnt[i]; j++, m++) r[A->col[m]] -= A->ele[m] * t;
+        }
+    } else {
+        /* device_jacobi 3-arg (device_amg.h:35-42): u = w D^-1 f; r = f - A u */
+        for (int i = 0; i < n; i++) u[i] = omega * f[i] * A->dinv[i];
+        long m = 0;
+        for (int i = 0; i < n; i++) {
+            double t = f[i];
+            for (int j = 0; j < A->cnt[i]; j++, m++) t -= A->ele[m] * u[A->col[m]];
+            r[i] = t;
+        }
+    }
+    restrict_simple(A, H->lv[l + 1].n, r, W[l + 1].f);
+    mg(H, W, l + 1, smoother, omega);
+    prolong_simple(A, W[l + 1].u, s);
+    if (smoother == 0) {
+        /* gauss_seidel_b 3-arg (amg.h:930-961) */
+        for (int i = 0; i < n; i++) u[i] += s[i];
+        long m = A->nnz;
+        for (int i = n - 1; i >= 0; i--) {
+            double t = f[i];
+            for (int j = 0; j < A->cnt[i]; j++) {
+                m--;
+                t -= A->ele[m] * u[A->col[m]];
+            }
+            u[i] += t * A->dinv[i];
+        }
+    } else {
+        /* add, then device_jacobi 2-arg (device_amg.h:27-34, 411-412) */
+        for (int i = 0; i < n; i++) u[i] += s[i];
+        long m = 0;
+        for (int i = 0; i < n; i++) {
+            double t = f[i];
+            for (int j = 0; j < A->cnt[i]; j++, m++) t -= A->ele[m] * u[A->col[m]];
+            r[i] = t;
+        }
+        for (int i = 0; i < n; i++) u[i] += omega * r[i] * A->dinv[i];
+    }
+}
+
+static or_work *work_alloc(const or_hierarchy *H)
+{
+    or_work *W = (or_work *)calloc(H->nlevels, sizeof(or_work));
+    for (int l = 0; l < H->nlevels; l++) {
+        int n = H->lv[l].n > 0 ? H->lv[l].n : 1;
+        W[l].u = (double *)calloc(n, sizeof(double));
+        W[l].f = (double *)calloc(n, sizeof(double));
+        W[l].s = (double *)calloc(n, sizeof(double));
+        W[l].r = (double *)calloc(n, sizeof(double));
+    }
+    return W;
+}
+
+static void work_free(const or_hierarchy *H, or_work *W)
+{
+    for (int l = 0; l < H->nlevels; l++) {
+        free(W[l].u); free(W[l].f); free(W[l].s); free(W[l].r);
+    }
+    free(W);
+}
+
+void or_vcycle(const or_hierarchy *H, int smoother, double omega,
+               const double *f, double *u)
+{
+    or_work *W = work_alloc(H);
+    memcpy(W[0].f, f, sizeof(double) * H->lv[0].n);
+    mg(H, W, 0, smoother, omega);
+    memcpy(u, W[0].u, sizeof(double) * H->lv[0].n);
+    work_free(H, W);
+}
+
+static double dot(int n, const double *x, const double *y)
+{
+    double s = 0.0;
+    for (int i = 0; i < n; i++) s += x[i] * y[i];
+    return s;
+}
+
+static double true_relres(const or_level *A, const double *b, const double *x,
+                          double *tmp)
+{
+    or_spmv(A->n, A->cnt, A->col, A->ele, x, tmp);
+    double rr = 0.0, bb = 0.0;
+    for (int i = 0; i < A->n; i++) {
+        double d = b[i] - tmp[i];
+        rr += d * d;
+        bb += b[i] * b[i];
+    }
+    return bb > 0 ? sqrt(rr / bb) : sqrt(rr);
+}
+
+/* conjugate_gradient::operator() (pcg.h:33-76) */
+int or_pcg(const or_hierarchy *H, int smoother, double omega, const double *b,
+           double *x, double eps, int max_it, int stop, double *relres)
+{
+    const or_level *A = &H->lv[0];
+    int n = A->n;
+    or_work *W = work_alloc(H);
+    double *r = (double *)malloc(sizeof(double) * n);
+    double *s = (double *)malloc(sizeof(double) * n);
+    double *v = (double *)malloc(sizeof(double) * n);
+    double *tmp = (double *)malloc(sizeof(double) * n);
+    memcpy(r, b, sizeof(double) * n);
+    memcpy(s, x, sizeof(double) * n);
+    or_spmv(n, A->cnt, A->col, A->ele, s, v);
+    for (int i = 0; i < n; i++) r[i] -= v[i] * 1.0;
+#define PREC(rin, vout)                                                      \
+    do {                                                                     \
+        memcpy(W[0].f, rin, sizeof(double) * n);                             \
+        mg(H, W, 0, smoother, omega);                                        \
+        memcpy(vout, W[0].u, sizeof(double) * n);                            \
+    } while (0)
+    PREC(r, v);
+    double sigma = dot(n, v, r);
+    if (sigma < 0.0) sigma = fabs(sigma);
+    for (int i = 0; i < n; i++) s[i] = s[i] * 0.0 + v[i];
+    double sigma_last = sigma, sigma_first = sigma;
+    if (sigma == 0.0) sigma_first = 1.0;
+    double tau = sigma / sigma_first;
+    double rel = stop == 1 ? true_relres(A, b, x, tmp) : 0.0;
+    int loop = 0;
+    while (++loop < max_it &&
+           (stop == 1 ? rel > eps : tau > eps * eps)) {
+        or_spmv(n, A->cnt, A->col, A->ele, s, v);
+        tau = dot(n, s, v);
+        if (tau < 0.0) tau = fabs(tau);
+        double alpha = sigma / tau;
+        for (int i = 0; i < n; i++) x[i] += s[i] * alpha;
+        for (int i = 0; i < n; i++) r[i] -= v[i] * alpha;
+        PREC(r, v);
+        sigma = dot(n, v, r);
+        if (sigma < 0.0) sigma = fabs(sigma);
+        double beta = sigma / sigma_last;
+        for (int i = 0; i < n; i++) s[i] = s[i] * beta + v[i];
+        sigma_last = sigma;
+        tau = sigma / sigma_first;
+        if (stop == 1) rel = true_relres(A, b, x, tmp);
+    }
+#undef PREC
+    if (relres) *relres = true_relres(A, b, x, tmp);
+    free(r); free(s); free(v); free(tmp);
+    work_free(H, W);
+    return loop;
+}
+
+/* compute.cpp:7-51 (epsilon 0, omega 1, 16 levels, min 1 node, GS) */
+int or_compute(const int *hdr, const int *cnt, const int *col,
+               const double *ele, const double *b, double *x, double eps,
+               int stop, int *iters, double *relres)
+{
+    or_hierarchy H;
+    or_amg_setup(hdr[0], cnt, col, ele, 16, 1, 0.0, &H);
+    int it = or_pcg(&H, 0, 1.0, b, x, eps, 10000, stop, relres);
+    if (iters) *iters = it;
+    or_amg_free(&H);
+    return 0;
+}
+
+/* flux_reconstruction.c:9-319 */
+void or_fluxes(int nx, int ny, int nz, double hx, double hy, double hz,
+               const double *p, const or_ele *perm, const or_bound *B,
+               const int bc_type[6], or_ele *v, double *divmin,
+               double *divmax)
+{
+    const int nxy = nx * ny;
+    int i, j, k, s;
+    for (k = 0; k < nz; k++)
+        for (j = 0; j < ny; j++)
+            for (i = 0; i < nx; i++) {
+                s = IDX(i, j, k);
+                if (j < ny - 1) v[s].u = hy * perm[s].u * (p[s] - p[s + nx]);
+                if (i < nx - 1) v[s].r = hx * perm[s].r * (p[s] - p[s + 1]);
+                if (j > 0) v[s].d = hy * perm[s].d * (p[s] - p[s - nx]);
+                if (i > 0) v[s].l = hx * perm[s].l * (p[s] - p[s - 1]);
+                if (k < nz - 1) v[s].t = hz * perm[s].t * (p[s] - p[s + nxy]);
+                if (k > 0) v[s].b = hz * perm[s].b * (p[s] - p[s - nxy]);
+            }
+    for (j = 0; j < ny; j++)
+        for (k = 0; k < nz; k++) {
+            int l = k * ny + j;
+            s = IDX(0, j, k);
+            v[s].l = bc_type[0] == 0 ? hx * perm[s].l * (p[s] - B->l[l]) : -B->l[l];
+            s = IDX(nx - 1, j, k);
+            v[s].r = bc_type[1] == 0 ? hx * perm[s].r * (p[s] - B->r[l]) : B->r[l];
+        }
+    for (i = 0; i < nx; i++)
+        for (k = 0; k < nz; k++) {
+            int l = k * nx + i;
+            s = IDX(i, 0, k);
+            v[s].d = bc_type[3] == 0 ? hy * perm[s].d * (p[s] - B->d[l]) : -B->d[l];
+            s = IDX(i, ny - 1, k);
+            v[s].u = bc_type[2] == 0 ? hy * perm[s].u * (p[s] - B->u[l]) : B->u[l];
+        }
+    for (i = 0; i < nx; i++)
+        for (j = 0; j < ny; j++) {
+            int l = j * nx + i;
+            s = IDX(i, j, nz - 1);
+            v[s].t = bc_type[4] == 0 ? hz * perm[s].t * (p[s] - B->t[l]) : B->t[l];
+            s = IDX(i, j, 0);
+            v[s].b = bc_type[5] == 0 ? hz * perm[s].b * (p[s] - B->b[l]) : -B->b[l];
+        }
+    /* divvel_pontual (flux_reconstruction.c:281-319) */
+    double mx = 0.0, mn = 100.0;
+    for (s = 0; s < nx * ny * nz; s++) {
+        double dv = v[s].r / hx + v[s].l / hx + v[s].d / hy + v[s].u / hy +
+                    v[s].b / hz + v[s].t / hz;
+        if (fabs(dv) > mx) mx = fabs(dv);
+        if (fabs(dv) < mn) mn = fabs(dv);
+    }
+    if (divmin) *divmin = mn;
+    if (divmax) *divmax = mx;
+}

@@ -1,0 +1,133 @@
+/*
+ * hmfem_oracle.h -- CPU restatement of hmfem's pressure-solve path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the correctness oracle: plain C, single
+ * threaded, following the reference algorithm step by step (each function
+ * cites the reference file:line it restates).  Only tests/, the smoke check
+ * and the bench's cpu_baseline leg may load it, and only as the checker or
+ * the timed CPU baseline.  The GPU product path never calls into it.
+ *
+ * Parity pinning: this restatement is checked against fixtures produced by
+ * the reference's own sources (compiled by oracle/Makefile into oracle/_ref/
+ * from the reference tree) -- see tests/golden/make_golden.py.
+ */
+#ifndef HMFEM_ORACLE_H
+#define HMFEM_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Layout-identical to the reference's ELE (structs.h:7-17) and IND
+ * (structs.h:38-48). */
+typedef struct { double u, d, l, r, c, t, b; } or_ele;
+typedef struct { int c, u, d, l, r, t, b; } or_ind;
+
+/* Face order used for boundary descriptions everywhere in this project:
+ * 0=l (x-), 1=r (x+), 2=u (y+), 3=d (y-), 4=t (z+), 5=b (z-) -- the order of
+ * val_bound[1..6] in main.c:140-145 / set_boundaries.c:8-40.
+ * bc_type: 0 = Dirichlet, 1 = Neumann (main.c:347-350). */
+
+/* Face-value arrays, one per face, indexed like the reference's Bound
+ * (pyzindex for l/r, pxzindex for u/d, pxyindex for t/b;
+ * solve_linearsystem_AMG.c:22-35). */
+typedef struct { const double *l, *r, *u, *d, *t, *b; } or_bound;
+
+/* permeabilities.c:188-193 */
+double or_hm(double a, double b);
+
+/* permeabilities.c:196-492 (permeabilidade_arestas). KI/WI may be NULL (0). */
+void or_assemble(int nx, int ny, int nz, double hx, double hy, double hz,
+                 double visc, const double *KX, const double *KY,
+                 const double *KZ, const int bc_type[6], const double *KI,
+                 const double *WI, or_ele *perm, or_ind *indcol);
+
+/* set_source_term.c:9-223 (source_term). b must be zero-initialised by the
+ * caller (reservoir.c:15).  KI/WI/pc/pw may be NULL (0). */
+void or_source_term(int nx, int ny, int nz, double hx, double hy, double hz,
+                    double visc, const or_bound *B, const int bc_type[6],
+                    const or_ele *perm, const double *KI, const double *WI,
+                    const double *pc, const double *pw, double *b);
+
+/* solve_linearsystem_AMG.c:37-157: AoS stencil -> count/col/ele (row order
+ * d,l,c,r,u,t,b).  Returns nnz; cnt/col/ele may be NULL for a count pass. */
+long or_pack_csr(int n, const or_ele *perm, const or_ind *indcol, int *cnt,
+                 int *col, double *ele);
+
+/* One AMG level (toolbox/inverse_operator/amg.h:1099-1239). */
+typedef struct {
+    int n;
+    long nnz;
+    int *cnt, *col;       /* row counts, row-concatenated columns */
+    double *ele;          /* values */
+    double *dinv;         /* 1 / (last stored diagonal entry) */
+    /* transfer to the next level (absent on the coarsest level) */
+    char *sel;            /* 1 = C, 2 = F (amg.h:1-32) */
+    long pnnz;
+    int *pcnt, *pcol;     /* P rows: coarse ids */
+    double *pele;         /* 1 / pcnt (amg.h:326-387) */
+} or_level;
+
+#define OR_MAX_LEVELS 32
+typedef struct {
+    int nlevels;          /* levels 0..nlevels-1; coarsest = nlevels-1 */
+    or_level lv[OR_MAX_LEVELS];
+} or_hierarchy;
+
+/* amg_solver ctor, amg.h:1135-1239 with parallel_coarsening (amg.h:37-223),
+ * parallel_interpolation (amg.h:228-406) and new_triple_product
+ * (amg.h:408-582), single rank.  The fine matrix is copied. */
+int or_amg_setup(int n, const int *cnt, const int *col, const double *ele,
+                 int max_level, int max_size, double eps, or_hierarchy *H);
+void or_amg_free(or_hierarchy *H);
+
+/* One V-cycle u = C f.
+ * smoother 0: the NOMPI Gauss-Seidel branch (amg.h:1315-1322, 759-784,
+ *             930-961), the path compute.cpp runs.
+ * smoother 1: the device design's damped Jacobi (device_amg.h:11-43,
+ *             396-411), with omega. */
+void or_vcycle(const or_hierarchy *H, int smoother, double omega,
+               const double *f, double *u);
+
+/* y = A x on level 0 layout (generic_operator.h:212-247). */
+void or_spmv(int n, const int *cnt, const int *col, const double *ele,
+             const double *x, double *y);
+
+/* PCG (pcg.h:13-76).  stop 0: the reference's test on the preconditioned
+ * residual, sigma/sigma0 <= eps^2.  stop 1: true residual
+ * ||b - A x|| / ||b|| <= eps, recomputed from x every iteration (used for
+ * parity runs).  x is the initial guess in, the solution out.  Returns the
+ * iteration count as pcg.h's iterations(); *relres receives the final true
+ * relative residual. */
+int or_pcg(const or_hierarchy *H, int smoother, double omega, const double *b,
+           double *x, double eps, int max_it, int stop, double *relres);
+
+/* compute.cpp:7-51 with a configurable tolerance/stop rule. */
+int or_compute(const int *hdr, const int *cnt, const int *col,
+               const double *ele, const double *b, double *x, double eps,
+               int stop, int *iters, double *relres);
+
+/* flux_reconstruction.c:9-279 (fluxos) and :281-319 (divvel_pontual).
+ * v[s].c is left untouched.  divmin/divmax may be NULL. */
+void or_fluxes(int nx, int ny, int nz, double hx, double hy, double hz,
+               const double *p, const or_ele *perm, const or_bound *B,
+               const int bc_type[6], or_ele *v, double *divmin,
+               double *divmax);
+
+/* Accessors for ctypes users: heap-allocated hierarchy, level sizes, and a
+ * copy-out of one level (sel/pcnt/pcol/pele untouched on the coarsest). */
+or_hierarchy *or_amg_create(int n, const int *cnt, const int *col,
+                            const double *ele, int max_level, int max_size,
+                            double eps);
+void or_amg_destroy(or_hierarchy *H);
+int or_amg_nlevels(const or_hierarchy *H);
+int or_level_info(const or_hierarchy *H, int l, int *n, long *nnz,
+                  long *pnnz);
+int or_level_copy(const or_hierarchy *H, int l, int *cnt, int *col,
+                  double *ele, double *dinv, char *sel, int *pcnt, int *pcol,
+                  double *pele);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

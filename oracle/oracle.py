@@ -1,0 +1,281 @@
+"""ctypes front-end of the correctness oracle.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
+and by ``bench.py``'s CPU-baseline leg, always as the checker or the timed CPU
+baseline, never by the GPU product path.
+
+Two back-ends with one interface:
+  * ``Port``: the C restatement (oracle/hmfem_oracle.c ->
+    oracle/_build/liboracle_port.so);
+  * ``Ref``: the reference's own sources compiled from the hmfem tree
+    (oracle/ref_harness.cpp -> oracle/_ref/libhmfem_ref.so), present only
+    where that build ran.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "_build", "liboracle_port.so")
+REF_SO = os.path.join(HERE, "_ref", "libhmfem_ref.so")
+
+ELE_FIELDS = ("u", "d", "l", "r", "c", "t", "b")   # structs.h:7-17
+IND_FIELDS = ("c", "u", "d", "l", "r", "t", "b")   # structs.h:38-48
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_cp = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
+
+
+def build(ref: bool = True) -> None:
+    """Compile the restatement (and the reference harness when the tree is
+    present) with oracle/Makefile."""
+    targets = ["port"] + (["ref"] if ref else [])
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class _Bound(C.Structure):
+    _fields_ = [(f, C.c_void_p) for f in ("l", "r", "u", "d", "t", "b")]
+
+
+class Hierarchy:
+    """Per-level arrays copied out of either back-end."""
+
+    def __init__(self):
+        self.levels = []   # dicts: n, cnt, col, ele, dinv, sel, pcnt, pcol, pele
+
+
+class Port:
+    """The C restatement of the reference algorithm."""
+
+    def __init__(self):
+        if not os.path.exists(PORT_SO):
+            build(ref=False)
+        L = C.CDLL(PORT_SO)
+        self.L = L
+        L.or_amg_create.restype = C.c_void_p
+        L.or_amg_create.argtypes = [C.c_int, _ip, _ip, _dp, C.c_int, C.c_int,
+                                    C.c_double]
+        L.or_amg_destroy.argtypes = [C.c_void_p]
+        L.or_amg_nlevels.argtypes = [C.c_void_p]
+        L.or_level_info.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                                    C.POINTER(C.c_long), C.POINTER(C.c_long)]
+        L.or_level_copy.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 8
+        L.or_vcycle.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp]
+        L.or_pcg.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp,
+                             C.c_double, C.c_int, C.c_int,
+                             C.POINTER(C.c_double)]
+        L.or_spmv.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp]
+        L.or_pack_csr.restype = C.c_long
+        L.or_pack_csr.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]
+        L.or_assemble.argtypes = [C.c_int] * 3 + [C.c_double] * 4 + [
+            _dp, _dp, _dp, _ip, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.or_source_term.argtypes = [C.c_int] * 3 + [C.c_double] * 4 + [
+            C.POINTER(_Bound), _ip, C.c_void_p] + [C.c_void_p] * 4 + [_dp]
+        L.or_fluxes.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [
+            _dp, C.c_void_p, C.POINTER(_Bound), _ip, C.c_void_p,
+            C.POINTER(C.c_double), C.POINTER(C.c_double)]
+
+    # -- assembly ------------------------------------------------------
+    def assemble(self, p):
+        """permeabilidade_arestas + source_term -> (perm[n,7], ind[n,7], b)."""
+        n = p.n
+        perm = np.zeros((n, 7), dtype=np.float64)
+        ind = np.full((n, 7), -1, dtype=np.int32)
+        bc = np.asarray(p.bc_type, dtype=np.int32)
+        self.L.or_assemble(p.nx, p.ny, p.nz, p.hx, p.hy, p.hz, p.visc, p.KX,
+                           p.KY, p.KZ, bc, None, None, _ptr(perm), _ptr(ind))
+        b = np.zeros(n)
+        faces = p.face_arrays()
+        B = _Bound(*[f.ctypes.data for f in faces])
+        self.L.or_source_term(p.nx, p.ny, p.nz, p.hx, p.hy, p.hz, p.visc,
+                              C.byref(B), bc, _ptr(perm), None, None, None,
+                              None, b)
+        return perm, ind, b
+
+    def pack(self, perm, ind):
+        n = perm.shape[0]
+        nnz = self.L.or_pack_csr(n, _ptr(perm), _ptr(ind), None, None, None)
+        cnt = np.zeros(n, np.int32)
+        col = np.zeros(nnz, np.int32)
+        ele = np.zeros(nnz)
+        self.L.or_pack_csr(n, _ptr(perm), _ptr(ind), _ptr(cnt), _ptr(col),
+                           _ptr(ele))
+        return cnt, col, ele
+
+    # -- AMG -----------------------------------------------------------
+    def amg(self, cnt, col, ele, max_level=16, max_size=1, eps=0.0):
+        h = self.L.or_amg_create(len(cnt), cnt, col, ele, max_level, max_size,
+                                 eps)
+        return _PortAMG(self, h)
+
+    def spmv(self, cnt, col, ele, x):
+        y = np.zeros(len(cnt))
+        self.L.or_spmv(len(cnt), cnt, col, ele, np.ascontiguousarray(x), y)
+        return y
+
+    def fluxes(self, p, perm, x):
+        n = p.n
+        v = np.zeros((n, 7))
+        faces = p.face_arrays()
+        B = _Bound(*[f.ctypes.data for f in faces])
+        dmin, dmax = C.c_double(), C.c_double()
+        bc = np.asarray(p.bc_type, dtype=np.int32)
+        self.L.or_fluxes(p.nx, p.ny, p.nz, p.hx, p.hy, p.hz,
+                         np.ascontiguousarray(x), _ptr(perm), C.byref(B), bc,
+                         _ptr(v), C.byref(dmin), C.byref(dmax))
+        return v, dmin.value, dmax.value
+
+
+class _PortAMG:
+    def __init__(self, port, h):
+        self.port, self.h = port, h
+        self.nlevels = port.L.or_amg_nlevels(C.c_void_p(h))
+
+    def __del__(self):
+        try:
+            self.port.L.or_amg_destroy(C.c_void_p(self.h))
+        except Exception:
+            pass
+
+    def level(self, l):
+        L = self.port.L
+        n, nnz, pnnz = C.c_int(), C.c_long(), C.c_long()
+        L.or_level_info(C.c_void_p(self.h), l, C.byref(n), C.byref(nnz),
+                        C.byref(pnnz))
+        d = dict(n=n.value, cnt=np.zeros(n.value, np.int32),
+                 col=np.zeros(nnz.value, np.int32), ele=np.zeros(nnz.value),
+                 dinv=np.zeros(n.value), sel=np.zeros(n.value, np.int8),
+                 pcnt=np.zeros(n.value, np.int32),
+                 pcol=np.zeros(pnnz.value, np.int32),
+                 pele=np.zeros(pnnz.value))
+        L.or_level_copy(C.c_void_p(self.h), l, *[
+            _ptr(d[k]) for k in ("cnt", "col", "ele", "dinv", "sel", "pcnt",
+                                 "pcol", "pele")])
+        if l == self.nlevels - 1:
+            for k in ("sel", "pcnt", "pcol", "pele"):
+                d[k] = d[k][:0]
+        return d
+
+    def vcycle(self, f, smoother=0, omega=1.0):
+        u = np.zeros(len(f))
+        self.port.L.or_vcycle(C.c_void_p(self.h), smoother, omega,
+                              np.ascontiguousarray(f), u)
+        return u
+
+    def pcg(self, b, x0=None, eps=1e-10, stop=1, smoother=0, omega=1.0,
+            max_it=10000):
+        x = np.zeros(len(b)) if x0 is None else np.array(x0, dtype=np.float64)
+        rel = C.c_double()
+        it = self.port.L.or_pcg(C.c_void_p(self.h), smoother, omega,
+                                np.ascontiguousarray(b), x, eps, max_it, stop,
+                                C.byref(rel))
+        return x, it, rel.value
+
+
+class Ref:
+    """The reference's own sources, compiled from the hmfem tree."""
+
+    def __init__(self):
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError(REF_SO)
+        L = C.CDLL(REF_SO)
+        self.L = L
+        L.ref_assemble.argtypes = [C.c_int] * 3 + [C.c_double] * 4 + [
+            _dp, _dp, _dp, _ip, _dp, C.c_void_p, C.c_void_p, _dp]
+        L.ref_pack.restype = C.c_long
+        L.ref_pack.argtypes = [C.c_int] * 3 + [C.c_void_p, C.c_void_p]
+        L.ref_packed.argtypes = [_ip, _ip, _dp]
+        L.ref_compute.argtypes = [C.c_int, C.c_long, _ip, _ip, _dp, _dp, _dp,
+                                  C.c_double, C.c_int] + [
+                                      C.POINTER(C.c_double)] * 3
+        L.ref_amg_build.argtypes = [C.c_int, C.c_long, _ip, _ip, _dp]
+        L.ref_amg_level.argtypes = [C.c_int, C.POINTER(C.c_int),
+                                    C.POINTER(C.c_long), C.POINTER(C.c_long)]
+        L.ref_amg_copy.argtypes = [C.c_int] + [C.c_void_p] * 8
+        L.ref_amg_apply.argtypes = [_dp, _dp]
+        L.ref_fluxes.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [
+            _ip, _dp, _dp, C.c_void_p, C.c_void_p]
+        L.ref_solve_all.argtypes = [C.c_int] * 3 + [C.c_double] * 4 + [
+            _dp, _dp, _dp, _ip, _dp, C.c_double, _dp, C.c_void_p, _dp,
+            C.POINTER(C.c_double)]
+
+    def assemble(self, p):
+        n = p.n
+        perm = np.zeros((n, 7))
+        ind = np.full((n, 7), -1, dtype=np.int32)
+        b = np.zeros(n)
+        self.L.ref_assemble(p.nx, p.ny, p.nz, p.hx, p.hy, p.hz, p.visc, p.KX,
+                            p.KY, p.KZ, np.asarray(p.bc_type, np.int32),
+                            np.asarray(p.bc_value, np.float64), _ptr(perm),
+                            _ptr(ind), b)
+        return perm, ind, b
+
+    def pack(self, p, perm, ind):
+        nnz = self.L.ref_pack(p.nx, p.ny, p.nz, _ptr(perm), _ptr(ind))
+        cnt = np.zeros(p.n, np.int32)
+        col = np.zeros(nnz, np.int32)
+        ele = np.zeros(nnz)
+        self.L.ref_packed(cnt, col, ele)
+        return cnt, col, ele
+
+    def compute(self, cnt, col, ele, b, x0=None, eps=1e-10, stop=2):
+        x = np.zeros(len(b)) if x0 is None else np.array(x0, dtype=np.float64)
+        ts, tv, rr = C.c_double(), C.c_double(), C.c_double()
+        it = self.L.ref_compute(len(cnt), len(col), cnt, col, ele,
+                                np.ascontiguousarray(b), x, eps, stop,
+                                C.byref(ts), C.byref(tv), C.byref(rr))
+        return x, it, rr.value, ts.value, tv.value
+
+    def hierarchy(self, cnt, col, ele):
+        nl = self.L.ref_amg_build(len(cnt), len(col), cnt, col, ele)
+        H = Hierarchy()
+        for l in range(nl):
+            n, nnz, pnnz = C.c_int(), C.c_long(), C.c_long()
+            self.L.ref_amg_level(l, C.byref(n), C.byref(nnz), C.byref(pnnz))
+            last = l == nl - 1
+            d = dict(n=n.value, cnt=np.zeros(n.value, np.int32),
+                     col=np.zeros(nnz.value, np.int32),
+                     ele=np.zeros(nnz.value), dinv=np.zeros(n.value),
+                     sel=np.zeros(0 if last else n.value, np.int8),
+                     pcnt=np.zeros(0 if last else n.value, np.int32),
+                     pcol=np.zeros(pnnz.value, np.int32),
+                     pele=np.zeros(pnnz.value))
+            self.L.ref_amg_copy(l, *[_ptr(d[k]) for k in (
+                "cnt", "col", "ele", "dinv", "sel", "pcnt", "pcol", "pele")])
+            H.levels.append(d)
+        return H
+
+    def vcycle(self, f):
+        u = np.zeros(len(f))
+        self.L.ref_amg_apply(np.ascontiguousarray(f), u)
+        return u
+
+    def fluxes(self, p, perm, x):
+        v = np.zeros((p.n, 7))
+        self.L.ref_fluxes(p.nx, p.ny, p.nz, p.hx, p.hy, p.hz,
+                          np.asarray(p.bc_type, np.int32),
+                          np.asarray(p.bc_value, np.float64),
+                          np.ascontiguousarray(x), _ptr(perm), _ptr(v))
+        return v
+
+    def solve_all(self, p, eps=1e-10):
+        x = np.zeros(p.n)
+        v = np.zeros((p.n, 7))
+        times = np.zeros(5)
+        rr = C.c_double()
+        it = self.L.ref_solve_all(p.nx, p.ny, p.nz, p.hx, p.hy, p.hz, p.visc,
+                                  p.KX, p.KY, p.KZ,
+                                  np.asarray(p.bc_type, np.int32),
+                                  np.asarray(p.bc_value, np.float64), eps, x,
+                                  _ptr(v), times, C.byref(rr))
+        return x, v, it, rr.value, times

@@ -1,0 +1,386 @@
+/*
+ * ref_harness.cpp -- drives the reference's OWN sources (compiled from the
+ * hmfem tree by oracle/Makefile, never copied) so that the C restatement in
+ * hmfem_oracle.c can be pinned against them and so that the reference CPU
+ * path can be timed as a baseline.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Output goes to oracle/_ref/ (git-ignored).
+ *
+ * What is the reference's code here: permeabilidade_arestas, create_boundary,
+ * source_term, solve_linsys (AoS -> CSR packing), fluxos, and the toolbox's
+ * amg_solver / conjugate_gradient / linear_operator / vector_product
+ * templates.  What is this harness's: the globals the application's main.c
+ * would define, a compute() that replaces compute.cpp so the tolerance and
+ * stopping rule can be chosen, and extern "C" wrappers for ctypes.
+ */
+#define NOMPI
+#include <sys/time.h>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+#include <sstream>
+#include <fstream>
+#include <string>
+#include <iostream>
+#include <algorithm>
+/* amg_solver keeps its hierarchy private; the harness reads it for the
+ * structure dumps. */
+#define private public
+#include "toolbox/toolbox.h"
+#undef private
+#include "structs.h"
+#include "functions.h"
+
+/* ---- globals normally defined by the application's main.c (variables.h) */
+Dim N;
+grid I, h;
+Perm *P;
+ELE *perm;
+IND *indcol;
+ELE *v;
+Bound *B;
+FACE boundary;
+FACEK *BoundKarst;
+IND *indcol1;
+ELEK *uc;
+Perm *KI;
+DimK *M;
+double *wi;
+int *IDwi;
+int Nwi;
+int ix0, ixf, jy0, jyf;
+double karst;
+double viscosidade;
+double **beta;
+double rho;
+int *n_brechas;
+int **brechas;
+double **pc_old;
+double **ucL_old;
+double **ucR_old;
+double *hs;
+double *Kc;
+double **cont_karst;
+int number_karst = 0;
+int Mmax;
+double **pc;
+double **C;
+double **C_contorno;
+double nxg, nyg, nzg;
+char fnam[1024];
+const char *fn;
+const char *fnwi;
+const char *dirname = ".";
+double time_total;
+double time_amg;
+int iter_amg;
+int layer;
+int lay;
+
+static double now()
+{
+    timeval t;
+    gettimeofday(&t, 0);
+    return t.tv_sec + 1e-6 * t.tv_usec;
+}
+
+/* ---- compute() replacement ------------------------------------------- */
+/* mode 0: capture the CSR that solve_linsys hands over;
+ * mode 1: the reference conjugate_gradient (pcg.h stop rule);
+ * mode 2: same operators, loop stopped on the true residual. */
+static int g_mode = 1;
+static double g_eps = 1e-8;
+static std::vector<int> g_cnt, g_col;
+static std::vector<double> g_ele;
+static double g_setup_s, g_solve_s, g_relres;
+
+static double true_relres(linear_operator<int, double> &lin,
+                          const vector<double> &b, const vector<double> &x)
+{
+    vector<double> r(b.size());
+    lin(x, r);
+    double rr = 0, bb = 0;
+    for (size_t i = 0; i < b.size(); i++) {
+        double d = b[i] - r[i];
+        rr += d * d;
+        bb += b[i] * b[i];
+    }
+    return bb > 0 ? sqrt(rr / bb) : sqrt(rr);
+}
+
+int compute(int *_hdr, int *_cnt, int *_col, double *_ele, double *_b, double *_x)
+{
+    int n = _hdr[0], nnz = _hdr[1];
+    if (g_mode == 0) {
+        g_cnt.assign(_cnt, _cnt + n);
+        g_col.assign(_col, _col + nnz);
+        g_ele.assign(_ele, _ele + nnz);
+        return 0;
+    }
+    vector<int> col(_col, _col + nnz), cnt(_cnt, _cnt + n), nod(n);
+    vector<double> ele(_ele, _ele + nnz), b(_b, _b + n), x(_x, _x + n);
+    for (int i = 0; i < n; i++) nod[i] = i;
+    communicator<int, double> com(nod);
+    linear_operator<int, double> lin(cnt, col, ele);
+    vector_product<int, double> sca(com);
+    double t0 = now();
+    /* compute.cpp:35-38 */
+    amg_solver<int, double> amg(nod, cnt, col, ele, 16, 1, 0.0, 1.0, true);
+    double t1 = now();
+    if (g_mode == 1) {
+        conjugate_gradient<int, double> cg(lin, amg, sca, g_eps, 10000, false);
+        cg(b, x);
+        iter_amg = cg.iterations();
+    } else {
+        /* pcg.h:33-76 with the test replaced by ||b-Ax||/||b|| <= eps */
+        vector<double> alpha(1, 1.0), beta(1, 0.0), sigma(1, 0.0),
+            sigma_last(1, 0.0), tau(1, 0.0);
+        vector<double> r(b), s(x), w(n);
+        lin(s, w);
+        sub_scale(r, w, alpha);
+        amg(r, w);
+        sca(w, r, sigma);
+        if (sigma[0] < 0.0) sigma[0] = fabs(sigma[0]);
+        scale_add(s, w, beta);
+        sigma_last[0] = sigma[0];
+        int loop = 0;
+        double rel = true_relres(lin, b, x);
+        while (++loop < 10000 && rel > g_eps) {
+            lin(s, w);
+            sca(s, w, tau);
+            if (tau[0] < 0.0) tau[0] = fabs(tau[0]);
+            alpha[0] = sigma[0] / tau[0];
+            add_scale(x, s, alpha);
+            sub_scale(r, w, alpha);
+            amg(r, w);
+            sca(w, r, sigma);
+            if (sigma[0] < 0.0) sigma[0] = fabs(sigma[0]);
+            beta[0] = sigma[0] / sigma_last[0];
+            scale_add(s, w, beta);
+            sigma_last[0] = sigma[0];
+            rel = true_relres(lin, b, x);
+        }
+        iter_amg = loop;
+    }
+    double t2 = now();
+    g_setup_s = t1 - t0;
+    g_solve_s = t2 - t1;
+    g_relres = true_relres(lin, b, x);
+    for (int i = 0; i < n; i++) _x[i] = x[i];
+    return 0;
+}
+
+/* ---- extern "C" wrappers ------------------------------------------------ */
+static void set_grid(int nx, int ny, int nz, double hx, double hy, double hz,
+                     const int bc[6], double visc)
+{
+    N.x = nx; N.y = ny; N.z = nz; N.xy = nx * ny; N.t = nx * ny * nz;
+    h.x = hx; h.y = hy; h.z = hz;
+    I.x = hx * nx; I.y = hy * ny; I.z = hz * nz;
+    boundary.l = bc[0]; boundary.r = bc[1]; boundary.u = bc[2];
+    boundary.d = bc[3]; boundary.t = bc[4]; boundary.b = bc[5];
+    viscosidade = visc;
+}
+
+static Bound *make_bound(const double val6[6])
+{
+    Bound *Bd = (Bound *)malloc(sizeof(Bound));
+    Bd->l = create_vector(N.t); Bd->r = create_vector(N.t);
+    Bd->u = create_vector(N.t); Bd->d = create_vector(N.t);
+    Bd->t = create_vector(N.t); Bd->b = create_vector(N.t);
+    /* val_bound[1..6] = L, R, U, D, T, B (main.c:140-152) */
+    double vb[7] = {0, val6[0], val6[1], val6[2], val6[3], val6[4], val6[5]};
+    create_boundary(vb, Bd, N, boundary);
+    return Bd;
+}
+
+static void free_bound(Bound *Bd)
+{
+    free(Bd->l); free(Bd->r); free(Bd->u); free(Bd->d); free(Bd->t); free(Bd->b);
+    free(Bd);
+}
+
+extern "C" {
+
+/* Assembly + RHS through permeabilidade_arestas and source_term.
+ * bc: l,r,u,d,t,b types; val6: l,r,u,d,t,b constant face values. */
+int ref_assemble(int nx, int ny, int nz, double hx, double hy, double hz,
+                 double visc, const double *KX, const double *KY,
+                 const double *KZ, const int *bc, const double *val6,
+                 ELE *perm_out, IND *ind_out, double *b_out)
+{
+    set_grid(nx, ny, nz, hx, hy, hz, bc, visc);
+    Perm K;
+    K.X = (double *)KX; K.Y = (double *)KY; K.Z = (double *)KZ;
+    Bound *Bd = make_bound(val6);
+    double *zero = create_vector(N.t);
+    for (int s = 0; s < N.t; s++) {
+        ind_out[s].c = ind_out[s].u = ind_out[s].d = ind_out[s].l = -1;
+        ind_out[s].r = ind_out[s].t = ind_out[s].b = -1;
+        b_out[s] = 0.0;
+    }
+    permeabilidade_arestas(&K, perm_out, ind_out, h, N, boundary, zero, zero,
+                           viscosidade);
+    source_term(Bd, perm_out, h, N, boundary, zero, zero, zero, zero,
+                viscosidade, b_out);
+    free(zero);
+    free_bound(Bd);
+    return 0;
+}
+
+/* solve_linsys packing; returns nnz, then ref_packed copies it out. */
+long ref_pack(int nx, int ny, int nz, ELE *perm_in, IND *ind_in)
+{
+    N.x = nx; N.y = ny; N.z = nz; N.xy = nx * ny; N.t = nx * ny * nz;
+    g_mode = 0;
+    std::vector<double> b(N.t, 0.0), x(N.t, 0.0);
+    solve_linsys(perm_in, ind_in, b.data(), x.data(), N);
+    return (long)g_col.size();
+}
+
+void ref_packed(int *cnt, int *col, double *ele)
+{
+    for (size_t i = 0; i < g_cnt.size(); i++) cnt[i] = g_cnt[i];
+    for (size_t i = 0; i < g_col.size(); i++) { col[i] = g_col[i]; ele[i] = g_ele[i]; }
+}
+
+/* AMG-PCG through compute(); stop 1 = pcg.h rule, 2 = true residual. */
+int ref_compute(int n, long nnz, const int *cnt, const int *col,
+                const double *ele, const double *b, double *x, double eps,
+                int stop, double *setup_s, double *solve_s, double *relres)
+{
+    int hdr[2] = {n, (int)nnz};
+    g_mode = stop;
+    g_eps = eps;
+    compute(hdr, (int *)cnt, (int *)col, (double *)ele, (double *)b, x);
+    if (setup_s) *setup_s = g_setup_s;
+    if (solve_s) *solve_s = g_solve_s;
+    if (relres) *relres = g_relres;
+    return iter_amg;
+}
+
+/* Hierarchy dump: the reference amg_solver is kept between calls. */
+static amg_solver<int, double> *g_amg;
+static std::vector<int> g_nod, g_hcnt, g_hcol;
+static std::vector<double> g_hele;
+static std::vector<std::vector<char> > g_sel;
+
+int ref_amg_build(int n, long nnz, const int *cnt, const int *col,
+                  const double *ele)
+{
+    delete g_amg;
+    g_nod.resize(n);
+    for (int i = 0; i < n; i++) g_nod[i] = i;
+    g_hcnt.assign(cnt, cnt + n);
+    g_hcol.assign(col, col + nnz);
+    g_hele.assign(ele, ele + nnz);
+    g_amg = new amg_solver<int, double>(g_nod, g_hcnt, g_hcol, g_hele, 16, 1,
+                                        0.0, 1.0, true);
+    /* C/F split per level: re-run the reference coarsening on each level. */
+    g_sel.assign(g_amg->_level, std::vector<char>());
+    for (int l = 0; l < g_amg->_level; l++) {
+        vector<double> adia;
+        vector<char> abou, acox;
+        communicator<int, double> com;
+        com.assign(g_amg->_anod[l]);
+        parallel_coarsening<int, double> coarsening;
+        coarsening(g_amg->_anod[l], g_amg->_acnt[l], g_amg->_acol[l],
+                   g_amg->_aele[l], adia, abou, g_sel[l], acox, com, 0.0);
+    }
+    return g_amg->_level + 1;
+}
+
+/* sizes of level l: rows, nnz, P nnz */
+int ref_amg_level(int l, int *n, long *nnz, long *pnnz)
+{
+    if (!g_amg || l > g_amg->_level) return -1;
+    *n = (int)g_amg->_acnt[l].size();
+    *nnz = (long)g_amg->_acol[l].size();
+    *pnnz = l < g_amg->_level ? (long)g_amg->_rcol[l].size() : 0;
+    return 0;
+}
+
+int ref_amg_copy(int l, int *cnt, int *col, double *ele, double *dinv,
+                 char *sel, int *pcnt, int *pcol, double *pele)
+{
+    if (!g_amg || l > g_amg->_level) return -1;
+    auto &A = *g_amg;
+    for (size_t i = 0; i < A._acnt[l].size(); i++) cnt[i] = A._acnt[l][i];
+    for (size_t i = 0; i < A._acol[l].size(); i++) { col[i] = A._acol[l][i]; ele[i] = A._aele[l][i]; }
+    for (size_t i = 0; i < A._adia[l].size(); i++) dinv[i] = A._adia[l][i];
+    if (l < A._level) {
+        for (size_t i = 0; i < g_sel[l].size(); i++) sel[i] = g_sel[l][i];
+        for (size_t i = 0; i < A._rcnt[l].size(); i++) pcnt[i] = A._rcnt[l][i];
+        for (size_t i = 0; i < A._rcol[l].size(); i++) { pcol[i] = A._rcol[l][i]; pele[i] = A._rele[l][i]; }
+    }
+    return 0;
+}
+
+/* one application of the reference V-cycle, u = C f */
+int ref_amg_apply(const double *f, double *u)
+{
+    if (!g_amg) return -1;
+    int n = (int)g_hcnt.size();
+    vector<double> ff(f, f + n), uu(n, 0.0);
+    (*g_amg)(ff, uu);
+    for (int i = 0; i < n; i++) u[i] = uu[i];
+    return 0;
+}
+
+void ref_amg_free()
+{
+    delete g_amg;
+    g_amg = 0;
+}
+
+/* fluxos + divvel_pontual; v_out is n ELE. */
+int ref_fluxes(int nx, int ny, int nz, double hx, double hy, double hz,
+               const int *bc, const double *val6, const double *p,
+               ELE *perm_in, ELE *v_out)
+{
+    set_grid(nx, ny, nz, hx, hy, hz, bc, viscosidade);
+    Bound *Bd = make_bound(val6);
+    fluxos((double *)p, perm_in, v_out, Bd, h, N);
+    free_bound(Bd);
+    return 0;
+}
+
+/* Whole reference CPU path for one problem, as reservoir() + fluxos run it:
+ * assembly, RHS, CSR packing + AMG-PCG (true-residual stop), flux.  times:
+ * [assemble, setup, solve, flux, total]. */
+int ref_solve_all(int nx, int ny, int nz, double hx, double hy, double hz,
+                  double visc, const double *KX, const double *KY,
+                  const double *KZ, const int *bc, const double *val6,
+                  double eps, double *p_out, ELE *v_out, double *times,
+                  double *relres)
+{
+    double t0 = now();
+    set_grid(nx, ny, nz, hx, hy, hz, bc, visc);
+    ELE *pm = (ELE *)calloc(N.t + 1, sizeof(ELE));
+    IND *ic = (IND *)malloc((N.t + 1) * sizeof(IND));
+    double *b = create_vector(N.t);
+    ref_assemble(nx, ny, nz, hx, hy, hz, visc, KX, KY, KZ, bc, val6, pm, ic, b);
+    double t1 = now();
+    for (int s = 0; s < N.t; s++) p_out[s] = 0.0;
+    g_mode = 2;
+    g_eps = eps;
+    solve_linsys(pm, ic, b, p_out, N);
+    double t2 = now();
+    fluxos(p_out, pm, v_out, B = make_bound(val6), h, N);
+    free_bound(B);
+    B = 0;
+    double t3 = now();
+    if (times) {
+        times[0] = t1 - t0;
+        times[1] = g_setup_s;
+        times[2] = g_solve_s;
+        times[3] = t3 - t2;
+        times[4] = t3 - t0;
+    }
+    if (relres) *relres = g_relres;
+    free(pm); free(ic); free(b);
+    return iter_amg;
+}
+
+}  // extern "C"
