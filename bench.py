@@ -1,0 +1,356 @@
+"""Benchmark: cells/s of hmfem's pressure solve on B200 to ||r||/||b|| <= 1e-10.
+
+One step = the hot path over one synthetic problem with the permeability
+field already resident in HBM: TPFA assembly -> AMG setup (C/F split,
+interpolation, Galerkin products, all on the device) -> CG to a true FP64
+relative residual <= 1e-10.  Workload: 256^3 cells, log10 K = -14 + 1.5 g
+(Gaussian field, correlation 8 cells) + 8 random-walk conduits at K = 1e-9,
+Dirichlet p=1 / p=0 on the x faces, no-flow elsewhere.
+
+The headline variant ("chosen") is the FP32 V-cycle inside FP64 flexible CG;
+the plain FP64 AMG-PCG drop-in is measured in the same run.  `e2e` is the
+same solve through the public C-ABI from host buffers (K uploaded, pressure
+downloaded inside the timed region).  `--impl reference` times the
+reference's own CPU path (oracle/_ref, compiled from the hmfem sources) on
+all host cores over a bounded sample of the same workload.
+
+Multi-GPU: the path does not shard; --gpus N runs N independent replicas,
+one per rank (weak scaling), and value is the sum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cells/s to ||r||/||b||<=1e-10 (256^3 lognormal+conduits), chosen=FP32 V-cycle in FP64 FCG"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=96)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- helpers --
+
+class Clocks:
+    """Samples nvidia-smi clocks/throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev, self.rows, self.proc = dev, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 2 + i and r[2 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_init(args):
+    import torch
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------- our arm -----
+
+def run_ours(args):
+    import torch
+
+    from hmfem_b200 import gpu
+    from hmfem_b200.problem import config_problem
+
+    rank, world, local = dist_init(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    prob = config_problem(2, size=args.size)  # same field on every replica
+    n = prob.n
+    K = torch.tensor(prob.KX, device=dev)     # resident in HBM (> L2)
+
+    def make(precision):
+        s = gpu.Solver(precision=precision, tol=args.tol,
+                       bf16_from=-1, check_every=2)
+        stream = torch.cuda.ExternalStream(s.stream)
+        return s, stream
+
+    def step(s, x):
+        s.assemble(prob, KX=K, KY=K, KZ=K)
+        s.setup()
+        x.zero_()
+        _, st = s.solve(x=x)
+        return st
+
+    results = {}
+    launches = {}
+    for name, precision in (("plain_fp64", 0), ("chosen", 1)):
+        s, stream = make(precision)
+        x = torch.zeros(n, dtype=torch.float64, device=dev)
+        for _ in range(args.warmup):
+            st = step(s, x)
+        torch.cuda.synchronize()
+        barrier(world)
+        times, stats = [], []
+        with Clocks(local) as ck:
+            for _ in range(args.steps):
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                st = step(s, x)
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+                stats.append(st)
+        torch.cuda.synchronize()
+        barrier(world)
+        total_ms = max_over_ranks(sum(times), world)
+        results[name] = dict(ms_per_step=total_ms / args.steps,
+                             value=world * n * args.steps / (total_ms / 1e3),
+                             iterations=stats[-1]["iterations"],
+                             relres=stats[-1]["relres"],
+                             levels=stats[-1]["levels"],
+                             setup_ms=stats[-1]["t_setup_ms"],
+                             solve_ms=stats[-1]["t_solve_ms"],
+                             clocks=ck.summary(), solver=s, stream=stream)
+        # kernel launches per step: assembly(2) + setup + CG (counted from
+        # the iteration structure: see DESIGN.md)
+        L = st["levels"]
+        per_iter = 4 + (4 * (L - 1) + 1) + (2 if precision == 1 else 0)
+        launches[name] = int(3 + 12 * (L - 1) + 2 * L + 4 + per_iter * (st["iterations"] + 2))
+    ch = results["chosen"]
+
+    # ---- roofline: the dominant kernel, timed live on the solver stream
+    s0 = results["plain_fp64"]["solver"]
+    ms0, by0 = s0.time_kernel(0, 0, reps=20)        # L0 SpMV FP64 (CG)
+    kern = {}
+    for lvl in range(min(3, results["plain_fp64"]["levels"] - 1)):
+        for w, nm in ((1, "pre64"), (2, "post64")):
+            kern[f"L{lvl}_{nm}"] = s0.time_kernel(w, lvl, reps=10)
+    s1 = ch["solver"]
+    for lvl in range(min(3, ch["levels"] - 1)):
+        for w, nm in ((3, "pre32"), (4, "post32")):
+            kern[f"L{lvl}_{nm}"] = s1.time_kernel(w, lvl, reps=10)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = by0 / (ms0 / 1e3) / 1e9
+    kernels_gbs = {k: round(b / (m / 1e3) / 1e9, 1) for k, (m, b) in kern.items()}
+
+    # ---- e2e through the public API with host buffers
+    s_e2e = gpu.Solver(precision=1, tol=args.tol, check_every=2)
+    xh = np.zeros(n)
+    for _ in range(max(1, args.warmup - 1)):
+        s_e2e.assemble(prob)
+        s_e2e.setup()
+        xh[:] = 0
+        s_e2e.solve(x=xh)
+    torch.cuda.synchronize()
+    barrier(world)
+    te = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        s_e2e.assemble(prob)          # KX/KY/KZ host -> device inside
+        s_e2e.setup()
+        xh[:] = 0
+        s_e2e.solve(x=xh)             # x host -> device, pressure device -> host
+        te.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(sum(te), world)
+    e2e = {"value": world * n * args.steps / e2e_s, "unit": "cells/s",
+           "h2d_bytes_per_step": 3 * n * 8 + n * 8, "d2h_bytes_per_step": n * 8}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(args.cpu_sample, cores=1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": ch["value"], "unit": "cells/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ch["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 CG / f32 V-cycle",
+            "data": "synthetic (seeded lognormal field + random-walk conduits)",
+            "config": {"workload": f"config2 {args.size}^3 lognormal+8 conduits",
+                       "cells": n, "tol": args.tol,
+                       "l2": "inputs (K 3x8 B/cell, matrix, hierarchy) larger than L2",
+                       "parallelism": f"replicas x{world}"},
+            "chosen": {k: v for k, v in ch.items() if k not in ("solver", "stream")},
+            "plain_fp64": {k: v for k, v in results["plain_fp64"].items()
+                           if k not in ("solver", "stream")},
+            "speedup_chosen_vs_plain": ch["value"] / results["plain_fp64"]["value"],
+            "e2e": e2e,
+            "roofline": {"bound": "hbm", "kernel": "k_spmv_dot (L0 SpMV FP64, SELL-32)",
+                         "achieved": round(achieved, 1), "peak": peak,
+                         "peak_source": peak_src, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4),
+                         "algorithmic_bytes": by0, "ms": ms0, "traffic": None},
+            "kernels_gbs": kernels_gbs,
+            "gpu_launches": launches["chosen"] * args.steps,
+            "cpu_baseline": cpu,
+            "clocks": ch["clocks"],
+        }
+        print(json.dumps(line), flush=True)
+    for r in results.values():
+        r["solver"].close()
+    s_e2e.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------ reference (CPU) ----
+
+def _ref_worker(args_tuple):
+    size, seed_off, tol = args_tuple
+    from hmfem_b200.problem import config_problem
+    from oracle.oracle import Ref
+    p = config_problem(2, realisation=seed_off, size=size)
+    t0 = time.perf_counter()
+    x, v, it, rel, times = Ref().solve_all(p, eps=tol)
+    dt = time.perf_counter() - t0
+    return p.n, dt, it, rel, list(times)
+
+
+def cpu_baseline_sample(size, cores=1, tol=1e-10):
+    """The reference's CPU path (oracle/_ref) on one sample of the workload."""
+    try:
+        n, dt, it, rel, times = _ref_worker((size, 0, tol))
+    except Exception as e:  # reference build missing
+        return {"value": None, "unavailable": str(e)}
+    return {"value": n / dt, "unit": "cells/s", "cores": cores,
+            "kind": "reference",
+            "sample": f"config2 generator at {size}^3 (same distribution), "
+                      f"full reference path: assembly + CSR + AMG setup + "
+                      f"PCG to true relres {tol} + flux; {it} iterations, "
+                      f"{dt:.1f} s",
+            "split_s": dict(zip(["assemble", "setup", "solve", "flux", "total"],
+                                [round(t, 3) for t in times]))}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    size = 64
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        for _ in range(args.warmup):
+            pool.map(_ref_worker, [(size, c, args.tol) for c in range(cores)])
+        t0 = time.perf_counter()
+        its = []
+        for _ in range(args.steps):
+            out = pool.map(_ref_worker, [(size, c, args.tol) for c in range(cores)])
+            its.append(out[0][2])
+        dt = time.perf_counter() - t0
+    cells = size ** 3 * cores * args.steps
+    value = cells / dt
+    line = {"impl": "reference", "metric": METRIC, "value": value,
+            "unit": "cells/s", "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"config2 generator at {size}^3 per core "
+                                   f"(bounded sample of the 256^3 workload)",
+                       "tol": args.tol},
+            "cpu_baseline": {"value": value, "unit": "cells/s", "cores": cores,
+                             "kind": "reference",
+                             "sample": f"{cores} independent {size}^3 solves per "
+                                       f"step, one per core, reference sources "
+                                       f"(oracle/_ref), {its[-1]} iterations"},
+            "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

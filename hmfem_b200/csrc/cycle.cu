@@ -1,0 +1,598 @@
+// cycle.cu -- V-cycle kernels (damped Jacobi on SELL-32, the device design
+// of device_amg.h:11-43, 370-432) and the CG vector kernels.
+//
+// FP64 instantiations use non-contracted arithmetic, so one V-cycle is
+// bit-identical to the oracle's Jacobi V-cycle; the FP32 ones (the mixed
+// precision preconditioner) use FMA.  Every kernel takes the CG control
+// block and returns at once when the solve is already finished, so a
+// captured iteration can be replayed past convergence at no cost.
+#include "solver.cuh"
+
+namespace hm {
+
+template <class T> struct Ar;
+template <> struct Ar<double> {
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double div(double a, double b) { return a / b; }
+};
+template <> struct Ar<float> {
+    static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
+    static __device__ __forceinline__ float add(float a, float b) { return a + b; }
+    static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
+    static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+};
+
+__device__ __forceinline__ double ld(const double *p, long long i) { return p[i]; }
+__device__ __forceinline__ float ld(const float *p, long long i) { return __ldg(p + i); }
+__device__ __forceinline__ float ld(const __nv_bfloat16 *p, long long i) { return __bfloat162float(p[i]); }
+
+__device__ __forceinline__ bool finished(const Ctl *c) { return c && *(volatile const int *)&c->done; }
+
+#define GRID_STRIDE(r, n)                                                     \
+    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < (n);       \
+         r += (long)gridDim.x * blockDim.x)
+
+// ---- smoother / transfer kernels --------------------------------------
+
+// Pre-smoother from zero and residual, fused (device_jacobi 3-arg,
+// device_amg.h:35-42):  u = w D^-1 f;  r = f - A u;  rs = r / |P row|
+// (the 1/c of simple_restriction, generic_operator.h:97-122, applied here).
+template <class T, class M>
+__global__ void __launch_bounds__(256)
+k_pre(const long long *__restrict__ sptr, const int *__restrict__ scol,
+      const M *__restrict__ sval, int n, const T *__restrict__ f,
+      const T *__restrict__ dinv, T w, const int *__restrict__ prow,
+      T *__restrict__ u, T *__restrict__ rs, const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    GRID_STRIDE(r, n) {
+        long q = r >> 5;
+        int lane = (int)(r & 31);
+        long long base = sptr[q];
+        int wd = (int)((sptr[q + 1] - base) >> 5);
+        T fr = f[r];
+        T t = fr;
+        for (int k = 0; k < wd; k++) {
+            long long o = base + (long long)k * 32 + lane;
+            int c = scol[o];
+            T uc = A::mul(A::mul(w, f[c]), dinv[c]);
+            t = A::sub(t, A::mul((T)ld(sval, o), uc));
+        }
+        u[r] = A::mul(A::mul(w, fr), dinv[r]);
+        int pc = prow[r + 1] - prow[r];
+        rs[r] = pc == 1 ? t : A::div(t, (T)pc);
+    }
+}
+
+// f_c[e] = sum_{i in R(e), ascending} rs_i  (simple_restriction's
+// accumulation order, generic_operator.h:86-128).
+template <class T>
+__global__ void __launch_bounds__(256)
+k_restrict(const int *__restrict__ rrow, const int *__restrict__ rcol, int nc,
+           const T *__restrict__ rs, T *__restrict__ fc, const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    GRID_STRIDE(e, nc) {
+        T acc = (T)0;
+        for (int k = rrow[e]; k < rrow[e + 1]; k++) acc = A::add(acc, rs[rcol[k]]);
+        fc[e] = acc;
+    }
+}
+
+// u += P u_c (simple_prolongation, generic_operator.h:18-64, then add).
+template <class T>
+__global__ void __launch_bounds__(256)
+k_prolong_add(const int *__restrict__ prow, const int *__restrict__ pcol, int n,
+              const T *__restrict__ uc, T *__restrict__ u, const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    GRID_STRIDE(i, n) {
+        int a = prow[i], c = prow[i + 1] - a;
+        if (c == 0) continue;
+        T s;
+        if (c == 1) s = uc[pcol[a]];
+        else {
+            T t = uc[pcol[a]];
+            for (int k = 1; k < c; k++) t = A::add(t, uc[pcol[a + k]]);
+            s = A::div(t, (T)c);
+        }
+        u[i] = A::add(u[i], s);
+    }
+}
+
+// Post-smoother (device_jacobi 2-arg, device_amg.h:27-34):
+// v = f - A u;  u_out = u + w v D^-1.  Optionally accumulates
+// dot(u_out, f) -> ctl->sigma (the PCG's (C r, r), pcg.h:66).
+template <class T, class M, bool DOT>
+__global__ void __launch_bounds__(256)
+k_post(const long long *__restrict__ sptr, const int *__restrict__ scol,
+       const M *__restrict__ sval, int n, const T *__restrict__ f,
+       const T *__restrict__ dinv, T w, const T *__restrict__ u,
+       T *__restrict__ uo, Ctl *ctl, double *part, int first)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    double dot = 0.0;
+    GRID_STRIDE(r, n) {
+        long q = r >> 5;
+        int lane = (int)(r & 31);
+        long long base = sptr[q];
+        int wd = (int)((sptr[q + 1] - base) >> 5);
+        T fr = f[r];
+        T t = fr;
+        for (int k = 0; k < wd; k++) {
+            long long o = base + (long long)k * 32 + lane;
+            t = A::sub(t, A::mul((T)ld(sval, o), u[scol[o]]));
+        }
+        T un = A::add(u[r], A::mul(A::mul(w, t), dinv[r]));
+        uo[r] = un;
+        if (DOT) dot += (double)un * (double)fr;
+    }
+    if (DOT) {
+        grid_reduce_sum(dot, part, &ctl->tickets[RED_SIGMA], [&](double s) {
+            // pcg.h:66-67 (and 46-47 on the first application)
+            if (s < 0.0) s = fabs(s);
+            if (!(s == s) || isinf(s)) { ctl->status = HMFEM_E_BREAKDOWN; ctl->done = 1; }
+            if (first) {
+                ctl->sigma_first = s == 0.0 ? 1.0 : s;
+                ctl->sigma_last = s;
+                ctl->beta = 0.0;
+            } else {
+                ctl->beta = s / ctl->sigma_last;
+            }
+            ctl->sigma = s;
+            if (ctl->stop_rule == 1 && s / ctl->sigma_first <= ctl->tol2) ctl->done = 1;
+        });
+    }
+}
+
+// coarsest level: v = D^-1 f (diagonal_solver, amg.h:1074-1097)
+template <class T>
+__global__ void k_diag_solve(int n, const T *__restrict__ dinv,
+                             const T *__restrict__ f, T *__restrict__ u,
+                             const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    GRID_STRIDE(i, n) u[i] = A::mul(dinv[i], f[i]);
+}
+
+// coarsest level: dense Cholesky solve, one block (L stored row-major,
+// lower triangle, FP64).
+template <class T>
+__global__ void k_dense_solve(int n, const double *__restrict__ Lf,
+                              const T *__restrict__ f, T *__restrict__ u,
+                              const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    extern __shared__ double y[];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (double)f[i];
+    __syncthreads();
+    // forward: L y = f (column-oriented so the block works on one column)
+    for (int j = 0; j < n; j++) {
+        if (threadIdx.x == 0) y[j] = y[j] / Lf[(long)j * n + j];
+        __syncthreads();
+        double yj = y[j];
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x)
+            y[i] -= Lf[(long)i * n + j] * yj;
+        __syncthreads();
+    }
+    // backward: L^T x = y
+    for (int j = n - 1; j >= 0; j--) {
+        if (threadIdx.x == 0) y[j] = y[j] / Lf[(long)j * n + j];
+        __syncthreads();
+        double yj = y[j];
+        for (int i = threadIdx.x; i < j; i += blockDim.x)
+            y[i] -= Lf[(long)j * n + i] * yj;
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) u[i] = (T)y[i];
+}
+
+// ---- CG kernels ---------------------------------------------------------
+
+// r = b - A x; rr = (r,r); bb = (b,b)
+__global__ void __launch_bounds__(256)
+k_resid(const long long *__restrict__ sptr, const int *__restrict__ scol,
+        const double *__restrict__ sval, int n, const double *__restrict__ b,
+        const double *__restrict__ x, double *__restrict__ r, Ctl *ctl,
+        double *part, int init)
+{
+    // init: 1 = start of the solve, 0 = convergence check (residual
+    // replacement), 2 = report only
+    if (init == 0 && (finished(ctl) || !ctl->check)) return;
+    double rr = 0.0, bb = 0.0;
+    GRID_STRIDE(i, n) {
+        long q = i >> 5;
+        int lane = (int)(i & 31);
+        long long base = sptr[q];
+        int wd = (int)((sptr[q + 1] - base) >> 5);
+        double s = 0.0;
+        for (int k = 0; k < wd; k++) {
+            long long o = base + (long long)k * 32 + lane;
+            s = dadd(s, dmul(sval[o], x[scol[o]]));
+        }
+        double bi = b[i];
+        double ri = dsub(bi, s);
+        r[i] = ri;
+        rr += ri * ri;
+        bb += bi * bi;
+    }
+    // two sums: reuse the single-value reduction twice through separate
+    // partial rows
+    double *p2 = part + kRedBlocks;
+    grid_reduce_sum(bb, p2, &ctl->tickets[RED_BB], [&](double s) { ctl->bb = s; });
+    grid_reduce_sum(rr, part, &ctl->tickets[RED_TRR], [&](double s) {
+        ctl->trr = s;
+        if (init == 2) return;
+        ctl->rr = s;
+        if (init == 1) {
+            ctl->iters = 0;
+            if (s <= ctl->tol2 * ctl->bb && ctl->stop_rule == 0) ctl->done = 1;
+        } else {
+            ctl->check = 0;
+            if (s <= ctl->tol2 * ctl->bb) ctl->done = 1;
+        }
+    });
+}
+
+// v = A s; tau = (s, v); alpha = sigma / tau (pcg.h:59-63)
+__global__ void __launch_bounds__(256)
+k_spmv_dot(const long long *__restrict__ sptr, const int *__restrict__ scol,
+           const double *__restrict__ sval, int n, const double *__restrict__ s,
+           double *__restrict__ v, Ctl *ctl, double *part)
+{
+    if (finished(ctl)) return;
+    double d = 0.0;
+    GRID_STRIDE(i, n) {
+        long q = i >> 5;
+        int lane = (int)(i & 31);
+        long long base = sptr[q];
+        int wd = (int)((sptr[q + 1] - base) >> 5);
+        double a = 0.0;
+        for (int k = 0; k < wd; k++) {
+            long long o = base + (long long)k * 32 + lane;
+            a = dadd(a, dmul(sval[o], s[scol[o]]));
+        }
+        v[i] = a;
+        d += s[i] * a;
+    }
+    grid_reduce_sum(d, part, &ctl->tickets[RED_TAU], [&](double t) {
+        if (t < 0.0) t = fabs(t);
+        ctl->tau = t;
+        if (!(t > 0.0) || isinf(t)) { ctl->status = HMFEM_E_BREAKDOWN; ctl->done = 1; return; }
+        ctl->alpha = ctl->sigma / t;
+    });
+}
+
+// x += alpha s; r -= alpha v; rr = (r, r)  (pcg.h:64-65)
+__global__ void __launch_bounds__(256)
+k_update(int n, double *__restrict__ x, double *__restrict__ r,
+         const double *__restrict__ s, const double *__restrict__ v, Ctl *ctl,
+         double *part)
+{
+    if (finished(ctl)) return;
+    const double al = ctl->alpha;
+    double rr = 0.0;
+    GRID_STRIDE(i, n) {
+        x[i] = dadd(x[i], dmul(s[i], al));
+        double ri = dsub(r[i], dmul(v[i], al));
+        r[i] = ri;
+        rr += ri * ri;
+    }
+    grid_reduce_sum(rr, part, &ctl->tickets[RED_RR], [&](double t) {
+        ctl->rr = t;
+        int it = ++ctl->iters;
+        if (ctl->stop_rule == 0 && t <= ctl->tol2 * ctl->bb) ctl->check = 1;
+        if (it >= ctl->max_iter) { ctl->status = HMFEM_E_NOTCONV; ctl->done = 1; }
+    });
+}
+
+// s = s * beta + z  (scale_add, pcg.h:69); sigma_last = sigma (pcg.h:70)
+__global__ void __launch_bounds__(256)
+k_sdir(int n, double *__restrict__ s, const double *__restrict__ z, Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    const double be = ctl->beta;
+    GRID_STRIDE(i, n) s[i] = dadd(dmul(s[i], be), z[i]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->sigma_last = ctl->sigma;
+}
+
+// z = (double) src; sigma = (z, r); for the flexible CG also (z, v) with
+// v = A s_old, giving beta = -(z, A s_old) / (s_old, A s_old) (one-term
+// flexible CG; equals the Polak-Ribiere formula).  Used after an FP32
+// V-cycle, and after a V-cycle that ends in the coarsest solve.
+template <class T>
+__global__ void __launch_bounds__(256)
+k_finish_z(int n, const T *__restrict__ src, const double *__restrict__ r,
+           const double *__restrict__ v, double *__restrict__ z, Ctl *ctl,
+           double *part, int first, int flexible)
+{
+    if (finished(ctl)) return;
+    double d1 = 0.0, d2 = 0.0;
+    GRID_STRIDE(i, n) {
+        double zi = (double)src[i];
+        z[i] = zi;
+        d1 += zi * r[i];
+        if (flexible && !first) d2 += zi * v[i];
+    }
+    double *p2 = part + kRedBlocks;
+    if (flexible && !first)
+        grid_reduce_sum(d2, p2, &ctl->tickets[RED_A], [&](double t) { ctl->rz_old = t; });
+    grid_reduce_sum(d1, part, &ctl->tickets[RED_SIGMA], [&](double s) {
+        if (!(s == s) || isinf(s)) { ctl->status = HMFEM_E_BREAKDOWN; ctl->done = 1; }
+        if (!flexible && s < 0.0) s = fabs(s);   // pcg.h:47, 68
+        if (first) {
+            ctl->sigma_first = s == 0.0 ? 1.0 : fabs(s);
+            ctl->sigma_last = s;
+            ctl->beta = 0.0;
+        } else if (flexible) {
+            ctl->beta = -ctl->rz_old / ctl->tau;
+        } else {
+            ctl->beta = s / ctl->sigma_last;
+        }
+        ctl->sigma = s;
+        if (ctl->stop_rule == 1 && fabs(s) / ctl->sigma_first <= ctl->tol2) ctl->done = 1;
+    });
+}
+
+__global__ void k_demote(int n, const double *__restrict__ r, float *__restrict__ f,
+                         const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    GRID_STRIDE(i, n) f[i] = (float)r[i];
+}
+
+// ---- host side ------------------------------------------------------------
+
+static int nb(long n, int threads = 256)
+{
+    long b = ceil_div(n, threads);
+    if (b < 1) b = 1;
+    return (int)(b < kRedBlocks ? b : kRedBlocks);
+}
+
+// One V-cycle from level l: f[l] holds the right-hand side, the result is
+// left in ub[l] (levels above the coarsest) or ua[l] (the coarsest).
+template <class T>
+static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
+{
+    Level &L = s.lv[l];
+    const int last = s.nlevels - 1;
+    Ctl *ctl = s.ctl_active ? s.ctl : nullptr;
+    T *f = s.vec_f<T>(l), *ua = s.vec_ua<T>(l), *ub = s.vec_ub<T>(l);
+    if (l == s.direct_level) {
+        k_dense_solve<T><<<1, 256, sizeof(double) * L.A.n, st>>>(
+            L.A.n, s.dense_L, f, ua, ctl);
+        HM_CUDA(cudaGetLastError());
+        return HMFEM_OK;
+    }
+    if (l == last) {
+        k_diag_solve<T><<<nb(L.A.n), 256, 0, st>>>(L.A.n, s.vec_dtrue<T>(l), f, ua, ctl);
+        HM_CUDA(cudaGetLastError());
+        return HMFEM_OK;
+    }
+    const T w = (T)s.opt.omega;
+    Level &C = s.lv[l + 1];
+    T *rs = s.vec_rs<T>(l);
+    const T *dv = s.vec_dinv<T>(l);
+    if (std::is_same<T, double>::value || !s.use_bf16(l)) {
+        k_pre<T, T><<<nb(L.A.n), 256, 0, st>>>(L.S.sptr, L.S.col, s.sval<T>(l),
+                                               L.A.n, f, dv, w, L.P.rowptr, ua, rs, ctl);
+    } else {
+        k_pre<T, __nv_bfloat16><<<nb(L.A.n), 256, 0, st>>>(
+            L.S.sptr, L.S.col, L.S.val16, L.A.n, f, dv, w, L.P.rowptr, ua, rs, ctl);
+    }
+    HM_CUDA(cudaGetLastError());
+    k_restrict<T><<<nb(L.nc), 256, 0, st>>>(L.R.rowptr, L.R.col, L.nc, rs,
+                                            s.vec_f<T>(l + 1), ctl);
+    HM_CUDA(cudaGetLastError());
+    HM_CHECK(cycle_t<T>(s, l + 1, st, false));
+    const T *uc = (l + 1 == last || l + 1 == s.direct_level) ? s.vec_ua<T>(l + 1)
+                                                             : s.vec_ub<T>(l + 1);
+    k_prolong_add<T><<<nb(L.A.n), 256, 0, st>>>(L.P.rowptr, L.P.col, L.A.n, uc, ua, ctl);
+    HM_CUDA(cudaGetLastError());
+    (void)C;
+    if (dot) {
+        k_post<T, T, true><<<nb(L.A.n), 256, 0, st>>>(
+            L.S.sptr, L.S.col, s.sval<T>(l), L.A.n, f, dv, w, ua, ub, s.ctl,
+            s.part, s.first_sigma);
+    } else if (std::is_same<T, double>::value || !s.use_bf16(l)) {
+        k_post<T, T, false><<<nb(L.A.n), 256, 0, st>>>(
+            L.S.sptr, L.S.col, s.sval<T>(l), L.A.n, f, dv, w, ua, ub, ctl,
+            nullptr, 0);
+    } else {
+        k_post<T, __nv_bfloat16, false><<<nb(L.A.n), 256, 0, st>>>(
+            L.S.sptr, L.S.col, L.S.val16, L.A.n, f, dv, w, ua, ub, ctl, nullptr, 0);
+    }
+    HM_CUDA(cudaGetLastError());
+    return HMFEM_OK;
+}
+
+int cycle_fp64(Solver &s, int l, cudaStream_t st, bool dot)
+{
+    return cycle_t<double>(s, l, st, dot);
+}
+
+int cycle_fp32(Solver &s, int l, cudaStream_t st, bool dot)
+{
+    return cycle_t<float>(s, l, st, dot);
+}
+
+// ---- CG iteration bodies (enqueued once, captured into a graph) -----------
+
+// z = C r, sigma = (z, r), beta (fused into the last V-cycle kernel where
+// the V-cycle is FP64 and has a coarse level)
+int cg_precondition(Solver &s, cudaStream_t st)
+{
+    Level &L0 = s.lv[0];
+    const int n = L0.A.n;
+    const bool top_is_coarse = s.nlevels == 1 || s.direct_level == 0;
+    if (s.opt.precision == 0) {
+        // the V-cycle reads f[0] = r in place; z lands in ub[0] = s.z
+        HM_CHECK(cycle_fp64(s, 0, st, !top_is_coarse));
+        if (top_is_coarse) {
+            k_finish_z<double><<<nb(n), 256, 0, st>>>(n, L0.ua, s.r, s.v, s.z,
+                                                      s.ctl, s.part,
+                                                      s.first_sigma, 0);
+            HM_CUDA(cudaGetLastError());
+        }
+        return HMFEM_OK;
+    }
+    k_demote<<<nb(n), 256, 0, st>>>(n, s.r, L0.f32, s.ctl);
+    HM_CUDA(cudaGetLastError());
+    HM_CHECK(cycle_fp32(s, 0, st, false));
+    const float *z32 = top_is_coarse ? L0.ua32 : L0.ub32;
+    k_finish_z<float><<<nb(n), 256, 0, st>>>(n, z32, s.r, s.v, s.z, s.ctl,
+                                             s.part, s.first_sigma, 1);
+    HM_CUDA(cudaGetLastError());
+    return HMFEM_OK;
+}
+
+int cg_init(Solver &s, cudaStream_t st)
+{
+    Level &L0 = s.lv[0];
+    const int n = L0.A.n;
+    k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
+                                   s.r, s.ctl, s.part, 1);
+    HM_CUDA(cudaGetLastError());
+    s.first_sigma = 1;
+    HM_CHECK(cg_precondition(s, st));
+    s.first_sigma = 0;
+    k_sdir<<<nb(n), 256, 0, st>>>(n, s.s, s.z, s.ctl);
+    HM_CUDA(cudaGetLastError());
+    return HMFEM_OK;
+}
+
+int cg_iteration(Solver &s, cudaStream_t st)
+{
+    Level &L0 = s.lv[0];
+    const int n = L0.A.n;
+    k_spmv_dot<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.s,
+                                      s.v, s.ctl, s.part);
+    HM_CUDA(cudaGetLastError());
+    k_update<<<nb(n), 256, 0, st>>>(n, s.x, s.r, s.s, s.v, s.ctl, s.part);
+    HM_CUDA(cudaGetLastError());
+    k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
+                                   s.r, s.ctl, s.part, 0);
+    HM_CUDA(cudaGetLastError());
+    HM_CHECK(cg_precondition(s, st));
+    k_sdir<<<nb(n), 256, 0, st>>>(n, s.s, s.z, s.ctl);
+    HM_CUDA(cudaGetLastError());
+    return HMFEM_OK;
+}
+
+// final true residual ||b - A x||^2 into ctl->trr (r is overwritten)
+int cg_final_residual(Solver &s, cudaStream_t st)
+{
+    Level &L0 = s.lv[0];
+    const int n = L0.A.n;
+    k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
+                                   s.r, s.ctl, s.part, 2);
+    HM_CUDA(cudaGetLastError());
+    return HMFEM_OK;
+}
+
+// plain SpMV on level l (inspection / tests)
+int level_spmv(Solver &s, int l, const double *x, double *y, cudaStream_t st)
+{
+    return launch_spmv(s.lv[l].S, x, y, st);
+}
+
+// Times `reps` back-to-back launches of one solve-phase kernel on level l
+// with CUDA events on the solver stream; returns the mean duration and the
+// kernel's algorithmic bytes per launch (no padding, every vector element
+// moved once):
+//   0 SpMV FP64            nnz*(8+4) + n*(8+8)
+//   1 pre-smoother FP64    nnz*(8+4) + n*(8 f + 8 d + 4 P-row + 8 u + 8 rs)
+//   2 post-smoother FP64   nnz*(8+4) + n*(8 f + 8 d + 8 u + 8 u_out)
+//   3 pre-smoother FP32    nnz*(4+4) + n*(4+4+4+4+4)
+//   4 post-smoother FP32   nnz*(4+4) + n*(4*4)
+// (values BF16 on levels >= bf16_from: 2 bytes instead of 4)
+int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
+{
+    if (l < 0 || l >= s.nlevels || reps < 1) return HMFEM_E_ARG;
+    if (which >= 1 && l == s.nlevels - 1) return HMFEM_E_ARG;
+    if (which >= 3 && s.opt.precision != 1) return HMFEM_E_ARG;
+    Level &L = s.lv[l];
+    cudaStream_t st = s.st;
+    const int n = L.A.n;
+    const double nnz = (double)L.A.nnz;
+    double *x = nullptr, *y = nullptr;
+    x = (double *)dalloc(sizeof(double) * n);
+    y = (double *)dalloc(sizeof(double) * n);
+    if (!x || !y) { dfree(x); dfree(y); return HMFEM_E_CUDA; }
+    HM_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+    float *xf = (float *)x, *yf = (float *)y;
+    const double w = s.opt.omega;
+    const int vb16 = s.use_bf16(l) ? 2 : 4;
+    auto launch = [&]() {
+        switch (which) {
+        case 0:
+            k_spmv_dot<<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, L.S.val, n, x, y,
+                                              s.ctl, s.part);
+            break;
+        case 1:
+            k_pre<double, double><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, L.S.val, n,
+                                                         x, L.dsm, w, L.P.rowptr, y,
+                                                         L.rs, nullptr);
+            break;
+        case 2:
+            k_post<double, double, false><<<nb(n), 256, 0, st>>>(
+                L.S.sptr, L.S.col, L.S.val, n, x, L.dsm, w, L.ua, y, nullptr, nullptr, 0);
+            break;
+        case 3:
+            if (vb16 == 2)
+                k_pre<float, __nv_bfloat16><<<nb(n), 256, 0, st>>>(
+                    L.S.sptr, L.S.col, L.S.val16, n, xf, L.dsm32, (float)w,
+                    L.P.rowptr, yf, L.rs32, nullptr);
+            else
+                k_pre<float, float><<<nb(n), 256, 0, st>>>(
+                    L.S.sptr, L.S.col, L.S.val32, n, xf, L.dsm32, (float)w,
+                    L.P.rowptr, yf, L.rs32, nullptr);
+            break;
+        default:
+            if (vb16 == 2)
+                k_post<float, __nv_bfloat16, false><<<nb(n), 256, 0, st>>>(
+                    L.S.sptr, L.S.col, L.S.val16, n, xf, L.dsm32, (float)w, L.ua32,
+                    yf, nullptr, nullptr, 0);
+            else
+                k_post<float, float, false><<<nb(n), 256, 0, st>>>(
+                    L.S.sptr, L.S.col, L.S.val32, n, xf, L.dsm32, (float)w, L.ua32,
+                    yf, nullptr, nullptr, 0);
+        }
+    };
+    // control block must not be in the finished state for case 0
+    HM_CUDA(cudaMemsetAsync(s.ctl, 0, sizeof(Ctl), st));
+    launch();
+    cudaEvent_t e0, e1;
+    HM_CUDA(cudaEventCreate(&e0));
+    HM_CUDA(cudaEventCreate(&e1));
+    HM_CUDA(cudaEventRecord(e0, st));
+    for (int i = 0; i < reps; i++) launch();
+    HM_CUDA(cudaEventRecord(e1, st));
+    HM_CUDA(cudaEventSynchronize(e1));
+    HM_CUDA(cudaGetLastError());
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    dfree(x);
+    dfree(y);
+    *ms = t / reps;
+    switch (which) {
+    case 0: *bytes = nnz * 12 + (double)n * 16; break;
+    case 1: *bytes = nnz * 12 + (double)n * 36; break;
+    case 2: *bytes = nnz * 12 + (double)n * 32; break;
+    case 3: *bytes = nnz * (vb16 + 4) + (double)n * 20; break;
+    default: *bytes = nnz * (vb16 + 4) + (double)n * 16; break;
+    }
+    return HMFEM_OK;
+}
+
+}  // namespace hm

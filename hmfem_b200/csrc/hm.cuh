@@ -1,0 +1,107 @@
+// hm.cuh -- solver data structures and launcher prototypes shared by the
+// hmfem B200 translation units.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace hm {
+
+// Compressed rows: rowptr[n+1], col/val[nnz].  Rows keep the producer's
+// column order (level 0: d,l,c,r,u,t,b as solve_linsys packs it; coarse
+// levels: ascending, as new_triple_product leaves them).
+struct Csr {
+    int n = 0;
+    long nnz = 0;
+    int *rowptr = nullptr;
+    int *col = nullptr;
+    double *val = nullptr;
+};
+
+// SELL-32: slices of 32 rows, each padded to its longest row; element k of
+// row r lives at sptr[r/32] + k*32 + r%32 (warp-coalesced).  Padding has
+// col = the row itself (or 0 past n) and value 0.
+struct Sell {
+    int n = 0;
+    int nslices = 0;
+    long len = 0;             // padded entries
+    long long *sptr = nullptr;  // nslices+1
+    int *col = nullptr;
+    double *val = nullptr;    // FP64 values
+    float *val32 = nullptr;   // FP32 copy (mixed-precision V-cycle)
+    __nv_bfloat16 *val16 = nullptr;  // BF16 copy (coarse levels)
+};
+
+struct Level {
+    Csr A;
+    Sell S;
+    double *dinv = nullptr;   // 1 / last stored diagonal entry (amg.h:1195)
+    float *dinv32 = nullptr;
+    double *dsm = nullptr;    // smoother diagonal inverse (Jacobi or l1)
+    float *dsm32 = nullptr;
+    // transfer to level+1 (absent on the coarsest)
+    signed char *sel = nullptr;  // 1 = C, 2 = F
+    int *cid = nullptr;          // coarse id of C rows (prefix count)
+    int nc = 0;
+    Csr P;                    // P rows: coarse ids in the fine row's order
+    double *pw = nullptr;     // 1 / pcnt per fine row (the P weights)
+    float *pw32 = nullptr;
+    Csr R;                    // P^T rows: fine ids ascending
+    // V-cycle vectors (FP64 and FP32 sets)
+    double *f = nullptr, *ua = nullptr, *ub = nullptr, *rs = nullptr;
+    float *f32 = nullptr, *ua32 = nullptr, *ub32 = nullptr, *rs32 = nullptr;
+};
+
+// Device-resident CG state; kernels read the scalars they need from here,
+// so an iteration runs without host round trips.
+struct Ctl {
+    double sigma, sigma_last, sigma_first, tau, alpha, beta;
+    double rr, bb, trr, tol2, rz_old;
+    int done, check, iters, status, max_iter, stop_rule, nrep, pad;
+    unsigned tickets[16];
+};
+
+// reduction slots (tickets[] index + partial buffer row)
+enum { RED_TAU = 0, RED_RR, RED_SIGMA, RED_TRR, RED_BB, RED_A, RED_B, RED_C,
+       RED_SLOTS };
+
+// ---- launchers (all enqueue on `st`) ---------------------------------
+// assembly / flux (assemble.cu)
+int launch_l0_rowcounts(int nx, int ny, int nz, int *cnt, cudaStream_t st);
+int launch_assemble(int nx, int ny, int nz, double hx, double hy, double hz,
+                    double visc, const double *KX, const double *KY,
+                    const double *KZ, const int bc[6], double *const face[6],
+                    const double *KI, const double *WI, const double *pc,
+                    const double *pw, const int *rowptr, int *col, double *val,
+                    double *b, cudaStream_t st);
+int launch_pack_stencil(int n, const hmfem_ele *perm, const hmfem_ind *ind,
+                        int *cnt, const int *rowptr, int *col, double *val,
+                        int pass, cudaStream_t st);
+int launch_flux(int nx, int ny, int nz, double hx, double hy, double hz,
+                double visc, const double *KX, const double *KY,
+                const double *KZ, const int bc[6], double *const face[6],
+                const double *p, hmfem_ele *v, double *mm, cudaStream_t st);
+
+// sparse utilities (sparse.cu)
+int scan_exclusive(const int *in, int *out, int n, cudaStream_t st);
+int rowptr_from_counts(int *rowptr, int n, cudaStream_t st, long *nnz_out);
+int csr_to_sell(const Csr &A, Sell &S, cudaStream_t st);
+int sell_fill_lowp(Sell &S, bool f32, bool bf16, cudaStream_t st);
+int launch_diag_inv(const Csr &A, double *dinv, float *dinv32, cudaStream_t st);
+int launch_spmv(const Sell &S, const double *x, double *y, cudaStream_t st);
+
+// AMG setup (amg_setup.cu)
+int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *err_dev);
+
+// cycle + CG (cycle.cu)
+struct Solver;
+int cycle_fp64(Solver &s, int l, cudaStream_t st, bool dot_into_sigma);
+int cycle_fp32(Solver &s, int l, cudaStream_t st, bool dot_into_sigma);
+
+void *dalloc(size_t bytes);
+void dfree(void *p);
+
+}  // namespace hm

@@ -1,0 +1,83 @@
+// solver.cuh -- the solver object behind the hmfem_* C-ABI.
+#pragma once
+#include <type_traits>
+#include <vector>
+
+#include "hm.cuh"
+
+namespace hm {
+
+struct Solver {
+    hmfem_options opt;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+
+    // grid problem (hmfem_assemble)
+    bool have_grid = false;
+    int nx = 0, ny = 0, nz = 0;
+    double hx = 0, hy = 0, hz = 0, visc = 1;
+    int bc[6] = {0, 0, 1, 1, 1, 1};
+    const double *KX = nullptr, *KY = nullptr, *KZ = nullptr;
+    double *Kown[3] = {nullptr, nullptr, nullptr};
+    double *face[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    double *mm = nullptr;  // flux min / max
+
+    // level-0 matrix and right-hand side
+    double *b = nullptr;
+    std::vector<Level> lv;
+    int nlevels = 0;
+    bool setup_done = false;
+    int direct_level = -1;
+    double *dense_L = nullptr;
+
+    // CG state
+    double *x = nullptr, *r = nullptr, *s = nullptr, *v = nullptr, *z = nullptr;
+    Ctl *ctl = nullptr;
+    Ctl *ctl_host = nullptr;  // pinned, 2 slots
+    double *part = nullptr;
+    int *dwork = nullptr;
+    bool ctl_active = false;
+    int first_sigma = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    hmfem_stats last{};
+
+    bool use_bf16(int l) const
+    {
+        return opt.precision == 1 && opt.bf16_from >= 0 && l >= opt.bf16_from;
+    }
+    // level vectors; level 0 of the FP64 cycle works on the CG's r and z
+    template <class T> T *vec_f(int l);
+    template <class T> T *vec_ua(int l);
+    template <class T> T *vec_ub(int l);
+    template <class T> T *vec_rs(int l);
+    template <class T> const T *vec_dinv(int l);  // smoother diagonal
+    template <class T> const T *vec_dtrue(int l); // 1 / a_ii
+    template <class T> const T *sval(int l);
+};
+
+template <> inline double *Solver::vec_f<double>(int l) { return l == 0 ? r : lv[l].f; }
+template <> inline float *Solver::vec_f<float>(int l) { return lv[l].f32; }
+template <> inline double *Solver::vec_ua<double>(int l) { return lv[l].ua; }
+template <> inline float *Solver::vec_ua<float>(int l) { return lv[l].ua32; }
+template <> inline double *Solver::vec_ub<double>(int l) { return l == 0 ? z : lv[l].ub; }
+template <> inline float *Solver::vec_ub<float>(int l) { return lv[l].ub32; }
+template <> inline double *Solver::vec_rs<double>(int l) { return lv[l].rs; }
+template <> inline float *Solver::vec_rs<float>(int l) { return lv[l].rs32; }
+template <> inline const double *Solver::vec_dinv<double>(int l) { return lv[l].dsm; }
+template <> inline const float *Solver::vec_dinv<float>(int l) { return lv[l].dsm32; }
+template <> inline const double *Solver::vec_dtrue<double>(int l) { return lv[l].dinv; }
+template <> inline const float *Solver::vec_dtrue<float>(int l) { return lv[l].dinv32; }
+template <> inline const double *Solver::sval<double>(int l) { return lv[l].S.val; }
+template <> inline const float *Solver::sval<float>(int l) { return lv[l].S.val32; }
+
+int cg_init(Solver &s, cudaStream_t st);
+int cg_iteration(Solver &s, cudaStream_t st);
+int cg_precondition(Solver &s, cudaStream_t st);
+int cg_final_residual(Solver &s, cudaStream_t st);
+int launch_smoother_diag(const Csr &A, int kind, double *dsm, float *dsm32,
+                         cudaStream_t st);
+int dense_factor(const Csr &A, double *Lf, int *err, cudaStream_t st);
+int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes);
+
+}  // namespace hm

@@ -1,0 +1,229 @@
+// sparse.cu -- scans, CSR -> SELL-32 conversion, diagonal extraction and the
+// FP64 SELL SpMV.
+#include <cub/device/device_scan.cuh>
+
+#include "hm.cuh"
+
+namespace hm {
+
+static char g_err[512];
+
+void set_last_error(const char *msg, const char *file, int line)
+{
+    snprintf(g_err, sizeof(g_err), "%s (%s:%d)", msg, file, line);
+}
+
+}  // namespace hm
+
+extern "C" const char *hmfem_last_error(void) { return hm::g_err; }
+
+namespace hm {
+
+void *dalloc(size_t bytes)
+{
+    void *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void dfree(void *p)
+{
+    if (p) cudaFree(p);
+}
+
+int scan_exclusive(const int *in, int *out, int n, cudaStream_t st)
+{
+    size_t tmp = 0;
+    HM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, st));
+    void *t = dalloc(tmp);
+    if (!t) { set_last_error("out of device memory (scan)", __FILE__, __LINE__); return HMFEM_E_CUDA; }
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(t, tmp, in, out, n, st);
+    cudaStreamSynchronize(st);
+    dfree(t);
+    HM_CUDA(e);
+    return HMFEM_OK;
+}
+
+// rowptr[0..n) holds counts on entry; on exit rowptr[0..n] is the exclusive
+// scan with rowptr[n] = total, which is returned in *nnz_out.
+int rowptr_from_counts(int *rowptr, int n, cudaStream_t st, long *nnz_out)
+{
+    int last = 0;
+    if (n > 0)
+        HM_CUDA(cudaMemcpyAsync(&last, rowptr + n - 1, sizeof(int),
+                                cudaMemcpyDeviceToHost, st));
+    HM_CHECK(scan_exclusive(rowptr, rowptr, n, st));
+    int base = 0;
+    if (n > 0)
+        HM_CUDA(cudaMemcpyAsync(&base, rowptr + n - 1, sizeof(int),
+                                cudaMemcpyDeviceToHost, st));
+    HM_CUDA(cudaStreamSynchronize(st));
+    long tot = (long)base + last;
+    if (tot > 2147483647L) {
+        set_last_error("more than 2^31-1 nonzeros", __FILE__, __LINE__);
+        return HMFEM_E_CAPACITY;
+    }
+    int t32 = (int)tot;
+    HM_CUDA(cudaMemcpyAsync(rowptr + n, &t32, sizeof(int),
+                            cudaMemcpyHostToDevice, st));
+    HM_CUDA(cudaStreamSynchronize(st));
+    *nnz_out = tot;
+    return HMFEM_OK;
+}
+
+namespace {
+
+__global__ void k_slice_len(const int *__restrict__ rowptr, int n, int nslices,
+                            long long *slen)
+{
+    int lane = threadIdx.x & 31;
+    for (long q = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+         q < nslices; q += ((long)gridDim.x * blockDim.x) >> 5) {
+        long r = q * 32 + lane;
+        int len = r < n ? rowptr[r + 1] - rowptr[r] : 0;
+        for (int o = 16; o > 0; o >>= 1)
+            len = max(len, __shfl_xor_sync(0xffffffffu, len, o));
+        if (lane == 0) slen[q] = (long long)len * 32;
+    }
+}
+
+__global__ void k_sell_fill(const int *__restrict__ rowptr,
+                            const int *__restrict__ col,
+                            const double *__restrict__ val, int n,
+                            long nrows_pad, const long long *__restrict__ sptr,
+                            int *scol, double *sval)
+{
+    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < nrows_pad;
+         r += (long)gridDim.x * blockDim.x) {
+        long q = r >> 5;
+        int lane = (int)(r & 31);
+        long long base = sptr[q];
+        int w = (int)((sptr[q + 1] - base) >> 5);
+        int a = 0, len = 0;
+        if (r < n) { a = rowptr[r]; len = rowptr[r + 1] - a; }
+        int self = r < n ? (int)r : 0;
+        for (int k = 0; k < w; k++) {
+            long long o = base + (long long)k * 32 + lane;
+            if (k < len) { scol[o] = col[a + k]; sval[o] = val[a + k]; }
+            else { scol[o] = self; sval[o] = 0.0; }
+        }
+    }
+}
+
+__global__ void k_to_lowp(const double *__restrict__ v, long len, float *f32,
+                          __nv_bfloat16 *b16)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < len;
+         i += (long)gridDim.x * blockDim.x) {
+        double x = v[i];
+        if (f32) f32[i] = (float)x;
+        if (b16) b16[i] = __float2bfloat16((float)x);
+    }
+}
+
+// amg.h:159-166 / 1216-1225: the LAST stored diagonal entry wins.
+__global__ void k_diag_inv(const int *__restrict__ rowptr,
+                           const int *__restrict__ col,
+                           const double *__restrict__ val, int n, double *dinv,
+                           float *dinv32)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x) {
+        double d = 0.0;
+        for (int k = rowptr[i]; k < rowptr[i + 1]; k++)
+            if (col[k] == i) d = val[k];
+        double v = 1.0 / d;
+        dinv[i] = v;
+        if (dinv32) dinv32[i] = (float)v;
+    }
+}
+
+// y = A x, one thread per row, row order kept (generic_operator.h:230-245).
+__global__ void __launch_bounds__(256)
+k_spmv(const long long *__restrict__ sptr, const int *__restrict__ scol,
+       const double *__restrict__ sval, int n, const double *__restrict__ x,
+       double *__restrict__ y)
+{
+    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < n;
+         r += (long)gridDim.x * blockDim.x) {
+        long q = r >> 5;
+        int lane = (int)(r & 31);
+        long long base = sptr[q];
+        int w = (int)((sptr[q + 1] - base) >> 5);
+        double s = 0.0;
+        for (int k = 0; k < w; k++) {
+            long long o = base + (long long)k * 32 + lane;
+            s = dadd(s, dmul(sval[o], x[scol[o]]));
+        }
+        y[r] = s;
+    }
+}
+
+int nblocks(long n, int threads, long cap = 148L * 16)
+{
+    long b = ceil_div(n, threads);
+    if (b < 1) b = 1;
+    return (int)(b < cap ? b : cap);
+}
+
+}  // namespace
+
+int csr_to_sell(const Csr &A, Sell &S, cudaStream_t st)
+{
+    S.n = A.n;
+    S.nslices = (int)ceil_div(A.n, 32);
+    S.sptr = (long long *)dalloc(sizeof(long long) * (S.nslices + 1));
+    if (!S.sptr) { set_last_error("out of device memory (sell)", __FILE__, __LINE__); return HMFEM_E_CUDA; }
+    k_slice_len<<<nblocks((long)S.nslices * 32, 256), 256, 0, st>>>(
+        A.rowptr, A.n, S.nslices, S.sptr);
+    HM_CUDA(cudaGetLastError());
+    size_t tmp = 0;
+    HM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, S.sptr, S.sptr,
+                                          S.nslices + 1, st));
+    void *t = dalloc(tmp);
+    HM_CUDA(cudaMemsetAsync(S.sptr + S.nslices, 0, sizeof(long long), st));
+    HM_CUDA(cub::DeviceScan::ExclusiveSum(t, tmp, S.sptr, S.sptr,
+                                          S.nslices + 1, st));
+    long long len = 0;
+    HM_CUDA(cudaMemcpyAsync(&len, S.sptr + S.nslices, sizeof(long long),
+                            cudaMemcpyDeviceToHost, st));
+    HM_CUDA(cudaStreamSynchronize(st));
+    dfree(t);
+    S.len = len;
+    S.col = (int *)dalloc(sizeof(int) * (len > 0 ? len : 1));
+    S.val = (double *)dalloc(sizeof(double) * (len > 0 ? len : 1));
+    if (!S.col || !S.val) { set_last_error("out of device memory (sell)", __FILE__, __LINE__); return HMFEM_E_CUDA; }
+    k_sell_fill<<<nblocks((long)S.nslices * 32, 256), 256, 0, st>>>(
+        A.rowptr, A.col, A.val, A.n, (long)S.nslices * 32, S.sptr, S.col, S.val);
+    HM_CUDA(cudaGetLastError());
+    return HMFEM_OK;
+}
+
+int sell_fill_lowp(Sell &S, bool f32, bool bf16, cudaStream_t st)
+{
+    if (f32 && !S.val32) S.val32 = (float *)dalloc(sizeof(float) * (S.len > 0 ? S.len : 1));
+    if (bf16 && !S.val16) S.val16 = (__nv_bfloat16 *)dalloc(2 * (S.len > 0 ? S.len : 1));
+    k_to_lowp<<<nblocks(S.len, 256), 256, 0, st>>>(S.val, S.len,
+                                                   f32 ? S.val32 : nullptr,
+                                                   bf16 ? S.val16 : nullptr);
+    HM_CUDA(cudaGetLastError());
+    return HMFEM_OK;
+}
+
+int launch_diag_inv(const Csr &A, double *dinv, float *dinv32, cudaStream_t st)
+{
+    k_diag_inv<<<nblocks(A.n, 256), 256, 0, st>>>(A.rowptr, A.col, A.val, A.n,
+                                                   dinv, dinv32);
+    HM_CUDA(cudaGetLastError());
+    return HMFEM_OK;
+}
+
+int launch_spmv(const Sell &S, const double *x, double *y, cudaStream_t st)
+{
+    k_spmv<<<nblocks(S.n, 256), 256, 0, st>>>(S.sptr, S.col, S.val, S.n, x, y);
+    HM_CUDA(cudaGetLastError());
+    return HMFEM_OK;
+}
+
+}  // namespace hm

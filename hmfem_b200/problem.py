@@ -100,7 +100,7 @@ def gaussian_field(rng: np.random.Generator, nx: int, ny: int, nz: int,
         kx = np.fft.rfftfreq(nx)[None, None, :]
         # Fourier transform of a unit-mass Gaussian of std `corr` cells
         ker = np.exp(-2.0 * (np.pi * corr) ** 2 * (kx**2 + ky**2 + kz**2))
-        g = np.fft.irfftn(np.fft.rfftn(g) * ker, s=(nz, ny, nx))
+        g = np.fft.irfftn(np.fft.rfftn(g) * ker, s=(nz, ny, nx), axes=(0, 1, 2))
     g = g - g.mean()
     sd = g.std()
     if sd > 0:

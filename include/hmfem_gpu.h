@@ -1,0 +1,185 @@
+/*
+ * hmfem_gpu.h -- C-ABI of the B200 (sm_100a) pressure solver for hmfem.
+ *
+ * Three layers, all plain C types (pointers, sizes, status codes):
+ *
+ *  1. The reference's own bridge, same names and argument meaning, so the
+ *     hmfem application links against this library instead of compute.cpp:
+ *       compute       -- replaces compute.cpp:7-51 (declared functions.h:53)
+ *       solve_linsys  -- replaces solve_linearsystem_AMG.c:37-157
+ *                        (declared functions.h:54)
+ *     The application compiles its .c files with g++ (makefile:40-41), so
+ *     both symbols are also exported under their C++ names.
+ *
+ *  2. The reference's device layer (toolbox/lib/toolbox.cu:22-608, declared
+ *     in device_pcg.h:1-9, device_amg.h:1-10, device_generic_operator.h:7-10,
+ *     device_binary_operator.h:7-9, device_communicator.h:5-8), the fifteen
+ *     _device_* entry points with their signatures, so toolbox host code that
+ *     drives device_vector / device_amg_solver / device_conjugate_gradient
+ *     links unchanged.  They run synchronously on the legacy default stream,
+ *     as the reference's do.
+ *
+ *  3. hmfem_* : the status-returning API (no counterpart in the reference,
+ *     which prints CUDA errors and continues, toolbox.h:21-26): assembly from
+ *     permeabilities on the device, AMG setup on the device, PCG / flexible
+ *     CG, flux reconstruction, hierarchy inspection.
+ *
+ * Memory kinds: functions taking `int mem` accept host pointers (mem = 0;
+ * the library copies in and out) or device pointers (mem = 1; the caller's
+ * CUDA allocations on the current device).
+ */
+#ifndef HMFEM_GPU_H
+#define HMFEM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------- */
+#define HMFEM_OK 0
+#define HMFEM_E_NOTCONV 1   /* iteration cap reached before the tolerance */
+#define HMFEM_E_BREAKDOWN 2 /* non-finite or zero curvature in CG */
+#define HMFEM_E_CUDA 3      /* a CUDA runtime call failed */
+#define HMFEM_E_ARG 4       /* invalid argument / state */
+#define HMFEM_E_TIMEOUT 5   /* a bounded device wait gave up */
+#define HMFEM_E_CAPACITY 6  /* a sparse row exceeded the setup kernels' limit */
+
+/* ---- reference data layouts (structs.h) ------------------------------ */
+/* ELE, structs.h:7-17: per-cell face coefficients u,d,l,r, centre c, t,b */
+typedef struct { double u, d, l, r, c, t, b; } hmfem_ele;
+/* IND, structs.h:38-48: matrix column per face, -1 = boundary (RHS) */
+typedef struct { int c, u, d, l, r, t, b; } hmfem_ind;
+/* Dim, structs.h:84-95 */
+typedef struct { int x, y, z, xy, t, px, pz, py; } hmfem_dim;
+
+/* ---- layer 1: the reference bridge ------------------------------------ */
+/* compute.cpp:7-51.  hdr[0] = rows, hdr[1] = nnz; cnt/col/ele row-by-count;
+ * b read-only; x = initial guess in, solution out.  AMG (16 levels, min 1
+ * node, epsilon 0) + PCG with the reference's stopping rule at 1e-8 unless
+ * HMFEM_TOL / HMFEM_STOP override it.  Returns 0 like the reference; the
+ * iteration count goes to iter_amg.  Errors: see hmfem_last_error(). */
+int compute(int *hdr, int *cnt, int *col, double *ele, double *b, double *x);
+/* solve_linearsystem_AMG.c:37-157: packs the AoS stencil on the device in
+ * the reference's row order (d,l,c,r,u,t,b) and solves as compute() does. */
+void solve_linsys(hmfem_ele *perm, hmfem_ind *indcol, double *b, double *x,
+                  hmfem_dim N);
+/* variables.h:63 -- defined weakly here; the application's definition wins */
+extern int iter_amg;
+
+/* ---- layer 2: the reference device layer (toolbox.cu) --------------- */
+void _device_add_scale(double *x, double *y, double s, unsigned int m);   /* toolbox.cu:22-33  x += s y */
+void _device_sub_scale(double *x, double *y, double s, unsigned int m);   /* toolbox.cu:52-63  x -= s y */
+void _device_scale_add(double *x, double *y, double s, unsigned int m);   /* toolbox.cu:82-93  x = s x + y */
+void _device_vector_product(double *x, double *y, double *z, unsigned int n,
+                            unsigned int m);                              /* toolbox.cu:102-143 z[0..m) partials */
+void _device_linear_operator(int *cnt, int *dsp, int *col, double *ele, int l,
+                             int m, int n, double *u, double *v);         /* toolbox.cu:150-240 SELL-32 v = A u */
+void _device_jacobi(int *cnt, int *dsp, int *col, double *ele, int l, int n,
+                    double *f, double *u, double *v);                     /* toolbox.cu:249-347 v = f - A u */
+void _device_set_mul(double *x, double *y, double *z, double omega,
+                     unsigned int m);                                     /* toolbox.cu:356-377 x = w y z */
+void _device_add_mul(double *x, double *y, double *z, double omega,
+                     unsigned int m);                                     /* toolbox.cu:386-407 x += w y z */
+void _device_diagonal_solver(double *x, double *y, double *z,
+                             unsigned int m);                             /* toolbox.cu:415-435 x = y z */
+void _device_com_snd(double *x, double *svec, int *rcom, unsigned int n);  /* toolbox.cu:443-464 svec = x[rcom] */
+void _device_com_rcv(double *x, double *rvec, int *rcom, unsigned int n);  /* toolbox.cu:472-506 x[rcom] += rvec */
+void _device_sub(double *x, double *y, unsigned int m);                   /* toolbox.cu:513-532 y -= x */
+void _device_add(double *x, double *y, unsigned int m);                   /* toolbox.cu:539-558 y += x */
+void _device_rsb(double *x, double *y, unsigned int m);                   /* toolbox.cu:565-584 y = x - y */
+void _device_matrix_conversion(int *acnt, int *adsp, int *acol, double *aele,
+                               int *tdsp, int *tcol, double *tele, int n); /* toolbox.cu:586-608 CSR -> SELL-32 */
+
+/* ---- layer 3: status-returning API ------------------------------------ */
+typedef struct hmfem_solver hmfem_solver;
+
+typedef struct {
+    int precision;     /* 0: FP64 V-cycle inside PCG (the plain drop-in);
+                          1: FP32 V-cycle (coarse values BF16 from level
+                          `bf16_from`) inside FP64 flexible CG */
+    int bf16_from;     /* first level stored in BF16 (precision 1); <0 = none */
+    int smoother;      /* 0: damped Jacobi with 1/a_ii (device_amg.h design);
+                          1: l1-Jacobi, 1/(a_ii + sum_j!=i |a_ij|) (default:
+                          SPD preconditioner for any SPD matrix) */
+    double omega;      /* Jacobi weight (compute.cpp:35 passes 1.0) */
+    double tol;        /* stopping tolerance */
+    int stop_rule;     /* 0: true residual ||b-Ax||/||b|| <= tol;
+                          1: reference rule (pcg.h:57) sigma/sigma0 <= tol^2 */
+    int max_iter;      /* CG iteration cap (compute.cpp:42: 10000) */
+    int max_levels;    /* compute.cpp:36: 16 */
+    int min_coarse;    /* compute.cpp:37: 1 */
+    int coarse_direct; /* solve the first level with <= this many rows by a
+                          dense FP64 Cholesky; 0 = the reference's diagonal
+                          solve on the coarsest level (amg.h:1353-1364) */
+    int check_every;   /* host polls convergence every k iterations */
+    int verbose;
+} hmfem_options;
+
+typedef struct {
+    int iterations;
+    int levels;
+    int status;
+    double relres;        /* final true ||b - A x|| / ||b|| (FP64) */
+    double t_assemble_ms, t_setup_ms, t_solve_ms, t_flux_ms;
+    double divmin, divmax; /* divvel_pontual min/max |div u| */
+} hmfem_stats;
+
+void hmfem_default_options(hmfem_options *opt);
+int hmfem_create(hmfem_solver **s, const hmfem_options *opt);
+int hmfem_destroy(hmfem_solver *s);
+/* Work on a caller stream (cudaStream_t passed as void*); NULL = the
+ * solver's own non-blocking stream. */
+int hmfem_set_stream(hmfem_solver *s, void *stream);
+void *hmfem_get_stream(hmfem_solver *s);
+const char *hmfem_last_error(void);
+
+/* TPFA assembly from permeabilities (permeabilities.c:196-492 and
+ * set_source_term.c:9-223 on the device).  K arrays are n = nx*ny*nz cells,
+ * s = i + j nx + k nx ny.  Faces l,r,u,d,t,b; bc_type 0 Dirichlet, 1
+ * Neumann; face_vals[f] (nullable) are per-face arrays in the Bound layout,
+ * else bc_value[f] everywhere.  KI/WI (nullable) are the well/karst indices
+ * of the diagonal and pc/pw the pressures they multiply in the RHS. */
+int hmfem_assemble(hmfem_solver *s, int nx, int ny, int nz, double hx,
+                   double hy, double hz, double visc, const double *KX,
+                   const double *KY, const double *KZ, const int bc_type[6],
+                   const double bc_value[6], const double *const *face_vals,
+                   int mem);
+/* A general symmetric matrix in the reference's row-by-count form. */
+int hmfem_set_matrix(hmfem_solver *s, int n, long nnz, const int *cnt,
+                     const int *col, const double *ele, const double *b,
+                     int mem);
+/* AoS stencil + index arrays as solve_linsys receives them. */
+int hmfem_set_stencil(hmfem_solver *s, int nx, int ny, int nz,
+                      const hmfem_ele *perm, const hmfem_ind *indcol,
+                      const double *b, int mem);
+/* AMG hierarchy on the device (structure bit-exact with amg.h). */
+int hmfem_setup(hmfem_solver *s);
+/* Solve A x = b (b NULL: the assembled right-hand side); x = initial guess
+ * in, solution out. */
+int hmfem_solve(hmfem_solver *s, const double *b, double *x, int mem,
+                hmfem_stats *st);
+/* Face fluxes (flux_reconstruction.c:9-279) into n ELE (c untouched) and the
+ * divvel_pontual min/max.  Needs hmfem_assemble. */
+int hmfem_fluxes(hmfem_solver *s, const double *p, hmfem_ele *v, int mem,
+                 double *divmin, double *divmax);
+/* Inspection for parity tests. */
+int hmfem_num_levels(hmfem_solver *s);
+int hmfem_level_info(hmfem_solver *s, int l, int *n, long *nnz, long *pnnz);
+int hmfem_level_copy(hmfem_solver *s, int l, int *cnt, int *col, double *ele,
+                     double *dinv, signed char *sel, int *pcnt, int *pcol);
+int hmfem_vcycle(hmfem_solver *s, const double *f, double *u, int mem);
+int hmfem_spmv(hmfem_solver *s, int level, const double *x, double *y,
+               int mem);
+int hmfem_rhs(hmfem_solver *s, double *b, int mem);
+int hmfem_last_stats(hmfem_solver *s, hmfem_stats *st);
+/* Measurement: mean duration of `reps` launches of one solve-phase kernel
+ * on level l (0 SpMV FP64, 1/2 pre/post smoother FP64, 3/4 pre/post
+ * smoother FP32) timed with CUDA events on the solver stream, and its
+ * algorithmic bytes per launch. */
+int hmfem_time_kernel(hmfem_solver *s, int which, int level, int reps,
+                      float *ms, double *bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -277,6 +277,21 @@ static void spmt(int arows, const int *acnt, const int *acol,
     *ccnt_o = ccnt; *ccol_o = ccol; *cele_o = cele; *csize_o = csize;
 }
 
+/* l1-Jacobi diagonal: a_ii + sum over the other stored entries of |a_ij|,
+ * accumulated in row order (project smoother, no reference counterpart). */
+static double *l1_inverse(const or_level *A, const double *dia)
+{
+    double *d = (double *)malloc(sizeof(double) * (A->n > 0 ? A->n : 1));
+    long m = 0;
+    for (int i = 0; i < A->n; i++) {
+        double t = 0.0;
+        for (int j = 0; j < A->cnt[i]; j++, m++)
+            if (A->col[m] != i) t = t + fabs(A->ele[m]);
+        d[i] = 1.0 / (dia[i] + t);
+    }
+    return d;
+}
+
 /* One coarsening step: parallel_coarsening (amg.h:37-223), then
  * parallel_interpolation (amg.h:228-406), then new_triple_product
  * (amg.h:567-582), for a single rank (no interface nodes). */
@@ -343,6 +358,7 @@ static void coarsen_level(double eps, or_level *A, or_level *Cn)
     /* 1/diag on this level (amg.h:1195) */
     A->dinv = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
     for (int i = 0; i < n; i++) A->dinv[i] = 1.0 / dia[i];
+    A->dl1inv = l1_inverse(A, dia);
     free(dia); free(cox); free(cid); free(dsp);
 }
 
@@ -374,13 +390,14 @@ int or_amg_setup(int n, const int *cnt, const int *col, const double *ele,
     /* coarsest level: 1/diag (amg.h:1214-1226) */
     or_level *C = &H->lv[l];
     C->dinv = (double *)malloc(sizeof(double) * (C->n > 0 ? C->n : 1));
+    double *cd = (double *)calloc(C->n > 0 ? C->n : 1, sizeof(double));
     for (long t = 0, i = 0; i < C->n; i++) {
-        double d = 0.0;
-        int have = 0;
         for (int j = 0; j < C->cnt[i]; j++, t++)
-            if (C->col[t] == i) { d = C->ele[t]; have = 1; }
-        C->dinv[i] = have ? 1.0 / d : 1.0 / 0.0;
+            if (C->col[t] == i) cd[i] = C->ele[t];
+        C->dinv[i] = 1.0 / cd[i];
     }
+    C->dl1inv = l1_inverse(C, cd);
+    free(cd);
     H->nlevels = l + 1;
     return H->nlevels;
 }
@@ -389,7 +406,7 @@ void or_amg_free(or_hierarchy *H)
 {
     for (int l = 0; l < H->nlevels; l++) {
         or_level *A = &H->lv[l];
-        free(A->cnt); free(A->col); free(A->ele); free(A->dinv);
+        free(A->cnt); free(A->col); free(A->ele); free(A->dinv); free(A->dl1inv);
         free(A->sel); free(A->pcnt); free(A->pcol); free(A->pele);
     }
     memset(H, 0, sizeof(*H));
@@ -505,7 +522,8 @@ static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
         }
     } else {
         /* device_jacobi 3-arg (device_amg.h:35-42): u = w D^-1 f; r = f - A u */
-        for (int i = 0; i < n; i++) u[i] = omega * f[i] * A->dinv[i];
+        const double *dv = smoother == 2 ? A->dl1inv : A->dinv;
+        for (int i = 0; i < n; i++) u[i] = omega * f[i] * dv[i];
         long m = 0;
         for (int i = 0; i < n; i++) {
             double t = f[i];
@@ -537,7 +555,8 @@ static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
             for (int j = 0; j < A->cnt[i]; j++, m++) t -= A->ele[m] * u[A->col[m]];
             r[i] = t;
         }
-        for (int i = 0; i < n; i++) u[i] += omega * r[i] * A->dinv[i];
+        const double *dv = smoother == 2 ? A->dl1inv : A->dinv;
+        for (int i = 0; i < n; i++) u[i] += omega * r[i] * dv[i];
     }
 }
 

@@ -61,6 +61,8 @@ typedef struct {
     int *cnt, *col;       /* row counts, row-concatenated columns */
     double *ele;          /* values */
     double *dinv;         /* 1 / (last stored diagonal entry) */
+    double *dl1inv;       /* 1 / (a_ii + sum_{j!=i} |a_ij|), row order: the
+                             l1-Jacobi diagonal (not in the reference) */
     /* transfer to the next level (absent on the coarsest level) */
     char *sel;            /* 1 = C, 2 = F (amg.h:1-32) */
     long pnnz;
@@ -85,7 +87,9 @@ void or_amg_free(or_hierarchy *H);
  * smoother 0: the NOMPI Gauss-Seidel branch (amg.h:1315-1322, 759-784,
  *             930-961), the path compute.cpp runs.
  * smoother 1: the device design's damped Jacobi (device_amg.h:11-43,
- *             396-411), with omega. */
+ *             396-411), with omega.
+ * smoother 2: the same cycle with the l1-Jacobi diagonal (dl1inv): the GPU
+ *             solver's default, an SPD preconditioner for any SPD matrix. */
 void or_vcycle(const or_hierarchy *H, int smoother, double omega,
                const double *f, double *u);
 
