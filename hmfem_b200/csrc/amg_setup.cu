@@ -18,6 +18,7 @@
 // increasing order through an atomic ticket, so a tile only ever waits on
 // tiles that are already resident; every wait is bounded.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "hm.cuh"
 
@@ -107,208 +108,231 @@ __global__ void k_hist(const int *__restrict__ key, long m, int *cnt)
         atomicAdd(cnt + key[i], 1);
 }
 
-// ---- sparse union of rows: warp (or block) per output row -------------
+// ---- Galerkin products: sparse union of rows ---------------------------
 //
-// Candidates of an output row are generated in the reference's summation
-// order; the distinct columns are sorted; each slot's value is the ordered
-// sum of its candidates.  MODE 0 counts distinct columns, MODE 1 writes
-// columns and values.
+// One output row is the union of several inner rows scaled by outer
+// entries:
+//   STAGE 0:  AP row i  = sum_{j in A(i), stored order}   a_ij w_j * P(j)
+//   STAGE 1:  Ac row e  = sum_{i in R(e), ascending}       w_i * AP(i)
+// (w = the P weight 1/|P row|).  Candidates are generated in exactly the
+// order sparse_multiply_transpose adds them (amg.h:520-546), tagged with
+// their generation index g, and sorted by (column, g); each run of equal
+// columns is then summed in g order with non-contracted adds, so every
+// value is bit-identical to the reference's.
 //
-// STAGE 0: AP row i   = sum_{j in A(i)} a_ij * w_j * e_{P(j)}
-// STAGE 1: Ac row e   = sum_{i in R(e), ascending} w_i * AP(i)
+// Pass A counts candidates per row (an upper bound of the row length);
+// pass B writes distinct columns and sums into a padded buffer (a warp per
+// row, sized by the row's candidate count; long rows fall through to wider
+// tiers); pass C compacts the padded rows into CSR.
 struct UnionArgs {
     int nrows;
-    // outer rows: stage 0 -> A, stage 1 -> R
-    const int *orow, *ocol;
-    const double *oval;  // stage 0: A values; stage 1: unused
-    const double *w;     // stage 0: P weight of column row; stage 1: of row i
-    // inner rows: stage 0 -> P (cols), stage 1 -> AP (cols, vals)
-    const int *irow, *icol;
-    const double *ival;
-    // output
-    int *cnt;            // MODE 0
-    const int *out_row;  // MODE 1
-    int *out_col;
-    double *out_val;
-    int *long_rows, *n_long;  // rows over capacity (first pass)
+    const int *orow, *ocol;  // outer rows: stage 0 A, stage 1 R
+    const double *oval;      // stage 0: A values
+    const double *w;         // P weight per fine row
+    const int *irow, *icol;  // inner rows: stage 0 P, stage 1 AP
+    const double *ival;      // stage 1: AP values
+    const long long *cptr;   // candidate offsets (pass A scan)
+    int *ucnt;               // distinct columns per row
+    int *pcol;               // padded output
+    double *pval;
+    int *list[2], *nlist[2]; // rows deferred to the next tier
     int *err;
 };
 
 template <int STAGE>
-__device__ __forceinline__ int cand_count(const UnionArgs &A, int r)
+__global__ void k_cand_count(UnionArgs A, long long *ccnt)
 {
-    int m = 0;
-    for (int k = A.orow[r]; k < A.orow[r + 1]; k++) {
-        int j = A.ocol[k];
-        m += A.irow[j + 1] - A.irow[j];
+    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < A.nrows;
+         r += (long)gridDim.x * blockDim.x) {
+        long long m = 0;
+        for (int k = A.orow[r]; k < A.orow[r + 1]; k++) {
+            int j = A.ocol[k];
+            m += A.irow[j + 1] - A.irow[j];
+        }
+        ccnt[r] = m;
     }
-    return m;
 }
 
-struct WarpG {
-    __device__ int rank() const { return threadIdx.x & 31; }
-    __device__ int size() const { return 32; }
-    __device__ void sync() const { __syncwarp(); }
-};
-struct BlockG {
-    __device__ int rank() const { return threadIdx.x; }
-    __device__ int size() const { return blockDim.x; }
-    __device__ void sync() const { __syncthreads(); }
-};
+__device__ __forceinline__ int key_col(unsigned long long k) { return (int)(k >> 32); }
+__device__ __forceinline__ int key_gen(unsigned long long k) { return (int)(k & 0xffffffffu); }
 
-// Gathers candidates of row r into cd/ct (generation order), sorts a copy
-// in sb, compacts distinct columns to the front of sb; returns the count.
-template <int STAGE, bool VALUES, class G>
-__device__ int row_union(const G &g, const UnionArgs &A, int r, int m,
-                         int *cd, double *ct, int *sb)
+// Bitonic sort of m (power of two) 64-bit keys in shared memory by a group
+// of `gs` threads with rank `gr`.
+template <bool BLOCK>
+__device__ void sort_keys(unsigned long long *a, int m, int gr, int gs)
 {
-    // generation: walk the outer row in order; each outer entry expands
-    // into a contiguous inner row.  Position of each inner entry = running
-    // offset, computed serially per outer entry (rows are short).
+    for (int k = 2; k <= m; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = gr; i < m; i += gs) {
+                int ixj = i ^ j;
+                if (ixj > i) {
+                    unsigned long long x = a[i], y = a[ixj];
+                    if ((x > y) == ((i & k) == 0)) { a[i] = y; a[ixj] = x; }
+                }
+            }
+            if (BLOCK) __syncthreads(); else __syncwarp();
+        }
+}
+
+// Generates the candidates of row r into keys/vals (group-parallel over the
+// outer entries: each thread expands one outer entry's inner row).
+template <int STAGE, bool BLOCK>
+__device__ void gen_row(const UnionArgs &A, int r, unsigned long long *keys,
+                        double *vals, int gr, int gs, int *s_scan)
+{
+    const int ob = A.orow[r], oe = A.orow[r + 1];
     int base = 0;
-    for (int k = A.orow[r]; k < A.orow[r + 1]; k++) {
-        int j = A.ocol[k];
-        int ib = A.irow[j], ie = A.irow[j + 1];
+    for (int c0 = ob; c0 < oe; c0 += gs) {
+        int k = c0 + gr;
+        bool ok = k < oe;
+        int j = ok ? A.ocol[k] : 0;
+        int ib = ok ? A.irow[j] : 0;
+        int len = ok ? A.irow[j + 1] - ib : 0;
         double s = 0.0;
-        if (VALUES) s = STAGE == 0 ? dmul(A.oval[k], A.w[j]) : A.w[j];
-        for (int q = ib + g.rank(); q < ie; q += g.size()) {
-            int d = A.icol[q];
-            cd[base + q - ib] = d;
-            sb[base + q - ib] = d;
-            // stage 0: t = a_ij * p_jd with p_jd = w_j (amg.h:537)
-            // stage 1: t = AP[i][d] * p_ie with p_ie = w_i (same line)
-            if (VALUES) ct[base + q - ib] = STAGE == 0 ? s : dmul(A.ival[q], s);
+        if (ok) s = STAGE == 0 ? dmul(A.oval[k], A.w[j]) : A.w[j];
+        // exclusive scan of len over the group
+        int off, tot;
+        if (!BLOCK) {
+            int lane = gr;
+            int x = len;
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            off = x - len;
+            tot = __shfl_sync(0xffffffffu, x, 31);
+        } else {
+            s_scan[gr] = len;
+            __syncthreads();
+            if (gr == 0) {
+                int t = 0;
+                for (int q = 0; q < gs; q++) { int v = s_scan[q]; s_scan[q] = t; t += v; }
+                s_scan[gs] = t;
+            }
+            __syncthreads();
+            off = s_scan[gr];
+            tot = s_scan[gs];
+            __syncthreads();
         }
-        base += ie - ib;
+        for (int q = 0; q < len; q++) {
+            int g = base + off + q;
+            int d = A.icol[ib + q];
+            keys[g] = ((unsigned long long)(unsigned)d << 32) | (unsigned)g;
+            // stage 0: t = a_ij * p_jd (p_jd = w_j); stage 1: t = AP[i][d] * w_i
+            vals[g] = STAGE == 0 ? s : dmul(A.ival[ib + q], s);
+        }
+        base += tot;
     }
-    int mp = next_pow2(m);
-    for (int q = m + g.rank(); q < mp; q += g.size()) sb[q] = 0x7fffffff;
-    g.sync();
-    if (g.size() == 32) warp_bitonic_sort(sb, mp);
-    else block_bitonic_sort(sb, mp);
-    // compact distinct values (one warp does it; others wait)
-    __shared__ int s_u;
+}
+
+// Distinct columns + ordered sums of sorted keys[0..m) into the padded
+// output at o; returns the number of distinct columns.  Done by one warp
+// (lane = gr & 31), chunk by chunk.
+__device__ int reduce_runs(const UnionArgs &A, const unsigned long long *keys,
+                           const double *vals, int m, long long o)
+{
+    const int lane = threadIdx.x & 31;
     int u = 0;
-    if (g.size() == 32 || threadIdx.x < 32) {
-        int lane = threadIdx.x & 31;
-        for (int c0 = 0; c0 < m; c0 += 32) {
-            int idx = c0 + lane;
-            int x = idx < m ? sb[idx] : 0;
-            bool head = idx < m && (idx == 0 || sb[idx - 1] != x);
-            unsigned bal = __ballot_sync(0xffffffffu, head);
-            int pos = u + __popc(bal & ((1u << lane) - 1));
-            __syncwarp();
-            if (head) sb[pos] = x;
-            __syncwarp();
-            u += __popc(bal);
+    for (int c0 = 0; c0 < m; c0 += 32) {
+        int idx = c0 + lane;
+        bool head = false;
+        int col = 0;
+        if (idx < m) {
+            col = key_col(keys[idx]);
+            head = idx == 0 || key_col(keys[idx - 1]) != col;
         }
-        if (g.size() != 32 && lane == 0) s_u = u;
+        unsigned bal = __ballot_sync(0xffffffffu, head);
+        if (head) {
+            int pos = u + __popc(bal & ((1u << lane) - 1));
+            double acc = vals[key_gen(keys[idx])];
+            for (int t = idx + 1; t < m && key_col(keys[t]) == col; t++)
+                acc = dadd(acc, vals[key_gen(keys[t])]);
+            A.pcol[o + pos] = col;
+            A.pval[o + pos] = acc;
+        }
+        u += __popc(bal);
     }
-    if (g.size() != 32) {
-        g.sync();
-        u = s_u;
-    }
-    g.sync();
     return u;
 }
 
-template <int STAGE, int MODE, class G>
-__device__ void union_row(const G &g, const UnionArgs &A, int r, int cap,
-                          int *cd, double *ct, int *sb)
+// Warp per row; rows with more candidates than CAP go to list[tier].
+template <int STAGE, int CAP, int WPB>
+__global__ void __launch_bounds__(32 * WPB)
+k_union_warp(UnionArgs A, const int *rows, const int *nrows_dev, int tier)
 {
-    int m = cand_count<STAGE>(A, r);
-    if (m > cap) {
-        // first (warp) pass only: defer to the block kernel
-        if (g.rank() == 0 && MODE == 0) {
-            int p = atomicAdd(A.n_long, 1);
-            A.long_rows[p] = r;
+    __shared__ unsigned long long s_keys[WPB][CAP];
+    __shared__ double s_vals[WPB][CAP];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned long long *keys = s_keys[w];
+    double *vals = s_vals[w];
+    const long nr = rows ? *nrows_dev : A.nrows;
+    for (long t = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; t < nr;
+         t += ((long)gridDim.x * blockDim.x) >> 5) {
+        const int r = rows ? rows[t] : (int)t;
+        const long long o = A.cptr[r];
+        const int m = (int)(A.cptr[r + 1] - o);
+        if (m > CAP) {
+            if (lane == 0) A.list[tier][atomicAdd(A.nlist[tier], 1)] = r;
+            continue;
         }
-        return;
+        gen_row<STAGE, false>(A, r, keys, vals, lane, 32, nullptr);
+        const int mp = next_pow2(m);
+        for (int q = m + lane; q < mp; q += 32) keys[q] = ~0ull;
+        __syncwarp();
+        sort_keys<false>(keys, mp, lane, 32);
+        int u = reduce_runs(A, keys, vals, m, o);
+        if (lane == 0) A.ucnt[r] = u;
+        __syncwarp();
     }
-    int u = row_union<STAGE, MODE == 1, G>(g, A, r, m, cd, ct, sb);
-    if (MODE == 0) {
-        if (g.rank() == 0) A.cnt[r] = u;
-        g.sync();
-        return;
-    }
-    int o = A.out_row[r];
-    if (A.out_row[r + 1] - o != u) {
-        if (g.rank() == 0) atomicExch(A.err, 2);
-        return;
-    }
-    // lane-owns-slot accumulation in generation order (amg.h:531-546)
-    for (int q = g.rank(); q < u; q += g.size()) {
-        int d = sb[q];
-        double acc = 0.0;
-        bool first = true;
-        for (int c = 0; c < m; c++) {
-            if (cd[c] != d) continue;
-            acc = first ? ct[c] : dadd(acc, ct[c]);
-            first = false;
-        }
-        A.out_col[o + q] = d;
-        A.out_val[o + q] = acc;
-    }
-    g.sync();
 }
 
-constexpr int kWarpCap = 1024;
-constexpr int kWarpsPerBlock = 4;
-
-template <int STAGE, int MODE>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock)
-k_union_warp(UnionArgs A)
-{
-    extern __shared__ unsigned char smem[];
-    int w = threadIdx.x >> 5;
-    size_t per = kWarpCap * (sizeof(int) * 2 + (MODE == 1 ? sizeof(double) : 0));
-    unsigned char *base = smem + per * w;
-    int *cd = (int *)base;
-    int *sb = cd + kWarpCap;
-    double *ct = (double *)(sb + kWarpCap);
-    WarpG g;
-    for (long r = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
-         r < A.nrows; r += ((long)gridDim.x * blockDim.x) >> 5)
-        union_row<STAGE, MODE>(g, A, (int)r, kWarpCap, cd, ct, sb);
-}
-
-// Long rows: one block per row with the whole dynamic shared memory.
-template <int STAGE, int MODE>
+// Block per row for the longest rows (dynamic shared memory, cap entries).
+template <int STAGE>
 __global__ void __launch_bounds__(256)
-k_union_block(UnionArgs A, const int *rows, int nrows, int cap)
+k_union_block(UnionArgs A, const int *rows, const int *nrows_dev, int cap)
 {
-    extern __shared__ unsigned char smem[];
-    int *cd = (int *)smem;
-    int *sb = cd + cap;
-    double *ct = (double *)(sb + cap);
-    BlockG g;
-    for (int t = blockIdx.x; t < nrows; t += gridDim.x) {
-        int r = rows[t];
-        int m = cand_count<STAGE>(A, r);
+    extern __shared__ unsigned long long s_dyn[];
+    __shared__ int s_scan[257];
+    unsigned long long *keys = s_dyn;
+    double *vals = (double *)(s_dyn + cap);
+    const long nr = *nrows_dev;
+    for (long t = blockIdx.x; t < nr; t += gridDim.x) {
+        const int r = rows[t];
+        const long long o = A.cptr[r];
+        const int m = (int)(A.cptr[r + 1] - o);
         if (m > cap) {
             if (threadIdx.x == 0) atomicExch(A.err, 3);
             return;
         }
-        int u = row_union<STAGE, MODE == 1, BlockG>(g, A, r, m, cd, ct, sb);
-        if (MODE == 0) {
-            if (threadIdx.x == 0) A.cnt[r] = u;
-            __syncthreads();
-            continue;
-        }
-        int o = A.out_row[r];
-        for (int q = threadIdx.x; q < u; q += blockDim.x) {
-            int d = sb[q];
-            double acc = 0.0;
-            bool first = true;
-            for (int c = 0; c < m; c++) {
-                if (cd[c] != d) continue;
-                acc = first ? ct[c] : dadd(acc, ct[c]);
-                first = false;
-            }
-            A.out_col[o + q] = d;
-            A.out_val[o + q] = acc;
+        gen_row<STAGE, true>(A, r, keys, vals, threadIdx.x, blockDim.x, s_scan);
+        const int mp = next_pow2(m);
+        for (int q = m + threadIdx.x; q < mp; q += blockDim.x) keys[q] = ~0ull;
+        __syncthreads();
+        sort_keys<true>(keys, mp, threadIdx.x, blockDim.x);
+        if (threadIdx.x < 32) {
+            int u = reduce_runs(A, keys, vals, m, o);
+            if (threadIdx.x == 0) A.ucnt[r] = u;
         }
         __syncthreads();
+    }
+}
+
+__global__ void k_compact(const long long *__restrict__ cptr,
+                          const int *__restrict__ rowptr, int n,
+                          const int *__restrict__ pcol,
+                          const double *__restrict__ pval, int *col,
+                          double *val)
+{
+    // a warp per row: rows are short and contiguous
+    const int lane = threadIdx.x & 31;
+    for (long r = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; r < n;
+         r += ((long)gridDim.x * blockDim.x) >> 5) {
+        const long long src = cptr[r];
+        const int dst = rowptr[r], len = rowptr[r + 1] - dst;
+        for (int q = lane; q < len; q += 32) {
+            col[dst + q] = pcol[src + q];
+            val[dst + q] = pval[src + q];
+        }
     }
 }
 
@@ -319,75 +343,85 @@ int nblk(long n, int threads, long cap = 148L * 16)
     return (int)(b < cap ? b : cap);
 }
 
-// Runs count + fill of one sparse-union stage into `out` (rowptr, col, val).
+// Runs passes A-C of one Galerkin stage into `out`.
 template <int STAGE>
 int run_union(UnionArgs A, Csr &out, int *dwork, cudaStream_t st)
 {
-    // dwork: [0] n_long, [1] err; long_rows separately
-    int *long_rows = (int *)dalloc(sizeof(int) * (A.nrows > 0 ? A.nrows : 1));
-    out.n = A.nrows;
-    out.rowptr = (int *)dalloc(sizeof(int) * (A.nrows + 1));
-    if (!long_rows || !out.rowptr) {
+    const int n = A.nrows;
+    out.n = n;
+    long long *cptr = (long long *)dalloc(sizeof(long long) * (n + 1));
+    out.rowptr = (int *)dalloc(sizeof(int) * (n + 1));
+    int *lists = (int *)dalloc(sizeof(int) * 2 * (n > 0 ? n : 1));
+    if (!cptr || !out.rowptr || !lists) {
         set_last_error("out of device memory (RAP)", __FILE__, __LINE__);
         return HMFEM_E_CUDA;
     }
-    HM_CUDA(cudaMemsetAsync(dwork, 0, 2 * sizeof(int), st));
-    A.cnt = out.rowptr;
-    A.long_rows = long_rows;
-    A.n_long = dwork;
-    A.err = dwork + 1;
-    const int thr = 32 * kWarpsPerBlock;
-    size_t smem0 = (size_t)kWarpsPerBlock * kWarpCap * 2 * sizeof(int);
-    size_t smem1 = (size_t)kWarpsPerBlock * kWarpCap * (2 * sizeof(int) + sizeof(double));
-    HM_CUDA(cudaFuncSetAttribute(k_union_warp<STAGE, 0>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0));
-    HM_CUDA(cudaFuncSetAttribute(k_union_warp<STAGE, 1>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
-    k_union_warp<STAGE, 0><<<nblk((long)A.nrows * 32, thr, 148L * 64), thr, smem0, st>>>(A);
+    // pass A
+    k_cand_count<STAGE><<<nblk(n, 256), 256, 0, st>>>(A, cptr);
     HM_CUDA(cudaGetLastError());
-    int h[2];
-    HM_CUDA(cudaMemcpyAsync(h, dwork, sizeof(h), cudaMemcpyDeviceToHost, st));
+    HM_CUDA(cudaMemsetAsync(cptr + n, 0, sizeof(long long), st));
+    {
+        size_t tmp = 0;
+        HM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, cptr, cptr, n + 1, st));
+        void *t = dalloc(tmp);
+        HM_CUDA(cub::DeviceScan::ExclusiveSum(t, tmp, cptr, cptr, n + 1, st));
+        dfree(t);
+    }
+    long long mtot = 0;
+    HM_CUDA(cudaMemcpyAsync(&mtot, cptr + n, sizeof(long long), cudaMemcpyDeviceToHost, st));
     HM_CUDA(cudaStreamSynchronize(st));
-    int nlong = h[0];
-    // 16 B per candidate: 128 KB; a power of two so the padded sort stays
-    // inside the column buffer
-    const int bcap = 8 * 1024;
-    size_t bsm = (size_t)bcap * (2 * sizeof(int) + sizeof(double));
-    if (nlong > 0) {
-        HM_CUDA(cudaFuncSetAttribute(k_union_block<STAGE, 0>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
-        HM_CUDA(cudaFuncSetAttribute(k_union_block<STAGE, 1>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
-        k_union_block<STAGE, 0><<<nblk(nlong, 1, 148L * 4), 256, bsm, st>>>(
-            A, long_rows, nlong, bcap);
+    A.cptr = cptr;
+    A.pcol = (int *)dalloc(sizeof(int) * (mtot > 0 ? mtot : 1));
+    A.pval = (double *)dalloc(sizeof(double) * (mtot > 0 ? mtot : 1));
+    if (!A.pcol || !A.pval) {
+        set_last_error("out of device memory (RAP)", __FILE__, __LINE__);
+        return HMFEM_E_CUDA;
+    }
+    A.ucnt = out.rowptr;
+    A.list[0] = lists;
+    A.list[1] = lists + n;
+    A.nlist[0] = dwork;
+    A.nlist[1] = dwork + 1;
+    A.err = dwork + 2;
+    HM_CUDA(cudaMemsetAsync(dwork, 0, 3 * sizeof(int), st));
+    // pass B: three tiers (<= 64 candidates, <= 1024, <= 8192)
+    k_union_warp<STAGE, 64, 8><<<nblk((long)n * 32, 256, 148L * 64), 256, 0, st>>>(
+        A, nullptr, nullptr, 0);
+    HM_CUDA(cudaGetLastError());
+    {
+        auto kmed = k_union_warp<STAGE, 1024, 2>;
+        HM_CUDA(cudaFuncSetAttribute(kmed, cudaFuncAttributeMaxDynamicSharedMemorySize, 0));
+        kmed<<<148 * 4, 64, 0, st>>>(A, A.list[0], A.nlist[0], 1);
         HM_CUDA(cudaGetLastError());
     }
-    HM_CHECK(rowptr_from_counts(out.rowptr, A.nrows, st, &out.nnz));
+    const int bcap = 4096;  // 16 B per candidate: 64 KB
+    const size_t bsm = (size_t)bcap * 16;
+    HM_CUDA(cudaFuncSetAttribute(k_union_block<STAGE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
+    k_union_block<STAGE><<<148 * 2, 256, bsm, st>>>(A, A.list[1], A.nlist[1], bcap);
+    HM_CUDA(cudaGetLastError());
+    // pass C
+    HM_CHECK(rowptr_from_counts(out.rowptr, n, st, &out.nnz));
+    int herr = 0;
+    HM_CUDA(cudaMemcpyAsync(&herr, A.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    HM_CUDA(cudaStreamSynchronize(st));
+    if (herr) {
+        set_last_error("sparse row over the Galerkin-product capacity", __FILE__, __LINE__);
+        return HMFEM_E_CAPACITY;
+    }
     out.col = (int *)dalloc(sizeof(int) * (out.nnz > 0 ? out.nnz : 1));
     out.val = (double *)dalloc(sizeof(double) * (out.nnz > 0 ? out.nnz : 1));
     if (!out.col || !out.val) {
         set_last_error("out of device memory (RAP)", __FILE__, __LINE__);
         return HMFEM_E_CUDA;
     }
-    A.out_row = out.rowptr;
-    A.out_col = out.col;
-    A.out_val = out.val;
-    k_union_warp<STAGE, 1><<<nblk((long)A.nrows * 32, thr, 148L * 64), thr, smem1, st>>>(A);
+    k_compact<<<nblk((long)n * 32, 256, 148L * 32), 256, 0, st>>>(
+        cptr, out.rowptr, n, A.pcol, A.pval, out.col, out.val);
     HM_CUDA(cudaGetLastError());
-    if (nlong > 0) {
-        k_union_block<STAGE, 1><<<nblk(nlong, 1, 148L * 4), 256, bsm, st>>>(
-            A, long_rows, nlong, bcap);
-        HM_CUDA(cudaGetLastError());
-    }
-    HM_CUDA(cudaMemcpyAsync(h, dwork, sizeof(h), cudaMemcpyDeviceToHost, st));
-    HM_CUDA(cudaStreamSynchronize(st));
-    dfree(long_rows);
-    if (h[1] != 0) {
-        set_last_error(h[1] == 3 ? "sparse row over the setup capacity"
-                                 : "inconsistent Galerkin row count",
-                       __FILE__, __LINE__);
-        return HMFEM_E_CAPACITY;
-    }
+    dfree(A.pcol);
+    dfree(A.pval);
+    dfree(cptr);
+    dfree(lists);
     return HMFEM_OK;
 }
 
@@ -408,6 +442,7 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork)
     int herr = 0;
     HM_CUDA(cudaMemcpyAsync(&herr, dwork, sizeof(int), cudaMemcpyDeviceToHost, st));
     HM_CUDA(cudaStreamSynchronize(st));
+    HM_PHASE("  C/F split", st);
     if (herr) {
         set_last_error("C/F split wavefront gave up waiting", __FILE__, __LINE__);
         return HMFEM_E_TIMEOUT;
@@ -418,6 +453,7 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork)
     HM_CUDA(cudaGetLastError());
     long nc = 0;
     HM_CHECK(rowptr_from_counts(L.cid, n, st, &nc));
+    HM_PHASE("  coarse ids", st);
     L.nc = (int)nc;
     // ---- P ---------------------------------------------------------------
     L.P.n = n;
@@ -459,6 +495,7 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork)
     }
     dfree(keys_out);
     dfree(pown);
+    HM_PHASE("  P and R", st);
     // ---- Galerkin product ---------------------------------------------
     Csr AP;
     UnionArgs a0{};
@@ -466,11 +503,13 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork)
     a0.orow = L.A.rowptr; a0.ocol = L.A.col; a0.oval = L.A.val; a0.w = L.pw;
     a0.irow = L.P.rowptr; a0.icol = L.P.col; a0.ival = nullptr;
     HM_CHECK(run_union<0>(a0, AP, dwork, st));
+    HM_PHASE("  A P", st);
     UnionArgs a1{};
     a1.nrows = L.nc;
     a1.orow = L.R.rowptr; a1.ocol = L.R.col; a1.oval = nullptr; a1.w = L.pw;
     a1.irow = AP.rowptr; a1.icol = AP.col; a1.ival = AP.val;
     HM_CHECK(run_union<1>(a1, C.A, dwork, st));
+    HM_PHASE("  P^T (A P)", st);
     HM_CUDA(cudaStreamSynchronize(st));
     dfree(AP.rowptr); dfree(AP.col); dfree(AP.val);
     return HMFEM_OK;

@@ -28,6 +28,15 @@ constexpr int kRedBlocks = 148 * 8; // max blocks of a grid-stride reduction
 
 void set_last_error(const char *msg, const char *file, int line);
 
+// Phase timing for diagnostics (HMFEM_VERBOSE=1 or options.verbose): syncs
+// the stream and prints the host time since the previous mark to stderr.
+extern int g_verbose;
+void phase_mark(const char *label, cudaStream_t st);
+#define HM_PHASE(label, st)                                                   \
+    do {                                                                      \
+        if (hm::g_verbose) hm::phase_mark(label, st);                         \
+    } while (0)
+
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b)
 {
     return (a + b - 1) / b;

@@ -151,6 +151,73 @@ k_post(const long long *__restrict__ sptr, const int *__restrict__ scol,
     }
 }
 
+// ---- multicolour Gauss-Seidel (coarse levels) ---------------------------
+
+// Forward sweep from zero, first colour: u_i = f_i / a_ii on colour 0,
+// 0 elsewhere (exactly what the colour-0 update gives from u = 0).
+template <class T>
+__global__ void __launch_bounds__(256)
+k_gs_init(int n, const signed char *__restrict__ color, const T *__restrict__ f,
+          const T *__restrict__ dinv, T *__restrict__ u, const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    GRID_STRIDE(i, n) u[i] = color[i] == 0 ? A::mul(f[i], dinv[i]) : (T)0;
+}
+
+// One colour: u_i += (f_i - sum_j a_ij u_j) / a_ii for the rows in slots
+// [s0, s1) of the colour-ordered SELL (no two rows of a colour couple).
+template <class T, class M>
+__global__ void __launch_bounds__(256)
+k_gs_sweep(const long long *__restrict__ sptr, const int *__restrict__ scol,
+           const M *__restrict__ sval, const int *__restrict__ cperm, long s0,
+           long s1, const T *__restrict__ f, const T *__restrict__ dinv,
+           T *__restrict__ u, const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    for (long s = s0 + blockIdx.x * (long)blockDim.x + threadIdx.x; s < s1;
+         s += (long)gridDim.x * blockDim.x) {
+        const int row = cperm[s];
+        if (row < 0) continue;
+        long q = s >> 5;
+        int lane = (int)(s & 31);
+        long long base = sptr[q];
+        int wd = (int)((sptr[q + 1] - base) >> 5);
+        T t = f[row];
+        for (int k = 0; k < wd; k++) {
+            long long o = base + (long long)k * 32 + lane;
+            t = A::sub(t, A::mul((T)ld(sval, o), u[scol[o]]));
+        }
+        u[row] = A::add(u[row], A::mul(t, dinv[row]));
+    }
+}
+
+// Residual after the pre-sweep, scaled for restriction: rs = (f - A u)/|P row|.
+template <class T, class M>
+__global__ void __launch_bounds__(256)
+k_resid_rs(const long long *__restrict__ sptr, const int *__restrict__ scol,
+           const M *__restrict__ sval, int n, const T *__restrict__ f,
+           const T *__restrict__ u, const int *__restrict__ prow,
+           T *__restrict__ rs, const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    GRID_STRIDE(r, n) {
+        long q = r >> 5;
+        int lane = (int)(r & 31);
+        long long base = sptr[q];
+        int wd = (int)((sptr[q + 1] - base) >> 5);
+        T t = f[r];
+        for (int k = 0; k < wd; k++) {
+            long long o = base + (long long)k * 32 + lane;
+            t = A::sub(t, A::mul((T)ld(sval, o), u[scol[o]]));
+        }
+        int pc = prow[r + 1] - prow[r];
+        rs[r] = pc == 1 ? t : A::div(t, (T)pc);
+    }
+}
+
 // coarsest level: v = D^-1 f (diagonal_solver, amg.h:1074-1097)
 template <class T>
 __global__ void k_diag_solve(int n, const T *__restrict__ dinv,
@@ -357,58 +424,93 @@ static int nb(long n, int threads = 256)
     return (int)(b < kRedBlocks ? b : kRedBlocks);
 }
 
+// Where a level leaves its correction: ub for Jacobi levels (ping-pong),
+// ua for Gauss-Seidel levels (in place) and for the coarse solves.
+template <class T>
+static T *cycle_out(Solver &s, int l)
+{
+    const int last = s.nlevels - 1;
+    if (l == last || l == s.direct_level || s.lv[l].gs) return s.vec_ua<T>(l);
+    return s.vec_ub<T>(l);
+}
+
+// Launches fn(values) with the level's matrix values in the cycle's
+// storage type: FP64, FP32, or BF16 on levels >= bf16_from.
+template <class T, class F>
+static void with_vals(Solver &s, const Sell &S, int l, F fn)
+{
+    if constexpr (std::is_same<T, double>::value) fn(S.val);
+    else if (s.use_bf16(l)) fn(S.val16);
+    else fn(S.val32);
+}
+
 // One V-cycle from level l: f[l] holds the right-hand side, the result is
-// left in ub[l] (levels above the coarsest) or ua[l] (the coarsest).
+// left in cycle_out(l).
 template <class T>
 static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
 {
     Level &L = s.lv[l];
     const int last = s.nlevels - 1;
+    const int n = L.A.n;
     Ctl *ctl = s.ctl_active ? s.ctl : nullptr;
     T *f = s.vec_f<T>(l), *ua = s.vec_ua<T>(l), *ub = s.vec_ub<T>(l);
     if (l == s.direct_level) {
-        k_dense_solve<T><<<1, 256, sizeof(double) * L.A.n, st>>>(
-            L.A.n, s.dense_L, f, ua, ctl);
+        k_dense_solve<T><<<1, 256, sizeof(double) * n, st>>>(n, s.dense_L, f, ua, ctl);
         HM_CUDA(cudaGetLastError());
         return HMFEM_OK;
     }
     if (l == last) {
-        k_diag_solve<T><<<nb(L.A.n), 256, 0, st>>>(L.A.n, s.vec_dtrue<T>(l), f, ua, ctl);
+        k_diag_solve<T><<<nb(n), 256, 0, st>>>(n, s.vec_dtrue<T>(l), f, ua, ctl);
         HM_CUDA(cudaGetLastError());
         return HMFEM_OK;
     }
     const T w = (T)s.opt.omega;
-    Level &C = s.lv[l + 1];
     T *rs = s.vec_rs<T>(l);
     const T *dv = s.vec_dinv<T>(l);
-    if (std::is_same<T, double>::value || !s.use_bf16(l)) {
-        k_pre<T, T><<<nb(L.A.n), 256, 0, st>>>(L.S.sptr, L.S.col, s.sval<T>(l),
-                                               L.A.n, f, dv, w, L.P.rowptr, ua, rs, ctl);
+    const T *dt = s.vec_dtrue<T>(l);
+    auto sweep = [&](int c) {
+        const long s0 = L.color_slot[c], s1 = L.color_slot[c + 1];
+        with_vals<T>(s, L.CS, l, [&](auto vals) {
+            k_gs_sweep<T><<<nb(s1 - s0), 256, 0, st>>>(L.CS.sptr, L.CS.col, vals,
+                                                      L.cperm, s0, s1, f, dt, ua, ctl);
+        });
+    };
+    // ---- pre-smoothing + residual (scaled for the restriction)
+    if (L.gs) {
+        k_gs_init<T><<<nb(n), 256, 0, st>>>(n, L.color, f, dt, ua, ctl);
+        for (int c = 1; c < L.ncolors; c++) sweep(c);
+        with_vals<T>(s, L.S, l, [&](auto vals) {
+            k_resid_rs<T><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, vals, n, f, ua,
+                                                L.P.rowptr, rs, ctl);
+        });
     } else {
-        k_pre<T, __nv_bfloat16><<<nb(L.A.n), 256, 0, st>>>(
-            L.S.sptr, L.S.col, L.S.val16, L.A.n, f, dv, w, L.P.rowptr, ua, rs, ctl);
+        with_vals<T>(s, L.S, l, [&](auto vals) {
+            k_pre<T><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, vals, n, f, dv, w,
+                                           L.P.rowptr, ua, rs, ctl);
+        });
     }
     HM_CUDA(cudaGetLastError());
     k_restrict<T><<<nb(L.nc), 256, 0, st>>>(L.R.rowptr, L.R.col, L.nc, rs,
                                             s.vec_f<T>(l + 1), ctl);
     HM_CUDA(cudaGetLastError());
     HM_CHECK(cycle_t<T>(s, l + 1, st, false));
-    const T *uc = (l + 1 == last || l + 1 == s.direct_level) ? s.vec_ua<T>(l + 1)
-                                                             : s.vec_ub<T>(l + 1);
-    k_prolong_add<T><<<nb(L.A.n), 256, 0, st>>>(L.P.rowptr, L.P.col, L.A.n, uc, ua, ctl);
+    k_prolong_add<T><<<nb(n), 256, 0, st>>>(L.P.rowptr, L.P.col, n,
+                                            cycle_out<T>(s, l + 1), ua, ctl);
     HM_CUDA(cudaGetLastError());
-    (void)C;
-    if (dot) {
-        k_post<T, T, true><<<nb(L.A.n), 256, 0, st>>>(
-            L.S.sptr, L.S.col, s.sval<T>(l), L.A.n, f, dv, w, ua, ub, s.ctl,
-            s.part, s.first_sigma);
-    } else if (std::is_same<T, double>::value || !s.use_bf16(l)) {
-        k_post<T, T, false><<<nb(L.A.n), 256, 0, st>>>(
-            L.S.sptr, L.S.col, s.sval<T>(l), L.A.n, f, dv, w, ua, ub, ctl,
-            nullptr, 0);
+    // ---- post-smoothing
+    if (L.gs) {
+        for (int c = L.ncolors - 1; c >= 0; c--) sweep(c);
+    } else if (dot) {
+        k_post<T, T, true><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, s.sval<T>(l), n,
+                                                   f, dv, w, ua, ub, s.ctl, s.part,
+                                                   s.first_sigma);
     } else {
-        k_post<T, __nv_bfloat16, false><<<nb(L.A.n), 256, 0, st>>>(
-            L.S.sptr, L.S.col, L.S.val16, L.A.n, f, dv, w, ua, ub, ctl, nullptr, 0);
+        with_vals<T>(s, L.S, l, [&](auto vals) {
+            k_post<T, typename std::remove_const<typename std::remove_pointer<
+                          decltype(vals)>::type>::type, false>
+                <<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, vals, n, f, dv, w, ua, ub,
+                                        ctl, nullptr, 0);
+        });
     }
     HM_CUDA(cudaGetLastError());
     return HMFEM_OK;
@@ -504,6 +606,11 @@ int level_spmv(Solver &s, int l, const double *x, double *y, cudaStream_t st)
     return launch_spmv(s.lv[l].S, x, y, st);
 }
 
+__global__ void k_fill_one(double *x, int n)
+{
+    GRID_STRIDE(i, n) x[i] = 1.0;
+}
+
 // Times `reps` back-to-back launches of one solve-phase kernel on level l
 // with CUDA events on the solver stream; returns the mean duration and the
 // kernel's algorithmic bytes per launch (no padding, every vector element
@@ -569,6 +676,8 @@ int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
     };
     // control block must not be in the finished state for case 0
     HM_CUDA(cudaMemsetAsync(s.ctl, 0, sizeof(Ctl), st));
+    // x = 1 keeps (x, A x) > 0, so the fused dot never flags a breakdown
+    k_fill_one<<<nb(n), 256, 0, st>>>(x, n);
     launch();
     cudaEvent_t e0, e1;
     HM_CUDA(cudaEventCreate(&e0));

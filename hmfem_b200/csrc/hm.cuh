@@ -53,6 +53,13 @@ struct Level {
     // V-cycle vectors (FP64 and FP32 sets)
     double *f = nullptr, *ua = nullptr, *ub = nullptr, *rs = nullptr;
     float *f32 = nullptr, *ua32 = nullptr, *ub32 = nullptr, *rs32 = nullptr;
+    // multicolour Gauss-Seidel smoother (levels >= gs_from)
+    bool gs = false;
+    int ncolors = 0;
+    signed char *color = nullptr;     // greedy natural-order colouring
+    int *cperm = nullptr;             // rows by colour, each colour padded to 32
+    Sell CS;                          // SELL over cperm (slot order)
+    std::vector<long> color_slot;     // first slot of each colour (+ end)
 };
 
 // Device-resident CG state; kernels read the scalars they need from here,
@@ -95,6 +102,9 @@ int launch_spmv(const Sell &S, const double *x, double *y, cudaStream_t st);
 
 // AMG setup (amg_setup.cu)
 int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *err_dev);
+// greedy colouring + colour-ordered SELL of a level; returns HMFEM_OK with
+// L.gs = false when the level needs more than 64 colours
+int color_level(Level &L, cudaStream_t st, int *dwork);
 
 // cycle + CG (cycle.cu)
 struct Solver;
@@ -103,5 +113,6 @@ int cycle_fp32(Solver &s, int l, cudaStream_t st, bool dot_into_sigma);
 
 void *dalloc(size_t bytes);
 void dfree(void *p);
+void set_alloc_stream(cudaStream_t st);  // stream that orders dalloc/dfree
 
 }  // namespace hm

@@ -115,6 +115,8 @@ static void free_level_setup(Level &L, bool keep_matrix)
     free_csr(L.P); free_csr(L.R);
     dfree(L.f); dfree(L.ua); dfree(L.ub); dfree(L.rs);
     dfree(L.f32); dfree(L.ua32); dfree(L.ub32); dfree(L.rs32);
+    dfree(L.color); dfree(L.cperm);
+    free_sell(L.CS);
     Csr a = L.A;
     L = Level();
     if (keep_matrix) L.A = a;
@@ -226,7 +228,9 @@ int setup(Solver &s)
         return HMFEM_E_ARG;
     }
     cudaStream_t st = s.st;
+    HM_PHASE(nullptr, st);
     free_hierarchy(s, true);
+    HM_PHASE("setup: free", st);
     s.lv.reserve(s.opt.max_levels + 1);
     // level loop (amg.h:1186-1213)
     int l = 0;
@@ -246,6 +250,7 @@ int setup(Solver &s)
         rel = (double)gcnt / (double)gold;
     }
     s.nlevels = l + 1;
+    HM_PHASE("setup: hierarchy", st);
     // solve-phase formats and vectors
     for (int k = 0; k < s.nlevels; k++) {
         Level &L = s.lv[k];
@@ -257,6 +262,7 @@ int setup(Solver &s)
             HM_CHECK(sell_fill_lowp(L.S, true, s.use_bf16(k), st));
         HM_CHECK(alloc_level_vectors(s, L));
     }
+    HM_PHASE("setup: SELL + vectors", st);
     // dense coarse solve on the first level small enough
     s.direct_level = -1;
     if (s.opt.coarse_direct > 0) {
@@ -278,6 +284,16 @@ int setup(Solver &s)
                 break;
             }
         }
+    }
+    // multicolour Gauss-Seidel on the coarse levels above the coarse solve
+    if (s.opt.gs_from >= 1) {
+        const int stop = s.direct_level >= 0 ? s.direct_level : s.nlevels - 1;
+        for (int k = s.opt.gs_from; k < stop; k++) {
+            HM_CHECK(color_level(s.lv[k], st, s.dwork));
+            if (s.lv[k].gs && s.opt.precision == 1)
+                HM_CHECK(sell_fill_lowp(s.lv[k].CS, true, s.use_bf16(k), st));
+        }
+        HM_PHASE("setup: colouring", st);
     }
     HM_CUDA(cudaStreamSynchronize(st));
     s.setup_done = true;
@@ -325,7 +341,9 @@ int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out)
     HM_CUDA(cudaEventCreate(&e1));
     HM_CUDA(cudaEventRecord(e0, st));
     s.ctl_active = true;
+    HM_PHASE(nullptr, st);
     int rc = cg_init(s, st);
+    HM_PHASE("solve: init", st);
     if (rc == HMFEM_OK && !s.gexec) rc = capture_iteration(s);
     s.ctl_active = false;
     if (rc != HMFEM_OK) return rc;
@@ -351,6 +369,7 @@ int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out)
         if (launched > s.opt.max_iter + 2 * k) break;
     }
     HM_CUDA(cudaStreamSynchronize(st));
+    HM_PHASE("solve: iterations", st);
     HM_CHECK(cg_final_residual(s, st));
     HM_CUDA(cudaEventRecord(e1, st));
     Ctl ch;
@@ -392,6 +411,7 @@ void hmfem_default_options(hmfem_options *o)
     o->precision = 0;
     o->bf16_from = -1;
     o->smoother = 1;
+    o->gs_from = 2;
     o->omega = 1.0;
     o->tol = 1e-10;
     o->stop_rule = 0;
@@ -408,6 +428,7 @@ int hmfem_create(hmfem_solver **out, const hmfem_options *opt)
     if (!out) return HMFEM_E_ARG;
     hmfem_solver *h = new hmfem_solver();
     Solver &s = h->s;
+    hm::set_alloc_stream(s.st);
     if (opt) s.opt = *opt;
     else hmfem_default_options(&s.opt);
     if (s.opt.max_levels < 1 || s.opt.max_levels > 64 || s.opt.tol < 0) {
@@ -422,6 +443,9 @@ int hmfem_create(hmfem_solver **out, const hmfem_options *opt)
         return HMFEM_E_CUDA;
     }
     s.own_stream = true;
+    hm::set_alloc_stream(s.st);
+    const char *ev = getenv("HMFEM_VERBOSE");
+    if (s.opt.verbose || (ev && atoi(ev) > 0)) hm::g_verbose = 1;
     s.ctl = (hm::Ctl *)hm::dalloc(sizeof(hm::Ctl));
     s.part = (double *)hm::dalloc(sizeof(double) * hm::kRedBlocks * 2);
     s.dwork = (int *)hm::dalloc(sizeof(int) * 64);
@@ -442,6 +466,7 @@ int hmfem_destroy(hmfem_solver *h)
 {
     if (!h) return HMFEM_OK;
     Solver &s = h->s;
+    hm::set_alloc_stream(s.st);
     if (s.st) cudaStreamSynchronize(s.st);
     hm::free_hierarchy(s, false);
     hm::free_vectors(s);
@@ -458,6 +483,7 @@ int hmfem_set_stream(hmfem_solver *h, void *stream)
 {
     if (!h) return HMFEM_E_ARG;
     Solver &s = h->s;
+    hm::set_alloc_stream(s.st);
     cudaStreamSynchronize(s.st);
     if (s.own_stream) cudaStreamDestroy(s.st);
     if (stream) {
@@ -492,7 +518,9 @@ int hmfem_assemble(hmfem_solver *h, int nx, int ny, int nz, double hx,
         return HMFEM_E_CAPACITY;
     }
     Solver &s = h->s;
+    hm::set_alloc_stream(s.st);
     cudaStream_t st = s.st;
+    HM_PHASE(nullptr, st);
     if (!s.have_grid || s.nx != nx || s.ny != ny || s.nz != nz || s.lv.empty() ||
         s.lv[0].A.n != n) {
         HM_CHECK(hm::new_level0(s, (int)n));
@@ -537,14 +565,17 @@ int hmfem_assemble(hmfem_solver *h, int nx, int ny, int nz, double hx,
         }
     }
     hm::Level &L = s.lv[0];
+    HM_PHASE("assemble: buffers + faces", st);
     HM_CHECK(hm::launch_l0_rowcounts(nx, ny, nz, L.A.rowptr, st));
     HM_CHECK(hm::rowptr_from_counts(L.A.rowptr, (int)n, st, &L.A.nnz));
     HM_ALLOC(L.A.col, int, L.A.nnz);
     HM_ALLOC(L.A.val, double, L.A.nnz);
+    HM_PHASE("assemble: row pointers", st);
     HM_CHECK(hm::launch_assemble(nx, ny, nz, hx, hy, hz, visc, s.KX, s.KY, s.KZ,
                                  s.bc, s.face, nullptr, nullptr, nullptr,
                                  nullptr, L.A.rowptr, L.A.col, L.A.val, s.b, st));
     HM_CUDA(cudaStreamSynchronize(st));
+    HM_PHASE("assemble: TPFA kernel", st);
     s.setup_done = false;
     return HMFEM_OK;
 }
@@ -556,6 +587,7 @@ int hmfem_set_matrix(hmfem_solver *h, int n, long nnz, const int *cnt,
     if (!h || n < 1 || nnz < 1 || !cnt || !col || !ele) return HMFEM_E_ARG;
     if (nnz > 2147483647L) return HMFEM_E_CAPACITY;
     Solver &s = h->s;
+    hm::set_alloc_stream(s.st);
     cudaStream_t st = s.st;
     HM_CHECK(hm::new_level0(s, n));
     s.have_grid = false;
@@ -585,6 +617,7 @@ int hmfem_set_stencil(hmfem_solver *h, int nx, int ny, int nz,
     if (!h || nx < 1 || ny < 1 || nz < 1 || !perm || !indcol) return HMFEM_E_ARG;
     long n = (long)nx * ny * nz;
     Solver &s = h->s;
+    hm::set_alloc_stream(s.st);
     cudaStream_t st = s.st;
     HM_CHECK(hm::new_level0(s, (int)n));
     s.have_grid = false;
@@ -628,6 +661,7 @@ int hmfem_setup(hmfem_solver *h)
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, h->s.st);
+    hm::set_alloc_stream(h->s.st);
     int rc = hm::setup(h->s);
     cudaEventRecord(e1, h->s.st);
     cudaEventSynchronize(e1);
@@ -644,6 +678,7 @@ int hmfem_solve(hmfem_solver *h, const double *b, double *x, int mem,
 {
     if (!h) return HMFEM_E_ARG;
     if (h->s.lv.empty()) return HMFEM_E_ARG;
+    hm::set_alloc_stream(h->s.st);
     return hm::solve(h->s, b, x, mem, st);
 }
 
@@ -652,6 +687,7 @@ int hmfem_fluxes(hmfem_solver *h, const double *p, hmfem_ele *v, int mem,
 {
     if (!h || !p || !v) return HMFEM_E_ARG;
     Solver &s = h->s;
+    hm::set_alloc_stream(s.st);
     if (!s.have_grid) {
         hm::set_last_error("fluxes need the grid problem (hmfem_assemble)", __FILE__, __LINE__);
         return HMFEM_E_ARG;
@@ -707,6 +743,7 @@ int hmfem_level_copy(hmfem_solver *h, int l, int *cnt, int *col, double *ele,
 {
     if (!h || l < 0 || l >= h->s.nlevels) return HMFEM_E_ARG;
     Solver &s = h->s;
+    hm::set_alloc_stream(s.st);
     hm::Level &L = s.lv[l];
     cudaStream_t st = s.st;
     const int n = L.A.n;
@@ -732,6 +769,7 @@ int hmfem_vcycle(hmfem_solver *h, const double *f, double *u, int mem)
 {
     if (!h || !f || !u) return HMFEM_E_ARG;
     Solver &s = h->s;
+    hm::set_alloc_stream(s.st);
     if (!s.setup_done) HM_CHECK(hm::setup(s));
     cudaStream_t st = s.st;
     const int n = s.lv[0].A.n;
@@ -749,6 +787,7 @@ int hmfem_spmv(hmfem_solver *h, int level, const double *x, double *y, int mem)
 {
     if (!h || level < 0 || !x || !y) return HMFEM_E_ARG;
     Solver &s = h->s;
+    hm::set_alloc_stream(s.st);
     if (level > 0 && !s.setup_done) HM_CHECK(hm::setup(s));
     if (level >= (int)s.lv.size()) return HMFEM_E_ARG;
     cudaStream_t st = s.st;
@@ -771,6 +810,7 @@ int hmfem_rhs(hmfem_solver *h, double *b, int mem)
 {
     if (!h || !b || h->s.lv.empty()) return HMFEM_E_ARG;
     Solver &s = h->s;
+    hm::set_alloc_stream(s.st);
     HM_CHECK(hm::download(b, (const double *)s.b, s.lv[0].A.n, mem, s.st));
     HM_CUDA(cudaStreamSynchronize(s.st));
     return HMFEM_OK;
@@ -787,6 +827,7 @@ int hmfem_time_kernel(hmfem_solver *h, int which, int level, int reps,
                       float *ms, double *bytes)
 {
     if (!h || !ms || !bytes) return HMFEM_E_ARG;
+    hm::set_alloc_stream(h->s.st);
     if (!h->s.setup_done) HM_CHECK(hm::setup(h->s));
     return hm::time_kernel(h->s, which, level, reps, ms, bytes);
 }

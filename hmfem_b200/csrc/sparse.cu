@@ -13,23 +13,54 @@ void set_last_error(const char *msg, const char *file, int line)
     snprintf(g_err, sizeof(g_err), "%s (%s:%d)", msg, file, line);
 }
 
+int g_verbose = 0;
+
+void phase_mark(const char *label, cudaStream_t st)
+{
+    static struct timespec last = {0, 0};
+    cudaStreamSynchronize(st);
+    struct timespec now;
+    clock_gettime(CLOCK_MONOTONIC, &now);
+    double ms = (now.tv_sec - last.tv_sec) * 1e3 + (now.tv_nsec - last.tv_nsec) * 1e-6;
+    if (last.tv_sec != 0 && label) fprintf(stderr, "[hmfem] %-28s %9.3f ms\n", label, ms);
+    last = now;
+}
+
 }  // namespace hm
 
 extern "C" const char *hmfem_last_error(void) { return hm::g_err; }
 
 namespace hm {
 
+// Device memory comes from the stream-ordered pool of the current device
+// with its release threshold raised, so the buffers a setup frees are handed
+// back to the next setup without synchronising cudaMalloc / cudaFree calls.
+static cudaStream_t g_astream = nullptr;
+static unsigned g_pool_ready = 0;  // bit per device
+
+void set_alloc_stream(cudaStream_t st) { g_astream = st; }
+
 void *dalloc(size_t bytes)
 {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 32 && !(g_pool_ready & (1u << dev))) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            unsigned long long keep = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        g_pool_ready |= 1u << dev;
+    }
     void *p = nullptr;
     if (bytes == 0) bytes = 16;
-    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    if (cudaMallocAsync(&p, bytes, g_astream) != cudaSuccess) return nullptr;
     return p;
 }
 
 void dfree(void *p)
 {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, g_astream);
 }
 
 int scan_exclusive(const int *in, int *out, int n, cudaStream_t st)

@@ -45,7 +45,8 @@ class Dim(C.Structure):  # structs.h:84-95
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("bf16_from", C.c_int),
-                ("smoother", C.c_int), ("omega", C.c_double),
+                ("smoother", C.c_int), ("gs_from", C.c_int),
+                ("omega", C.c_double),
                 ("tol", C.c_double), ("stop_rule", C.c_int),
                 ("max_iter", C.c_int), ("max_levels", C.c_int),
                 ("min_coarse", C.c_int), ("coarse_direct", C.c_int),

@@ -101,6 +101,11 @@ typedef struct {
     int smoother;      /* 0: damped Jacobi with 1/a_ii (device_amg.h design);
                           1: l1-Jacobi, 1/(a_ii + sum_j!=i |a_ij|) (default:
                           SPD preconditioner for any SPD matrix) */
+    int gs_from;       /* levels >= gs_from (below the coarse solve) use a
+                          multicolour Gauss-Seidel smoother instead: forward
+                          sweep over greedy natural-order colours before the
+                          restriction, backward sweep after the
+                          prolongation; < 0 disables (default 2) */
     double omega;      /* Jacobi weight (compute.cpp:35 passes 1.0) */
     double tol;        /* stopping tolerance */
     int stop_rule;     /* 0: true residual ||b-Ax||/||b|| <= tol;

@@ -277,6 +277,27 @@ static void spmt(int arows, const int *acnt, const int *acol,
     *ccnt_o = ccnt; *ccol_o = ccol; *cele_o = cele; *csize_o = csize;
 }
 
+/* Greedy colouring in natural row order: each row takes the smallest colour
+ * not used by a lower-numbered neighbour (project smoother setup). */
+static int greedy_colour(or_level *A)
+{
+    A->color = (signed char *)malloc(A->n > 0 ? A->n : 1);
+    long m = 0;
+    int nc = 0;
+    for (int i = 0; i < A->n; i++) {
+        unsigned long long used = 0;
+        for (int j = 0; j < A->cnt[i]; j++, m++) {
+            int c = A->col[m];
+            if (c < i) used |= 1ull << A->color[c];
+        }
+        int k = 0;
+        while (k < 63 && (used & (1ull << k))) k++;
+        A->color[i] = (signed char)k;
+        if (k + 1 > nc) nc = k + 1;
+    }
+    return nc;
+}
+
 /* l1-Jacobi diagonal: a_ii + sum over the other stored entries of |a_ij|,
  * accumulated in row order (project smoother, no reference counterpart). */
 static double *l1_inverse(const or_level *A, const double *dia)
@@ -359,6 +380,7 @@ static void coarsen_level(double eps, or_level *A, or_level *Cn)
     A->dinv = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
     for (int i = 0; i < n; i++) A->dinv[i] = 1.0 / dia[i];
     A->dl1inv = l1_inverse(A, dia);
+    A->ncolors = greedy_colour(A);
     free(dia); free(cox); free(cid); free(dsp);
 }
 
@@ -407,6 +429,7 @@ void or_amg_free(or_hierarchy *H)
     for (int l = 0; l < H->nlevels; l++) {
         or_level *A = &H->lv[l];
         free(A->cnt); free(A->col); free(A->ele); free(A->dinv); free(A->dl1inv);
+        free(A->color);
         free(A->sel); free(A->pcnt); free(A->pcol); free(A->pele);
     }
     memset(H, 0, sizeof(*H));
@@ -500,6 +523,19 @@ static void prolong_simple(const or_level *A, const double *u, double *s)
 
 typedef struct { double *u, *f, *s, *r; } or_work;
 
+/* One colour of a Gauss-Seidel sweep: rows of colour c, each
+ * u_i += (f_i - sum_j a_ij u_j) / a_ii with the sum in row order. */
+static void gs_colour(const or_level *A, int c, const double *f, double *u)
+{
+    long m = 0;
+    for (int i = 0; i < A->n; i++) {
+        if (A->color[i] != c) { m += A->cnt[i]; continue; }
+        double t = f[i];
+        for (int j = 0; j < A->cnt[i]; j++, m++) t -= A->ele[m] * u[A->col[m]];
+        u[i] += t * A->dinv[i];
+    }
+}
+
 static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
                double omega)
 {
@@ -511,7 +547,20 @@ static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
         for (int i = 0; i < n; i++) u[i] = A->dinv[i] * f[i];
         return;
     }
-    if (smoother == 0) {
+    const int gs_from = smoother >= 10 ? smoother - 10 : 1 << 30;
+    if (l >= gs_from) {
+        /* multicolour Gauss-Seidel, forward over colours from zero, then the
+         * residual (the GPU smoother on coarse levels; no reference
+         * counterpart -- the reference's own GS is lexicographic) */
+        for (int i = 0; i < n; i++) u[i] = 0.0;
+        for (int c = 0; c < A->ncolors; c++) gs_colour(A, c, f, u);
+        long m = 0;
+        for (int i = 0; i < n; i++) {
+            double t = f[i];
+            for (int j = 0; j < A->cnt[i]; j++, m++) t -= A->ele[m] * u[A->col[m]];
+            r[i] = t;
+        }
+    } else if (smoother == 0) {
         /* gauss_seidel_f 3-arg (amg.h:759-784) */
         for (int i = 0; i < n; i++) r[i] = f[i];
         long m = 0;
@@ -522,7 +571,7 @@ static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
         }
     } else {
         /* device_jacobi 3-arg (device_amg.h:35-42): u = w D^-1 f; r = f - A u */
-        const double *dv = smoother == 2 ? A->dl1inv : A->dinv;
+        const double *dv = smoother != 1 ? A->dl1inv : A->dinv;
         for (int i = 0; i < n; i++) u[i] = omega * f[i] * dv[i];
         long m = 0;
         for (int i = 0; i < n; i++) {
@@ -534,7 +583,10 @@ static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
     restrict_simple(A, H->lv[l + 1].n, r, W[l + 1].f);
     mg(H, W, l + 1, smoother, omega);
     prolong_simple(A, W[l + 1].u, s);
-    if (smoother == 0) {
+    if (l >= gs_from) {
+        for (int i = 0; i < n; i++) u[i] += s[i];
+        for (int c = A->ncolors - 1; c >= 0; c--) gs_colour(A, c, f, u);
+    } else if (smoother == 0) {
         /* gauss_seidel_b 3-arg (amg.h:930-961) */
         for (int i = 0; i < n; i++) u[i] += s[i];
         long m = A->nnz;
@@ -555,7 +607,7 @@ static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
             for (int j = 0; j < A->cnt[i]; j++, m++) t -= A->ele[m] * u[A->col[m]];
             r[i] = t;
         }
-        const double *dv = smoother == 2 ? A->dl1inv : A->dinv;
+        const double *dv = smoother != 1 ? A->dl1inv : A->dinv;
         for (int i = 0; i < n; i++) u[i] += omega * r[i] * dv[i];
     }
 }

@@ -63,6 +63,9 @@ typedef struct {
     double *dinv;         /* 1 / (last stored diagonal entry) */
     double *dl1inv;       /* 1 / (a_ii + sum_{j!=i} |a_ij|), row order: the
                              l1-Jacobi diagonal (not in the reference) */
+    signed char *color;   /* greedy natural-order colouring (not in the
+                             reference) and its number of colours */
+    int ncolors;
     /* transfer to the next level (absent on the coarsest level) */
     char *sel;            /* 1 = C, 2 = F (amg.h:1-32) */
     long pnnz;
@@ -88,8 +91,11 @@ void or_amg_free(or_hierarchy *H);
  *             930-961), the path compute.cpp runs.
  * smoother 1: the device design's damped Jacobi (device_amg.h:11-43,
  *             396-411), with omega.
- * smoother 2: the same cycle with the l1-Jacobi diagonal (dl1inv): the GPU
- *             solver's default, an SPD preconditioner for any SPD matrix. */
+ * smoother 2: the same cycle with the l1-Jacobi diagonal (dl1inv): an SPD
+ *             preconditioner for any SPD matrix.
+ * smoother 10+g: l1-Jacobi on levels < g, multicolour Gauss-Seidel (forward
+ *             pre-sweep over colours 0..C-1 from zero, backward post-sweep)
+ *             on levels >= g -- the GPU solver's default with g = 2. */
 void or_vcycle(const or_hierarchy *H, int smoother, double omega,
                const double *f, double *u);
 

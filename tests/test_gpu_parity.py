@@ -92,11 +92,12 @@ def test_hierarchy_bit_exact(case):
             np.testing.assert_array_equal(g[k], o[k], err_msg=f"L{l} {k}")
 
 
-@pytest.mark.parametrize("smoother,oracle_smoother,omega",
-                         [(0, 1, 1.0), (0, 1, 0.6), (1, 2, 1.0)])
-def test_vcycle_bit_exact(case, smoother, oracle_smoother, omega):
+@pytest.mark.parametrize("smoother,gs_from,oracle_smoother,omega",
+                         [(0, -1, 1, 1.0), (0, -1, 1, 0.6), (1, -1, 2, 1.0),
+                          (1, 2, 12, 1.0), (1, 1, 11, 1.0)])
+def test_vcycle_bit_exact(case, smoother, gs_from, oracle_smoother, omega):
     name, p, (perm, ind, b, csr, H) = case
-    s = gpu.Solver(smoother=smoother, omega=omega)
+    s = gpu.Solver(smoother=smoother, gs_from=gs_from, omega=omega)
     s.assemble(p)
     s.setup()
     f = np.random.default_rng(11).standard_normal(p.n)
