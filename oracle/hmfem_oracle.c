@@ -547,8 +547,12 @@ static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
         for (int i = 0; i < n; i++) u[i] = A->dinv[i] * f[i];
         return;
     }
-    const int gs_from = smoother >= 10 ? smoother - 10 : 1 << 30;
-    if (l >= gs_from) {
+    /* smoother 10+g: GS on levels >= g; 100+10g+t: GS on levels [g, t) */
+    const int gs_from = smoother >= 100 ? (smoother / 10) % 10
+                        : smoother >= 10 ? smoother - 10 : 1 << 30;
+    const int gs_to = smoother >= 100 ? smoother % 10 : 1 << 30;
+    const int use_gs = l >= gs_from && l < gs_to;
+    if (use_gs) {
         /* multicolour Gauss-Seidel, forward over colours from zero, then the
          * residual (the GPU smoother on coarse levels; no reference
          * counterpart -- the reference's own GS is lexicographic) */
@@ -583,7 +587,7 @@ static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
     restrict_simple(A, H->lv[l + 1].n, r, W[l + 1].f);
     mg(H, W, l + 1, smoother, omega);
     prolong_simple(A, W[l + 1].u, s);
-    if (l >= gs_from) {
+    if (use_gs) {
         for (int i = 0; i < n; i++) u[i] += s[i];
         for (int c = A->ncolors - 1; c >= 0; c--) gs_colour(A, c, f, u);
     } else if (smoother == 0) {
