@@ -19,7 +19,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=default", "--expt-relaxed-constexpr",
          "--extended-lambda"]
 SOURCES = ["assemble.cu", "sparse.cu", "amg_setup.cu", "smoother_setup.cu", "cycle.cu", "solver.cu",
-           "device_abi.cu"]
+           "device_abi.cu", "noalloc.cu"]
 
 
 def _deps():

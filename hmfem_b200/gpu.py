@@ -78,8 +78,10 @@ EXPORTS = [
     "hmfem_assemble", "hmfem_set_matrix", "hmfem_set_stencil", "hmfem_setup",
     "hmfem_solve", "hmfem_fluxes", "hmfem_num_levels", "hmfem_level_info",
     "hmfem_level_copy", "hmfem_vcycle", "hmfem_spmv", "hmfem_rhs",
-    "hmfem_last_stats", "hmfem_time_kernel",
+    "hmfem_last_stats", "hmfem_time_kernel", "hmfem_fluxes_noalloc",
 ]
+
+NOALLOC_MAX_FACE = 262144  # HMFEM_NOALLOC_MAX_FACE in include/hmfem_gpu.h
 
 
 def lib():
@@ -115,6 +117,10 @@ def lib():
         L.hmfem_last_stats.argtypes = [vp, C.POINTER(Stats)]
         L.hmfem_time_kernel.argtypes = [vp, ip, ip, ip, C.POINTER(C.c_float),
                                         C.POINTER(C.c_double)]
+        L.hmfem_fluxes_noalloc.argtypes = [ip, ip, ip, dp, dp, dp, dp, vp, vp,
+                                           vp, vp, vp, vp, vp,
+                                           C.POINTER(C.c_double),
+                                           C.POINTER(C.c_double), vp]
         L.compute.argtypes = [vp] * 6
         L.solve_linsys.argtypes = [vp, vp, vp, vp, Dim]
         L.solve_linsys.restype = None
@@ -324,3 +330,25 @@ def solve_linsys(perm, indcol, b, x, nx, ny, nz):
 
 def iter_amg() -> int:
     return C.c_int.in_dll(lib(), "iter_amg").value
+
+
+def fluxes_noalloc(prob, KX, KY, KZ, p, v, stream=None):
+    """hmfem_fluxes_noalloc: fluxes of device pressure p into device v
+    (n x 7 float64, c untouched) with no device allocation by the library;
+    returns (divmin, divmax).  For callers that cannot let the library
+    allocate (see include/hmfem_gpu.h)."""
+    L = lib()
+    bc = (C.c_int * 6)(*prob.bc_type)
+    bv = (C.c_double * 6)(*prob.bc_value)
+    dmin, dmax = C.c_double(), C.c_double()
+    ptrs = []
+    for a in (KX, KY, KZ, p, v):
+        pa, mem = _ptr(a)
+        if mem != 1:
+            raise ValueError("fluxes_noalloc takes device arrays only")
+        ptrs.append(pa)
+    _check(L.hmfem_fluxes_noalloc(prob.nx, prob.ny, prob.nz, prob.hx, prob.hy,
+                                  prob.hz, prob.visc, ptrs[0], ptrs[1], ptrs[2],
+                                  bc, bv, ptrs[3], ptrs[4], C.byref(dmin),
+                                  C.byref(dmax), C.c_void_p(stream)))
+    return dmin.value, dmax.value

@@ -184,6 +184,27 @@ int hmfem_last_stats(hmfem_solver *s, hmfem_stats *st);
 int hmfem_time_kernel(hmfem_solver *s, int which, int level, int reps,
                       float *ms, double *bytes);
 
+/* Flux reconstruction that allocates nothing.  No counterpart in the
+ * reference.  For callers that cannot let a library allocate device memory
+ * (their device memory is already reserved by their own or a framework's
+ * caching allocator, or they run where allocation is not permitted): the
+ * same fluxes and divvel_pontual bounds as hmfem_fluxes, with constant
+ * boundary values per face, from device arrays K*, p and into device v
+ * (c untouched); divmin/divmax are host doubles.  All scratch lives in one
+ * fixed __device__ array inside the library, so every boundary face must
+ * have at most HMFEM_NOALLOC_MAX_FACE cells (else HMFEM_E_CAPACITY).  The
+ * array is shared by all calls on a device and keeps the last call's
+ * contents: calls that overlap on the GPU race.  The first call on a device
+ * looks the array's address up; make it before any stream capture.
+ * stream: cudaStream_t as void*, NULL = the legacy default stream. */
+#define HMFEM_NOALLOC_MAX_FACE 262144
+int hmfem_fluxes_noalloc(int nx, int ny, int nz, double hx, double hy,
+                         double hz, double visc, const double *KX,
+                         const double *KY, const double *KZ,
+                         const int bc_type[6], const double bc_value[6],
+                         const double *p, hmfem_ele *v, double *divmin,
+                         double *divmax, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
