@@ -34,6 +34,38 @@ __device__ __forceinline__ bool finished(const Ctl *c) { return c && *(volatile 
     for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < (n);       \
          r += (long)gridDim.x * blockDim.x)
 
+// t - sum_k a_k x(c_k) (SUB) or t + sum_k a_k x(c_k) over one SELL-32 row
+// (entries at o, o+32, ...), in stored order.  Column indices, values and
+// the gathered x are loaded four entries at a time so the dependent gathers
+// overlap; the summation order is unchanged.
+template <class T, bool SUB, int CH = 8, class M, class X>
+__device__ __forceinline__ T row_acc(T t, const int *__restrict__ scol,
+                                     const M *__restrict__ sval, long long o,
+                                     int wd, X x)
+{
+    using A = Ar<T>;
+    for (int k0 = 0; k0 < wd; k0 += CH, o += 32 * CH) {
+        int c[CH];
+        T a[CH], xv[CH];
+#pragma unroll
+        for (int q = 0; q < CH; q++) {
+            const bool ok = k0 + q < wd;
+            c[q] = ok ? scol[o + 32 * q] : 0;
+            a[q] = ok ? (T)ld(sval, o + 32 * q) : (T)0;
+        }
+#pragma unroll
+        for (int q = 0; q < CH; q++) xv[q] = k0 + q < wd ? x(c[q]) : (T)0;
+#pragma unroll
+        for (int q = 0; q < CH; q++) {
+            if (k0 + q < wd) {
+                const T ax = A::mul(a[q], xv[q]);
+                t = SUB ? A::sub(t, ax) : A::add(t, ax);
+            }
+        }
+    }
+    return t;
+}
+
 // ---- smoother / transfer kernels --------------------------------------
 
 // Pre-smoother from zero and residual, fused (device_jacobi 3-arg,
@@ -55,12 +87,9 @@ k_pre(const long long *__restrict__ sptr, const int *__restrict__ scol,
         int wd = (int)((sptr[q + 1] - base) >> 5);
         T fr = f[r];
         T t = fr;
-        for (int k = 0; k < wd; k++) {
-            long long o = base + (long long)k * 32 + lane;
-            int c = scol[o];
-            T uc = A::mul(A::mul(w, f[c]), dinv[c]);
-            t = A::sub(t, A::mul((T)ld(sval, o), uc));
-        }
+        t = row_acc<T, true>(t, scol, sval, base + lane, wd, [&](int c) {
+            return A::mul(A::mul(w, f[c]), dinv[c]);
+        });
         u[r] = A::mul(A::mul(w, fr), dinv[r]);
         int pc = prow[r + 1] - prow[r];
         rs[r] = pc == 1 ? t : A::div(t, (T)pc);
@@ -125,10 +154,7 @@ k_post(const long long *__restrict__ sptr, const int *__restrict__ scol,
         int wd = (int)((sptr[q + 1] - base) >> 5);
         T fr = f[r];
         T t = fr;
-        for (int k = 0; k < wd; k++) {
-            long long o = base + (long long)k * 32 + lane;
-            t = A::sub(t, A::mul((T)ld(sval, o), u[scol[o]]));
-        }
+        t = row_acc<T, true>(t, scol, sval, base + lane, wd, [&](int c) { return u[c]; });
         T un = A::add(u[r], A::mul(A::mul(w, t), dinv[r]));
         uo[r] = un;
         if (DOT) dot += (double)un * (double)fr;
@@ -185,10 +211,7 @@ k_gs_sweep(const long long *__restrict__ sptr, const int *__restrict__ scol,
         long long base = sptr[q];
         int wd = (int)((sptr[q + 1] - base) >> 5);
         T t = f[row];
-        for (int k = 0; k < wd; k++) {
-            long long o = base + (long long)k * 32 + lane;
-            t = A::sub(t, A::mul((T)ld(sval, o), u[scol[o]]));
-        }
+        t = row_acc<T, true, 16>(t, scol, sval, base + lane, wd, [&](int c) { return u[c]; });
         u[row] = A::add(u[row], A::mul(t, dinv[row]));
     }
 }
@@ -209,10 +232,7 @@ k_resid_rs(const long long *__restrict__ sptr, const int *__restrict__ scol,
         long long base = sptr[q];
         int wd = (int)((sptr[q + 1] - base) >> 5);
         T t = f[r];
-        for (int k = 0; k < wd; k++) {
-            long long o = base + (long long)k * 32 + lane;
-            t = A::sub(t, A::mul((T)ld(sval, o), u[scol[o]]));
-        }
+        t = row_acc<T, true>(t, scol, sval, base + lane, wd, [&](int c) { return u[c]; });
         int pc = prow[r + 1] - prow[r];
         rs[r] = pc == 1 ? t : A::div(t, (T)pc);
     }
@@ -229,36 +249,23 @@ __global__ void k_diag_solve(int n, const T *__restrict__ dinv,
     GRID_STRIDE(i, n) u[i] = A::mul(dinv[i], f[i]);
 }
 
-// coarsest level: dense Cholesky solve, one block (L stored row-major,
-// lower triangle, FP64).
+// Coarse solve by the explicit inverse: u = A^-1 f, a warp per row (FP64
+// accumulation, the inverse stored row-major).
 template <class T>
-__global__ void k_dense_solve(int n, const double *__restrict__ Lf,
-                              const T *__restrict__ f, T *__restrict__ u,
-                              const Ctl *ctl)
+__global__ void __launch_bounds__(256)
+k_dense_solve(int n, const double *__restrict__ Minv, const T *__restrict__ f,
+              T *__restrict__ u, const Ctl *ctl)
 {
     if (finished(ctl)) return;
-    extern __shared__ double y[];
-    for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (double)f[i];
-    __syncthreads();
-    // forward: L y = f (column-oriented so the block works on one column)
-    for (int j = 0; j < n; j++) {
-        if (threadIdx.x == 0) y[j] = y[j] / Lf[(long)j * n + j];
-        __syncthreads();
-        double yj = y[j];
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x)
-            y[i] -= Lf[(long)i * n + j] * yj;
-        __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (long i = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; i < n;
+         i += ((long)gridDim.x * blockDim.x) >> 5) {
+        const double *row = Minv + i * (long)n;
+        double acc = 0.0;
+        for (int j = lane; j < n; j += 32) acc += row[j] * (double)f[j];
+        acc = warp_sum(acc);
+        if (lane == 0) u[i] = (T)acc;
     }
-    // backward: L^T x = y
-    for (int j = n - 1; j >= 0; j--) {
-        if (threadIdx.x == 0) y[j] = y[j] / Lf[(long)j * n + j];
-        __syncthreads();
-        double yj = y[j];
-        for (int i = threadIdx.x; i < j; i += blockDim.x)
-            y[i] -= Lf[(long)j * n + i] * yj;
-        __syncthreads();
-    }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) u[i] = (T)y[i];
 }
 
 // ---- CG kernels ---------------------------------------------------------
@@ -280,10 +287,7 @@ k_resid(const long long *__restrict__ sptr, const int *__restrict__ scol,
         long long base = sptr[q];
         int wd = (int)((sptr[q + 1] - base) >> 5);
         double s = 0.0;
-        for (int k = 0; k < wd; k++) {
-            long long o = base + (long long)k * 32 + lane;
-            s = dadd(s, dmul(sval[o], x[scol[o]]));
-        }
+        s = row_acc<double, false>(s, scol, sval, base + lane, wd, [&](int c) { return x[c]; });
         double bi = b[i];
         double ri = dsub(bi, s);
         r[i] = ri;
@@ -322,10 +326,7 @@ k_spmv_dot(const long long *__restrict__ sptr, const int *__restrict__ scol,
         long long base = sptr[q];
         int wd = (int)((sptr[q + 1] - base) >> 5);
         double a = 0.0;
-        for (int k = 0; k < wd; k++) {
-            long long o = base + (long long)k * 32 + lane;
-            a = dadd(a, dmul(sval[o], s[scol[o]]));
-        }
+        a = row_acc<double, false>(a, scol, sval, base + lane, wd, [&](int c) { return s[c]; });
         v[i] = a;
         d += s[i] * a;
     }
@@ -455,7 +456,8 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
     Ctl *ctl = s.ctl_active ? s.ctl : nullptr;
     T *f = s.vec_f<T>(l), *ua = s.vec_ua<T>(l), *ub = s.vec_ub<T>(l);
     if (l == s.direct_level) {
-        k_dense_solve<T><<<1, 256, sizeof(double) * n, st>>>(n, s.dense_L, f, ua, ctl);
+        k_dense_solve<T><<<(int)ceil_div((long)n * 32, 256), 256, 0, st>>>(n, s.dense_L, f, ua,
+                                                                         ctl);
         HM_CUDA(cudaGetLastError());
         return HMFEM_OK;
     }

@@ -114,5 +114,9 @@ int cycle_fp32(Solver &s, int l, cudaStream_t st, bool dot_into_sigma);
 void *dalloc(size_t bytes);
 void dfree(void *p);
 void set_alloc_stream(cudaStream_t st);  // stream that orders dalloc/dfree
+struct AllocCache;                       // per-solver exact-size block cache
+void set_alloc_context(cudaStream_t st, AllocCache *c);
+AllocCache *alloc_cache_new();
+void alloc_cache_release(AllocCache *c);
 
 }  // namespace hm

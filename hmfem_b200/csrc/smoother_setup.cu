@@ -1,13 +1,11 @@
 // smoother_setup.cu -- setup of the multicolour Gauss-Seidel smoother used on
-// the coarse levels: a greedy colouring in natural row order (each row takes
-// the smallest colour not used by a lower-numbered neighbour) and a SELL-32
+// the coarse levels: a colouring and a SELL-32
 // copy of the level with rows grouped by colour, so one colour is one
 // coalesced, conflict-free kernel.
 //
-// The colouring is sequential by definition; like the C/F split it runs as
-// a dependency wavefront (a row is coloured once all its lower neighbours
-// are), with row tiles handed out in increasing order by an atomic ticket
-// and every wait bounded.
+// The colouring is Jones-Plassmann with fixed pseudo-random priorities
+// (a round per launch, double-buffered, so the result is deterministic and
+// the oracle reproduces it exactly).
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -18,44 +16,44 @@ namespace hm {
 namespace {
 
 constexpr int kTile = 256;
-constexpr long long kMaxPolls = 1ll << 22;
 constexpr int kMaxColors = 63;
 
-__global__ void __launch_bounds__(kTile)
-k_greedy_color(const int *__restrict__ rowptr, const int *__restrict__ col,
-               int n, signed char *color, unsigned *ticket, int *err, int *ncol)
+// Jones-Plassmann colouring, one round: a row still uncoloured (old < 0)
+// whose (priority, index) key beats every uncoloured neighbour's takes the
+// smallest colour not used by its coloured neighbours.  Reads `old`, writes
+// `nw` (double-buffered rounds), so the result is order-independent.
+__device__ __forceinline__ unsigned long long jp_key(int v)
 {
-    __shared__ int s_tile;
-    if (threadIdx.x == 0) s_tile = (int)atomicAdd(ticket, 1u);
-    __syncthreads();
-    const long v = (long)s_tile * kTile + threadIdx.x;
-    if (v >= n) return;
-    volatile signed char *vc = color;
-    volatile int *verr = err;
-    const int a = rowptr[v], e = rowptr[v + 1];
-    long long polls = 0;
-    for (;;) {
+    unsigned x = (unsigned)v;
+    x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
+    return ((unsigned long long)x << 32) | (unsigned)v;
+}
+
+__global__ void __launch_bounds__(kTile)
+k_jp_round(const int *__restrict__ rowptr, const int *__restrict__ col, int n,
+           const signed char *__restrict__ old, signed char *__restrict__ nw,
+           int *left, int *ncol, int *err)
+{
+    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < n;
+         v += (long)gridDim.x * blockDim.x) {
+        signed char cv = old[v];
+        if (cv >= 0) { nw[v] = cv; continue; }
+        const unsigned long long kv = jp_key((int)v);
         unsigned long long used = 0;
-        bool ready = true;
-        for (int k = a; k < e; k++) {
+        bool ok = true;
+        for (int k = rowptr[v]; k < rowptr[v + 1]; k++) {
             int u = col[k];
-            if (u >= v) continue;
-            signed char c = vc[u];
-            if (c < 0) { ready = false; break; }
-            used |= 1ull << c;
+            if (u == v) continue;
+            signed char c = old[u];
+            if (c >= 0) used |= 1ull << c;
+            else if (jp_key(u) > kv) { ok = false; break; }
         }
-        if (ready) {
-            int c = __ffsll((long long)~used) - 1;
-            if (c < 0 || c >= kMaxColors) {  // too many colours: flag, park
-                atomicExch(err, 2);
-                c = kMaxColors;
-            }
-            vc[v] = (signed char)c;
-            atomicMax(ncol, c + 1);
-            return;
-        }
-        if (++polls > kMaxPolls || *verr == 1) { atomicExch(err, 1); return; }
-        if (polls > 32) __nanosleep(64);
+        if (!ok) { nw[v] = -1; continue; }
+        int c = __ffsll((long long)~used) - 1;
+        if (c < 0 || c >= kMaxColors) { atomicExch(err, 2); c = kMaxColors; }
+        nw[v] = (signed char)c;
+        atomicSub(left, 1);
+        atomicMax(ncol, c + 1);
     }
 }
 
@@ -147,20 +145,32 @@ int color_level(Level &L, cudaStream_t st, int *dwork)
     L.gs = false;
     if (n < 1) return HMFEM_OK;
     L.color = (signed char *)dalloc(n);
-    if (!L.color) return HMFEM_E_CUDA;
+    signed char *tmpc = (signed char *)dalloc(n);
+    if (!L.color || !tmpc) return HMFEM_E_CUDA;
     HM_CUDA(cudaMemsetAsync(L.color, 0xff, n, st));
-    HM_CUDA(cudaMemsetAsync(dwork, 0, 4 * sizeof(int), st));
-    k_greedy_color<<<(int)ceil_div(n, kTile), kTile, 0, st>>>(
-        L.A.rowptr, L.A.col, n, L.color, (unsigned *)(dwork + 2), dwork, dwork + 1);
-    HM_CUDA(cudaGetLastError());
-    int h[2];
+    int h0[3] = {n, 0, 0};  // left, colours, error
+    HM_CUDA(cudaMemcpyAsync(dwork, h0, sizeof(h0), cudaMemcpyHostToDevice, st));
+    signed char *a = L.color, *b = tmpc;
+    int h[3] = {n, 0, 0};
+    for (int round = 0; round < 4096 && h[0] > 0; round++) {
+        k_jp_round<<<nb(n), kTile, 0, st>>>(L.A.rowptr, L.A.col, n, a, b, dwork,
+                                            dwork + 1, dwork + 2);
+        HM_CUDA(cudaGetLastError());
+        signed char *t = a; a = b; b = t;
+        if ((round & 3) == 3 || round < 4) {
+            HM_CUDA(cudaMemcpyAsync(h, dwork, sizeof(h), cudaMemcpyDeviceToHost, st));
+            HM_CUDA(cudaStreamSynchronize(st));
+        }
+    }
+    if (a != L.color) HM_CUDA(cudaMemcpyAsync(L.color, a, n, cudaMemcpyDeviceToDevice, st));
     HM_CUDA(cudaMemcpyAsync(h, dwork, sizeof(h), cudaMemcpyDeviceToHost, st));
     HM_CUDA(cudaStreamSynchronize(st));
-    if (h[0] == 1) {
-        set_last_error("colouring wavefront gave up waiting", __FILE__, __LINE__);
+    dfree(tmpc);
+    if (h[0] > 0) {
+        set_last_error("colouring did not finish", __FILE__, __LINE__);
         return HMFEM_E_TIMEOUT;
     }
-    if (h[0] == 2) return HMFEM_OK;  // over 63 colours: keep l1-Jacobi here
+    if (h[2] == 2) return HMFEM_OK;  // over 63 colours: keep l1-Jacobi here
     const int nc = h[1];
     // rows grouped by colour (stable: ascending within a colour)
     int *key = (int *)dalloc(sizeof(int) * n), *row = (int *)dalloc(sizeof(int) * n);

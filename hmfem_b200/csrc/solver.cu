@@ -42,37 +42,40 @@ int launch_smoother_diag(const Csr &A, int kind, double *dsm, float *dsm32,
     return HMFEM_OK;
 }
 
-// Dense FP64 Cholesky of a small SPD level, one block, in place (lower
-// triangle of a row-major n x n array).
+// Explicit FP64 inverse of a small SPD level by in-place Gauss-Jordan
+// elimination (one block; SPD, so no pivoting): the coarse solve then is a
+// single dense mat-vec.  err = 1 on a non-positive pivot.
 __global__ void k_dense_factor(int n, const int *__restrict__ rowptr,
                                const int *__restrict__ col,
-                               const double *__restrict__ val, double *Lf,
+                               const double *__restrict__ val, double *M,
                                int *err)
 {
     const long nn = (long)n * n;
-    for (long q = threadIdx.x; q < nn; q += blockDim.x) Lf[q] = 0.0;
+    for (long q = threadIdx.x; q < nn; q += blockDim.x) M[q] = 0.0;
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x)
-        for (int k = rowptr[i]; k < rowptr[i + 1]; k++) Lf[(long)i * n + col[k]] += val[k];
+        for (int k = rowptr[i]; k < rowptr[i + 1]; k++) M[(long)i * n + col[k]] += val[k];
     __syncthreads();
-    __shared__ double s_d;
-    for (int j = 0; j < n; j++) {
+    __shared__ double s_pinv;
+    for (int k = 0; k < n; k++) {
         if (threadIdx.x == 0) {
-            double d = Lf[(long)j * n + j];
-            if (!(d > 0.0)) { *err = 1; d = 1.0; }
-            s_d = sqrt(d);
-            Lf[(long)j * n + j] = s_d;
+            double p = M[(long)k * n + k];
+            if (!(p > 0.0)) { *err = 1; p = 1.0; }
+            s_pinv = 1.0 / p;
         }
         __syncthreads();
-        double ljj = s_d;
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) Lf[(long)i * n + j] /= ljj;
+        const double pinv = s_pinv;
+        for (int j = threadIdx.x; j < n; j += blockDim.x)
+            if (j != k) M[(long)k * n + j] *= pinv;
         __syncthreads();
-        const int m = n - j - 1;
-        const long pairs = (long)m * m;
-        for (long q = threadIdx.x; q < pairs; q += blockDim.x) {
-            int i = j + 1 + (int)(q / m), k = j + 1 + (int)(q % m);
-            if (k <= i) Lf[(long)i * n + k] -= Lf[(long)i * n + j] * Lf[(long)k * n + j];
+        for (long q = threadIdx.x; q < nn; q += blockDim.x) {
+            const int i = (int)(q / n), j = (int)(q % n);
+            if (i != k && j != k) M[q] -= M[(long)i * n + k] * M[(long)k * n + j];
         }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            if (i != k) M[(long)i * n + k] *= -pinv;
+        if (threadIdx.x == 0) M[(long)k * n + k] = pinv;
         __syncthreads();
     }
 }
@@ -418,7 +421,7 @@ void hmfem_default_options(hmfem_options *o)
     o->max_iter = 10000;
     o->max_levels = 16;
     o->min_coarse = 1;
-    o->coarse_direct = 0;
+    o->coarse_direct = 512;
     o->check_every = 2;
     o->verbose = 0;
 }
@@ -428,7 +431,7 @@ int hmfem_create(hmfem_solver **out, const hmfem_options *opt)
     if (!out) return HMFEM_E_ARG;
     hmfem_solver *h = new hmfem_solver();
     Solver &s = h->s;
-    hm::set_alloc_stream(s.st);
+    hm::set_alloc_context(s.st, s.cache);
     if (opt) s.opt = *opt;
     else hmfem_default_options(&s.opt);
     if (s.opt.max_levels < 1 || s.opt.max_levels > 64 || s.opt.tol < 0) {
@@ -443,7 +446,8 @@ int hmfem_create(hmfem_solver **out, const hmfem_options *opt)
         return HMFEM_E_CUDA;
     }
     s.own_stream = true;
-    hm::set_alloc_stream(s.st);
+    s.cache = hm::alloc_cache_new();
+    hm::set_alloc_context(s.st, s.cache);
     const char *ev = getenv("HMFEM_VERBOSE");
     if (s.opt.verbose || (ev && atoi(ev) > 0)) hm::g_verbose = 1;
     s.ctl = (hm::Ctl *)hm::dalloc(sizeof(hm::Ctl));
@@ -466,14 +470,18 @@ int hmfem_destroy(hmfem_solver *h)
 {
     if (!h) return HMFEM_OK;
     Solver &s = h->s;
-    hm::set_alloc_stream(s.st);
+    hm::set_alloc_context(s.st, s.cache);
     if (s.st) cudaStreamSynchronize(s.st);
     hm::free_hierarchy(s, false);
     hm::free_vectors(s);
     for (int i = 0; i < 3; i++) hm::dfree(s.Kown[i]);
     for (int f = 0; f < 6; f++) hm::dfree(s.face[f]);
     hm::dfree(s.ctl); hm::dfree(s.part); hm::dfree(s.dwork); hm::dfree(s.mm);
+    hm::alloc_cache_release(s.cache);
+    s.cache = nullptr;
+    hm::set_alloc_context(s.st, nullptr);
     if (s.ctl_host) cudaFreeHost(s.ctl_host);
+    if (s.st) cudaStreamSynchronize(s.st);
     if (s.own_stream && s.st) cudaStreamDestroy(s.st);
     delete h;
     return HMFEM_OK;
@@ -483,7 +491,7 @@ int hmfem_set_stream(hmfem_solver *h, void *stream)
 {
     if (!h) return HMFEM_E_ARG;
     Solver &s = h->s;
-    hm::set_alloc_stream(s.st);
+    hm::set_alloc_context(s.st, s.cache);
     cudaStreamSynchronize(s.st);
     if (s.own_stream) cudaStreamDestroy(s.st);
     if (stream) {
@@ -518,7 +526,7 @@ int hmfem_assemble(hmfem_solver *h, int nx, int ny, int nz, double hx,
         return HMFEM_E_CAPACITY;
     }
     Solver &s = h->s;
-    hm::set_alloc_stream(s.st);
+    hm::set_alloc_context(s.st, s.cache);
     cudaStream_t st = s.st;
     HM_PHASE(nullptr, st);
     if (!s.have_grid || s.nx != nx || s.ny != ny || s.nz != nz || s.lv.empty() ||
@@ -587,7 +595,7 @@ int hmfem_set_matrix(hmfem_solver *h, int n, long nnz, const int *cnt,
     if (!h || n < 1 || nnz < 1 || !cnt || !col || !ele) return HMFEM_E_ARG;
     if (nnz > 2147483647L) return HMFEM_E_CAPACITY;
     Solver &s = h->s;
-    hm::set_alloc_stream(s.st);
+    hm::set_alloc_context(s.st, s.cache);
     cudaStream_t st = s.st;
     HM_CHECK(hm::new_level0(s, n));
     s.have_grid = false;
@@ -617,7 +625,7 @@ int hmfem_set_stencil(hmfem_solver *h, int nx, int ny, int nz,
     if (!h || nx < 1 || ny < 1 || nz < 1 || !perm || !indcol) return HMFEM_E_ARG;
     long n = (long)nx * ny * nz;
     Solver &s = h->s;
-    hm::set_alloc_stream(s.st);
+    hm::set_alloc_context(s.st, s.cache);
     cudaStream_t st = s.st;
     HM_CHECK(hm::new_level0(s, (int)n));
     s.have_grid = false;
@@ -661,7 +669,7 @@ int hmfem_setup(hmfem_solver *h)
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, h->s.st);
-    hm::set_alloc_stream(h->s.st);
+    hm::set_alloc_context(h->s.st, h->s.cache);
     int rc = hm::setup(h->s);
     cudaEventRecord(e1, h->s.st);
     cudaEventSynchronize(e1);
@@ -678,7 +686,7 @@ int hmfem_solve(hmfem_solver *h, const double *b, double *x, int mem,
 {
     if (!h) return HMFEM_E_ARG;
     if (h->s.lv.empty()) return HMFEM_E_ARG;
-    hm::set_alloc_stream(h->s.st);
+    hm::set_alloc_context(h->s.st, h->s.cache);
     return hm::solve(h->s, b, x, mem, st);
 }
 
@@ -687,7 +695,7 @@ int hmfem_fluxes(hmfem_solver *h, const double *p, hmfem_ele *v, int mem,
 {
     if (!h || !p || !v) return HMFEM_E_ARG;
     Solver &s = h->s;
-    hm::set_alloc_stream(s.st);
+    hm::set_alloc_context(s.st, s.cache);
     if (!s.have_grid) {
         hm::set_last_error("fluxes need the grid problem (hmfem_assemble)", __FILE__, __LINE__);
         return HMFEM_E_ARG;
@@ -743,7 +751,7 @@ int hmfem_level_copy(hmfem_solver *h, int l, int *cnt, int *col, double *ele,
 {
     if (!h || l < 0 || l >= h->s.nlevels) return HMFEM_E_ARG;
     Solver &s = h->s;
-    hm::set_alloc_stream(s.st);
+    hm::set_alloc_context(s.st, s.cache);
     hm::Level &L = s.lv[l];
     cudaStream_t st = s.st;
     const int n = L.A.n;
@@ -769,7 +777,7 @@ int hmfem_vcycle(hmfem_solver *h, const double *f, double *u, int mem)
 {
     if (!h || !f || !u) return HMFEM_E_ARG;
     Solver &s = h->s;
-    hm::set_alloc_stream(s.st);
+    hm::set_alloc_context(s.st, s.cache);
     if (!s.setup_done) HM_CHECK(hm::setup(s));
     cudaStream_t st = s.st;
     const int n = s.lv[0].A.n;
@@ -787,7 +795,7 @@ int hmfem_spmv(hmfem_solver *h, int level, const double *x, double *y, int mem)
 {
     if (!h || level < 0 || !x || !y) return HMFEM_E_ARG;
     Solver &s = h->s;
-    hm::set_alloc_stream(s.st);
+    hm::set_alloc_context(s.st, s.cache);
     if (level > 0 && !s.setup_done) HM_CHECK(hm::setup(s));
     if (level >= (int)s.lv.size()) return HMFEM_E_ARG;
     cudaStream_t st = s.st;
@@ -810,7 +818,7 @@ int hmfem_rhs(hmfem_solver *h, double *b, int mem)
 {
     if (!h || !b || h->s.lv.empty()) return HMFEM_E_ARG;
     Solver &s = h->s;
-    hm::set_alloc_stream(s.st);
+    hm::set_alloc_context(s.st, s.cache);
     HM_CHECK(hm::download(b, (const double *)s.b, s.lv[0].A.n, mem, s.st));
     HM_CUDA(cudaStreamSynchronize(s.st));
     return HMFEM_OK;
@@ -827,7 +835,7 @@ int hmfem_time_kernel(hmfem_solver *h, int which, int level, int reps,
                       float *ms, double *bytes)
 {
     if (!h || !ms || !bytes) return HMFEM_E_ARG;
-    hm::set_alloc_stream(h->s.st);
+    hm::set_alloc_context(h->s.st, h->s.cache);
     if (!h->s.setup_done) HM_CHECK(hm::setup(h->s));
     return hm::time_kernel(h->s, which, level, reps, ms, bytes);
 }

@@ -11,6 +11,7 @@ struct Solver {
     hmfem_options opt;
     cudaStream_t st = nullptr;
     bool own_stream = false;
+    AllocCache *cache = nullptr;
 
     // grid problem (hmfem_assemble)
     bool have_grid = false;

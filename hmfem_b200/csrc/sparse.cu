@@ -1,6 +1,8 @@
 // sparse.cu -- scans, CSR -> SELL-32 conversion, diagonal extraction and the
 // FP64 SELL SpMV.
 #include <cub/device/device_scan.cuh>
+#include <map>
+#include <unordered_map>
 
 #include "hm.cuh"
 
@@ -38,9 +40,53 @@ namespace hm {
 static cudaStream_t g_astream = nullptr;
 static unsigned g_pool_ready = 0;  // bit per device
 
+// Per-solver cache of freed blocks keyed by exact size: a solver that sets
+// up the same grid again gets every buffer back without touching the pool.
+struct AllocCache {
+    std::unordered_map<void *, size_t> live;
+    std::multimap<size_t, void *> idle;
+};
+static AllocCache *g_cache = nullptr;
+
 void set_alloc_stream(cudaStream_t st) { g_astream = st; }
 
+void set_alloc_context(cudaStream_t st, AllocCache *c)
+{
+    g_astream = st;
+    g_cache = c;
+}
+
+AllocCache *alloc_cache_new() { return new AllocCache(); }
+
+void alloc_cache_release(AllocCache *c)
+{
+    if (!c) return;
+    for (auto &kv : c->idle) cudaFreeAsync(kv.second, g_astream);
+    for (auto &kv : c->live) cudaFreeAsync(kv.first, g_astream);
+    if (g_cache == c) g_cache = nullptr;
+    delete c;
+}
+
+static void *pool_alloc(size_t bytes);
+
 void *dalloc(size_t bytes)
+{
+    bytes = bytes == 0 ? 256 : (bytes + 255) & ~(size_t)255;
+    if (g_cache) {
+        auto it = g_cache->idle.find(bytes);
+        if (it != g_cache->idle.end()) {
+            void *p = it->second;
+            g_cache->idle.erase(it);
+            g_cache->live[p] = bytes;
+            return p;
+        }
+    }
+    void *p = pool_alloc(bytes);
+    if (p && g_cache) g_cache->live[p] = bytes;
+    return p;
+}
+
+static void *pool_alloc(size_t bytes)
 {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -60,7 +106,16 @@ void *dalloc(size_t bytes)
 
 void dfree(void *p)
 {
-    if (p) cudaFreeAsync(p, g_astream);
+    if (!p) return;
+    if (g_cache) {
+        auto it = g_cache->live.find(p);
+        if (it != g_cache->live.end()) {
+            g_cache->idle.insert({it->second, p});
+            g_cache->live.erase(it);
+            return;
+        }
+    }
+    cudaFreeAsync(p, g_astream);
 }
 
 int scan_exclusive(const int *in, int *out, int n, cudaStream_t st)

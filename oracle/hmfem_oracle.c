@@ -277,24 +277,60 @@ static void spmt(int arows, const int *acnt, const int *acol,
     *ccnt_o = ccnt; *ccol_o = ccol; *cele_o = cele; *csize_o = csize;
 }
 
-/* Greedy colouring in natural row order: each row takes the smallest colour
- * not used by a lower-numbered neighbour (project smoother setup). */
+/* Colouring for the multicolour Gauss-Seidel smoother (project setup, no
+ * reference counterpart): Jones-Plassmann rounds with fixed pseudo-random
+ * priorities.  In each round every uncoloured row whose (priority, index)
+ * key exceeds those of all its uncoloured neighbours takes the smallest
+ * colour not used by its already-coloured neighbours; those rows form an
+ * independent set, so a round's result does not depend on the order the
+ * rows are visited in (the GPU visits them in parallel). */
+static unsigned jp_prio(unsigned x)
+{
+    x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
+    return x;
+}
+
+static unsigned long long jp_key(int v)
+{
+    return ((unsigned long long)jp_prio((unsigned)v) << 32) | (unsigned)v;
+}
+
 static int greedy_colour(or_level *A)
 {
-    A->color = (signed char *)malloc(A->n > 0 ? A->n : 1);
-    long m = 0;
-    int nc = 0;
-    for (int i = 0; i < A->n; i++) {
-        unsigned long long used = 0;
-        for (int j = 0; j < A->cnt[i]; j++, m++) {
-            int c = A->col[m];
-            if (c < i) used |= 1ull << A->color[c];
+    const int n = A->n;
+    A->color = (signed char *)malloc(n > 0 ? n : 1);
+    signed char *nw = (signed char *)malloc(n > 0 ? n : 1);
+    long *dsp = offsets(n, A->cnt);
+    for (int i = 0; i < n; i++) A->color[i] = -1;
+    int left = n, nc = 0;
+    while (left > 0) {
+        for (int v = 0; v < n; v++) {
+            nw[v] = A->color[v];
+            if (A->color[v] >= 0) continue;
+            unsigned long long used = 0, kv = jp_key(v);
+            int ok = 1;
+            for (long j = dsp[v]; j < dsp[v + 1]; j++) {
+                int u = A->col[j];
+                if (u == v) continue;
+                signed char c = A->color[u];
+                if (c >= 0) used |= 1ull << c;
+                else if (jp_key(u) > kv) { ok = 0; break; }
+            }
+            if (!ok) continue;
+            int k = 0;
+            while (k < 63 && (used & (1ull << k))) k++;
+            nw[v] = (signed char)k;
         }
-        int k = 0;
-        while (k < 63 && (used & (1ull << k))) k++;
-        A->color[i] = (signed char)k;
-        if (k + 1 > nc) nc = k + 1;
+        for (int v = 0; v < n; v++) {
+            if (A->color[v] < 0 && nw[v] >= 0) {
+                left--;
+                if (nw[v] + 1 > nc) nc = nw[v] + 1;
+            }
+            A->color[v] = nw[v];
+        }
     }
+    free(nw);
+    free(dsp);
     return nc;
 }
 

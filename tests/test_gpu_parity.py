@@ -97,7 +97,9 @@ def test_hierarchy_bit_exact(case):
                           (1, 2, 12, 1.0), (1, 1, 11, 1.0)])
 def test_vcycle_bit_exact(case, smoother, gs_from, oracle_smoother, omega):
     name, p, (perm, ind, b, csr, H) = case
-    s = gpu.Solver(smoother=smoother, gs_from=gs_from, omega=omega)
+    # coarse_direct=0: the reference's diagonal solve on the coarsest level
+    s = gpu.Solver(smoother=smoother, gs_from=gs_from, omega=omega,
+                   coarse_direct=0)
     s.assemble(p)
     s.setup()
     f = np.random.default_rng(11).standard_normal(p.n)
