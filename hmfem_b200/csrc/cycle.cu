@@ -191,50 +191,88 @@ k_gs_init(int n, const signed char *__restrict__ color, const T *__restrict__ f,
     GRID_STRIDE(i, n) u[i] = color[i] == 0 ? A::mul(f[i], dinv[i]) : (T)0;
 }
 
-// One colour: u_i += (f_i - sum_j a_ij u_j) / a_ii for the rows in slots
-// [s0, s1) of the colour-ordered SELL (no two rows of a colour couple).
+// sum_j a_ij x_j of CSR row `row` by the eight threads of a warp quarter
+// (g = thread within the group): thread g adds entries g, g+8, ... in
+// order (four entries per round, so the gathers overlap), the eight
+// partial sums are combined by xor offsets 4, 2, 1 and thread 0's value is
+// returned to the group -- the order the oracle's row_dot8 reproduces.
+// Every thread of the warp must call this (a group with no row passes
+// a = e = 0).
+template <class T, class M>
+__device__ __forceinline__ T row_dot8(int a, int e, const int *__restrict__ col,
+                                      const M *__restrict__ val,
+                                      const T *__restrict__ x, int g)
+{
+    using A = Ar<T>;
+    T p = (T)0;
+    for (int k0 = a + g; k0 < e; k0 += 32) {
+        int c[4];
+        T v[4], xv[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int k = k0 + 8 * q;
+            c[q] = k < e ? col[k] : 0;
+            v[q] = k < e ? (T)ld(val, k) : (T)0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) xv[q] = k0 + 8 * q < e ? x[c[q]] : (T)0;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (k0 + 8 * q < e) p = A::add(p, A::mul(v[q], xv[q]));
+    }
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) p = A::add(p, __shfl_xor_sync(0xffffffffu, p, o));
+    return __shfl_sync(0xffffffffu, p, (threadIdx.x & 31) & ~7);
+}
+
+// One colour of a Gauss-Seidel sweep, four rows per warp: rows crows[r0..r1)
+// (no two rows of a colour couple), u_i += (f_i - sum_j a_ij u_j) / a_ii.
 template <class T, class M>
 __global__ void __launch_bounds__(256)
-k_gs_sweep(const long long *__restrict__ sptr, const int *__restrict__ scol,
-           const M *__restrict__ sval, const int *__restrict__ cperm, long s0,
-           long s1, const T *__restrict__ f, const T *__restrict__ dinv,
+k_gs_sweep(const int *__restrict__ rowptr, const int *__restrict__ col,
+           const M *__restrict__ val, const int *__restrict__ crows, long r0,
+           long r1, const T *__restrict__ f, const T *__restrict__ dinv,
            T *__restrict__ u, const Ctl *ctl)
 {
     if (finished(ctl)) return;
     using A = Ar<T>;
-    for (long s = s0 + blockIdx.x * (long)blockDim.x + threadIdx.x; s < s1;
-         s += (long)gridDim.x * blockDim.x) {
-        const int row = cperm[s];
-        if (row < 0) continue;
-        long q = s >> 5;
-        int lane = (int)(s & 31);
-        long long base = sptr[q];
-        int wd = (int)((sptr[q + 1] - base) >> 5);
-        T t = f[row];
-        t = row_acc<T, true, 16>(t, scol, sval, base + lane, wd, [&](int c) { return u[c]; });
-        u[row] = A::add(u[row], A::mul(t, dinv[row]));
+    const int g = threadIdx.x & 7;
+    const long nw = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long w = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+         r0 + 4 * w < r1; w += nw) {
+        const long t = r0 + 4 * w + ((threadIdx.x & 31) >> 3);
+        const bool on = t < r1;
+        const int row = on ? crows[t] : 0;
+        const int a = on ? rowptr[row] : 0, e = on ? rowptr[row + 1] : 0;
+        const T sum = row_dot8<T>(a, e, col, val, u, g);
+        if (on && g == 0) u[row] = A::add(u[row], A::mul(A::sub(f[row], sum), dinv[row]));
     }
 }
 
-// Residual after the pre-sweep, scaled for restriction: rs = (f - A u)/|P row|.
+// Residual after the pre-sweep, scaled for restriction, four rows per warp:
+// rs = (f - A u) / |P row|.
 template <class T, class M>
 __global__ void __launch_bounds__(256)
-k_resid_rs(const long long *__restrict__ sptr, const int *__restrict__ scol,
-           const M *__restrict__ sval, int n, const T *__restrict__ f,
+k_resid_rs(const int *__restrict__ rowptr, const int *__restrict__ col,
+           const M *__restrict__ val, int n, const T *__restrict__ f,
            const T *__restrict__ u, const int *__restrict__ prow,
            T *__restrict__ rs, const Ctl *ctl)
 {
     if (finished(ctl)) return;
     using A = Ar<T>;
-    GRID_STRIDE(r, n) {
-        long q = r >> 5;
-        int lane = (int)(r & 31);
-        long long base = sptr[q];
-        int wd = (int)((sptr[q + 1] - base) >> 5);
-        T t = f[r];
-        t = row_acc<T, true>(t, scol, sval, base + lane, wd, [&](int c) { return u[c]; });
-        int pc = prow[r + 1] - prow[r];
-        rs[r] = pc == 1 ? t : A::div(t, (T)pc);
+    const int g = threadIdx.x & 7;
+    const long nw = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long w = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; 4 * w < n;
+         w += nw) {
+        const long r = 4 * w + ((threadIdx.x & 31) >> 3);
+        const bool on = r < n;
+        const int a = on ? rowptr[r] : 0, e = on ? rowptr[r + 1] : 0;
+        const T sum = row_dot8<T>(a, e, col, val, u, g);
+        if (on && g == 0) {
+            const T t = A::sub(f[r], sum);
+            const int pc = prow[r + 1] - prow[r];
+            rs[r] = pc == 1 ? t : A::div(t, (T)pc);
+        }
     }
 }
 
@@ -470,20 +508,25 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
     T *rs = s.vec_rs<T>(l);
     const T *dv = s.vec_dinv<T>(l);
     const T *dt = s.vec_dtrue<T>(l);
+    auto csr_vals = [&](auto fn) {
+        if constexpr (std::is_same<T, double>::value) fn(L.A.val);
+        else if (s.use_bf16(l)) fn(L.aval16);
+        else fn(L.aval32);
+    };
     auto sweep = [&](int c) {
-        const long s0 = L.color_slot[c], s1 = L.color_slot[c + 1];
-        with_vals<T>(s, L.CS, l, [&](auto vals) {
-            k_gs_sweep<T><<<nb(s1 - s0), 256, 0, st>>>(L.CS.sptr, L.CS.col, vals,
-                                                      L.cperm, s0, s1, f, dt, ua, ctl);
+        const long r0 = L.color_slot[c], r1 = L.color_slot[c + 1];
+        csr_vals([&](auto vals) {
+            k_gs_sweep<T><<<nb(ceil_div(r1 - r0, 4) * 32), 256, 0, st>>>(
+                L.A.rowptr, L.A.col, vals, L.crows, r0, r1, f, dt, ua, ctl);
         });
     };
     // ---- pre-smoothing + residual (scaled for the restriction)
     if (L.gs) {
         k_gs_init<T><<<nb(n), 256, 0, st>>>(n, L.color, f, dt, ua, ctl);
         for (int c = 1; c < L.ncolors; c++) sweep(c);
-        with_vals<T>(s, L.S, l, [&](auto vals) {
-            k_resid_rs<T><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, vals, n, f, ua,
-                                                L.P.rowptr, rs, ctl);
+        csr_vals([&](auto vals) {
+            k_resid_rs<T><<<nb(ceil_div(n, 4) * 32), 256, 0, st>>>(
+                L.A.rowptr, L.A.col, vals, n, f, ua, L.P.rowptr, rs, ctl);
         });
     } else {
         with_vals<T>(s, L.S, l, [&](auto vals) {

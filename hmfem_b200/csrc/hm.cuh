@@ -56,10 +56,11 @@ struct Level {
     // multicolour Gauss-Seidel smoother (levels >= gs_from)
     bool gs = false;
     int ncolors = 0;
-    signed char *color = nullptr;     // greedy natural-order colouring
-    int *cperm = nullptr;             // rows by colour, each colour padded to 32
-    Sell CS;                          // SELL over cperm (slot order)
-    std::vector<long> color_slot;     // first slot of each colour (+ end)
+    signed char *color = nullptr;     // Jones-Plassmann colouring
+    int *crows = nullptr;             // rows grouped by colour
+    std::vector<long> color_slot;     // first row of each colour in crows
+    float *aval32 = nullptr;          // CSR values in FP32 / BF16 (GS levels)
+    __nv_bfloat16 *aval16 = nullptr;
 };
 
 // Device-resident CG state; kernels read the scalars they need from here,
@@ -97,13 +98,15 @@ int scan_exclusive(const int *in, int *out, int n, cudaStream_t st);
 int rowptr_from_counts(int *rowptr, int n, cudaStream_t st, long *nnz_out);
 int csr_to_sell(const Csr &A, Sell &S, cudaStream_t st);
 int sell_fill_lowp(Sell &S, bool f32, bool bf16, cudaStream_t st);
+struct Level;
+int csr_fill_lowp(Level &L, bool bf16, cudaStream_t st);
 int launch_diag_inv(const Csr &A, double *dinv, float *dinv32, cudaStream_t st);
 int launch_spmv(const Sell &S, const double *x, double *y, cudaStream_t st);
 
 // AMG setup (amg_setup.cu)
 int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *err_dev);
-// greedy colouring + colour-ordered SELL of a level; returns HMFEM_OK with
-// L.gs = false when the level needs more than 64 colours
+// colouring + rows grouped by colour; returns HMFEM_OK with L.gs = false
+// when the level needs more than 63 colours
 int color_level(Level &L, cudaStream_t st, int *dwork);
 
 // cycle + CG (cycle.cu)

@@ -1,7 +1,6 @@
 // smoother_setup.cu -- setup of the multicolour Gauss-Seidel smoother used on
-// the coarse levels: a colouring and a SELL-32
-// copy of the level with rows grouped by colour, so one colour is one
-// coalesced, conflict-free kernel.
+// the coarse levels: a colouring and the list of rows grouped by colour, so
+// one colour is one conflict-free kernel over the level's CSR rows.
 //
 // The colouring is Jones-Plassmann with fixed pseudo-random priorities
 // (a round per launch, double-buffered, so the result is deterministic and
@@ -75,61 +74,6 @@ __global__ void k_color_hist(const signed char *__restrict__ color, int n,
         atomicAdd(cnt + color[i], 1);
 }
 
-// cperm[slot]: the rows of colour c occupy slots [dst[c], dst[c] + cnt[c]),
-// padded with -1 up to dst[c+1] (a multiple of 32).
-__global__ void k_cperm(const int *__restrict__ sorted_rows,
-                        const long *__restrict__ src, const long *__restrict__ dst,
-                        int ncolors, long nslots, int *cperm)
-{
-    for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < nslots;
-         s += (long)gridDim.x * blockDim.x) {
-        int c = 0;
-        while (c + 1 < ncolors && dst[c + 1] <= s) c++;
-        long k = s - dst[c];
-        long cnt = src[c + 1] - src[c];
-        cperm[s] = k < cnt ? sorted_rows[src[c] + k] : -1;
-    }
-}
-
-__global__ void k_cslice_len(const int *__restrict__ rowptr,
-                             const int *__restrict__ cperm, long nslices,
-                             long long *slen)
-{
-    const int lane = threadIdx.x & 31;
-    for (long q = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; q < nslices;
-         q += ((long)gridDim.x * blockDim.x) >> 5) {
-        int r = cperm[q * 32 + lane];
-        int len = r >= 0 ? rowptr[r + 1] - rowptr[r] : 0;
-        for (int o = 16; o > 0; o >>= 1)
-            len = max(len, __shfl_xor_sync(0xffffffffu, len, o));
-        if (lane == 0) slen[q] = (long long)len * 32;
-    }
-}
-
-__global__ void k_csell_fill(const int *__restrict__ rowptr,
-                             const int *__restrict__ col,
-                             const double *__restrict__ val,
-                             const int *__restrict__ cperm, long nslots,
-                             const long long *__restrict__ sptr, int *scol,
-                             double *sval)
-{
-    for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < nslots;
-         s += (long)gridDim.x * blockDim.x) {
-        long q = s >> 5;
-        int lane = (int)(s & 31);
-        long long base = sptr[q];
-        int w = (int)((sptr[q + 1] - base) >> 5);
-        int r = cperm[s];
-        int a = 0, len = 0;
-        if (r >= 0) { a = rowptr[r]; len = rowptr[r + 1] - a; }
-        for (int k = 0; k < w; k++) {
-            long long o = base + (long long)k * 32 + lane;
-            if (k < len) { scol[o] = col[a + k]; sval[o] = val[a + k]; }
-            else { scol[o] = 0; sval[o] = 0.0; }
-        }
-    }
-}
-
 int nb(long n, int threads = 256, long cap = 148L * 16)
 {
     long b = ceil_div(n, threads);
@@ -190,51 +134,13 @@ int color_level(Level &L, cudaStream_t st, int *dwork)
     int hh[64];
     HM_CUDA(cudaMemcpyAsync(hh, hist, sizeof(int) * 64, cudaMemcpyDeviceToHost, st));
     HM_CUDA(cudaStreamSynchronize(st));
-    std::vector<long> src(nc + 1), dst(nc + 1);
-    src[0] = dst[0] = 0;
-    for (int c = 0; c < nc; c++) {
-        src[c + 1] = src[c] + hh[c];
-        dst[c + 1] = dst[c] + ceil_div(hh[c], 32) * 32;
-    }
-    const long nslots = dst[nc];
-    long *dsrc = (long *)dalloc(sizeof(long) * (nc + 1));
-    long *ddst = (long *)dalloc(sizeof(long) * (nc + 1));
-    L.cperm = (int *)dalloc(sizeof(int) * nslots);
-    if (!dsrc || !ddst || !L.cperm) return HMFEM_E_CUDA;
-    HM_CUDA(cudaMemcpyAsync(dsrc, src.data(), sizeof(long) * (nc + 1), cudaMemcpyHostToDevice, st));
-    HM_CUDA(cudaMemcpyAsync(ddst, dst.data(), sizeof(long) * (nc + 1), cudaMemcpyHostToDevice, st));
-    k_cperm<<<nb(nslots), 256, 0, st>>>(srow, dsrc, ddst, nc, nslots, L.cperm);
-    HM_CUDA(cudaGetLastError());
-    // SELL over the colour-ordered slots
-    Sell &S = L.CS;
-    S.n = (int)nslots;
-    S.nslices = (int)(nslots / 32);
-    S.sptr = (long long *)dalloc(sizeof(long long) * (S.nslices + 1));
-    k_cslice_len<<<nb((long)S.nslices * 32), 256, 0, st>>>(L.A.rowptr, L.cperm,
-                                                           S.nslices, S.sptr);
-    HM_CUDA(cudaGetLastError());
-    HM_CUDA(cudaMemsetAsync(S.sptr + S.nslices, 0, sizeof(long long), st));
-    {
-        size_t tmp = 0;
-        HM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, S.sptr, S.sptr, S.nslices + 1, st));
-        void *t = dalloc(tmp);
-        HM_CUDA(cub::DeviceScan::ExclusiveSum(t, tmp, S.sptr, S.sptr, S.nslices + 1, st));
-        dfree(t);
-    }
-    long long len = 0;
-    HM_CUDA(cudaMemcpyAsync(&len, S.sptr + S.nslices, sizeof(long long), cudaMemcpyDeviceToHost, st));
-    HM_CUDA(cudaStreamSynchronize(st));
-    S.len = len;
-    S.col = (int *)dalloc(sizeof(int) * (len > 0 ? len : 1));
-    S.val = (double *)dalloc(sizeof(double) * (len > 0 ? len : 1));
-    if (!S.col || !S.val) return HMFEM_E_CUDA;
-    k_csell_fill<<<nb(nslots), 256, 0, st>>>(L.A.rowptr, L.A.col, L.A.val, L.cperm,
-                                             nslots, S.sptr, S.col, S.val);
-    HM_CUDA(cudaGetLastError());
-    dfree(key); dfree(row); dfree(skey); dfree(srow); dfree(hist);
-    dfree(dsrc); dfree(ddst);
+    std::vector<long> off(nc + 1);
+    off[0] = 0;
+    for (int c = 0; c < nc; c++) off[c + 1] = off[c] + hh[c];
+    dfree(key); dfree(row); dfree(skey); dfree(hist);
+    L.crows = srow;          // rows by colour, ascending within a colour
     L.ncolors = nc;
-    L.color_slot = dst;
+    L.color_slot = off;      // first row of each colour in crows (+ end)
     L.gs = true;
     return HMFEM_OK;
 }

@@ -118,8 +118,7 @@ static void free_level_setup(Level &L, bool keep_matrix)
     free_csr(L.P); free_csr(L.R);
     dfree(L.f); dfree(L.ua); dfree(L.ub); dfree(L.rs);
     dfree(L.f32); dfree(L.ua32); dfree(L.ub32); dfree(L.rs32);
-    dfree(L.color); dfree(L.cperm);
-    free_sell(L.CS);
+    dfree(L.color); dfree(L.crows); dfree(L.aval32); dfree(L.aval16);
     Csr a = L.A;
     L = Level();
     if (keep_matrix) L.A = a;
@@ -294,7 +293,7 @@ int setup(Solver &s)
         for (int k = s.opt.gs_from; k < stop; k++) {
             HM_CHECK(color_level(s.lv[k], st, s.dwork));
             if (s.lv[k].gs && s.opt.precision == 1)
-                HM_CHECK(sell_fill_lowp(s.lv[k].CS, true, s.use_bf16(k), st));
+                HM_CHECK(csr_fill_lowp(s.lv[k], s.use_bf16(k), st));
         }
         HM_PHASE("setup: colouring", st);
     }

@@ -297,6 +297,18 @@ int sell_fill_lowp(Sell &S, bool f32, bool bf16, cudaStream_t st)
     return HMFEM_OK;
 }
 
+int csr_fill_lowp(Level &L, bool bf16, cudaStream_t st)
+{
+    const long len = L.A.nnz;
+    if (!L.aval32) L.aval32 = (float *)dalloc(sizeof(float) * (len > 0 ? len : 1));
+    if (bf16 && !L.aval16) L.aval16 = (__nv_bfloat16 *)dalloc(2 * (len > 0 ? len : 1));
+    if (!L.aval32 || (bf16 && !L.aval16)) return HMFEM_E_CUDA;
+    k_to_lowp<<<nblocks(len, 256), 256, 0, st>>>(L.A.val, len, L.aval32,
+                                                 bf16 ? L.aval16 : nullptr);
+    HM_CUDA(cudaGetLastError());
+    return HMFEM_OK;
+}
+
 int launch_diag_inv(const Csr &A, double *dinv, float *dinv32, cudaStream_t st)
 {
     k_diag_inv<<<nblocks(A.n, 256), 256, 0, st>>>(A.rowptr, A.col, A.val, A.n,

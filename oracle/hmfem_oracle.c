@@ -561,14 +561,36 @@ typedef struct { double *u, *f, *s, *r; } or_work;
 
 /* One colour of a Gauss-Seidel sweep: rows of colour c, each
  * u_i += (f_i - sum_j a_ij u_j) / a_ii with the sum in row order. */
+/* sum_j a_ij x_j for the coarse-level smoother in the order the GPU forms
+ * it with eight threads per row: thread g sums entries g, g+8, g+16, ...
+ * of the row in order, then the eight partial sums are combined pairwise
+ * by offsets 4, 2, 1 and thread 0's value is used. */
+static double row_dot8(const or_level *A, long m0, int cnt, const double *x)
+{
+    double p[8], q[8];
+    for (int g = 0; g < 8; g++) {
+        double t = 0.0;
+        for (int k = g; k < cnt; k += 8) t += A->ele[m0 + k] * x[A->col[m0 + k]];
+        p[g] = t;
+    }
+    for (int o = 4; o > 0; o >>= 1) {
+        for (int g = 0; g < 8; g++) q[g] = p[g] + p[g ^ o];
+        for (int g = 0; g < 8; g++) p[g] = q[g];
+    }
+    return p[0];
+}
+
+/* One colour of a Gauss-Seidel sweep: rows of colour c, each
+ * u_i += (f_i - sum_j a_ij u_j) / a_ii. */
 static void gs_colour(const or_level *A, int c, const double *f, double *u)
 {
     long m = 0;
     for (int i = 0; i < A->n; i++) {
-        if (A->color[i] != c) { m += A->cnt[i]; continue; }
-        double t = f[i];
-        for (int j = 0; j < A->cnt[i]; j++, m++) t -= A->ele[m] * u[A->col[m]];
-        u[i] += t * A->dinv[i];
+        if (A->color[i] == c) {
+            double t = f[i] - row_dot8(A, m, A->cnt[i], u);
+            u[i] += t * A->dinv[i];
+        }
+        m += A->cnt[i];
     }
 }
 
@@ -596,9 +618,8 @@ static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
         for (int c = 0; c < A->ncolors; c++) gs_colour(A, c, f, u);
         long m = 0;
         for (int i = 0; i < n; i++) {
-            double t = f[i];
-            for (int j = 0; j < A->cnt[i]; j++, m++) t -= A->ele[m] * u[A->col[m]];
-            r[i] = t;
+            r[i] = f[i] - row_dot8(A, m, A->cnt[i], u);
+            m += A->cnt[i];
         }
     } else if (smoother == 0) {
         /* gauss_seidel_f 3-arg (amg.h:759-784) */
