@@ -167,6 +167,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier(world)
         times, stats = [], []
+        c0 = gpu.launch_count()
         with Clocks(local) as ck:
             for _ in range(args.steps):
                 torch.cuda.synchronize()
@@ -179,6 +180,7 @@ def run_ours(args):
                 times.append(e0.elapsed_time(e1))
                 stats.append(st)
         torch.cuda.synchronize()
+        launches[name] = gpu.launch_count() - c0
         barrier(world)
         total_ms = max_over_ranks(sum(times), world)
         results[name] = dict(ms_per_step=total_ms / args.steps,
@@ -189,11 +191,6 @@ def run_ours(args):
                              setup_ms=stats[-1]["t_setup_ms"],
                              solve_ms=stats[-1]["t_solve_ms"],
                              clocks=ck.summary(), solver=s, stream=stream)
-        # kernel launches per step: assembly(2) + setup + CG (counted from
-        # the iteration structure: see DESIGN.md)
-        L = st["levels"]
-        per_iter = 4 + (4 * (L - 1) + 1) + (2 if precision == 1 else 0)
-        launches[name] = int(3 + 12 * (L - 1) + 2 * L + 4 + per_iter * (st["iterations"] + 2))
     ch = results["chosen"]
 
     # ---- roofline: the dominant kernel, timed live on the solver stream
@@ -265,7 +262,8 @@ def run_ours(args):
                          "frac": round(achieved / peak, 4),
                          "algorithmic_bytes": by0, "ms": ms0, "traffic": None},
             "kernels_gbs": kernels_gbs,
-            "gpu_launches": launches["chosen"] * args.steps,
+            "gpu_launches": launches["chosen"],
+            "gpu_launches_per_step": launches["chosen"] / args.steps,
             "cpu_baseline": cpu,
             "clocks": ch["clocks"],
         }

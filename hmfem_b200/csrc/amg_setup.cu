@@ -286,6 +286,135 @@ k_union_warp(UnionArgs A, const int *rows, const int *nrows_dev, int tier)
     }
 }
 
+// Warp per row with a shared-memory hash table: candidates are walked in
+// generation order, 32 at a time; lanes holding the same column in a chunk
+// are grouped (match_any) and the group's lowest lane adds their values to
+// the column's slot in lane (= generation) order, so every sum keeps the
+// reference's order.  Only the distinct columns are sorted at the end.
+// Rows with more than HCAP/2 candidates go to list[tier].
+template <int STAGE, int HCAP>
+__global__ void __launch_bounds__(128)
+k_union_hash(UnionArgs A, const int *rows, const int *nrows_dev, int tier)
+{
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    struct WarpMem {
+        int key[HCAP];
+        double val[HCAP];
+        unsigned long long sorted[HCAP / 2];
+        double cv[32];
+        int off[33], ib[32];
+        double sc[32];
+    };
+    static_assert(sizeof(WarpMem) % 8 == 0, "alignment");
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpMem &M = ((WarpMem *)s_raw)[w];
+    const long nr = rows ? *nrows_dev : A.nrows;
+    for (long t = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; t < nr;
+         t += ((long)gridDim.x * blockDim.x) >> 5) {
+        const int r = rows ? rows[t] : (int)t;
+        const long long o = A.cptr[r];
+        const int m = (int)(A.cptr[r + 1] - o);
+        if (m > HCAP / 2) {
+            if (lane == 0) A.list[tier][atomicAdd(A.nlist[tier], 1)] = r;
+            continue;
+        }
+        for (int q = lane; q < HCAP; q += 32) M.key[q] = -1;
+        __syncwarp();
+        const int ob = A.orow[r], oe = A.orow[r + 1];
+        for (int c0 = ob; c0 < oe; c0 += 32) {
+            // this group's outer entries: inner row start, length, scale
+            const int k = c0 + lane;
+            const bool ok = k < oe;
+            const int j = ok ? A.ocol[k] : 0;
+            const int ib = ok ? A.irow[j] : 0;
+            const int len = ok ? A.irow[j + 1] - ib : 0;
+            double sc = 0.0;
+            if (ok) sc = STAGE == 0 ? dmul(A.oval[k], A.w[j]) : A.w[j];
+            int x = len;
+            for (int d = 1; d < 32; d <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, x, d);
+                if (lane >= d) x += y;
+            }
+            M.off[lane] = x - len;
+            M.ib[lane] = ib;
+            M.sc[lane] = sc;
+            const int tot = __shfl_sync(0xffffffffu, x, 31);
+            const int nk = min(32, oe - c0);
+            __syncwarp();
+            for (int g0 = 0; g0 < tot; g0 += 32) {
+                const int g = g0 + lane;
+                const bool on = g < tot;
+                int col = -1;
+                double tv = 0.0;
+                if (on) {
+                    int lo = 0, hi = nk - 1;  // largest kk with off[kk] <= g
+                    while (lo < hi) {
+                        int mid = (lo + hi + 1) >> 1;
+                        if (M.off[mid] <= g) lo = mid; else hi = mid - 1;
+                    }
+                    const int q = M.ib[lo] + (g - M.off[lo]);
+                    col = A.icol[q];
+                    // stage 0: a_ij * p_jd (= w_j); stage 1: AP[i][d] * w_i
+                    tv = STAGE == 0 ? M.sc[lo] : dmul(A.ival[q], M.sc[lo]);
+                }
+                M.cv[lane] = tv;
+                const unsigned grp = __match_any_sync(0xffffffffu, col);
+                __syncwarp();
+                if (on && lane == __ffs(grp) - 1) {
+                    unsigned h = ((unsigned)col * 2654435761u) & (HCAP - 1);
+                    bool fresh = false;
+                    for (;;) {
+                        int prev = atomicCAS(&M.key[h], -1, col);
+                        if (prev == -1) { fresh = true; break; }
+                        if (prev == col) break;
+                        h = (h + 1) & (HCAP - 1);
+                    }
+                    unsigned mm = grp;
+                    double acc = fresh ? M.cv[__ffs(mm) - 1] : dadd(M.val[h], M.cv[__ffs(mm) - 1]);
+                    mm &= mm - 1;
+                    while (mm) {
+                        acc = dadd(acc, M.cv[__ffs(mm) - 1]);
+                        mm &= mm - 1;
+                    }
+                    M.val[h] = acc;
+                }
+                __syncwarp();
+            }
+        }
+        // distinct columns, sorted
+        int u = 0;
+        for (int q0 = 0; q0 < HCAP; q0 += 32) {
+            const int q = q0 + lane;
+            const int kq = M.key[q];
+            const bool occ = kq >= 0;
+            const unsigned bal = __ballot_sync(0xffffffffu, occ);
+            if (occ)
+                M.sorted[u + __popc(bal & ((1u << lane) - 1))] =
+                    ((unsigned long long)(unsigned)kq << 32) | (unsigned)q;
+            u += __popc(bal);
+        }
+        __syncwarp();
+        const int up = next_pow2(u);
+        for (int q = u + lane; q < up; q += 32) M.sorted[q] = ~0ull;
+        __syncwarp();
+        sort_keys<false>(M.sorted, up, lane, 32);
+        for (int q = lane; q < u; q += 32) {
+            const unsigned long long kk = M.sorted[q];
+            A.pcol[o + q] = key_col(kk);
+            A.pval[o + q] = M.val[key_gen(kk)];
+        }
+        if (lane == 0) A.ucnt[r] = u;
+        __syncwarp();
+    }
+}
+
+template <int STAGE, int HCAP>
+size_t hash_smem()
+{
+    return 4 * (sizeof(int) * HCAP + sizeof(double) * HCAP + 8 * (HCAP / 2) +
+                8 * 32 + 4 * 33 + 4 * 32 + 8 * 32 + 4);
+}
+
 // Block per row for the longest rows (dynamic shared memory, cap entries).
 template <int STAGE>
 __global__ void __launch_bounds__(256)
@@ -358,7 +487,7 @@ int run_union(UnionArgs A, Csr &out, int *dwork, cudaStream_t st)
     }
     // pass A
     k_cand_count<STAGE><<<nblk(n, 256), 256, 0, st>>>(A, cptr);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     HM_CUDA(cudaMemsetAsync(cptr + n, 0, sizeof(long long), st));
     {
         size_t tmp = 0;
@@ -384,22 +513,24 @@ int run_union(UnionArgs A, Csr &out, int *dwork, cudaStream_t st)
     A.nlist[1] = dwork + 1;
     A.err = dwork + 2;
     HM_CUDA(cudaMemsetAsync(dwork, 0, 3 * sizeof(int), st));
-    // pass B: three tiers (<= 64 candidates, <= 1024, <= 8192)
-    k_union_warp<STAGE, 64, 8><<<nblk((long)n * 32, 256, 148L * 64), 256, 0, st>>>(
-        A, nullptr, nullptr, 0);
-    HM_CUDA(cudaGetLastError());
+    // pass B: three tiers (<= 64 candidates, <= 1024, <= 4096)
     {
-        auto kmed = k_union_warp<STAGE, 1024, 2>;
-        HM_CUDA(cudaFuncSetAttribute(kmed, cudaFuncAttributeMaxDynamicSharedMemorySize, 0));
-        kmed<<<148 * 4, 64, 0, st>>>(A, A.list[0], A.nlist[0], 1);
-        HM_CUDA(cudaGetLastError());
+        auto k0 = k_union_hash<STAGE, 128>;
+        auto k1 = k_union_hash<STAGE, 2048>;
+        const size_t m0 = hash_smem<STAGE, 128>(), m1 = hash_smem<STAGE, 2048>();
+        HM_CUDA(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m0));
+        HM_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m1));
+        k0<<<nblk((long)n * 32, 128, 148L * 64), 128, m0, st>>>(A, nullptr, nullptr, 0);
+        HM_LAUNCHED();
+        k1<<<148 * 4, 128, m1, st>>>(A, A.list[0], A.nlist[0], 1);
+        HM_LAUNCHED();
     }
     const int bcap = 4096;  // 16 B per candidate: 64 KB
     const size_t bsm = (size_t)bcap * 16;
     HM_CUDA(cudaFuncSetAttribute(k_union_block<STAGE>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
     k_union_block<STAGE><<<148 * 2, 256, bsm, st>>>(A, A.list[1], A.nlist[1], bcap);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     // pass C
     HM_CHECK(rowptr_from_counts(out.rowptr, n, st, &out.nnz));
     int herr = 0;
@@ -417,7 +548,7 @@ int run_union(UnionArgs A, Csr &out, int *dwork, cudaStream_t st)
     }
     k_compact<<<nblk((long)n * 32, 256, 148L * 32), 256, 0, st>>>(
         cptr, out.rowptr, n, A.pcol, A.pval, out.col, out.val);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     dfree(A.pcol);
     dfree(A.pval);
     dfree(cptr);
@@ -437,7 +568,7 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork)
     if (n > 0) {
         k_lfmis<<<(int)ceil_div(n, kMisTile), kMisTile, 0, st>>>(
             L.A.rowptr, L.A.col, n, L.sel, (unsigned *)(dwork + 2), dwork);
-        HM_CUDA(cudaGetLastError());
+        HM_LAUNCHED();
     }
     int herr = 0;
     HM_CUDA(cudaMemcpyAsync(&herr, dwork, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -450,7 +581,7 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork)
     // ---- coarse numbering ---------------------------------------------
     L.cid = (int *)dalloc(sizeof(int) * (n + 1));
     k_cflag<<<nblk(n, 256), 256, 0, st>>>(L.sel, n, L.cid);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     long nc = 0;
     HM_CHECK(rowptr_from_counts(L.cid, n, st, &nc));
     HM_PHASE("  coarse ids", st);
@@ -459,7 +590,7 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork)
     L.P.n = n;
     L.P.rowptr = (int *)dalloc(sizeof(int) * (n + 1));
     k_pcount<<<nblk(n, 256), 256, 0, st>>>(L.A.rowptr, L.A.col, L.sel, n, L.P.rowptr);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     HM_CHECK(rowptr_from_counts(L.P.rowptr, n, st, &L.P.nnz));
     L.P.col = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
     int *pown = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
@@ -467,7 +598,7 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork)
     L.pw32 = (float *)dalloc(sizeof(float) * (n > 0 ? n : 1));
     k_pfill<<<nblk(n, 256), 256, 0, st>>>(L.A.rowptr, L.A.col, L.sel, L.cid, n,
                                           L.P.rowptr, L.P.col, pown, L.pw, L.pw32);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     // ---- R = P^T, fine rows ascending (stable radix sort on coarse id) -
     L.R.n = L.nc;
     L.R.nnz = L.P.nnz;
@@ -476,7 +607,7 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork)
     int *keys_out = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
     HM_CUDA(cudaMemsetAsync(L.R.rowptr, 0, sizeof(int) * (L.nc + 1), st));
     k_hist<<<nblk(L.P.nnz, 256), 256, 0, st>>>(L.P.col, L.P.nnz, L.R.rowptr);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     long rn = 0;
     HM_CHECK(rowptr_from_counts(L.R.rowptr, L.nc, st, &rn));
     {

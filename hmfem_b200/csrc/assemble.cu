@@ -247,7 +247,7 @@ int launch_l0_rowcounts(int nx, int ny, int nz, int *cnt, cudaStream_t st)
 {
     long n = (long)nx * ny * nz;
     k_l0_rowcounts<<<grid_for(n, 256), 256, 0, st>>>(nx, ny, nz, cnt);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -263,7 +263,7 @@ int launch_assemble(int nx, int ny, int nz, double hx, double hy, double hz,
     long n = (long)nx * ny * nz;
     k_assemble<<<grid_for(n, 256), 256, 0, st>>>(g, KX, KY, KZ, fv, KI, WI, pc,
                                                  pw, rowptr, col, val, b);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -273,7 +273,7 @@ int launch_pack_stencil(int n, const hmfem_ele *perm, const hmfem_ind *ind,
 {
     k_pack_stencil<<<grid_for(n, 256), 256, 0, st>>>(n, perm, ind, cnt, rowptr,
                                                      col, val, pass);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -291,7 +291,7 @@ int launch_flux(int nx, int ny, int nz, double hx, double hy, double hz,
     HM_CUDA(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, st));
     k_flux<<<grid_for(n, 256), 256, 0, st>>>(g, KX, KY, KZ, fv, p, v,
                                              (unsigned long long *)mm);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 

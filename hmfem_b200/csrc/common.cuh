@@ -28,6 +28,16 @@ constexpr int kRedBlocks = 148 * 8; // max blocks of a grid-stride reduction
 
 void set_last_error(const char *msg, const char *file, int line);
 
+// Number of this library's kernels launched (captured launches count once
+// at capture; graph replays add the captured count).
+extern unsigned long long g_nlaunch;
+#define HM_COUNT() (++hm::g_nlaunch)
+#define HM_LAUNCHED()                                                         \
+    do {                                                                      \
+        HM_COUNT();                                                           \
+        HM_CUDA(cudaGetLastError());                                          \
+    } while (0)
+
 // Phase timing for diagnostics (HMFEM_VERBOSE=1 or options.verbose): syncs
 // the stream and prints the host time since the previous mark to stderr.
 extern int g_verbose;

@@ -496,12 +496,12 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
     if (l == s.direct_level) {
         k_dense_solve<T><<<(int)ceil_div((long)n * 32, 256), 256, 0, st>>>(n, s.dense_L, f, ua,
                                                                          ctl);
-        HM_CUDA(cudaGetLastError());
+        HM_LAUNCHED();
         return HMFEM_OK;
     }
     if (l == last) {
         k_diag_solve<T><<<nb(n), 256, 0, st>>>(n, s.vec_dtrue<T>(l), f, ua, ctl);
-        HM_CUDA(cudaGetLastError());
+        HM_LAUNCHED();
         return HMFEM_OK;
     }
     const T w = (T)s.opt.omega;
@@ -518,30 +518,34 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
         csr_vals([&](auto vals) {
             k_gs_sweep<T><<<nb(ceil_div(r1 - r0, 4) * 32), 256, 0, st>>>(
                 L.A.rowptr, L.A.col, vals, L.crows, r0, r1, f, dt, ua, ctl);
+            HM_COUNT();
         });
     };
     // ---- pre-smoothing + residual (scaled for the restriction)
     if (L.gs) {
         k_gs_init<T><<<nb(n), 256, 0, st>>>(n, L.color, f, dt, ua, ctl);
+        HM_COUNT();
         for (int c = 1; c < L.ncolors; c++) sweep(c);
         csr_vals([&](auto vals) {
             k_resid_rs<T><<<nb(ceil_div(n, 4) * 32), 256, 0, st>>>(
                 L.A.rowptr, L.A.col, vals, n, f, ua, L.P.rowptr, rs, ctl);
+            HM_COUNT();
         });
     } else {
         with_vals<T>(s, L.S, l, [&](auto vals) {
             k_pre<T><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, vals, n, f, dv, w,
                                            L.P.rowptr, ua, rs, ctl);
+            HM_COUNT();
         });
     }
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     k_restrict<T><<<nb(L.nc), 256, 0, st>>>(L.R.rowptr, L.R.col, L.nc, rs,
                                             s.vec_f<T>(l + 1), ctl);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     HM_CHECK(cycle_t<T>(s, l + 1, st, false));
     k_prolong_add<T><<<nb(n), 256, 0, st>>>(L.P.rowptr, L.P.col, n,
                                             cycle_out<T>(s, l + 1), ua, ctl);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     // ---- post-smoothing
     if (L.gs) {
         for (int c = L.ncolors - 1; c >= 0; c--) sweep(c);
@@ -549,15 +553,17 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
         k_post<T, T, true><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, s.sval<T>(l), n,
                                                    f, dv, w, ua, ub, s.ctl, s.part,
                                                    s.first_sigma);
+        HM_COUNT();
     } else {
         with_vals<T>(s, L.S, l, [&](auto vals) {
             k_post<T, typename std::remove_const<typename std::remove_pointer<
                           decltype(vals)>::type>::type, false>
                 <<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, vals, n, f, dv, w, ua, ub,
                                         ctl, nullptr, 0);
+            HM_COUNT();
         });
     }
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -587,17 +593,17 @@ int cg_precondition(Solver &s, cudaStream_t st)
             k_finish_z<double><<<nb(n), 256, 0, st>>>(n, L0.ua, s.r, s.v, s.z,
                                                       s.ctl, s.part,
                                                       s.first_sigma, 0);
-            HM_CUDA(cudaGetLastError());
+            HM_LAUNCHED();
         }
         return HMFEM_OK;
     }
     k_demote<<<nb(n), 256, 0, st>>>(n, s.r, L0.f32, s.ctl);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     HM_CHECK(cycle_fp32(s, 0, st, false));
     const float *z32 = top_is_coarse ? L0.ua32 : L0.ub32;
     k_finish_z<float><<<nb(n), 256, 0, st>>>(n, z32, s.r, s.v, s.z, s.ctl,
                                              s.part, s.first_sigma, 1);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -607,12 +613,12 @@ int cg_init(Solver &s, cudaStream_t st)
     const int n = L0.A.n;
     k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
                                    s.r, s.ctl, s.part, 1);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     s.first_sigma = 1;
     HM_CHECK(cg_precondition(s, st));
     s.first_sigma = 0;
     k_sdir<<<nb(n), 256, 0, st>>>(n, s.s, s.z, s.ctl);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -622,15 +628,15 @@ int cg_iteration(Solver &s, cudaStream_t st)
     const int n = L0.A.n;
     k_spmv_dot<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.s,
                                       s.v, s.ctl, s.part);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     k_update<<<nb(n), 256, 0, st>>>(n, s.x, s.r, s.s, s.v, s.ctl, s.part);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
                                    s.r, s.ctl, s.part, 0);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     HM_CHECK(cg_precondition(s, st));
     k_sdir<<<nb(n), 256, 0, st>>>(n, s.s, s.z, s.ctl);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -641,7 +647,7 @@ int cg_final_residual(Solver &s, cudaStream_t st)
     const int n = L0.A.n;
     k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
                                    s.r, s.ctl, s.part, 2);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -731,7 +737,7 @@ int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
     for (int i = 0; i < reps; i++) launch();
     HM_CUDA(cudaEventRecord(e1, st));
     HM_CUDA(cudaEventSynchronize(e1));
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     float t = 0;
     cudaEventElapsedTime(&t, e0, e1);
     cudaEventDestroy(e0);

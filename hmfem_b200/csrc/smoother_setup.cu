@@ -99,7 +99,7 @@ int color_level(Level &L, cudaStream_t st, int *dwork)
     for (int round = 0; round < 4096 && h[0] > 0; round++) {
         k_jp_round<<<nb(n), kTile, 0, st>>>(L.A.rowptr, L.A.col, n, a, b, dwork,
                                             dwork + 1, dwork + 2);
-        HM_CUDA(cudaGetLastError());
+        HM_LAUNCHED();
         signed char *t = a; a = b; b = t;
         if ((round & 3) == 3 || round < 4) {
             HM_CUDA(cudaMemcpyAsync(h, dwork, sizeof(h), cudaMemcpyDeviceToHost, st));
@@ -122,8 +122,10 @@ int color_level(Level &L, cudaStream_t st, int *dwork)
     int *hist = (int *)dalloc(sizeof(int) * 64);
     if (!key || !row || !skey || !srow || !hist) return HMFEM_E_CUDA;
     k_color_key<<<nb(n), 256, 0, st>>>(L.color, n, key, row);
+    HM_LAUNCHED();
     HM_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * 64, st));
     k_color_hist<<<nb(n), 256, 0, st>>>(L.color, n, hist);
+    HM_LAUNCHED();
     {
         size_t tmp = 0;
         HM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, skey, row, srow, n, 0, 6, st));

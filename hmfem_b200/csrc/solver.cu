@@ -38,7 +38,7 @@ int launch_smoother_diag(const Csr &A, int kind, double *dsm, float *dsm32,
     long b = ceil_div(A.n, 256);
     k_smoother_diag<<<(int)(b < 2368 ? (b > 0 ? b : 1) : 2368), 256, 0, st>>>(
         A.rowptr, A.col, A.val, A.n, kind, dsm, dsm32);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -83,7 +83,7 @@ __global__ void k_dense_factor(int n, const int *__restrict__ rowptr,
 int dense_factor(const Csr &A, double *Lf, int *err, cudaStream_t st)
 {
     k_dense_factor<<<1, 1024, 0, st>>>(A.n, A.rowptr, A.col, A.val, Lf, err);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -310,7 +310,9 @@ static int capture_iteration(Solver &s)
     cudaStream_t cs;
     HM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     HM_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    const unsigned long long before = g_nlaunch;
     int rc = cg_iteration(s, cs);
+    s.graph_kernels = g_nlaunch - before;
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);
@@ -357,7 +359,10 @@ int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out)
     int slot = 0, launched = 0;
     bool pending = false;
     for (;;) {
-        for (int i = 0; i < k; i++) HM_CUDA(cudaGraphLaunch(s.gexec, st));
+        for (int i = 0; i < k; i++) {
+            HM_CUDA(cudaGraphLaunch(s.gexec, st));
+            g_nlaunch += s.graph_kernels;
+        }
         launched += k;
         HM_CUDA(cudaMemcpyAsync(&s.ctl_host[slot], s.ctl, sizeof(Ctl),
                                 cudaMemcpyDeviceToHost, st));
@@ -568,7 +573,7 @@ int hmfem_assemble(hmfem_solver *h, int nx, int ny, int nz, double hx,
             double v = bc_value ? bc_value[f] : 0.0;
             hm::k_fill<<<(int)hm::ceil_div(fsz[f], 256) < 1024 ? (int)hm::ceil_div(fsz[f], 256) : 1024,
                          256, 0, st>>>(s.face[f], fsz[f], v);
-            HM_CUDA(cudaGetLastError());
+            HM_LAUNCHED();
         }
     }
     hm::Level &L = s.lv[0];
@@ -924,3 +929,5 @@ void solve_linsys_cxx(hmfem_ele *perm, hmfem_ind *indcol, double *b, double *x,
 {
     solve_linsys(perm, indcol, b, x, N);
 }
+
+extern "C" unsigned long long hmfem_launch_count(void) { return hm::g_nlaunch; }

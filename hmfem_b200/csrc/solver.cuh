@@ -41,6 +41,7 @@ struct Solver {
     int first_sigma = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    unsigned long long graph_kernels = 0;  // kernels in one captured iteration
     hmfem_stats last{};
 
     bool use_bf16(int l) const

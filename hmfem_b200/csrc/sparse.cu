@@ -16,6 +16,7 @@ void set_last_error(const char *msg, const char *file, int line)
 }
 
 int g_verbose = 0;
+unsigned long long g_nlaunch = 0;
 
 void phase_mark(const char *label, cudaStream_t st)
 {
@@ -263,7 +264,7 @@ int csr_to_sell(const Csr &A, Sell &S, cudaStream_t st)
     if (!S.sptr) { set_last_error("out of device memory (sell)", __FILE__, __LINE__); return HMFEM_E_CUDA; }
     k_slice_len<<<nblocks((long)S.nslices * 32, 256), 256, 0, st>>>(
         A.rowptr, A.n, S.nslices, S.sptr);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     size_t tmp = 0;
     HM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, S.sptr, S.sptr,
                                           S.nslices + 1, st));
@@ -282,7 +283,7 @@ int csr_to_sell(const Csr &A, Sell &S, cudaStream_t st)
     if (!S.col || !S.val) { set_last_error("out of device memory (sell)", __FILE__, __LINE__); return HMFEM_E_CUDA; }
     k_sell_fill<<<nblocks((long)S.nslices * 32, 256), 256, 0, st>>>(
         A.rowptr, A.col, A.val, A.n, (long)S.nslices * 32, S.sptr, S.col, S.val);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -293,7 +294,7 @@ int sell_fill_lowp(Sell &S, bool f32, bool bf16, cudaStream_t st)
     k_to_lowp<<<nblocks(S.len, 256), 256, 0, st>>>(S.val, S.len,
                                                    f32 ? S.val32 : nullptr,
                                                    bf16 ? S.val16 : nullptr);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -305,7 +306,7 @@ int csr_fill_lowp(Level &L, bool bf16, cudaStream_t st)
     if (!L.aval32 || (bf16 && !L.aval16)) return HMFEM_E_CUDA;
     k_to_lowp<<<nblocks(len, 256), 256, 0, st>>>(L.A.val, len, L.aval32,
                                                  bf16 ? L.aval16 : nullptr);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
@@ -313,14 +314,14 @@ int launch_diag_inv(const Csr &A, double *dinv, float *dinv32, cudaStream_t st)
 {
     k_diag_inv<<<nblocks(A.n, 256), 256, 0, st>>>(A.rowptr, A.col, A.val, A.n,
                                                    dinv, dinv32);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 
 int launch_spmv(const Sell &S, const double *x, double *y, cudaStream_t st)
 {
     k_spmv<<<nblocks(S.n, 256), 256, 0, st>>>(S.sptr, S.col, S.val, S.n, x, y);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 

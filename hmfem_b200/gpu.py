@@ -79,6 +79,7 @@ EXPORTS = [
     "hmfem_solve", "hmfem_fluxes", "hmfem_num_levels", "hmfem_level_info",
     "hmfem_level_copy", "hmfem_vcycle", "hmfem_spmv", "hmfem_rhs",
     "hmfem_last_stats", "hmfem_time_kernel", "hmfem_fluxes_noalloc",
+    "hmfem_launch_count",
 ]
 
 NOALLOC_MAX_FACE = 262144  # HMFEM_NOALLOC_MAX_FACE in include/hmfem_gpu.h
@@ -121,6 +122,7 @@ def lib():
                                            vp, vp, vp, vp, vp,
                                            C.POINTER(C.c_double),
                                            C.POINTER(C.c_double), vp]
+        L.hmfem_launch_count.restype = C.c_ulonglong
         L.compute.argtypes = [vp] * 6
         L.solve_linsys.argtypes = [vp, vp, vp, vp, Dim]
         L.solve_linsys.restype = None
@@ -326,6 +328,11 @@ def solve_linsys(perm, indcol, b, x, nx, ny, nz):
     N = Dim(nx, ny, nz, nx * ny, nx * ny * nz, 0, 0, 0)
     L.solve_linsys(perm.ctypes.data, indcol.ctypes.data, b.ctypes.data,
                    x.ctypes.data, N)
+
+
+def launch_count() -> int:
+    """Kernels of this library launched so far (graph replays included)."""
+    return int(lib().hmfem_launch_count())
 
 
 def iter_amg() -> int:

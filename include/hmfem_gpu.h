@@ -185,6 +185,10 @@ int hmfem_last_stats(hmfem_solver *s, hmfem_stats *st);
 int hmfem_time_kernel(hmfem_solver *s, int which, int level, int reps,
                       float *ms, double *bytes);
 
+/* Number of this library's kernels launched so far in the process
+ * (graph replays included): a measurement aid. */
+unsigned long long hmfem_launch_count(void);
+
 /* Flux reconstruction that allocates nothing.  No counterpart in the
  * reference.  For callers that cannot let a library allocate device memory
  * (their device memory is already reserved by their own or a framework's
