@@ -45,6 +45,10 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=96)
+    ap.add_argument("--profile-step", type=int, default=-1, metavar="PRECISION",
+                    help="run one untimed step (assembly + setup + solve) of "
+                         "the plain (0) or chosen (1) variant and exit: the "
+                         "command the ncu summaries under profiles/ profile")
     return ap.parse_args()
 
 
@@ -60,6 +64,7 @@ class Clocks:
 
     def __init__(self, dev):
         self.dev, self.rows, self.proc = dev, [], None
+        self.t0, self.t1 = None, None
 
     def __enter__(self):
         try:
@@ -75,7 +80,12 @@ class Clocks:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([c.strip() for c in line.split(",")])
+            self.rows.append((time.perf_counter(),
+                              [c.strip() for c in line.split(",")]))
+
+    def window(self, t0, t1):
+        """Samples taken while [t0, t1] (the timed region) was running."""
+        self.t0, self.t1 = t0, t1
 
     def __exit__(self, *a):
         if self.proc:
@@ -86,17 +96,19 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
+        rows = [r for t, r in self.rows
+                if self.t0 is None or self.t0 <= t <= self.t1 + 0.15]
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
                  "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4)
+        reasons = sorted({names[i] for r in rows for i in range(4)
                           if len(r) > 2 + i and r[2 + i].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.rows)}
+                "samples": len(rows)}
 
 
 def dist_init(args):
@@ -162,13 +174,16 @@ def run_ours(args):
     for name, precision in (("plain_fp64", 0), ("chosen", 1)):
         s, stream = make(precision)
         x = torch.zeros(n, dtype=torch.float64, device=dev)
-        for _ in range(args.warmup):
-            st = step(s, x)
-        torch.cuda.synchronize()
-        barrier(world)
-        times, stats = [], []
-        c0 = gpu.launch_count()
+        # the clock sampler starts before the warm-up (its start-up stalls
+        # the driver) and only its samples from the timed region are kept
         with Clocks(local) as ck:
+            for _ in range(args.warmup):
+                st = step(s, x)
+            torch.cuda.synchronize()
+            barrier(world)
+            times, stats = [], []
+            c0 = gpu.launch_count()
+            tw0 = time.perf_counter()
             for _ in range(args.steps):
                 torch.cuda.synchronize()
                 e0 = torch.cuda.Event(enable_timing=True)
@@ -179,6 +194,7 @@ def run_ours(args):
                 e1.synchronize()
                 times.append(e0.elapsed_time(e1))
                 stats.append(st)
+            ck.window(tw0, time.perf_counter())
         torch.cuda.synchronize()
         launches[name] = gpu.launch_count() - c0
         barrier(world)
@@ -342,9 +358,29 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def profile_step(args):
+    import torch
+
+    from hmfem_b200 import gpu
+    from hmfem_b200.problem import config_problem
+    prob = config_problem(2, size=args.size)
+    K = torch.tensor(prob.KX, device="cuda")
+    s = gpu.Solver(precision=args.profile_step, tol=args.tol)
+    x = torch.zeros(prob.n, dtype=torch.float64, device="cuda")
+    s.assemble(prob, KX=K, KY=K, KZ=K)
+    s.setup()
+    _, st = s.solve(x=x)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_step": args.profile_step, "size": args.size,
+                      "iterations": st["iterations"], "relres": st["relres"],
+                      "launches": gpu.launch_count()}))
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.profile_step >= 0:
+        profile_step(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -558,14 +558,17 @@ int run_union(UnionArgs A, Csr &out, int *dwork, cudaStream_t st)
 
 }  // namespace
 
-int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork)
+int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
+                const int *grid3)
 {
     const int n = L.A.n;
     // ---- C/F split ----------------------------------------------------
     L.sel = (signed char *)dalloc(n > 0 ? n : 1);
     HM_CUDA(cudaMemsetAsync(L.sel, 0, n > 0 ? n : 1, st));
     HM_CUDA(cudaMemsetAsync(dwork, 0, 4 * sizeof(int), st));
-    if (n > 0) {
+    if (grid3) {
+        HM_CHECK(stencil_parity_split(grid3[0], grid3[1], grid3[2], L.sel, st));
+    } else if (n > 0) {
         k_lfmis<<<(int)ceil_div(n, kMisTile), kMisTile, 0, st>>>(
             L.A.rowptr, L.A.col, n, L.sel, (unsigned *)(dwork + 2), dwork);
         HM_LAUNCHED();
@@ -628,6 +631,11 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork)
     dfree(pown);
     HM_PHASE("  P and R", st);
     // ---- Galerkin product ---------------------------------------------
+    if (grid3) {
+        HM_CHECK(stencil_galerkin(grid3[0], grid3[1], grid3[2], L, C.A, st));
+        HM_PHASE("  P^T A P (stencil)", st);
+        return HMFEM_OK;
+    }
     Csr AP;
     UnionArgs a0{};
     a0.nrows = n;

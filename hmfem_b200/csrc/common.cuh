@@ -9,7 +9,7 @@
 namespace hm {
 
 constexpr int kSlice = 32;          // SELL slice height = warp width
-constexpr int kRedBlocks = 148 * 8; // max blocks of a grid-stride reduction
+constexpr int kRedBlocks = 148 * 6; // max blocks of a grid-stride reduction (6 resident per SM at 40 registers)
 
 // Status plumbing: every host entry returns an hmfem status code.
 #define HM_CUDA(call)                                                         \

@@ -38,7 +38,7 @@ __device__ __forceinline__ bool finished(const Ctl *c) { return c && *(volatile 
 // (entries at o, o+32, ...), in stored order.  Column indices, values and
 // the gathered x are loaded four entries at a time so the dependent gathers
 // overlap; the summation order is unchanged.
-template <class T, bool SUB, int CH = 8, class M, class X>
+template <class T, bool SUB, int CH = 4, class M, class X>
 __device__ __forceinline__ T row_acc(T t, const int *__restrict__ scol,
                                      const M *__restrict__ sval, long long o,
                                      int wd, X x)
@@ -72,7 +72,7 @@ __device__ __forceinline__ T row_acc(T t, const int *__restrict__ scol,
 // device_amg.h:35-42):  u = w D^-1 f;  r = f - A u;  rs = r / |P row|
 // (the 1/c of simple_restriction, generic_operator.h:97-122, applied here).
 template <class T, class M>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 6)
 k_pre(const long long *__restrict__ sptr, const int *__restrict__ scol,
       const M *__restrict__ sval, int n, const T *__restrict__ f,
       const T *__restrict__ dinv, T w, const int *__restrict__ prow,
@@ -138,7 +138,7 @@ k_prolong_add(const int *__restrict__ prow, const int *__restrict__ pcol, int n,
 // v = f - A u;  u_out = u + w v D^-1.  Optionally accumulates
 // dot(u_out, f) -> ctl->sigma (the PCG's (C r, r), pcg.h:66).
 template <class T, class M, bool DOT>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 6)
 k_post(const long long *__restrict__ sptr, const int *__restrict__ scol,
        const M *__restrict__ sval, int n, const T *__restrict__ f,
        const T *__restrict__ dinv, T w, const T *__restrict__ u,
@@ -309,7 +309,7 @@ k_dense_solve(int n, const double *__restrict__ Minv, const T *__restrict__ f,
 // ---- CG kernels ---------------------------------------------------------
 
 // r = b - A x; rr = (r,r); bb = (b,b)
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 6)
 k_resid(const long long *__restrict__ sptr, const int *__restrict__ scol,
         const double *__restrict__ sval, int n, const double *__restrict__ b,
         const double *__restrict__ x, double *__restrict__ r, Ctl *ctl,
@@ -351,7 +351,7 @@ k_resid(const long long *__restrict__ sptr, const int *__restrict__ scol,
 }
 
 // v = A s; tau = (s, v); alpha = sigma / tau (pcg.h:59-63)
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 6)
 k_spmv_dot(const long long *__restrict__ sptr, const int *__restrict__ scol,
            const double *__restrict__ sval, int n, const double *__restrict__ s,
            double *__restrict__ v, Ctl *ctl, double *part)

@@ -104,7 +104,14 @@ int launch_diag_inv(const Csr &A, double *dinv, float *dinv32, cudaStream_t st);
 int launch_spmv(const Sell &S, const double *x, double *y, cudaStream_t st);
 
 // AMG setup (amg_setup.cu)
-int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *err_dev);
+// grid3 (nx, ny, nz) marks a level-0 matrix assembled on the device: its
+// split and Galerkin product then come from the 7-point structure
+// (rap_stencil.cu), bit-identical to the generic kernels.
+int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *err_dev,
+                const int *grid3 = nullptr);
+int stencil_parity_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st);
+int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
+                     cudaStream_t st);
 // colouring + rows grouped by colour; returns HMFEM_OK with L.gs = false
 // when the level needs more than 63 colours
 int color_level(Level &L, cudaStream_t st, int *dwork);

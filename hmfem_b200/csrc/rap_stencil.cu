@@ -1,0 +1,251 @@
+// rap_stencil.cu -- the first coarsening step of a matrix assembled on the
+// device (hmfem_assemble), computed from its known 7-point structure.
+//
+// For the TPFA stencil in natural order the reference's greedy C/F split
+// (amg.h:1-32, 219-223) is the parity colouring: a cell is C iff i+j+k is
+// even (every odd cell has a lower even neighbour, every even cell's lower
+// neighbours are odd).  P then takes each F cell's neighbours (all C) with
+// weight 1/degree, and the Galerkin row of a coarse cell c involves only c
+// and its six F neighbours: the 19 coarse cells at offsets 0, +-2e_a and
+// +-e_a+-e_b.  Each coarse row is formed here by one thread, adding every
+// contribution in the same order sparse_multiply_transpose would
+// (amg.h:520-546: A P in A-row order d,l,c,r,u,t,b, then P^T (A P) over
+// fine rows in ascending order), without FMA contraction -- so the result
+// is bit-identical to the generic Galerkin kernels (and to the reference),
+// at a fraction of their cost.
+#include "hm.cuh"
+
+namespace hm {
+
+namespace {
+
+// storage order of a level-0 row (solve_linearsystem_AMG.c:103-139)
+enum { DD = 0, DL, DC, DR, DU, DT, DB };
+
+struct SG {
+    int nx, ny, nz;
+    long nxy;
+};
+
+__device__ __forceinline__ unsigned present(const SG &g, int i, int j, int k)
+{
+    return (unsigned)(j > 0) << DD | (unsigned)(i > 0) << DL | 1u << DC |
+           (unsigned)(i < g.nx - 1) << DR | (unsigned)(j < g.ny - 1) << DU |
+           (unsigned)(k < g.nz - 1) << DT | (unsigned)(k > 0) << DB;
+}
+
+// a_{s, s+dir} of row s (dir present)
+__device__ __forceinline__ double aval(const int *__restrict__ rowptr,
+                                       const double *__restrict__ val, long s,
+                                       unsigned pm, int dir)
+{
+    return val[rowptr[s] + __popc(pm & ((1u << dir) - 1))];
+}
+
+__constant__ signed char c_off[19][3] = {
+    {0, 0, 0},  {2, 0, 0},   {-2, 0, 0}, {0, 2, 0},  {0, -2, 0}, {0, 0, 2},
+    {0, 0, -2}, {1, 1, 0},   {1, -1, 0}, {-1, 1, 0}, {-1, -1, 0}, {1, 0, 1},
+    {1, 0, -1}, {-1, 0, 1},  {-1, 0, -1}, {0, 1, 1}, {0, 1, -1}, {0, -1, 1},
+    {0, -1, -1}};
+
+// The in-grid coarse neighbours of even cell (i,j,k), as offsets sorted by
+// fine index (= by coarse id).  Returns how many.
+__device__ __forceinline__ int coarse_nbrs(const SG &g, int i, int j, int k,
+                                           int q[19])
+{
+    int m = 0;
+    long key[19];
+    for (int t = 0; t < 19; t++) {
+        const int a = i + c_off[t][0], b = j + c_off[t][1], c = k + c_off[t][2];
+        if (a < 0 || a >= g.nx || b < 0 || b >= g.ny || c < 0 || c >= g.nz) continue;
+        const long lin = (long)c_off[t][0] + (long)c_off[t][1] * g.nx + (long)c_off[t][2] * g.nxy;
+        int p = m++;
+        while (p > 0 && key[p - 1] > lin) { key[p] = key[p - 1]; q[p] = q[p - 1]; p--; }
+        key[p] = lin;
+        q[p] = t;
+    }
+    return m;
+}
+
+__global__ void k_parity(SG g, signed char *sel)
+{
+    const long n = g.nxy * g.nz;
+    for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < n;
+         s += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(s % g.nx), j = (int)((s / g.nx) % g.ny), k = (int)(s / g.nxy);
+        sel[s] = ((i + j + k) & 1) == 0 ? 1 : 2;
+    }
+}
+
+__global__ void k_sg_count(SG g, const int *__restrict__ cid, int *cnt)
+{
+    const long n = g.nxy * g.nz;
+    for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < n;
+         s += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(s % g.nx), j = (int)((s / g.nx) % g.ny), k = (int)(s / g.nxy);
+        if ((i + j + k) & 1) continue;
+        int q[19];
+        cnt[cid[s]] = coarse_nbrs(g, i, j, k, q);
+    }
+}
+
+__host__ __device__ constexpr int slot_of(int dx, int dy, int dz)
+{
+    return (dx == 0 && dy == 0 && dz == 0) ? 0
+         : (dx == 2 && dy == 0 && dz == 0) ? 1 : (dx == -2 && dy == 0 && dz == 0) ? 2
+         : (dx == 0 && dy == 2 && dz == 0) ? 3 : (dx == 0 && dy == -2 && dz == 0) ? 4
+         : (dx == 0 && dy == 0 && dz == 2) ? 5 : (dx == 0 && dy == 0 && dz == -2) ? 6
+         : (dx == 1 && dy == 1 && dz == 0) ? 7 : (dx == 1 && dy == -1 && dz == 0) ? 8
+         : (dx == -1 && dy == 1 && dz == 0) ? 9 : (dx == -1 && dy == -1 && dz == 0) ? 10
+         : (dx == 1 && dy == 0 && dz == 1) ? 11 : (dx == 1 && dy == 0 && dz == -1) ? 12
+         : (dx == -1 && dy == 0 && dz == 1) ? 13 : (dx == -1 && dy == 0 && dz == -1) ? 14
+         : (dx == 0 && dy == 1 && dz == 1) ? 15 : (dx == 0 && dy == 1 && dz == -1) ? 16
+         : (dx == 0 && dy == -1 && dz == 1) ? 17 : (dx == 0 && dy == -1 && dz == -1) ? 18
+         : -1;
+}
+
+__host__ __device__ constexpr int DX(int d) { return d == DL ? -1 : d == DR ? 1 : 0; }
+__host__ __device__ constexpr int DY(int d) { return d == DD ? -1 : d == DU ? 1 : 0; }
+__host__ __device__ constexpr int DZ(int d) { return d == DB ? -1 : d == DT ? 1 : 0; }
+
+// acc[slot] += t in order; the first contribution initialises the slot
+#define SG_ADD(slot, t)                                                        \
+    do {                                                                       \
+        const double t_ = (t);                                                 \
+        if (hv & (1u << (slot))) acc[slot] = dadd(acc[slot], t_);              \
+        else { acc[slot] = t_; hv |= 1u << (slot); }                           \
+    } while (0)
+
+// One coarse row c: Ac[c][q] = sum over the fine rows f of R(c) in ascending
+// index order {c-nxy, c-nx, c-1, c, c+1, c+nx, c+nxy} of AP[f][q] * w_f,
+// where
+//   AP[c][q] = sum over c's row in stored order (d,l,c,r,u,t,b) of
+//              a_cj * w_j for each F neighbour j adjacent to q, and a_cc for
+//              q = c;
+//   AP[f][q] = a_fq + a_ff * w_f for an F neighbour f and each of its C
+//              neighbours q (a sum of two terms, so its order is free).
+// Slots are the 19 offsets of c_off; every index below is a compile-time
+// constant once the direction loops are unrolled, so acc stays in
+// registers.
+__global__ void __launch_bounds__(128)
+k_sg_fill(SG g, const int *__restrict__ rowptr, const double *__restrict__ val,
+          const double *__restrict__ pw, const int *__restrict__ cid,
+          const int *__restrict__ crow, int *ccol, double *cval)
+{
+    const long n = g.nxy * g.nz;
+    for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < n;
+         s += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(s % g.nx), j = (int)((s / g.nx) % g.ny), k = (int)(s / g.nxy);
+        if ((i + j + k) & 1) continue;
+        const unsigned pmc = present(g, i, j, k);
+        // ---- AP[c][.], in c's row order
+        double ap[19];
+        unsigned hv = 0;
+        double *acc = ap;
+        const int adir[7] = {DD, DL, DC, DR, DU, DT, DB};
+#pragma unroll
+        for (int aa = 0; aa < 7; aa++) {
+            const int e = adir[aa];
+            if (!(pmc & (1u << e))) continue;
+            const double a_ce = aval(rowptr, val, s, pmc, e);
+            if (e == DC) {
+                SG_ADD(0, a_ce);
+                continue;
+            }
+            const long f = s + DX(e) + (long)DY(e) * g.nx + (long)DZ(e) * g.nxy;
+            const double t = dmul(a_ce, pw[f]);
+            // the C neighbours of f = c + e: c, c + 2e, c + e +- (perpendicular)
+#pragma unroll
+            for (int b2 = 0; b2 < 7; b2++) {
+                if (b2 == DC) continue;
+                const int qx = DX(e) + DX(b2), qy = DY(e) + DY(b2), qz = DZ(e) + DZ(b2);
+                const int sl = slot_of(qx, qy, qz);
+                if (sl < 0) continue;
+                if (!(present(g, i + DX(e), j + DY(e), k + DZ(e)) & (1u << b2))) continue;
+                SG_ADD(sl, t);
+            }
+        }
+        const unsigned hap = hv;
+        // ---- P^T (A P): fine rows of R(c) in ascending order
+        double out[19];
+        hv = 0;
+        acc = out;
+        const int rdir[7] = {DB, DD, DL, DC, DR, DU, DT};
+#pragma unroll
+        for (int rr = 0; rr < 7; rr++) {
+            const int d = rdir[rr];
+            if (!(pmc & (1u << d))) continue;
+            if (d == DC) {
+#pragma unroll
+                for (int sl = 0; sl < 19; sl++)
+                    if (hap & (1u << sl)) SG_ADD(sl, ap[sl]);  // * w_c = 1
+                continue;
+            }
+            const long f = s + DX(d) + (long)DY(d) * g.nx + (long)DZ(d) * g.nxy;
+            const unsigned pmf = present(g, i + DX(d), j + DY(d), k + DZ(d));
+            const double wf = pw[f];
+            const double dg = dmul(aval(rowptr, val, f, pmf, DC), wf);
+#pragma unroll
+            for (int b2 = 0; b2 < 7; b2++) {
+                if (b2 == DC || !(pmf & (1u << b2))) continue;
+                const int sl = slot_of(DX(d) + DX(b2), DY(d) + DY(b2), DZ(d) + DZ(b2));
+                if (sl < 0) continue;
+                SG_ADD(sl, dmul(dadd(aval(rowptr, val, f, pmf, b2), dg), wf));
+            }
+        }
+        // ---- emit in coarse-id order (ascending fine index)
+        int q[19];
+        const int m = coarse_nbrs(g, i, j, k, q);
+        const long o = crow[cid[s]];
+        for (int t = 0; t < m; t++) {
+            const int sl = q[t];
+            const long cq = s + c_off[sl][0] + (long)c_off[sl][1] * g.nx +
+                            (long)c_off[sl][2] * g.nxy;
+            double v = 0.0;
+#pragma unroll
+            for (int u = 0; u < 19; u++)
+                if (u == sl) v = out[u];
+            ccol[o + t] = cid[cq];
+            cval[o + t] = v;
+        }
+    }
+}
+
+int nbk(long n)
+{
+    long b = ceil_div(n, 256);
+    if (b < 1) b = 1;
+    return (int)(b < 148L * 16 ? b : 148L * 16);
+}
+
+}  // namespace
+
+int stencil_parity_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st)
+{
+    SG g{nx, ny, nz, (long)nx * ny};
+    k_parity<<<nbk(g.nxy * nz), 256, 0, st>>>(g, sel);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
+                     cudaStream_t st)
+{
+    SG g{nx, ny, nz, (long)nx * ny};
+    const long n = g.nxy * nz;
+    out.n = L.nc;
+    out.rowptr = (int *)dalloc(sizeof(int) * (L.nc + 1));
+    if (!out.rowptr) return HMFEM_E_CUDA;
+    k_sg_count<<<nbk(n), 256, 0, st>>>(g, L.cid, out.rowptr);
+    HM_LAUNCHED();
+    HM_CHECK(rowptr_from_counts(out.rowptr, L.nc, st, &out.nnz));
+    out.col = (int *)dalloc(sizeof(int) * (out.nnz > 0 ? out.nnz : 1));
+    out.val = (double *)dalloc(sizeof(double) * (out.nnz > 0 ? out.nnz : 1));
+    if (!out.col || !out.val) return HMFEM_E_CUDA;
+    k_sg_fill<<<nbk(n), 128, 0, st>>>(g, L.A.rowptr, L.A.val, L.pw, L.cid, out.rowptr,
+                                      out.col, out.val);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+}  // namespace hm

@@ -245,7 +245,10 @@ int setup(Solver &s)
         HM_CHECK(launch_diag_inv(L.A, L.dinv, L.dinv32, st));
         if (!(l < s.opt.max_levels - 1 && gcnt > s.opt.min_coarse && rel < 1.0)) break;
         s.lv.emplace_back();
-        HM_CHECK(amg_coarsen(s.lv[l], s.lv[l + 1], st, s.dwork));
+        const int grid3[3] = {s.nx, s.ny, s.nz};
+        const bool stencil = l == 0 && s.have_grid && s.opt.generic_setup == 0;
+        HM_CHECK(amg_coarsen(s.lv[l], s.lv[l + 1], st, s.dwork,
+                             stencil ? grid3 : nullptr));
         l++;
         long gold = gcnt;
         gcnt = s.lv[l].A.n;

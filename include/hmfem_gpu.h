@@ -118,6 +118,9 @@ typedef struct {
                           the reference's diagonal solve on the coarsest
                           level (amg.h:1353-1364) */
     int check_every;   /* host polls convergence every k iterations */
+    int generic_setup; /* 1: coarsen an assembled level 0 with the generic
+                          kernels too (default 0: from its 7-point
+                          structure; both give the identical hierarchy) */
     int verbose;
 } hmfem_options;
 

@@ -79,9 +79,13 @@ def test_stencil_packing_bit_exact(case):
     np.testing.assert_array_equal(d["ele"], csr[2])
 
 
-def test_hierarchy_bit_exact(case):
+@pytest.mark.parametrize("generic_setup", [0, 1])
+def test_hierarchy_bit_exact(case, generic_setup):
+    """Level 0 from hmfem_assemble is coarsened from its 7-point structure
+    (generic_setup=0) or by the generic kernels; both must equal the
+    reference's hierarchy bit for bit."""
     name, p, (perm, ind, b, csr, H) = case
-    s = gpu.Solver()
+    s = gpu.Solver(generic_setup=generic_setup)
     s.assemble(p)
     s.setup()
     assert s.num_levels() == H.nlevels
