@@ -42,29 +42,68 @@ __device__ __forceinline__ double aval(const int *__restrict__ rowptr,
     return val[rowptr[s] + __popc(pm & ((1u << dir) - 1))];
 }
 
-__constant__ signed char c_off[19][3] = {
-    {0, 0, 0},  {2, 0, 0},   {-2, 0, 0}, {0, 2, 0},  {0, -2, 0}, {0, 0, 2},
-    {0, 0, -2}, {1, 1, 0},   {1, -1, 0}, {-1, 1, 0}, {-1, -1, 0}, {1, 0, 1},
-    {1, 0, -1}, {-1, 0, 1},  {-1, 0, -1}, {0, 1, 1}, {0, 1, -1}, {0, -1, 1},
-    {0, -1, -1}};
-
-// The in-grid coarse neighbours of even cell (i,j,k), as offsets sorted by
-// fine index (= by coarse id).  Returns how many.
-__device__ __forceinline__ int coarse_nbrs(const SG &g, int i, int j, int k,
-                                           int q[19])
+// The 19 coarse offsets of a level-1 row, by slot: 0, +-2e_x, +-2e_y,
+// +-2e_z, then the 12 offsets +-e_a +- e_b.
+__host__ __device__ constexpr int OX(int t)
 {
-    int m = 0;
-    long key[19];
+    return t == 1 ? 2 : t == 2 ? -2 : (t == 7 || t == 8 || t == 11 || t == 12) ? 1
+         : (t == 9 || t == 10 || t == 13 || t == 14) ? -1 : 0;
+}
+__host__ __device__ constexpr int OY(int t)
+{
+    return t == 3 ? 2 : t == 4 ? -2 : (t == 7 || t == 9 || t == 15 || t == 16) ? 1
+         : (t == 8 || t == 10 || t == 17 || t == 18) ? -1 : 0;
+}
+__host__ __device__ constexpr int OZ(int t)
+{
+    return t == 5 ? 2 : t == 6 ? -2 : (t == 11 || t == 13 || t == 15 || t == 17) ? 1
+         : (t == 12 || t == 14 || t == 16 || t == 18) ? -1 : 0;
+}
+
+// Per-grid slot table: the fine-index offset of each slot and, for each
+// slot, the mask of slots with a smaller offset.  Two in-grid coarse
+// neighbours never share an offset, so the rank of a present slot among the
+// present ones, popc(present & less[slot]), is its position in the coarse
+// row (columns ascend with fine index).
+struct SGT {
+    long lin[19];
+    unsigned less[19];
+};
+
+SGT slot_table(const SG &g)
+{
+    SGT t;
+    for (int a = 0; a < 19; a++)
+        t.lin[a] = OX(a) + (long)OY(a) * g.nx + (long)OZ(a) * g.nxy;
+    for (int a = 0; a < 19; a++) {
+        t.less[a] = 0;
+        for (int b = 0; b < 19; b++)
+            if (t.lin[b] < t.lin[a] || (t.lin[b] == t.lin[a] && b < a)) t.less[a] |= 1u << b;
+    }
+    return t;
+}
+
+// mask of the slots whose coarse neighbour of even cell (i,j,k) is in grid
+__device__ __forceinline__ unsigned in_grid(const SG &g, int i, int j, int k)
+{
+    unsigned m = 0;
+#pragma unroll
     for (int t = 0; t < 19; t++) {
-        const int a = i + c_off[t][0], b = j + c_off[t][1], c = k + c_off[t][2];
-        if (a < 0 || a >= g.nx || b < 0 || b >= g.ny || c < 0 || c >= g.nz) continue;
-        const long lin = (long)c_off[t][0] + (long)c_off[t][1] * g.nx + (long)c_off[t][2] * g.nxy;
-        int p = m++;
-        while (p > 0 && key[p - 1] > lin) { key[p] = key[p - 1]; q[p] = q[p - 1]; p--; }
-        key[p] = lin;
-        q[p] = t;
+        const int a = i + OX(t), b = j + OY(t), c = k + OZ(t);
+        m |= (unsigned)(a >= 0 && a < g.nx && b >= 0 && b < g.ny && c >= 0 && c < g.nz) << t;
     }
     return m;
+}
+
+// Threads walk the even cells only: (nx+1)/2 per x-row.
+__device__ __forceinline__ bool even_cell(const SG &g, long t, int &i, int &j, int &k)
+{
+    const int hx = (g.nx + 1) >> 1;
+    const long r = t / hx;
+    j = (int)(r % g.ny);
+    k = (int)(r / g.ny);
+    i = 2 * (int)(t - r * hx) + ((j + k) & 1);
+    return i < g.nx;
 }
 
 __global__ void k_parity(SG g, signed char *sel)
@@ -79,13 +118,12 @@ __global__ void k_parity(SG g, signed char *sel)
 
 __global__ void k_sg_count(SG g, const int *__restrict__ cid, int *cnt)
 {
-    const long n = g.nxy * g.nz;
-    for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < n;
-         s += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(s % g.nx), j = (int)((s / g.nx) % g.ny), k = (int)(s / g.nxy);
-        if ((i + j + k) & 1) continue;
-        int q[19];
-        cnt[cid[s]] = coarse_nbrs(g, i, j, k, q);
+    const long n = (long)((g.nx + 1) >> 1) * g.ny * g.nz;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+         t += (long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        if (!even_cell(g, t, i, j, k)) continue;
+        cnt[cid[i + (long)j * g.nx + (long)k * g.nxy]] = __popc(in_grid(g, i, j, k));
     }
 }
 
@@ -124,19 +162,21 @@ __host__ __device__ constexpr int DZ(int d) { return d == DB ? -1 : d == DT ? 1 
 //              q = c;
 //   AP[f][q] = a_fq + a_ff * w_f for an F neighbour f and each of its C
 //              neighbours q (a sum of two terms, so its order is free).
-// Slots are the 19 offsets of c_off; every index below is a compile-time
+// Slots are numbered as in OX/OY/OZ; every index below is a compile-time
 // constant once the direction loops are unrolled, so acc stays in
 // registers.
 __global__ void __launch_bounds__(128)
-k_sg_fill(SG g, const int *__restrict__ rowptr, const double *__restrict__ val,
-          const double *__restrict__ pw, const int *__restrict__ cid,
-          const int *__restrict__ crow, int *ccol, double *cval)
+k_sg_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
+          const double *__restrict__ val, const double *__restrict__ pw,
+          const int *__restrict__ cid, const int *__restrict__ crow, int *ccol,
+          double *cval)
 {
-    const long n = g.nxy * g.nz;
-    for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < n;
-         s += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(s % g.nx), j = (int)((s / g.nx) % g.ny), k = (int)(s / g.nxy);
-        if ((i + j + k) & 1) continue;
+    const long n = (long)((g.nx + 1) >> 1) * g.ny * g.nz;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+         t += (long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        if (!even_cell(g, t, i, j, k)) continue;
+        const long s = i + (long)j * g.nx + (long)k * g.nxy;
         const unsigned pmc = present(g, i, j, k);
         // ---- AP[c][.], in c's row order
         double ap[19];
@@ -194,22 +234,25 @@ k_sg_fill(SG g, const int *__restrict__ rowptr, const double *__restrict__ val,
             }
         }
         // ---- emit in coarse-id order (ascending fine index)
-        int q[19];
-        const int m = coarse_nbrs(g, i, j, k, q);
+        const unsigned in = in_grid(g, i, j, k);
         const long o = crow[cid[s]];
-        for (int t = 0; t < m; t++) {
-            const int sl = q[t];
-            const long cq = s + c_off[sl][0] + (long)c_off[sl][1] * g.nx +
-                            (long)c_off[sl][2] * g.nxy;
-            double v = 0.0;
 #pragma unroll
-            for (int u = 0; u < 19; u++)
-                if (u == sl) v = out[u];
-            ccol[o + t] = cid[cq];
-            cval[o + t] = v;
+        for (int sl = 0; sl < 19; sl++) {
+            if (!(in & (1u << sl))) continue;
+            const long e = o + __popc(in & tb.less[sl]);
+            ccol[e] = cid[s + tb.lin[sl]];
+            cval[e] = out[sl];
         }
     }
 }
+
+constexpr bool slots_consistent()
+{
+    for (int t = 0; t < 19; t++)
+        if (slot_of(OX(t), OY(t), OZ(t)) != t) return false;
+    return true;
+}
+static_assert(slots_consistent(), "slot numbering");
 
 int nbk(long n)
 {
@@ -236,14 +279,14 @@ int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
     out.n = L.nc;
     out.rowptr = (int *)dalloc(sizeof(int) * (L.nc + 1));
     if (!out.rowptr) return HMFEM_E_CUDA;
-    k_sg_count<<<nbk(n), 256, 0, st>>>(g, L.cid, out.rowptr);
+    k_sg_count<<<nbk(n / 2), 256, 0, st>>>(g, L.cid, out.rowptr);
     HM_LAUNCHED();
     HM_CHECK(rowptr_from_counts(out.rowptr, L.nc, st, &out.nnz));
     out.col = (int *)dalloc(sizeof(int) * (out.nnz > 0 ? out.nnz : 1));
     out.val = (double *)dalloc(sizeof(double) * (out.nnz > 0 ? out.nnz : 1));
     if (!out.col || !out.val) return HMFEM_E_CUDA;
-    k_sg_fill<<<nbk(n), 128, 0, st>>>(g, L.A.rowptr, L.A.val, L.pw, L.cid, out.rowptr,
-                                      out.col, out.val);
+    k_sg_fill<<<nbk(n / 2), 128, 0, st>>>(g, slot_table(g), L.A.rowptr, L.A.val, L.pw,
+                                          L.cid, out.rowptr, out.col, out.val);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
