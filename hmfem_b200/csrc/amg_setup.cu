@@ -20,6 +20,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
+#include "grid19.cuh"
 #include "hm.cuh"
 
 namespace hm {
@@ -632,7 +633,16 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
     HM_PHASE("  P and R", st);
     // ---- Galerkin product ---------------------------------------------
     if (grid3) {
-        HM_CHECK(stencil_galerkin(grid3[0], grid3[1], grid3[2], L, C.A, st));
+        double *g19v = nullptr;
+        if (g19_applies(grid3[0], grid3[1], grid3[2])) {
+            g19v = (double *)dalloc(sizeof(double) * kQ19 * (size_t)L.nc);
+            if (!g19v) return HMFEM_E_CUDA;
+            C.g19.nx = grid3[0];
+            C.g19.ny = grid3[1];
+            C.g19.nz = grid3[2];
+            C.g19.v = g19v;
+        }
+        HM_CHECK(stencil_galerkin(grid3[0], grid3[1], grid3[2], L, C.A, g19v, st));
         HM_PHASE("  P^T A P (stencil)", st);
         return HMFEM_OK;
     }

@@ -6,33 +6,9 @@
 // precision preconditioner) use FMA.  Every kernel takes the CG control
 // block and returns at once when the solve is already finished, so a
 // captured iteration can be replayed past convergence at no cost.
-#include "solver.cuh"
+#include "cycle.cuh"
 
 namespace hm {
-
-template <class T> struct Ar;
-template <> struct Ar<double> {
-    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
-    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
-    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
-    static __device__ __forceinline__ double div(double a, double b) { return a / b; }
-};
-template <> struct Ar<float> {
-    static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
-    static __device__ __forceinline__ float add(float a, float b) { return a + b; }
-    static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
-    static __device__ __forceinline__ float div(float a, float b) { return a / b; }
-};
-
-__device__ __forceinline__ double ld(const double *p, long long i) { return p[i]; }
-__device__ __forceinline__ float ld(const float *p, long long i) { return __ldg(p + i); }
-__device__ __forceinline__ float ld(const __nv_bfloat16 *p, long long i) { return __bfloat162float(p[i]); }
-
-__device__ __forceinline__ bool finished(const Ctl *c) { return c && *(volatile const int *)&c->done; }
-
-#define GRID_STRIDE(r, n)                                                     \
-    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < (n);       \
-         r += (long)gridDim.x * blockDim.x)
 
 // t - sum_k a_k x(c_k) (SUB) or t + sum_k a_k x(c_k) over one SELL-32 row
 // (entries at o, o+32, ...), in stored order.  Column indices, values and
@@ -160,20 +136,8 @@ k_post(const long long *__restrict__ sptr, const int *__restrict__ scol,
         if (DOT) dot += (double)un * (double)fr;
     }
     if (DOT) {
-        grid_reduce_sum(dot, part, &ctl->tickets[RED_SIGMA], [&](double s) {
-            // pcg.h:66-67 (and 46-47 on the first application)
-            if (s < 0.0) s = fabs(s);
-            if (!(s == s) || isinf(s)) { ctl->status = HMFEM_E_BREAKDOWN; ctl->done = 1; }
-            if (first) {
-                ctl->sigma_first = s == 0.0 ? 1.0 : s;
-                ctl->sigma_last = s;
-                ctl->beta = 0.0;
-            } else {
-                ctl->beta = s / ctl->sigma_last;
-            }
-            ctl->sigma = s;
-            if (ctl->stop_rule == 1 && s / ctl->sigma_first <= ctl->tol2) ctl->done = 1;
-        });
+        grid_reduce_sum(dot, part, &ctl->tickets[RED_SIGMA],
+                        [&](double s) { sigma_finish(ctl, s, first); });
     }
 }
 
@@ -336,18 +300,8 @@ k_resid(const long long *__restrict__ sptr, const int *__restrict__ scol,
     // partial rows
     double *p2 = part + kRedBlocks;
     grid_reduce_sum(bb, p2, &ctl->tickets[RED_BB], [&](double s) { ctl->bb = s; });
-    grid_reduce_sum(rr, part, &ctl->tickets[RED_TRR], [&](double s) {
-        ctl->trr = s;
-        if (init == 2) return;
-        ctl->rr = s;
-        if (init == 1) {
-            ctl->iters = 0;
-            if (s <= ctl->tol2 * ctl->bb && ctl->stop_rule == 0) ctl->done = 1;
-        } else {
-            ctl->check = 0;
-            if (s <= ctl->tol2 * ctl->bb) ctl->done = 1;
-        }
-    });
+    grid_reduce_sum(rr, part, &ctl->tickets[RED_TRR],
+                    [&](double s) { trr_finish(ctl, s, init); });
 }
 
 // v = A s; tau = (s, v); alpha = sigma / tau (pcg.h:59-63)
@@ -368,12 +322,8 @@ k_spmv_dot(const long long *__restrict__ sptr, const int *__restrict__ scol,
         v[i] = a;
         d += s[i] * a;
     }
-    grid_reduce_sum(d, part, &ctl->tickets[RED_TAU], [&](double t) {
-        if (t < 0.0) t = fabs(t);
-        ctl->tau = t;
-        if (!(t > 0.0) || isinf(t)) { ctl->status = HMFEM_E_BREAKDOWN; ctl->done = 1; return; }
-        ctl->alpha = ctl->sigma / t;
-    });
+    grid_reduce_sum(d, part, &ctl->tickets[RED_TAU],
+                    [&](double t) { tau_finish(ctl, t); });
 }
 
 // x += alpha s; r -= alpha v; rr = (r, r)  (pcg.h:64-65)
@@ -505,6 +455,8 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
         return HMFEM_OK;
     }
     const T w = (T)s.opt.omega;
+    const bool g7 = s.use_g7(l), g19 = s.use_g19(l);
+    const bool bf16 = !std::is_same<T, double>::value && s.use_bf16(l);
     T *rs = s.vec_rs<T>(l);
     const T *dv = s.vec_dinv<T>(l);
     const T *dt = s.vec_dtrue<T>(l);
@@ -531,6 +483,11 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
                 L.A.rowptr, L.A.col, vals, n, f, ua, L.P.rowptr, rs, ctl);
             HM_COUNT();
         });
+    } else if (g7) {
+        HM_CHECK((g7_pre<T, T>(L, f, dv, w, ua, rs, ctl, st)));
+    } else if (g19) {
+        if (bf16) HM_CHECK((g19_pre<T, __nv_bfloat16>(L, f, dv, w, ua, rs, ctl, st)));
+        else HM_CHECK((g19_pre<T, T>(L, f, dv, w, ua, rs, ctl, st)));
     } else {
         with_vals<T>(s, L.S, l, [&](auto vals) {
             k_pre<T><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, vals, n, f, dv, w,
@@ -539,16 +496,34 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
         });
     }
     HM_LAUNCHED();
-    k_restrict<T><<<nb(L.nc), 256, 0, st>>>(L.R.rowptr, L.R.col, L.nc, rs,
-                                            s.vec_f<T>(l + 1), ctl);
-    HM_LAUNCHED();
+    if (g7) {
+        HM_CHECK((g7_restrict<T>(L, rs, s.vec_f<T>(l + 1), ctl, st)));
+    } else {
+        k_restrict<T><<<nb(L.nc), 256, 0, st>>>(L.R.rowptr, L.R.col, L.nc, rs,
+                                                s.vec_f<T>(l + 1), ctl);
+        HM_LAUNCHED();
+    }
     HM_CHECK(cycle_t<T>(s, l + 1, st, false));
-    k_prolong_add<T><<<nb(n), 256, 0, st>>>(L.P.rowptr, L.P.col, n,
-                                            cycle_out<T>(s, l + 1), ua, ctl);
-    HM_LAUNCHED();
+    if (g7) {
+        HM_CHECK((g7_prolong<T>(L, cycle_out<T>(s, l + 1), ua, ctl, st)));
+    } else {
+        k_prolong_add<T><<<nb(n), 256, 0, st>>>(L.P.rowptr, L.P.col, n,
+                                                cycle_out<T>(s, l + 1), ua, ctl);
+        HM_LAUNCHED();
+    }
     // ---- post-smoothing
     if (L.gs) {
         for (int c = L.ncolors - 1; c >= 0; c--) sweep(c);
+    } else if (g7) {
+        if constexpr (std::is_same<T, double>::value) {
+            if (dot) HM_CHECK((g7_post<T, T, true>(L, f, dv, w, ua, ub, s.ctl, s.part, s.first_sigma, st)));
+            else HM_CHECK((g7_post<T, T, false>(L, f, dv, w, ua, ub, ctl, nullptr, 0, st)));
+        } else {
+            HM_CHECK((g7_post<T, T, false>(L, f, dv, w, ua, ub, ctl, nullptr, 0, st)));
+        }
+    } else if (g19 && !dot) {
+        if (bf16) HM_CHECK((g19_post<T, __nv_bfloat16>(L, f, dv, w, ua, ub, ctl, st)));
+        else HM_CHECK((g19_post<T, T>(L, f, dv, w, ua, ub, ctl, st)));
     } else if (dot) {
         k_post<T, T, true><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, s.sval<T>(l), n,
                                                    f, dv, w, ua, ub, s.ctl, s.part,
@@ -611,9 +586,13 @@ int cg_init(Solver &s, cudaStream_t st)
 {
     Level &L0 = s.lv[0];
     const int n = L0.A.n;
-    k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
-                                   s.r, s.ctl, s.part, 1);
-    HM_LAUNCHED();
+    if (s.use_g7(0)) {
+        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 1, st));
+    } else {
+        k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
+                                       s.r, s.ctl, s.part, 1);
+        HM_LAUNCHED();
+    }
     s.first_sigma = 1;
     HM_CHECK(cg_precondition(s, st));
     s.first_sigma = 0;
@@ -626,14 +605,23 @@ int cg_iteration(Solver &s, cudaStream_t st)
 {
     Level &L0 = s.lv[0];
     const int n = L0.A.n;
-    k_spmv_dot<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.s,
-                                      s.v, s.ctl, s.part);
-    HM_LAUNCHED();
+    const bool g7 = s.use_g7(0);
+    if (g7) {
+        HM_CHECK(g7_spmv_dot(L0, s.s, s.v, s.ctl, s.part, st));
+    } else {
+        k_spmv_dot<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.s,
+                                          s.v, s.ctl, s.part);
+        HM_LAUNCHED();
+    }
     k_update<<<nb(n), 256, 0, st>>>(n, s.x, s.r, s.s, s.v, s.ctl, s.part);
     HM_LAUNCHED();
-    k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
-                                   s.r, s.ctl, s.part, 0);
-    HM_LAUNCHED();
+    if (g7) {
+        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 0, st));
+    } else {
+        k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
+                                       s.r, s.ctl, s.part, 0);
+        HM_LAUNCHED();
+    }
     HM_CHECK(cg_precondition(s, st));
     k_sdir<<<nb(n), 256, 0, st>>>(n, s.s, s.z, s.ctl);
     HM_LAUNCHED();
@@ -645,15 +633,22 @@ int cg_final_residual(Solver &s, cudaStream_t st)
 {
     Level &L0 = s.lv[0];
     const int n = L0.A.n;
-    k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
-                                   s.r, s.ctl, s.part, 2);
-    HM_LAUNCHED();
+    if (s.use_g7(0)) {
+        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 2, st));
+    } else {
+        k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
+                                       s.r, s.ctl, s.part, 2);
+        HM_LAUNCHED();
+    }
     return HMFEM_OK;
 }
 
 // plain SpMV on level l (inspection / tests)
 int level_spmv(Solver &s, int l, const double *x, double *y, cudaStream_t st)
 {
+    if (s.use_g7(l)) return g7_spmv(s.lv[l], x, y, st);
+    if (s.use_g19(l)) return g19_spmv(s.lv[l], x, y, st);
+    if (!s.lv[l].S.sptr) HM_CHECK(csr_to_sell(s.lv[l].A, s.lv[l].S, st));
     return launch_spmv(s.lv[l].S, x, y, st);
 }
 
@@ -671,14 +666,28 @@ __global__ void k_fill_one(double *x, int n)
 //   2 post-smoother FP64   nnz*(8+4) + n*(8 f + 8 d + 8 u + 8 u_out)
 //   3 pre-smoother FP32    nnz*(4+4) + n*(4+4+4+4+4)
 //   4 post-smoother FP32   nnz*(4+4) + n*(4*4)
-// (values BF16 on levels >= bf16_from: 2 bytes instead of 4)
+// (values BF16 on levels >= bf16_from: 2 bytes instead of 4); the SELL
+// form is built for the call where the level solves in a structured form.
+// Structured forms (level 0: 4 coefficient arrays; level 1: 19 arrays of
+// which the in-grid ones count), same vectors as above:
+//   5 SpMV FP64 (level 0)           n*4*8 + n*(8+8)
+//   6 pre-smoother FP32 (level 0)   n*4*4 + n*(4 f + 4 d + 4 u + 4 rs)
+//   7 post-smoother FP32 (level 0)  n*4*4 + n*4*4
+//   8 pre-smoother FP32 (level 1)   nnz*4 + n*(4+4+4+4+4)
+//   9 post-smoother FP32 (level 1)  nnz*4 + n*4*4
 int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
 {
-    if (l < 0 || l >= s.nlevels || reps < 1) return HMFEM_E_ARG;
+    if (l < 0 || l >= s.nlevels || reps < 1 || which < 0 || which > 9) return HMFEM_E_ARG;
     if (which >= 1 && l == s.nlevels - 1) return HMFEM_E_ARG;
     if (which >= 3 && s.opt.precision != 1) return HMFEM_E_ARG;
+    if (which >= 5 && which <= 7 && !s.use_g7(l)) return HMFEM_E_ARG;
+    if (which >= 8 && (!s.use_g19(l) || s.use_bf16(l))) return HMFEM_E_ARG;
     Level &L = s.lv[l];
     cudaStream_t st = s.st;
+    if (which <= 4 && !L.S.sptr) {
+        HM_CHECK(csr_to_sell(L.A, L.S, st));
+        if (s.opt.precision == 1) HM_CHECK(sell_fill_lowp(L.S, true, s.use_bf16(l), st));
+    }
     const int n = L.A.n;
     const double nnz = (double)L.A.nnz;
     double *x = nullptr, *y = nullptr;
@@ -714,6 +723,14 @@ int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
                     L.S.sptr, L.S.col, L.S.val32, n, xf, L.dsm32, (float)w,
                     L.P.rowptr, yf, L.rs32, nullptr);
             break;
+        case 5: g7_spmv_dot(L, x, y, s.ctl, s.part, st); break;
+        case 6: g7_pre<float, float>(L, xf, L.dsm32, (float)w, yf, L.rs32, nullptr, st); break;
+        case 7:
+            g7_post<float, float, false>(L, xf, L.dsm32, (float)w, L.ua32, yf, nullptr,
+                                         nullptr, 0, st);
+            break;
+        case 8: g19_pre<float, float>(L, xf, L.dsm32, (float)w, yf, L.rs32, nullptr, st); break;
+        case 9: g19_post<float, float>(L, xf, L.dsm32, (float)w, L.ua32, yf, nullptr, st); break;
         default:
             if (vb16 == 2)
                 k_post<float, __nv_bfloat16, false><<<nb(n), 256, 0, st>>>(
@@ -750,7 +767,12 @@ int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
     case 1: *bytes = nnz * 12 + (double)n * 36; break;
     case 2: *bytes = nnz * 12 + (double)n * 32; break;
     case 3: *bytes = nnz * (vb16 + 4) + (double)n * 20; break;
-    default: *bytes = nnz * (vb16 + 4) + (double)n * 16; break;
+    case 4: *bytes = nnz * (vb16 + 4) + (double)n * 16; break;
+    case 5: *bytes = (double)n * 48; break;
+    case 6: *bytes = (double)n * 32; break;
+    case 7: *bytes = (double)n * 32; break;
+    case 8: *bytes = nnz * 4 + (double)n * 20; break;
+    default: *bytes = nnz * 4 + (double)n * 16; break;
     }
     return HMFEM_OK;
 }

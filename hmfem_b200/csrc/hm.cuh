@@ -35,8 +35,31 @@ struct Sell {
     __nv_bfloat16 *val16 = nullptr;  // BF16 copy (coarse levels)
 };
 
+// Solve-phase forms of the two finest levels of a matrix assembled on the
+// device (stencil_cycle.cu).  Level 0: the 7-point stencil as a_cc and the
+// couplings to the +x, +y, +z neighbours (0 where absent); the coupling to
+// -x is the -x neighbour's +x one, and so on (the matrix is checked to be
+// bitwise symmetric first).
+struct Grid7 {
+    int nx = 0, ny = 0, nz = 0;
+    double *c = nullptr, *px = nullptr, *py = nullptr, *pz = nullptr;
+    float *c32 = nullptr, *px32 = nullptr, *py32 = nullptr, *pz32 = nullptr;
+};
+
+// Level 1 of the parity split (nx even, nx >= 4, ny >= 4): even cell s has
+// coarse id s >> 1, and row c's coefficient at offset q (grid19.cuh) is
+// v[q * n + c] (0 where the neighbour is outside the grid).
+struct Grid19 {
+    int nx = 0, ny = 0, nz = 0;
+    double *v = nullptr;
+    float *v32 = nullptr;
+    __nv_bfloat16 *v16 = nullptr;
+};
+
 struct Level {
     Csr A;
+    Grid7 g7;      // set on level 0 when the structured form applies
+    Grid19 g19;    // set on level 1 when the structured form applies
     Sell S;
     double *dinv = nullptr;   // 1 / last stored diagonal entry (amg.h:1195)
     float *dinv32 = nullptr;
@@ -111,10 +134,18 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *err_dev,
                 const int *grid3 = nullptr);
 int stencil_parity_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st);
 int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
-                     cudaStream_t st);
+                     double *g19v, cudaStream_t st);
 // colouring + rows grouped by colour; returns HMFEM_OK with L.gs = false
 // when the level needs more than 63 colours
 int color_level(Level &L, cudaStream_t st, int *dwork);
+// structured solve-phase forms (stencil_cycle.cu): g7_build fills L.g7 from
+// the assembled CSR and returns HMFEM_OK with L.g7.c == nullptr when the
+// matrix is not bitwise symmetric; g19 values come from stencil_galerkin.
+int g7_build(Level &L, int nx, int ny, int nz, bool f32, cudaStream_t st, int *dwork);
+void g7_free(Grid7 &g);
+bool g19_applies(int nx, int ny, int nz);
+int g19_lowp(Grid19 &g, int n, bool f32, bool bf16, cudaStream_t st);
+void g19_free(Grid19 &g);
 
 // cycle + CG (cycle.cu)
 struct Solver;

@@ -13,6 +13,7 @@
 // fine rows in ascending order), without FMA contraction -- so the result
 // is bit-identical to the generic Galerkin kernels (and to the reference),
 // at a fraction of their cost.
+#include "grid19.cuh"
 #include "hm.cuh"
 
 namespace hm {
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(128)
 k_sg_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
           const double *__restrict__ val, const double *__restrict__ pw,
           const int *__restrict__ cid, const int *__restrict__ crow, int *ccol,
-          double *cval)
+          double *cval, double *g19v, long nc)
 {
     const long n = (long)((g.nx + 1) >> 1) * g.ny * g.nz;
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
@@ -235,10 +236,13 @@ k_sg_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
         }
         // ---- emit in coarse-id order (ascending fine index)
         const unsigned in = in_grid(g, i, j, k);
-        const long o = crow[cid[s]];
+        const int c = cid[s];
+        const long o = crow[c];
 #pragma unroll
         for (int sl = 0; sl < 19; sl++) {
-            if (!(in & (1u << sl))) continue;
+            const bool on = in & (1u << sl);
+            if (g19v) g19v[q19_of(OX(sl), OY(sl), OZ(sl)) * nc + c] = on ? out[sl] : 0.0;
+            if (!on) continue;
             const long e = o + __popc(in & tb.less[sl]);
             ccol[e] = cid[s + tb.lin[sl]];
             cval[e] = out[sl];
@@ -272,7 +276,7 @@ int stencil_parity_split(int nx, int ny, int nz, signed char *sel, cudaStream_t 
 }
 
 int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
-                     cudaStream_t st)
+                     double *g19v, cudaStream_t st)
 {
     SG g{nx, ny, nz, (long)nx * ny};
     const long n = g.nxy * nz;
@@ -286,7 +290,8 @@ int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
     out.val = (double *)dalloc(sizeof(double) * (out.nnz > 0 ? out.nnz : 1));
     if (!out.col || !out.val) return HMFEM_E_CUDA;
     k_sg_fill<<<nbk(n / 2), 128, 0, st>>>(g, slot_table(g), L.A.rowptr, L.A.val, L.pw,
-                                          L.cid, out.rowptr, out.col, out.val);
+                                          L.cid, out.rowptr, out.col, out.val, g19v,
+                                          (long)L.nc);
     HM_LAUNCHED();
     return HMFEM_OK;
 }

@@ -119,6 +119,8 @@ static void free_level_setup(Level &L, bool keep_matrix)
     dfree(L.f); dfree(L.ua); dfree(L.ub); dfree(L.rs);
     dfree(L.f32); dfree(L.ua32); dfree(L.ub32); dfree(L.rs32);
     dfree(L.color); dfree(L.crows); dfree(L.aval32); dfree(L.aval16);
+    g7_free(L.g7);
+    g19_free(L.g19);
     Csr a = L.A;
     L = Level();
     if (keep_matrix) L.A = a;
@@ -256,15 +258,28 @@ int setup(Solver &s)
     }
     s.nlevels = l + 1;
     HM_PHASE("setup: hierarchy", st);
+    // structured forms of the two finest levels of an assembled grid
+    const bool low = s.opt.precision == 1;
+    if (s.have_grid && s.opt.generic_setup == 0)
+        HM_CHECK(g7_build(s.lv[0], s.nx, s.ny, s.nz, low, st, s.dwork));
+    if (s.nlevels > 1 && s.lv[1].g19.v) {
+        const bool smoothed = 1 < s.nlevels - 1 && !(s.opt.gs_from >= 1 && s.opt.gs_from <= 1);
+        if (s.use_g7(0) && smoothed)
+            HM_CHECK(g19_lowp(s.lv[1].g19, s.lv[1].A.n, low && !s.use_bf16(1),
+                              low && s.use_bf16(1), st));
+        else
+            g19_free(s.lv[1].g19);
+    }
     // solve-phase formats and vectors
     for (int k = 0; k < s.nlevels; k++) {
         Level &L = s.lv[k];
-        HM_CHECK(csr_to_sell(L.A, L.S, st));
+        if (!s.use_g7(k) && !s.use_g19(k)) {
+            HM_CHECK(csr_to_sell(L.A, L.S, st));
+            if (low) HM_CHECK(sell_fill_lowp(L.S, true, s.use_bf16(k), st));
+        }
         HM_ALLOC(L.dsm, double, L.A.n);
         HM_ALLOC(L.dsm32, float, L.A.n);
         HM_CHECK(launch_smoother_diag(L.A, s.opt.smoother, L.dsm, L.dsm32, st));
-        if (s.opt.precision == 1)
-            HM_CHECK(sell_fill_lowp(L.S, true, s.use_bf16(k), st));
         HM_CHECK(alloc_level_vectors(s, L));
     }
     HM_PHASE("setup: SELL + vectors", st);
@@ -807,13 +822,12 @@ int hmfem_spmv(hmfem_solver *h, int level, const double *x, double *y, int mem)
     if (level >= (int)s.lv.size()) return HMFEM_E_ARG;
     cudaStream_t st = s.st;
     hm::Level &L = s.lv[level];
-    if (!L.S.sptr) HM_CHECK(hm::csr_to_sell(L.A, L.S, st));
     const int n = L.A.n;
     double *dx = nullptr, *dy = nullptr;
     HM_ALLOC(dx, double, n);
     HM_ALLOC(dy, double, n);
     HM_CHECK(hm::upload(dx, x, n, mem, st));
-    HM_CHECK(hm::launch_spmv(L.S, dx, dy, st));
+    HM_CHECK(hm::level_spmv(s, level, dx, dy, st));
     HM_CHECK(hm::download(y, (const double *)dy, n, mem, st));
     HM_CUDA(cudaStreamSynchronize(st));
     hm::dfree(dx);

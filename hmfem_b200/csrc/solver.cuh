@@ -48,6 +48,9 @@ struct Solver {
     {
         return opt.precision == 1 && opt.bf16_from >= 0 && l >= opt.bf16_from;
     }
+    // structured solve-phase forms (stencil_cycle.cu), when setup built them
+    bool use_g7(int l) const { return l == 0 && !lv.empty() && lv[0].g7.c; }
+    bool use_g19(int l) const { return l == 1 && (int)lv.size() > 1 && lv[1].g19.v; }
     // level vectors; level 0 of the FP64 cycle works on the CG's r and z
     template <class T> T *vec_f(int l);
     template <class T> T *vec_ua(int l);
@@ -81,5 +84,31 @@ int launch_smoother_diag(const Csr &A, int kind, double *dsm, float *dsm32,
                          cudaStream_t st);
 int dense_factor(const Csr &A, double *Lf, int *err, cudaStream_t st);
 int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes);
+int level_spmv(Solver &s, int l, const double *x, double *y, cudaStream_t st);
+
+// structured level-0 / level-1 kernels (stencil_cycle.cu); V is the
+// coefficient storage type
+template <class T, class V>
+int g7_pre(const Level &L, const T *f, const T *dinv, T w, T *u, T *rs, const Ctl *ctl,
+            cudaStream_t st);
+template <class T>
+int g7_restrict(const Level &L, const T *rs, T *fc, const Ctl *ctl, cudaStream_t st);
+template <class T>
+int g7_prolong(const Level &L, const T *uc, T *u, const Ctl *ctl, cudaStream_t st);
+template <class T, class V, bool DOT>
+int g7_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo, Ctl *ctl,
+             double *part, int first, cudaStream_t st);
+int g7_spmv_dot(const Level &L, const double *x, double *y, Ctl *ctl, double *part,
+                 cudaStream_t st);
+int g7_resid(const Level &L, const double *b, const double *x, double *r, Ctl *ctl,
+              double *part, int init, cudaStream_t st);
+int g7_spmv(const Level &L, const double *x, double *y, cudaStream_t st);
+template <class T, class V>
+int g19_pre(const Level &L, const T *f, const T *dinv, T w, T *u, T *rs, const Ctl *ctl,
+             cudaStream_t st);
+template <class T, class V>
+int g19_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo,
+              const Ctl *ctl, cudaStream_t st);
+int g19_spmv(const Level &L, const double *x, double *y, cudaStream_t st);
 
 }  // namespace hm

@@ -1,0 +1,600 @@
+// stencil_cycle.cu -- solve-phase kernels for the two finest levels of a
+// matrix assembled on the device, stored by their grid structure instead of
+// SELL-32, so no column index is read.
+//
+// Level 0 is the 7-point TPFA stencil: per cell a_cc and the couplings to
+// the +x, +y, +z neighbours; the coupling to -x is the -x neighbour's +x
+// one, and so on.  That needs the assembled matrix to be bitwise symmetric
+// (hm(a,b) = 2ab/(a+b) is, and every pair is checked before this form is
+// used).  A row costs 4 coefficients instead of 7 values + 7 column
+// indices.  Level 1 -- the Galerkin operator of the parity split -- couples
+// each even cell to the even cells at the 19 offsets of grid19.cuh; with nx
+// even the even cell s has coarse id s >> 1, so the 19 coefficients of a
+// row sit in 19 unit-stride arrays.
+//
+// Every row is summed in the CSR's column order (level 0: d,l,c,r,u,t,b as
+// solve_linearsystem_AMG.c:103-139 packs it; level 1: ascending), with the
+// operations of the SELL kernels, so FP64 results are bit-identical to
+// them; the level-0 transfers follow the parity split's P and R rows
+// (C rows: the cell itself; F rows: the six neighbours, in row order).
+#include "cycle.cuh"
+#include "grid19.cuh"
+
+namespace hm {
+
+namespace {
+
+// (i, j, k) of cell s
+__device__ __forceinline__ void cell_ijk(unsigned s, unsigned nx, unsigned ny, int &i,
+                                         int &j, int &k)
+{
+    const unsigned r = s / nx;
+    i = (int)(s - r * nx);
+    k = (int)(r / ny);
+    j = (int)(r - (unsigned)k * ny);
+}
+
+template <class V> struct G7v {
+    const V *c, *px, *py, *pz;
+    int nx, ny, nz;
+};
+
+// t -/+ sum over row s of a_sj x(j), in the order d,l,c,r,u,t,b
+template <class T, bool SUB, class V, class X>
+__device__ __forceinline__ T g7_row(T t, const G7v<V> &g, long s, int i, int j, int k,
+                                    X x)
+{
+    using A = Ar<T>;
+    const long nx = g.nx, nxy = (long)g.nx * g.ny;
+    const bool hd = j > 0, hl = i > 0, hr = i < g.nx - 1, hu = j < g.ny - 1,
+               ht = k < g.nz - 1, hb = k > 0;
+    // all loads first, so they overlap
+    const T ad = hd ? (T)ld(g.py, s - nx) : (T)0, xd = hd ? x(s - nx) : (T)0;
+    const T al = hl ? (T)ld(g.px, s - 1) : (T)0, xl = hl ? x(s - 1) : (T)0;
+    const T ac = (T)ld(g.c, s), xc = x(s);
+    const T ar = hr ? (T)ld(g.px, s) : (T)0, xr = hr ? x(s + 1) : (T)0;
+    const T au = hu ? (T)ld(g.py, s) : (T)0, xu = hu ? x(s + nx) : (T)0;
+    const T at = ht ? (T)ld(g.pz, s) : (T)0, xt = ht ? x(s + nxy) : (T)0;
+    const T ab = hb ? (T)ld(g.pz, s - nxy) : (T)0, xb = hb ? x(s - nxy) : (T)0;
+    auto acc = [&](T a, T xv) {
+        const T p = A::mul(a, xv);
+        t = SUB ? A::sub(t, p) : A::add(t, p);
+    };
+    if (hd) acc(ad, xd);
+    if (hl) acc(al, xl);
+    acc(ac, xc);
+    if (hr) acc(ar, xr);
+    if (hu) acc(au, xu);
+    if (ht) acc(at, xt);
+    if (hb) acc(ab, xb);
+    return t;
+}
+
+// number of neighbours of cell (i,j,k) = the P-row length of an F cell
+__device__ __forceinline__ int g7_degree(int i, int j, int k, int nx, int ny, int nz)
+{
+    return (j > 0) + (i > 0) + (i < nx - 1) + (j < ny - 1) + (k < nz - 1) + (k > 0);
+}
+
+template <class V> struct G19v {
+    const V *v;
+    long n;  // coarse rows (the array stride)
+    int nx, ny, nz;
+};
+
+// t -/+ sum over level-1 row c of a_cq x(q), ascending q
+template <class T, bool SUB, class V, class X>
+__device__ __forceinline__ T g19_row(T t, const G19v<V> &g, long c, X x)
+{
+    using A = Ar<T>;
+    const int hx = g.nx >> 1;
+    const long row = c / hx;
+    const int j = (int)(row % g.ny), k = (int)(row / g.ny);
+    const int i = 2 * (int)(c - row * hx) + ((j + k) & 1);
+    const long s = i + row * g.nx, nxy = (long)g.nx * g.ny;
+    T a[kQ19], xv[kQ19];
+    bool on[kQ19];
+#pragma unroll
+    for (int q = 0; q < kQ19; q++) {
+        const int ii = i + q19x(q), jj = j + q19y(q), kk = k + q19z(q);
+        on[q] = ii >= 0 && ii < g.nx && jj >= 0 && jj < g.ny && kk >= 0 && kk < g.nz;
+        a[q] = on[q] ? (T)ld(g.v, q * g.n + c) : (T)0;
+        xv[q] = on[q] ? x((s + q19_lin(q, g.nx, nxy)) >> 1) : (T)0;
+    }
+#pragma unroll
+    for (int q = 0; q < kQ19; q++) {
+        if (!on[q]) continue;
+        const T p = A::mul(a[q], xv[q]);
+        t = SUB ? A::sub(t, p) : A::add(t, p);
+    }
+    return t;
+}
+
+// ---- level 0 ------------------------------------------------------------
+
+// u = w D^-1 f;  r = f - A u;  rs = r / |P row|  (k_pre on the stencil)
+template <class T, class V>
+__global__ void __launch_bounds__(256)
+k_g7_pre(G7v<V> g, int n, const T *__restrict__ f, const T *__restrict__ dinv, T w,
+         T *__restrict__ u, T *__restrict__ rs, const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    GRID_STRIDE(s, n) {
+        int i, j, k;
+        cell_ijk((unsigned)s, g.nx, g.ny, i, j, k);
+        const T fr = f[s];
+        const T t = g7_row<T, true>(fr, g, s, i, j, k, [&](long c) {
+            return A::mul(A::mul(w, f[c]), dinv[c]);
+        });
+        u[s] = A::mul(A::mul(w, fr), dinv[s]);
+        const int pc = ((i + j + k) & 1) ? g7_degree(i, j, k, g.nx, g.ny, g.nz) : 1;
+        rs[s] = pc == 1 ? t : A::div(t, (T)pc);
+    }
+}
+
+// f_c = sum over R(c) of rs, fine rows ascending: b, d, l, c, r, u, t
+template <class T>
+__global__ void __launch_bounds__(256)
+k_g7_restrict(int nx, int ny, int nz, const int *__restrict__ cid,
+              const T *__restrict__ rs, T *__restrict__ fc, const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    const int hx = (nx + 1) >> 1;
+    const long nxy = (long)nx * ny, m = (long)hx * ny * nz;
+    GRID_STRIDE(t, m) {
+        const long r = t / hx;
+        const int j = (int)(r % ny), k = (int)(r / ny);
+        const int i = 2 * (int)(t - r * hx) + ((j + k) & 1);
+        if (i >= nx) continue;
+        const long s = i + r * nx;
+        const T vb = k > 0 ? rs[s - nxy] : (T)0, vd = j > 0 ? rs[s - nx] : (T)0;
+        const T vl = i > 0 ? rs[s - 1] : (T)0, vc = rs[s];
+        const T vr = i < nx - 1 ? rs[s + 1] : (T)0, vu = j < ny - 1 ? rs[s + nx] : (T)0;
+        const T vt = k < nz - 1 ? rs[s + nxy] : (T)0;
+        T acc = (T)0;
+        if (k > 0) acc = A::add(acc, vb);
+        if (j > 0) acc = A::add(acc, vd);
+        if (i > 0) acc = A::add(acc, vl);
+        acc = A::add(acc, vc);
+        if (i < nx - 1) acc = A::add(acc, vr);
+        if (j < ny - 1) acc = A::add(acc, vu);
+        if (k < nz - 1) acc = A::add(acc, vt);
+        fc[cid[s]] = acc;
+    }
+}
+
+// u += P u_c: C cells take their own coarse value, F cells the average of
+// their neighbours' in row order d, l, r, u, t, b (k_prolong_add's sums)
+template <class T>
+__global__ void __launch_bounds__(256)
+k_g7_prolong(int nx, int ny, int nz, const int *__restrict__ cid,
+             const T *__restrict__ uc, T *__restrict__ u, const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    const long nxy = (long)nx * ny, n = nxy * nz;
+    GRID_STRIDE(s, n) {
+        int i, j, k;
+        cell_ijk((unsigned)s, nx, ny, i, j, k);
+        T add;
+        if (((i + j + k) & 1) == 0) {
+            add = uc[cid[s]];
+        } else {
+            const bool h[6] = {j > 0, i > 0, i < nx - 1, j < ny - 1, k < nz - 1, k > 0};
+            const long o[6] = {-nx, -1, 1, nx, nxy, -nxy};
+            T v[6];
+#pragma unroll
+            for (int d = 0; d < 6; d++) v[d] = h[d] ? uc[cid[s + o[d]]] : (T)0;
+            T t = (T)0;
+            int c = 0;
+#pragma unroll
+            for (int d = 0; d < 6; d++) {
+                if (!h[d]) continue;
+                t = c == 0 ? v[d] : A::add(t, v[d]);
+                c++;
+            }
+            add = c == 1 ? t : A::div(t, (T)c);
+        }
+        u[s] = A::add(u[s], add);
+    }
+}
+
+// v = f - A u;  u_out = u + w v D^-1;  optionally sigma = (u_out, f)
+template <class T, class V, bool DOT>
+__global__ void __launch_bounds__(256)
+k_g7_post(G7v<V> g, int n, const T *__restrict__ f, const T *__restrict__ dinv, T w,
+          const T *__restrict__ u, T *__restrict__ uo, Ctl *ctl, double *part, int first)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    double dot = 0.0;
+    GRID_STRIDE(s, n) {
+        int i, j, k;
+        cell_ijk((unsigned)s, g.nx, g.ny, i, j, k);
+        const T fr = f[s];
+        const T t = g7_row<T, true>(fr, g, s, i, j, k, [&](long c) { return u[c]; });
+        const T un = A::add(u[s], A::mul(A::mul(w, t), dinv[s]));
+        uo[s] = un;
+        if (DOT) dot += (double)un * (double)fr;
+    }
+    if (DOT)
+        grid_reduce_sum(dot, part, &ctl->tickets[RED_SIGMA],
+                        [&](double s) { sigma_finish(ctl, s, first); });
+}
+
+// v = A s; tau = (s, v); alpha = sigma / tau   (k_spmv_dot on the stencil)
+__global__ void __launch_bounds__(256)
+k_g7_spmv_dot(G7v<double> g, int n, const double *__restrict__ x, double *__restrict__ y,
+              Ctl *ctl, double *part)
+{
+    if (finished(ctl)) return;
+    double d = 0.0;
+    GRID_STRIDE(s, n) {
+        int i, j, k;
+        cell_ijk((unsigned)s, g.nx, g.ny, i, j, k);
+        const double a = g7_row<double, false>(0.0, g, s, i, j, k, [&](long c) { return x[c]; });
+        y[s] = a;
+        d += x[s] * a;
+    }
+    grid_reduce_sum(d, part, &ctl->tickets[RED_TAU], [&](double t) { tau_finish(ctl, t); });
+}
+
+// plain y = A x (inspection)
+__global__ void __launch_bounds__(256)
+k_g7_spmv(G7v<double> g, int n, const double *__restrict__ x, double *__restrict__ y)
+{
+    GRID_STRIDE(s, n) {
+        int i, j, k;
+        cell_ijk((unsigned)s, g.nx, g.ny, i, j, k);
+        y[s] = g7_row<double, false>(0.0, g, s, i, j, k, [&](long c) { return x[c]; });
+    }
+}
+
+// r = b - A x; (r, r); (b, b)   (k_resid on the stencil)
+__global__ void __launch_bounds__(256)
+k_g7_resid(G7v<double> g, int n, const double *__restrict__ b, const double *__restrict__ x,
+           double *__restrict__ r, Ctl *ctl, double *part, int init)
+{
+    if (init == 0 && (finished(ctl) || !ctl->check)) return;
+    double rr = 0.0, bb = 0.0;
+    GRID_STRIDE(s, n) {
+        int i, j, k;
+        cell_ijk((unsigned)s, g.nx, g.ny, i, j, k);
+        const double a = g7_row<double, false>(0.0, g, s, i, j, k, [&](long c) { return x[c]; });
+        const double bi = b[s];
+        const double ri = dsub(bi, a);
+        r[s] = ri;
+        rr += ri * ri;
+        bb += bi * bi;
+    }
+    double *p2 = part + kRedBlocks;
+    grid_reduce_sum(bb, p2, &ctl->tickets[RED_BB], [&](double s) { ctl->bb = s; });
+    grid_reduce_sum(rr, part, &ctl->tickets[RED_TRR],
+                    [&](double s) { trr_finish(ctl, s, init); });
+}
+
+// ---- level 1 ------------------------------------------------------------
+
+template <class T, class V>
+__global__ void __launch_bounds__(256)
+k_g19_pre(G19v<V> g, const T *__restrict__ f, const T *__restrict__ dinv, T w,
+          const int *__restrict__ prow, T *__restrict__ u, T *__restrict__ rs,
+          const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    GRID_STRIDE(c, g.n) {
+        const T fr = f[c];
+        const T t = g19_row<T, true>(fr, g, c, [&](long q) {
+            return A::mul(A::mul(w, f[q]), dinv[q]);
+        });
+        u[c] = A::mul(A::mul(w, fr), dinv[c]);
+        const int pc = prow[c + 1] - prow[c];
+        rs[c] = pc == 1 ? t : A::div(t, (T)pc);
+    }
+}
+
+template <class T, class V>
+__global__ void __launch_bounds__(256)
+k_g19_post(G19v<V> g, const T *__restrict__ f, const T *__restrict__ dinv, T w,
+           const T *__restrict__ u, T *__restrict__ uo, const Ctl *ctl)
+{
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    GRID_STRIDE(c, g.n) {
+        const T fr = f[c];
+        const T t = g19_row<T, true>(fr, g, c, [&](long q) { return u[q]; });
+        uo[c] = A::add(u[c], A::mul(A::mul(w, t), dinv[c]));
+    }
+}
+
+__global__ void __launch_bounds__(256)
+k_g19_spmv(G19v<double> g, const double *__restrict__ x, double *__restrict__ y)
+{
+    GRID_STRIDE(c, g.n) y[c] = g19_row<double, false>(0.0, g, c, [&](long q) { return x[q]; });
+}
+
+// ---- setup ----------------------------------------------------------------
+
+// a_cc, a_{c,c+1}, a_{c,c+nx}, a_{c,c+nxy} from the assembled rows (order
+// d,l,c,r,u,t,b over the in-grid neighbours), and a bitwise check of
+// a_{c,c+e} == a_{c+e,c} for the three + directions
+__global__ void k_g7_extract(int nx, int ny, int nz, const int *__restrict__ rowptr,
+                             const int *__restrict__ col, const double *__restrict__ val,
+                             double *c, double *px, double *py, double *pz, float *c32,
+                             float *px32, float *py32, float *pz32, int *bad)
+{
+    const long nxy = (long)nx * ny, n = nxy * nz;
+    GRID_STRIDE(s, n) {
+        int i, j, k;
+        cell_ijk((unsigned)s, nx, ny, i, j, k);
+        const int o = rowptr[s];
+        // position of each direction in the row
+        const int pd = o, pl = pd + (j > 0), pc = pl + (i > 0), pr = pc + 1;
+        const int pu = pr + (i < nx - 1), pt = pu + (j < ny - 1), pb = pt + (k < nz - 1);
+        const int e = pb + (k > 0);
+        bool ok = e == rowptr[s + 1] && col[pc] == (int)s;
+        const double vc = val[pc];
+        double vr = 0.0, vu = 0.0, vt = 0.0;
+        if (i < nx - 1) {
+            vr = val[pr];
+            const long q = s + 1;
+            const int oq = rowptr[q] + (j > 0);  // its l entry
+            ok = ok && col[pr] == (int)q && col[oq] == (int)s &&
+                 __double_as_longlong(val[oq]) == __double_as_longlong(vr);
+        }
+        if (j < ny - 1) {
+            vu = val[pu];
+            const long q = s + nx;
+            const int oq = rowptr[q];  // its d entry (first)
+            ok = ok && col[pu] == (int)q && col[oq] == (int)s &&
+                 __double_as_longlong(val[oq]) == __double_as_longlong(vu);
+        }
+        if (k < nz - 1) {
+            vt = val[pt];
+            const long q = s + nxy;
+            const int oq = rowptr[q + 1] - 1;  // its b entry (last)
+            ok = ok && col[pt] == (int)q && col[oq] == (int)s &&
+                 __double_as_longlong(val[oq]) == __double_as_longlong(vt);
+        }
+        c[s] = vc; px[s] = vr; py[s] = vu; pz[s] = vt;
+        if (c32) { c32[s] = (float)vc; px32[s] = (float)vr; py32[s] = (float)vu; pz32[s] = (float)vt; }
+        if (!ok) atomicOr(bad, 1);
+    }
+}
+
+__device__ __forceinline__ void cvt(double v, float *o) { *o = (float)v; }
+__device__ __forceinline__ void cvt(double v, __nv_bfloat16 *o) { *o = __float2bfloat16((float)v); }
+
+template <class D>
+__global__ void k_g19_cast(const double *__restrict__ v, long m, D *out)
+{
+    GRID_STRIDE(t, m) cvt(v[t], out + t);
+}
+
+int nb(long n)
+{
+    long b = ceil_div(n, 256);
+    if (b < 1) b = 1;
+    return (int)(b < kRedBlocks ? b : kRedBlocks);
+}
+
+template <class V> G7v<V> g7v(const Grid7 &g);
+template <> G7v<double> g7v<double>(const Grid7 &g)
+{
+    return {g.c, g.px, g.py, g.pz, g.nx, g.ny, g.nz};
+}
+template <> G7v<float> g7v<float>(const Grid7 &g)
+{
+    return {g.c32, g.px32, g.py32, g.pz32, g.nx, g.ny, g.nz};
+}
+
+template <class V> G19v<V> g19v(const Grid19 &g, long n);
+template <> G19v<double> g19v<double>(const Grid19 &g, long n) { return {g.v, n, g.nx, g.ny, g.nz}; }
+template <> G19v<float> g19v<float>(const Grid19 &g, long n) { return {g.v32, n, g.nx, g.ny, g.nz}; }
+template <> G19v<__nv_bfloat16> g19v<__nv_bfloat16>(const Grid19 &g, long n)
+{
+    return {g.v16, n, g.nx, g.ny, g.nz};
+}
+
+}  // namespace
+
+bool g19_applies(int nx, int ny, int nz)
+{
+    (void)nz;
+    return nx % 2 == 0 && nx >= 4 && ny >= 4;
+}
+
+void g7_free(Grid7 &g)
+{
+    dfree(g.c); dfree(g.px); dfree(g.py); dfree(g.pz);
+    dfree(g.c32); dfree(g.px32); dfree(g.py32); dfree(g.pz32);
+    g = Grid7();
+}
+
+void g19_free(Grid19 &g)
+{
+    dfree(g.v); dfree(g.v32); dfree(g.v16);
+    g = Grid19();
+}
+
+int g7_build(Level &L, int nx, int ny, int nz, bool f32, cudaStream_t st, int *dwork)
+{
+    g7_free(L.g7);
+    const long n = (long)nx * ny * nz;
+    if (n != L.A.n || n <= 0) return HMFEM_OK;
+    Grid7 g;
+    g.nx = nx; g.ny = ny; g.nz = nz;
+    double **d64[4] = {&g.c, &g.px, &g.py, &g.pz};
+    float **d32[4] = {&g.c32, &g.px32, &g.py32, &g.pz32};
+    for (int a = 0; a < 4; a++) {
+        *d64[a] = (double *)dalloc(sizeof(double) * n);
+        if (f32) *d32[a] = (float *)dalloc(sizeof(float) * n);
+        if (!*d64[a] || (f32 && !*d32[a])) { g7_free(g); return HMFEM_E_CUDA; }
+    }
+    HM_CUDA(cudaMemsetAsync(dwork, 0, sizeof(int), st));
+    k_g7_extract<<<nb(n), 256, 0, st>>>(nx, ny, nz, L.A.rowptr, L.A.col, L.A.val, g.c, g.px,
+                                        g.py, g.pz, g.c32, g.px32, g.py32, g.pz32, dwork);
+    HM_LAUNCHED();
+    int bad = 0;
+    HM_CUDA(cudaMemcpyAsync(&bad, dwork, sizeof(int), cudaMemcpyDeviceToHost, st));
+    HM_CUDA(cudaStreamSynchronize(st));
+    if (bad) { g7_free(g); return HMFEM_OK; }
+    L.g7 = g;
+    return HMFEM_OK;
+}
+
+int g19_lowp(Grid19 &g, int n, bool f32, bool bf16, cudaStream_t st)
+{
+    const long m = (long)kQ19 * n;
+    if (f32 && !g.v32) {
+        g.v32 = (float *)dalloc(sizeof(float) * m);
+        if (!g.v32) return HMFEM_E_CUDA;
+        k_g19_cast<float><<<nb(m), 256, 0, st>>>(g.v, m, g.v32);
+        HM_LAUNCHED();
+    }
+    if (bf16 && !g.v16) {
+        g.v16 = (__nv_bfloat16 *)dalloc(sizeof(__nv_bfloat16) * m);
+        if (!g.v16) return HMFEM_E_CUDA;
+        k_g19_cast<__nv_bfloat16><<<nb(m), 256, 0, st>>>(g.v, m, g.v16);
+        HM_LAUNCHED();
+    }
+    return HMFEM_OK;
+}
+
+// ---- launchers used by the cycle and the CG --------------------------------
+
+template <class T, class V>
+int g7_pre(const Level &L, const T *f, const T *dinv, T w, T *u, T *rs, const Ctl *ctl,
+            cudaStream_t st)
+{
+    const int n = L.A.n;
+    k_g7_pre<T, V><<<nb(n), 256, 0, st>>>(g7v<V>(L.g7), n, f, dinv, w, u, rs, ctl);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+template <class T>
+int g7_restrict(const Level &L, const T *rs, T *fc, const Ctl *ctl, cudaStream_t st)
+{
+    const Grid7 &g = L.g7;
+    const long m = (long)((g.nx + 1) >> 1) * g.ny * g.nz;
+    k_g7_restrict<T><<<nb(m), 256, 0, st>>>(g.nx, g.ny, g.nz, L.cid, rs, fc, ctl);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+template <class T>
+int g7_prolong(const Level &L, const T *uc, T *u, const Ctl *ctl, cudaStream_t st)
+{
+    const Grid7 &g = L.g7;
+    k_g7_prolong<T><<<nb(L.A.n), 256, 0, st>>>(g.nx, g.ny, g.nz, L.cid, uc, u, ctl);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+template <class T, class V, bool DOT>
+int g7_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo, Ctl *ctl,
+             double *part, int first, cudaStream_t st)
+{
+    const int n = L.A.n;
+    k_g7_post<T, V, DOT><<<nb(n), 256, 0, st>>>(g7v<V>(L.g7), n, f, dinv, w, u, uo, ctl,
+                                                part, first);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+int g7_spmv_dot(const Level &L, const double *x, double *y, Ctl *ctl, double *part,
+                 cudaStream_t st)
+{
+    const int n = L.A.n;
+    k_g7_spmv_dot<<<nb(n), 256, 0, st>>>(g7v<double>(L.g7), n, x, y, ctl, part);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+int g7_resid(const Level &L, const double *b, const double *x, double *r, Ctl *ctl,
+              double *part, int init, cudaStream_t st)
+{
+    const int n = L.A.n;
+    k_g7_resid<<<nb(n), 256, 0, st>>>(g7v<double>(L.g7), n, b, x, r, ctl, part, init);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+int g7_spmv(const Level &L, const double *x, double *y, cudaStream_t st)
+{
+    const int n = L.A.n;
+    k_g7_spmv<<<nb(n), 256, 0, st>>>(g7v<double>(L.g7), n, x, y);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+template <class T, class V>
+int g19_pre(const Level &L, const T *f, const T *dinv, T w, T *u, T *rs, const Ctl *ctl,
+             cudaStream_t st)
+{
+    const G19v<V> g = g19v<V>(L.g19, L.A.n);
+    k_g19_pre<T, V><<<nb(g.n), 256, 0, st>>>(g, f, dinv, w, L.P.rowptr, u, rs, ctl);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+template <class T, class V>
+int g19_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo,
+              const Ctl *ctl, cudaStream_t st)
+{
+    const G19v<V> g = g19v<V>(L.g19, L.A.n);
+    k_g19_post<T, V><<<nb(g.n), 256, 0, st>>>(g, f, dinv, w, u, uo, ctl);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+int g19_spmv(const Level &L, const double *x, double *y, cudaStream_t st)
+{
+    const G19v<double> g = g19v<double>(L.g19, L.A.n);
+    k_g19_spmv<<<nb(g.n), 256, 0, st>>>(g, x, y);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+template int g7_pre<double, double>(const Level &, const double *, const double *, double,
+                                     double *, double *, const Ctl *, cudaStream_t);
+template int g7_pre<float, float>(const Level &, const float *, const float *, float,
+                                   float *, float *, const Ctl *, cudaStream_t);
+template int g7_restrict<double>(const Level &, const double *, double *, const Ctl *,
+                                  cudaStream_t);
+template int g7_restrict<float>(const Level &, const float *, float *, const Ctl *,
+                                 cudaStream_t);
+template int g7_prolong<double>(const Level &, const double *, double *, const Ctl *,
+                                 cudaStream_t);
+template int g7_prolong<float>(const Level &, const float *, float *, const Ctl *,
+                                cudaStream_t);
+template int g7_post<double, double, true>(const Level &, const double *, const double *,
+                                            double, const double *, double *, Ctl *,
+                                            double *, int, cudaStream_t);
+template int g7_post<double, double, false>(const Level &, const double *, const double *,
+                                             double, const double *, double *, Ctl *,
+                                             double *, int, cudaStream_t);
+template int g7_post<float, float, false>(const Level &, const float *, const float *,
+                                           float, const float *, float *, Ctl *, double *,
+                                           int, cudaStream_t);
+template int g19_pre<double, double>(const Level &, const double *, const double *, double,
+                                      double *, double *, const Ctl *, cudaStream_t);
+template int g19_pre<float, float>(const Level &, const float *, const float *, float,
+                                    float *, float *, const Ctl *, cudaStream_t);
+template int g19_pre<float, __nv_bfloat16>(const Level &, const float *, const float *,
+                                            float, float *, float *, const Ctl *,
+                                            cudaStream_t);
+template int g19_post<double, double>(const Level &, const double *, const double *,
+                                       double, const double *, double *, const Ctl *,
+                                       cudaStream_t);
+template int g19_post<float, float>(const Level &, const float *, const float *, float,
+                                     const float *, float *, const Ctl *, cudaStream_t);
+template int g19_post<float, __nv_bfloat16>(const Level &, const float *, const float *,
+                                             float, const float *, float *, const Ctl *,
+                                             cudaStream_t);
+
+}  // namespace hm

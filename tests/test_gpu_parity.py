@@ -36,6 +36,7 @@ CASES.update({
     "ragged_5x3x7": lambda: make_problem(5, 3, 7, log10k=(-14.0, 2.0, 1.0),
                                          n_conduits=1, seed=9),
     "conduit_40": lambda: config_problem(1, size=40),
+    "slab_8x6x1": lambda: make_problem(8, 6, 1, log10k=(-13.0, 1.0, 1.0), seed=4),
 })
 
 # Pressure / flux tolerance against the FP64 oracle when both are solved to
@@ -99,20 +100,26 @@ def test_hierarchy_bit_exact(case, generic_setup):
 @pytest.mark.parametrize("smoother,gs_from,oracle_smoother,omega",
                          [(0, -1, 1, 1.0), (0, -1, 1, 0.6), (1, -1, 2, 1.0),
                           (1, 2, 12, 1.0), (1, 1, 11, 1.0)])
-def test_vcycle_bit_exact(case, smoother, gs_from, oracle_smoother, omega):
+@pytest.mark.parametrize("generic_setup", [0, 1])
+def test_vcycle_bit_exact(case, smoother, gs_from, oracle_smoother, omega,
+                          generic_setup):
+    """generic_setup=0 runs the two finest levels of an assembled grid in
+    their structured forms (7-point stencil, 19-offset level 1),
+    generic_setup=1 everything on SELL-32; both equal the oracle's cycle."""
     name, p, (perm, ind, b, csr, H) = case
     # coarse_direct=0: the reference's diagonal solve on the coarsest level
     s = gpu.Solver(smoother=smoother, gs_from=gs_from, omega=omega,
-                   coarse_direct=0)
+                   coarse_direct=0, generic_setup=generic_setup)
     s.assemble(p)
     s.setup()
     f = np.random.default_rng(11).standard_normal(p.n)
     np.testing.assert_array_equal(s.vcycle(f), H.vcycle(f, oracle_smoother, omega))
 
 
-def test_spmv_bit_exact(case, port):
+@pytest.mark.parametrize("generic_setup", [0, 1])
+def test_spmv_bit_exact(case, port, generic_setup):
     name, p, (perm, ind, b, csr, H) = case
-    s = gpu.Solver()
+    s = gpu.Solver(generic_setup=generic_setup)
     s.assemble(p)
     s.setup()
     x = np.random.default_rng(3).standard_normal(p.n)
