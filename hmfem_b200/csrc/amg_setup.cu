@@ -635,8 +635,10 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
     if (grid3) {
         double *g19v = nullptr;
         if (g19_applies(grid3[0], grid3[1], grid3[2])) {
-            g19v = (double *)dalloc(sizeof(double) * kQ19 * (size_t)L.nc);
+            const long long m = slice_len(L.nc, kQ19);
+            g19v = (double *)dalloc(sizeof(double) * m);
             if (!g19v) return HMFEM_E_CUDA;
+            HM_CUDA(cudaMemsetAsync(g19v, 0, sizeof(double) * m, st));  // last slice's tail
             C.g19.nx = grid3[0];
             C.g19.ny = grid3[1];
             C.g19.nz = grid3[2];

@@ -44,15 +44,16 @@ __device__ __forceinline__ T row_acc(T t, const int *__restrict__ scol,
 
 // ---- smoother / transfer kernels --------------------------------------
 
-// Pre-smoother from zero and residual, fused (device_jacobi 3-arg,
-// device_amg.h:35-42):  u = w D^-1 f;  r = f - A u;  rs = r / |P row|
-// (the 1/c of simple_restriction, generic_operator.h:97-122, applied here).
+// Residual after the pre-smoother from zero (device_jacobi 3-arg,
+// device_amg.h:35-42), whose iterate u = w D^-1 f the producer of f has
+// already written (Seed):  r = f - A u;  rs = r / |P row| (the 1/c of
+// simple_restriction, generic_operator.h:97-122, applied here).
 template <class T, class M>
 __global__ void __launch_bounds__(256, 6)
 k_pre(const long long *__restrict__ sptr, const int *__restrict__ scol,
       const M *__restrict__ sval, int n, const T *__restrict__ f,
-      const T *__restrict__ dinv, T w, const int *__restrict__ prow,
-      T *__restrict__ u, T *__restrict__ rs, const Ctl *ctl)
+      const T *__restrict__ u, const int *__restrict__ prow, T *__restrict__ rs,
+      const Ctl *ctl)
 {
     if (finished(ctl)) return;
     using A = Ar<T>;
@@ -61,15 +62,19 @@ k_pre(const long long *__restrict__ sptr, const int *__restrict__ scol,
         int lane = (int)(r & 31);
         long long base = sptr[q];
         int wd = (int)((sptr[q + 1] - base) >> 5);
-        T fr = f[r];
-        T t = fr;
-        t = row_acc<T, true>(t, scol, sval, base + lane, wd, [&](int c) {
-            return A::mul(A::mul(w, f[c]), dinv[c]);
-        });
-        u[r] = A::mul(A::mul(w, fr), dinv[r]);
+        T t = f[r];
+        t = row_acc<T, true>(t, scol, sval, base + lane, wd, [&](int c) { return u[c]; });
         int pc = prow[r + 1] - prow[r];
         rs[r] = pc == 1 ? t : A::div(t, (T)pc);
     }
+}
+
+// u = (w f) D^-1 on level 0 where no producer seeded it (a V-cycle applied
+// on its own, hmfem_vcycle)
+template <class T>
+__global__ void k_seed(int n, const T *__restrict__ f, Seed<T> sd)
+{
+    GRID_STRIDE(i, n) sd.put(i, f[i]);
 }
 
 // f_c[e] = sum_{i in R(e), ascending} rs_i  (simple_restriction's
@@ -77,7 +82,7 @@ k_pre(const long long *__restrict__ sptr, const int *__restrict__ scol,
 template <class T>
 __global__ void __launch_bounds__(256)
 k_restrict(const int *__restrict__ rrow, const int *__restrict__ rcol, int nc,
-           const T *__restrict__ rs, T *__restrict__ fc, const Ctl *ctl)
+           const T *__restrict__ rs, T *__restrict__ fc, Seed<T> sd, const Ctl *ctl)
 {
     if (finished(ctl)) return;
     using A = Ar<T>;
@@ -85,6 +90,7 @@ k_restrict(const int *__restrict__ rrow, const int *__restrict__ rcol, int nc,
         T acc = (T)0;
         for (int k = rrow[e]; k < rrow[e + 1]; k++) acc = A::add(acc, rs[rcol[k]]);
         fc[e] = acc;
+        sd.put(e, acc);
     }
 }
 
@@ -277,7 +283,7 @@ __global__ void __launch_bounds__(256, 6)
 k_resid(const long long *__restrict__ sptr, const int *__restrict__ scol,
         const double *__restrict__ sval, int n, const double *__restrict__ b,
         const double *__restrict__ x, double *__restrict__ r, Ctl *ctl,
-        double *part, int init)
+        double *part, int init, Seed<double> sd)
 {
     // init: 1 = start of the solve, 0 = convergence check (residual
     // replacement), 2 = report only
@@ -293,6 +299,7 @@ k_resid(const long long *__restrict__ sptr, const int *__restrict__ scol,
         double bi = b[i];
         double ri = dsub(bi, s);
         r[i] = ri;
+        if (init != 2) sd.put(i, ri);
         rr += ri * ri;
         bb += bi * bi;
     }
@@ -330,7 +337,7 @@ k_spmv_dot(const long long *__restrict__ sptr, const int *__restrict__ scol,
 __global__ void __launch_bounds__(256)
 k_update(int n, double *__restrict__ x, double *__restrict__ r,
          const double *__restrict__ s, const double *__restrict__ v, Ctl *ctl,
-         double *part)
+         double *part, Seed<double> sd)
 {
     if (finished(ctl)) return;
     const double al = ctl->alpha;
@@ -339,6 +346,7 @@ k_update(int n, double *__restrict__ x, double *__restrict__ r,
         x[i] = dadd(x[i], dmul(s[i], al));
         double ri = dsub(r[i], dmul(v[i], al));
         r[i] = ri;
+        sd.put(i, ri);
         rr += ri * ri;
     }
     grid_reduce_sum(rr, part, &ctl->tickets[RED_RR], [&](double t) {
@@ -398,10 +406,14 @@ k_finish_z(int n, const T *__restrict__ src, const double *__restrict__ r,
 }
 
 __global__ void k_demote(int n, const double *__restrict__ r, float *__restrict__ f,
-                         const Ctl *ctl)
+                         Seed<float> sd, const Ctl *ctl)
 {
     if (finished(ctl)) return;
-    GRID_STRIDE(i, n) f[i] = (float)r[i];
+    GRID_STRIDE(i, n) {
+        const float fi = (float)r[i];
+        f[i] = fi;
+        sd.put(i, fi);
+    }
 }
 
 // ---- host side ------------------------------------------------------------
@@ -423,6 +435,16 @@ static T *cycle_out(Solver &s, int l)
     return s.vec_ub<T>(l);
 }
 
+// The seed (first Jacobi iterate) a producer of level l's right-hand side
+// writes: none unless level l is Jacobi-smoothed.
+template <class T>
+static Seed<T> seed_of(Solver &s, int l)
+{
+    const int last = s.nlevels - 1;
+    if (l >= last || l == s.direct_level || s.lv[l].gs) return {nullptr, nullptr, (T)0};
+    return {s.vec_ua<T>(l), s.vec_dinv<T>(l), (T)s.opt.omega};
+}
+
 // Launches fn(values) with the level's matrix values in the cycle's
 // storage type: FP64, FP32, or BF16 on levels >= bf16_from.
 template <class T, class F>
@@ -436,7 +458,7 @@ static void with_vals(Solver &s, const Sell &S, int l, F fn)
 // One V-cycle from level l: f[l] holds the right-hand side, the result is
 // left in cycle_out(l).
 template <class T>
-static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
+static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
 {
     Level &L = s.lv[l];
     const int last = s.nlevels - 1;
@@ -455,6 +477,10 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
         return HMFEM_OK;
     }
     const T w = (T)s.opt.omega;
+    if (!seeded && seed_of<T>(s, l).u) {
+        k_seed<T><<<nb(n), 256, 0, st>>>(n, f, seed_of<T>(s, l));
+        HM_LAUNCHED();
+    }
     const bool g7 = s.use_g7(l), g19 = s.use_g19(l);
     const bool bf16 = !std::is_same<T, double>::value && s.use_bf16(l);
     T *rs = s.vec_rs<T>(l);
@@ -484,26 +510,27 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
             HM_COUNT();
         });
     } else if (g7) {
-        HM_CHECK((g7_pre<T, T>(L, f, dv, w, ua, rs, ctl, st)));
+        HM_CHECK((g7_pre<T, T>(L, f, ua, rs, ctl, st)));
     } else if (g19) {
-        if (bf16) HM_CHECK((g19_pre<T, __nv_bfloat16>(L, f, dv, w, ua, rs, ctl, st)));
-        else HM_CHECK((g19_pre<T, T>(L, f, dv, w, ua, rs, ctl, st)));
+        if (bf16) HM_CHECK((g19_pre<T, __nv_bfloat16>(L, f, ua, rs, ctl, st)));
+        else HM_CHECK((g19_pre<T, T>(L, f, ua, rs, ctl, st)));
     } else {
         with_vals<T>(s, L.S, l, [&](auto vals) {
-            k_pre<T><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, vals, n, f, dv, w,
-                                           L.P.rowptr, ua, rs, ctl);
+            k_pre<T><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, vals, n, f, ua,
+                                           L.P.rowptr, rs, ctl);
             HM_COUNT();
         });
     }
     HM_LAUNCHED();
     if (g7) {
-        HM_CHECK((g7_restrict<T>(L, rs, s.vec_f<T>(l + 1), ctl, st)));
+        HM_CHECK((g7_restrict<T>(L, rs, s.vec_f<T>(l + 1), seed_of<T>(s, l + 1), ctl, st)));
     } else {
         k_restrict<T><<<nb(L.nc), 256, 0, st>>>(L.R.rowptr, L.R.col, L.nc, rs,
-                                                s.vec_f<T>(l + 1), ctl);
+                                                s.vec_f<T>(l + 1), seed_of<T>(s, l + 1),
+                                                ctl);
         HM_LAUNCHED();
     }
-    HM_CHECK(cycle_t<T>(s, l + 1, st, false));
+    HM_CHECK(cycle_t<T>(s, l + 1, st, false, true));
     if (g7) {
         HM_CHECK((g7_prolong<T>(L, cycle_out<T>(s, l + 1), ua, ctl, st)));
     } else {
@@ -542,17 +569,25 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot)
     return HMFEM_OK;
 }
 
-int cycle_fp64(Solver &s, int l, cudaStream_t st, bool dot)
+int cycle_fp64(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
 {
-    return cycle_t<double>(s, l, st, dot);
+    return cycle_t<double>(s, l, st, dot, seeded);
 }
 
-int cycle_fp32(Solver &s, int l, cudaStream_t st, bool dot)
+int cycle_fp32(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
 {
-    return cycle_t<float>(s, l, st, dot);
+    return cycle_t<float>(s, l, st, dot, seeded);
 }
 
 // ---- CG iteration bodies (enqueued once, captured into a graph) -----------
+
+// The FP64 cycle's level-0 seed, written by the CG kernels that produce r
+// (the FP32 cycle seeds in k_demote instead)
+static Seed<double> cg_seed(Solver &s)
+{
+    if (s.opt.precision != 0) return {nullptr, nullptr, 0.0};
+    return seed_of<double>(s, 0);
+}
 
 // z = C r, sigma = (z, r), beta (fused into the last V-cycle kernel where
 // the V-cycle is FP64 and has a coarse level)
@@ -563,7 +598,7 @@ int cg_precondition(Solver &s, cudaStream_t st)
     const bool top_is_coarse = s.nlevels == 1 || s.direct_level == 0;
     if (s.opt.precision == 0) {
         // the V-cycle reads f[0] = r in place; z lands in ub[0] = s.z
-        HM_CHECK(cycle_fp64(s, 0, st, !top_is_coarse));
+        HM_CHECK(cycle_fp64(s, 0, st, !top_is_coarse, true));
         if (top_is_coarse) {
             k_finish_z<double><<<nb(n), 256, 0, st>>>(n, L0.ua, s.r, s.v, s.z,
                                                       s.ctl, s.part,
@@ -572,9 +607,9 @@ int cg_precondition(Solver &s, cudaStream_t st)
         }
         return HMFEM_OK;
     }
-    k_demote<<<nb(n), 256, 0, st>>>(n, s.r, L0.f32, s.ctl);
+    k_demote<<<nb(n), 256, 0, st>>>(n, s.r, L0.f32, seed_of<float>(s, 0), s.ctl);
     HM_LAUNCHED();
-    HM_CHECK(cycle_fp32(s, 0, st, false));
+    HM_CHECK(cycle_fp32(s, 0, st, false, true));
     const float *z32 = top_is_coarse ? L0.ua32 : L0.ub32;
     k_finish_z<float><<<nb(n), 256, 0, st>>>(n, z32, s.r, s.v, s.z, s.ctl,
                                              s.part, s.first_sigma, 1);
@@ -587,10 +622,10 @@ int cg_init(Solver &s, cudaStream_t st)
     Level &L0 = s.lv[0];
     const int n = L0.A.n;
     if (s.use_g7(0)) {
-        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 1, st));
+        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 1, cg_seed(s), st));
     } else {
         k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
-                                       s.r, s.ctl, s.part, 1);
+                                       s.r, s.ctl, s.part, 1, cg_seed(s));
         HM_LAUNCHED();
     }
     s.first_sigma = 1;
@@ -613,13 +648,13 @@ int cg_iteration(Solver &s, cudaStream_t st)
                                           s.v, s.ctl, s.part);
         HM_LAUNCHED();
     }
-    k_update<<<nb(n), 256, 0, st>>>(n, s.x, s.r, s.s, s.v, s.ctl, s.part);
+    k_update<<<nb(n), 256, 0, st>>>(n, s.x, s.r, s.s, s.v, s.ctl, s.part, cg_seed(s));
     HM_LAUNCHED();
     if (g7) {
-        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 0, st));
+        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 0, cg_seed(s), st));
     } else {
         k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
-                                       s.r, s.ctl, s.part, 0);
+                                       s.r, s.ctl, s.part, 0, cg_seed(s));
         HM_LAUNCHED();
     }
     HM_CHECK(cg_precondition(s, st));
@@ -634,10 +669,10 @@ int cg_final_residual(Solver &s, cudaStream_t st)
     Level &L0 = s.lv[0];
     const int n = L0.A.n;
     if (s.use_g7(0)) {
-        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 2, st));
+        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 2, Seed<double>{}, st));
     } else {
         k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
-                                       s.r, s.ctl, s.part, 2);
+                                       s.r, s.ctl, s.part, 2, Seed<double>{});
         HM_LAUNCHED();
     }
     return HMFEM_OK;
@@ -662,24 +697,24 @@ __global__ void k_fill_one(double *x, int n)
 // kernel's algorithmic bytes per launch (no padding, every vector element
 // moved once):
 //   0 SpMV FP64            nnz*(8+4) + n*(8+8)
-//   1 pre-smoother FP64    nnz*(8+4) + n*(8 f + 8 d + 4 P-row + 8 u + 8 rs)
+//   1 pre-smoother FP64    nnz*(8+4) + n*(8 f + 8 u + 4 P-row + 8 rs)
 //   2 post-smoother FP64   nnz*(8+4) + n*(8 f + 8 d + 8 u + 8 u_out)
-//   3 pre-smoother FP32    nnz*(4+4) + n*(4+4+4+4+4)
+//   3 pre-smoother FP32    nnz*(4+4) + n*(4 f + 4 u + 4 P-row + 4 rs)
 //   4 post-smoother FP32   nnz*(4+4) + n*(4*4)
 // (values BF16 on levels >= bf16_from: 2 bytes instead of 4); the SELL
 // form is built for the call where the level solves in a structured form.
 // Structured forms (level 0: 4 coefficient arrays; level 1: 19 arrays of
 // which the in-grid ones count), same vectors as above:
 //   5 SpMV FP64 (level 0)           n*4*8 + n*(8+8)
-//   6 pre-smoother FP32 (level 0)   n*4*4 + n*(4 f + 4 d + 4 u + 4 rs)
+//   6 pre-smoother FP32 (level 0)   n*4*4 + n*(4 f + 4 u + 4 rs)
 //   7 post-smoother FP32 (level 0)  n*4*4 + n*4*4
-//   8 pre-smoother FP32 (level 1)   nnz*4 + n*(4+4+4+4+4)
+//   8 pre-smoother FP32 (level 1)   nnz*4 + n*(4 f + 4 u + 4 P-row + 4 rs)
 //   9 post-smoother FP32 (level 1)  nnz*4 + n*4*4
 int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
 {
     if (l < 0 || l >= s.nlevels || reps < 1 || which < 0 || which > 9) return HMFEM_E_ARG;
     if (which >= 1 && l == s.nlevels - 1) return HMFEM_E_ARG;
-    if (which >= 3 && s.opt.precision != 1) return HMFEM_E_ARG;
+    if (((which >= 3 && which <= 4) || which >= 6) && s.opt.precision != 1) return HMFEM_E_ARG;
     if (which >= 5 && which <= 7 && !s.use_g7(l)) return HMFEM_E_ARG;
     if (which >= 8 && (!s.use_g19(l) || s.use_bf16(l))) return HMFEM_E_ARG;
     Level &L = s.lv[l];
@@ -706,8 +741,7 @@ int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
             break;
         case 1:
             k_pre<double, double><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, L.S.val, n,
-                                                         x, L.dsm, w, L.P.rowptr, y,
-                                                         L.rs, nullptr);
+                                                         x, L.ua, L.P.rowptr, y, nullptr);
             break;
         case 2:
             k_post<double, double, false><<<nb(n), 256, 0, st>>>(
@@ -716,20 +750,18 @@ int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
         case 3:
             if (vb16 == 2)
                 k_pre<float, __nv_bfloat16><<<nb(n), 256, 0, st>>>(
-                    L.S.sptr, L.S.col, L.S.val16, n, xf, L.dsm32, (float)w,
-                    L.P.rowptr, yf, L.rs32, nullptr);
+                    L.S.sptr, L.S.col, L.S.val16, n, xf, L.ua32, L.P.rowptr, yf, nullptr);
             else
                 k_pre<float, float><<<nb(n), 256, 0, st>>>(
-                    L.S.sptr, L.S.col, L.S.val32, n, xf, L.dsm32, (float)w,
-                    L.P.rowptr, yf, L.rs32, nullptr);
+                    L.S.sptr, L.S.col, L.S.val32, n, xf, L.ua32, L.P.rowptr, yf, nullptr);
             break;
         case 5: g7_spmv_dot(L, x, y, s.ctl, s.part, st); break;
-        case 6: g7_pre<float, float>(L, xf, L.dsm32, (float)w, yf, L.rs32, nullptr, st); break;
+        case 6: g7_pre<float, float>(L, xf, L.ua32, yf, nullptr, st); break;
         case 7:
             g7_post<float, float, false>(L, xf, L.dsm32, (float)w, L.ua32, yf, nullptr,
                                          nullptr, 0, st);
             break;
-        case 8: g19_pre<float, float>(L, xf, L.dsm32, (float)w, yf, L.rs32, nullptr, st); break;
+        case 8: g19_pre<float, float>(L, xf, L.ua32, yf, nullptr, st); break;
         case 9: g19_post<float, float>(L, xf, L.dsm32, (float)w, L.ua32, yf, nullptr, st); break;
         default:
             if (vb16 == 2)
@@ -764,14 +796,14 @@ int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
     *ms = t / reps;
     switch (which) {
     case 0: *bytes = nnz * 12 + (double)n * 16; break;
-    case 1: *bytes = nnz * 12 + (double)n * 36; break;
+    case 1: *bytes = nnz * 12 + (double)n * 28; break;
     case 2: *bytes = nnz * 12 + (double)n * 32; break;
-    case 3: *bytes = nnz * (vb16 + 4) + (double)n * 20; break;
+    case 3: *bytes = nnz * (vb16 + 4) + (double)n * 16; break;
     case 4: *bytes = nnz * (vb16 + 4) + (double)n * 16; break;
     case 5: *bytes = (double)n * 48; break;
-    case 6: *bytes = (double)n * 32; break;
+    case 6: *bytes = (double)n * 28; break;
     case 7: *bytes = (double)n * 32; break;
-    case 8: *bytes = nnz * 4 + (double)n * 20; break;
+    case 8: *bytes = nnz * 4 + (double)n * 16; break;
     default: *bytes = nnz * 4 + (double)n * 16; break;
     }
     return HMFEM_OK;

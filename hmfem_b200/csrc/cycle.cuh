@@ -28,6 +28,21 @@ __device__ __forceinline__ bool finished(const Ctl *c) { return c && *(volatile 
     for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < (n);       \
          r += (long)gridDim.x * blockDim.x)
 
+// The first Jacobi iterate from zero, u = (w f) D^-1 (device_jacobi 3-arg,
+// device_amg.h:35-42), written by the kernel that produces f (restriction,
+// demotion, the CG residual update) so the pre-smoother reads u once
+// instead of recomputing it from f and D^-1 at every neighbour.  u ==
+// nullptr: the level is not Jacobi-smoothed.
+template <class T> struct Seed {
+    T *u;
+    const T *d;
+    T w;
+    __device__ __forceinline__ void put(long i, T f) const
+    {
+        if (u) u[i] = Ar<T>::mul(Ar<T>::mul(w, f), d[i]);
+    }
+};
+
 // sigma = (C r, r) once the preconditioner is applied (pcg.h:66-67, and
 // 46-47 on the first application); run by the last block of the fused
 // reduction.

@@ -36,25 +36,40 @@ struct Sell {
 };
 
 // Solve-phase forms of the two finest levels of a matrix assembled on the
-// device (stencil_cycle.cu).  Level 0: the 7-point stencil as a_cc and the
-// couplings to the +x, +y, +z neighbours (0 where absent); the coupling to
-// -x is the -x neighbour's +x one, and so on (the matrix is checked to be
-// bitwise symmetric first).
+// device (stencil_cycle.cu).  Both keep their coefficients slice-interleaved
+// like SELL-32 without column indices: the coefficients of rows 32t..32t+31
+// form one contiguous block, coefficient k of row r at
+// (r / 32) * K * 32 + k * 32 + r % 32, so a warp reads one stream.
+//
+// Level 0 (K = 4): the 7-point stencil as a_cc and the couplings to the +x,
+// +y, +z neighbours (0 where absent); the coupling to -x is the -x
+// neighbour's +x one, and so on (the matrix is checked to be bitwise
+// symmetric first).
 struct Grid7 {
     int nx = 0, ny = 0, nz = 0;
-    double *c = nullptr, *px = nullptr, *py = nullptr, *pz = nullptr;
-    float *c32 = nullptr, *px32 = nullptr, *py32 = nullptr, *pz32 = nullptr;
+    double *cf = nullptr;
+    float *cf32 = nullptr;
 };
 
-// Level 1 of the parity split (nx even, nx >= 4, ny >= 4): even cell s has
-// coarse id s >> 1, and row c's coefficient at offset q (grid19.cuh) is
-// v[q * n + c] (0 where the neighbour is outside the grid).
+// Level 1 of the parity split (K = 19; nx even, nx >= 4, ny >= 4): even
+// cell s has coarse id s >> 1; coefficient q (grid19.cuh) of a row is 0
+// where that neighbour is outside the grid.
 struct Grid19 {
     int nx = 0, ny = 0, nz = 0;
     double *v = nullptr;
     float *v32 = nullptr;
     __nv_bfloat16 *v16 = nullptr;
 };
+
+// index of coefficient k of row r in a slice-interleaved array of K per row
+__host__ __device__ __forceinline__ long long slice_at(long long r, int k, int K)
+{
+    return (r >> 5) * (32LL * K) + k * 32 + (r & 31);
+}
+__host__ __device__ __forceinline__ long long slice_len(long long n, int K)
+{
+    return ((n + 31) >> 5) * 32LL * K;
+}
 
 struct Level {
     Csr A;
@@ -149,9 +164,12 @@ void g19_free(Grid19 &g);
 
 // cycle + CG (cycle.cu)
 struct Solver;
-int cycle_fp64(Solver &s, int l, cudaStream_t st, bool dot_into_sigma);
-int cycle_fp32(Solver &s, int l, cudaStream_t st, bool dot_into_sigma);
+// seeded: the level-0 smoother's first iterate was written by the producer
+// of the right-hand side (the CG kernels); otherwise the cycle writes it
+int cycle_fp64(Solver &s, int l, cudaStream_t st, bool dot_into_sigma, bool seeded);
+int cycle_fp32(Solver &s, int l, cudaStream_t st, bool dot_into_sigma, bool seeded);
 
+int occ_blocks(const void *kernel, long n, int threads, int cap);
 void *dalloc(size_t bytes);
 void dfree(void *p);
 void set_alloc_stream(cudaStream_t st);  // stream that orders dalloc/dfree

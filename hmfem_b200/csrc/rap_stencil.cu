@@ -241,7 +241,7 @@ k_sg_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
 #pragma unroll
         for (int sl = 0; sl < 19; sl++) {
             const bool on = in & (1u << sl);
-            if (g19v) g19v[q19_of(OX(sl), OY(sl), OZ(sl)) * nc + c] = on ? out[sl] : 0.0;
+            if (g19v) g19v[slice_at(c, q19_of(OX(sl), OY(sl), OZ(sl)), kQ19)] = on ? out[sl] : 0.0;
             if (!on) continue;
             const long e = o + __popc(in & tb.less[sl]);
             ccol[e] = cid[s + tb.lin[sl]];

@@ -807,7 +807,7 @@ int hmfem_vcycle(hmfem_solver *h, const double *f, double *u, int mem)
     HM_CHECK(hm::upload(s.r, f, n, mem, st));
     s.ctl_active = false;
     const bool top_coarse = s.nlevels == 1 || s.direct_level == 0;
-    HM_CHECK(hm::cycle_fp64(s, 0, st, false));
+    HM_CHECK(hm::cycle_fp64(s, 0, st, false, false));
     HM_CHECK(hm::download(u, (const double *)(top_coarse ? s.lv[0].ua : s.z), n, mem, st));
     HM_CUDA(cudaStreamSynchronize(st));
     return HMFEM_OK;

@@ -7,6 +7,8 @@
 
 namespace hm {
 
+template <class T> struct Seed;  // cycle.cuh
+
 struct Solver {
     hmfem_options opt;
     cudaStream_t st = nullptr;
@@ -49,7 +51,7 @@ struct Solver {
         return opt.precision == 1 && opt.bf16_from >= 0 && l >= opt.bf16_from;
     }
     // structured solve-phase forms (stencil_cycle.cu), when setup built them
-    bool use_g7(int l) const { return l == 0 && !lv.empty() && lv[0].g7.c; }
+    bool use_g7(int l) const { return l == 0 && !lv.empty() && lv[0].g7.cf; }
     bool use_g19(int l) const { return l == 1 && (int)lv.size() > 1 && lv[1].g19.v; }
     // level vectors; level 0 of the FP64 cycle works on the CG's r and z
     template <class T> T *vec_f(int l);
@@ -89,10 +91,10 @@ int level_spmv(Solver &s, int l, const double *x, double *y, cudaStream_t st);
 // structured level-0 / level-1 kernels (stencil_cycle.cu); V is the
 // coefficient storage type
 template <class T, class V>
-int g7_pre(const Level &L, const T *f, const T *dinv, T w, T *u, T *rs, const Ctl *ctl,
-            cudaStream_t st);
+int g7_pre(const Level &L, const T *f, const T *u, T *rs, const Ctl *ctl, cudaStream_t st);
 template <class T>
-int g7_restrict(const Level &L, const T *rs, T *fc, const Ctl *ctl, cudaStream_t st);
+int g7_restrict(const Level &L, const T *rs, T *fc, Seed<T> sd, const Ctl *ctl,
+                cudaStream_t st);
 template <class T>
 int g7_prolong(const Level &L, const T *uc, T *u, const Ctl *ctl, cudaStream_t st);
 template <class T, class V, bool DOT>
@@ -101,11 +103,10 @@ int g7_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo, C
 int g7_spmv_dot(const Level &L, const double *x, double *y, Ctl *ctl, double *part,
                  cudaStream_t st);
 int g7_resid(const Level &L, const double *b, const double *x, double *r, Ctl *ctl,
-              double *part, int init, cudaStream_t st);
+             double *part, int init, Seed<double> sd, cudaStream_t st);
 int g7_spmv(const Level &L, const double *x, double *y, cudaStream_t st);
 template <class T, class V>
-int g19_pre(const Level &L, const T *f, const T *dinv, T w, T *u, T *rs, const Ctl *ctl,
-             cudaStream_t st);
+int g19_pre(const Level &L, const T *f, const T *u, T *rs, const Ctl *ctl, cudaStream_t st);
 template <class T, class V>
 int g19_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo,
               const Ctl *ctl, cudaStream_t st);

@@ -2,6 +2,7 @@
 // FP64 SELL SpMV.
 #include <cub/device/device_scan.cuh>
 #include <map>
+#include <mutex>
 #include <unordered_map>
 
 #include "hm.cuh"
@@ -69,6 +70,40 @@ void alloc_cache_release(AllocCache *c)
 }
 
 static void *pool_alloc(size_t bytes);
+
+// Blocks for a grid-stride kernel over n items: every block the SMs can
+// hold at once for this kernel (its register / shared-memory occupancy), so
+// the grid is one full wave; fewer when n is small; at most cap.
+int occ_blocks(const void *kernel, long n, int threads, int cap)
+{
+    static std::mutex mu;
+    static std::unordered_map<const void *, int> cache;
+    static int nsm = 0;
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        if (nsm == 0) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            if (nsm <= 0) nsm = 148;
+        }
+        auto it = cache.find(kernel);
+        if (it == cache.end()) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) !=
+                    cudaSuccess || per_sm < 1)
+                per_sm = 1;
+            cache[kernel] = per_sm;
+        } else {
+            per_sm = it->second;
+        }
+    }
+    long b = ceil_div(n, threads);
+    const long full = (long)nsm * per_sm;
+    if (b > full) b = full;
+    if (b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
 
 void *dalloc(size_t bytes)
 {

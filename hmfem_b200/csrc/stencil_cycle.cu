@@ -35,7 +35,7 @@ __device__ __forceinline__ void cell_ijk(unsigned s, unsigned nx, unsigned ny, i
 }
 
 template <class V> struct G7v {
-    const V *c, *px, *py, *pz;
+    const V *cf;  // slice-interleaved: a_cc, +x, +y, +z
     int nx, ny, nz;
 };
 
@@ -49,13 +49,13 @@ __device__ __forceinline__ T g7_row(T t, const G7v<V> &g, long s, int i, int j, 
     const bool hd = j > 0, hl = i > 0, hr = i < g.nx - 1, hu = j < g.ny - 1,
                ht = k < g.nz - 1, hb = k > 0;
     // all loads first, so they overlap
-    const T ad = hd ? (T)ld(g.py, s - nx) : (T)0, xd = hd ? x(s - nx) : (T)0;
-    const T al = hl ? (T)ld(g.px, s - 1) : (T)0, xl = hl ? x(s - 1) : (T)0;
-    const T ac = (T)ld(g.c, s), xc = x(s);
-    const T ar = hr ? (T)ld(g.px, s) : (T)0, xr = hr ? x(s + 1) : (T)0;
-    const T au = hu ? (T)ld(g.py, s) : (T)0, xu = hu ? x(s + nx) : (T)0;
-    const T at = ht ? (T)ld(g.pz, s) : (T)0, xt = ht ? x(s + nxy) : (T)0;
-    const T ab = hb ? (T)ld(g.pz, s - nxy) : (T)0, xb = hb ? x(s - nxy) : (T)0;
+    const T ad = hd ? (T)ld(g.cf, slice_at(s - nx, 2, 4)) : (T)0, xd = hd ? x(s - nx) : (T)0;
+    const T al = hl ? (T)ld(g.cf, slice_at(s - 1, 1, 4)) : (T)0, xl = hl ? x(s - 1) : (T)0;
+    const T ac = (T)ld(g.cf, slice_at(s, 0, 4)), xc = x(s);
+    const T ar = hr ? (T)ld(g.cf, slice_at(s, 1, 4)) : (T)0, xr = hr ? x(s + 1) : (T)0;
+    const T au = hu ? (T)ld(g.cf, slice_at(s, 2, 4)) : (T)0, xu = hu ? x(s + nx) : (T)0;
+    const T at = ht ? (T)ld(g.cf, slice_at(s, 3, 4)) : (T)0, xt = ht ? x(s + nxy) : (T)0;
+    const T ab = hb ? (T)ld(g.cf, slice_at(s - nxy, 3, 4)) : (T)0, xb = hb ? x(s - nxy) : (T)0;
     auto acc = [&](T a, T xv) {
         const T p = A::mul(a, xv);
         t = SUB ? A::sub(t, p) : A::add(t, p);
@@ -77,57 +77,65 @@ __device__ __forceinline__ int g7_degree(int i, int j, int k, int nx, int ny, in
 }
 
 template <class V> struct G19v {
-    const V *v;
-    long n;  // coarse rows (the array stride)
+    const V *v;   // slice-interleaved, 19 per row
+    int n;        // coarse rows
     int nx, ny, nz;
 };
 
-// t -/+ sum over level-1 row c of a_cq x(q), ascending q
+// t -/+ sum over level-1 row c of a_cq x(q), ascending q.  No bounds test:
+// the coefficient of a neighbour outside the grid is stored as +0, and its
+// x index is clamped into the vector, so it adds t -/+ 0 * x = t (x finite;
+// the SELL kernels' zero padding behaves the same).  Entries are loaded in
+// chunks of five so the gathers overlap without holding all 19 in
+// registers; the summation order is unchanged.
 template <class T, bool SUB, class V, class X>
-__device__ __forceinline__ T g19_row(T t, const G19v<V> &g, long c, X x)
+__device__ __forceinline__ T g19_row(T t, const G19v<V> &g, int c, X x)
 {
     using A = Ar<T>;
-    const int hx = g.nx >> 1;
-    const long row = c / hx;
-    const int j = (int)(row % g.ny), k = (int)(row / g.ny);
-    const int i = 2 * (int)(c - row * hx) + ((j + k) & 1);
-    const long s = i + row * g.nx, nxy = (long)g.nx * g.ny;
-    T a[kQ19], xv[kQ19];
-    bool on[kQ19];
+    constexpr int CH = 5;
+    const unsigned hx = (unsigned)g.nx >> 1, cu = (unsigned)c;
+    const unsigned row = cu / hx, k = row / (unsigned)g.ny, j = row - k * (unsigned)g.ny;
+    const int s = 2 * c + (int)((j + k) & 1);  // fine index (nx even)
+    const int nx = g.nx, nxy = g.nx * g.ny, last = g.n - 1;
 #pragma unroll
-    for (int q = 0; q < kQ19; q++) {
-        const int ii = i + q19x(q), jj = j + q19y(q), kk = k + q19z(q);
-        on[q] = ii >= 0 && ii < g.nx && jj >= 0 && jj < g.ny && kk >= 0 && kk < g.nz;
-        a[q] = on[q] ? (T)ld(g.v, q * g.n + c) : (T)0;
-        xv[q] = on[q] ? x((s + q19_lin(q, g.nx, nxy)) >> 1) : (T)0;
-    }
+    for (int q0 = 0; q0 < kQ19; q0 += CH) {
+        T a[CH], xv[CH];
 #pragma unroll
-    for (int q = 0; q < kQ19; q++) {
-        if (!on[q]) continue;
-        const T p = A::mul(a[q], xv[q]);
-        t = SUB ? A::sub(t, p) : A::add(t, p);
+        for (int d = 0; d < CH; d++) {
+            const int q = q0 + d;
+            if (q < kQ19) {
+                a[d] = (T)ld(g.v, slice_at(c, q, kQ19));
+                int e = (s + q19x(q) + q19y(q) * nx + q19z(q) * nxy) >> 1;
+                e = e < 0 ? 0 : (e > last ? last : e);
+                xv[d] = x(e);
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < CH; d++) {
+            if (q0 + d < kQ19) {
+                const T p = A::mul(a[d], xv[d]);
+                t = SUB ? A::sub(t, p) : A::add(t, p);
+            }
+        }
     }
     return t;
 }
 
 // ---- level 0 ------------------------------------------------------------
 
-// u = w D^-1 f;  r = f - A u;  rs = r / |P row|  (k_pre on the stencil)
+// r = f - A u (u the seeded first Jacobi iterate);  rs = r / |P row|
+// (k_pre on the stencil)
 template <class T, class V>
 __global__ void __launch_bounds__(256)
-k_g7_pre(G7v<V> g, int n, const T *__restrict__ f, const T *__restrict__ dinv, T w,
-         T *__restrict__ u, T *__restrict__ rs, const Ctl *ctl)
+k_g7_pre(G7v<V> g, int n, const T *__restrict__ f, const T *__restrict__ u,
+         T *__restrict__ rs, const Ctl *ctl)
 {
     if (finished(ctl)) return;
     using A = Ar<T>;
     GRID_STRIDE(s, n) {
         int i, j, k;
         cell_ijk((unsigned)s, g.nx, g.ny, i, j, k);
-        const T fr = f[s];
-        const T t = g7_row<T, true>(fr, g, s, i, j, k, [&](long c) {
-            return A::mul(A::mul(w, f[c]), dinv[c]);
-        });
-        u[s] = A::mul(A::mul(w, fr), dinv[s]);
+        const T t = g7_row<T, true>(f[s], g, s, i, j, k, [&](long c) { return u[c]; });
         const int pc = ((i + j + k) & 1) ? g7_degree(i, j, k, g.nx, g.ny, g.nz) : 1;
         rs[s] = pc == 1 ? t : A::div(t, (T)pc);
     }
@@ -137,18 +145,18 @@ k_g7_pre(G7v<V> g, int n, const T *__restrict__ f, const T *__restrict__ dinv, T
 template <class T>
 __global__ void __launch_bounds__(256)
 k_g7_restrict(int nx, int ny, int nz, const int *__restrict__ cid,
-              const T *__restrict__ rs, T *__restrict__ fc, const Ctl *ctl)
+              const T *__restrict__ rs, T *__restrict__ fc, Seed<T> sd, const Ctl *ctl)
 {
     if (finished(ctl)) return;
     using A = Ar<T>;
-    const int hx = (nx + 1) >> 1;
+    const unsigned hx = (unsigned)(nx + 1) >> 1;
     const long nxy = (long)nx * ny, m = (long)hx * ny * nz;
     GRID_STRIDE(t, m) {
-        const long r = t / hx;
-        const int j = (int)(r % ny), k = (int)(r / ny);
-        const int i = 2 * (int)(t - r * hx) + ((j + k) & 1);
+        const unsigned tu = (unsigned)t, r = tu / hx, kk0 = r / (unsigned)ny;
+        const int j = (int)(r - kk0 * (unsigned)ny), k = (int)kk0;
+        const int i = 2 * (int)(tu - r * hx) + ((j + k) & 1);
         if (i >= nx) continue;
-        const long s = i + r * nx;
+        const long s = i + (long)r * nx;
         const T vb = k > 0 ? rs[s - nxy] : (T)0, vd = j > 0 ? rs[s - nx] : (T)0;
         const T vl = i > 0 ? rs[s - 1] : (T)0, vc = rs[s];
         const T vr = i < nx - 1 ? rs[s + 1] : (T)0, vu = j < ny - 1 ? rs[s + nx] : (T)0;
@@ -161,7 +169,9 @@ k_g7_restrict(int nx, int ny, int nz, const int *__restrict__ cid,
         if (i < nx - 1) acc = A::add(acc, vr);
         if (j < ny - 1) acc = A::add(acc, vu);
         if (k < nz - 1) acc = A::add(acc, vt);
-        fc[cid[s]] = acc;
+        const int e = cid[s];
+        fc[e] = acc;
+        sd.put(e, acc);
     }
 }
 
@@ -255,7 +265,7 @@ k_g7_spmv(G7v<double> g, int n, const double *__restrict__ x, double *__restrict
 // r = b - A x; (r, r); (b, b)   (k_resid on the stencil)
 __global__ void __launch_bounds__(256)
 k_g7_resid(G7v<double> g, int n, const double *__restrict__ b, const double *__restrict__ x,
-           double *__restrict__ r, Ctl *ctl, double *part, int init)
+           double *__restrict__ r, Ctl *ctl, double *part, int init, Seed<double> sd)
 {
     if (init == 0 && (finished(ctl) || !ctl->check)) return;
     double rr = 0.0, bb = 0.0;
@@ -266,6 +276,7 @@ k_g7_resid(G7v<double> g, int n, const double *__restrict__ b, const double *__r
         const double bi = b[s];
         const double ri = dsub(bi, a);
         r[s] = ri;
+        if (init != 2) sd.put(s, ri);
         rr += ri * ri;
         bb += bi * bi;
     }
@@ -279,18 +290,13 @@ k_g7_resid(G7v<double> g, int n, const double *__restrict__ b, const double *__r
 
 template <class T, class V>
 __global__ void __launch_bounds__(256)
-k_g19_pre(G19v<V> g, const T *__restrict__ f, const T *__restrict__ dinv, T w,
-          const int *__restrict__ prow, T *__restrict__ u, T *__restrict__ rs,
-          const Ctl *ctl)
+k_g19_pre(G19v<V> g, const T *__restrict__ f, const T *__restrict__ u,
+          const int *__restrict__ prow, T *__restrict__ rs, const Ctl *ctl)
 {
     if (finished(ctl)) return;
     using A = Ar<T>;
     GRID_STRIDE(c, g.n) {
-        const T fr = f[c];
-        const T t = g19_row<T, true>(fr, g, c, [&](long q) {
-            return A::mul(A::mul(w, f[q]), dinv[q]);
-        });
-        u[c] = A::mul(A::mul(w, fr), dinv[c]);
+        const T t = g19_row<T, true>(f[c], g, (int)c, [&](long q) { return u[q]; });
         const int pc = prow[c + 1] - prow[c];
         rs[c] = pc == 1 ? t : A::div(t, (T)pc);
     }
@@ -305,7 +311,7 @@ k_g19_post(G19v<V> g, const T *__restrict__ f, const T *__restrict__ dinv, T w,
     using A = Ar<T>;
     GRID_STRIDE(c, g.n) {
         const T fr = f[c];
-        const T t = g19_row<T, true>(fr, g, c, [&](long q) { return u[q]; });
+        const T t = g19_row<T, true>(fr, g, (int)c, [&](long q) { return u[q]; });
         uo[c] = A::add(u[c], A::mul(A::mul(w, t), dinv[c]));
     }
 }
@@ -313,7 +319,7 @@ k_g19_post(G19v<V> g, const T *__restrict__ f, const T *__restrict__ dinv, T w,
 __global__ void __launch_bounds__(256)
 k_g19_spmv(G19v<double> g, const double *__restrict__ x, double *__restrict__ y)
 {
-    GRID_STRIDE(c, g.n) y[c] = g19_row<double, false>(0.0, g, c, [&](long q) { return x[q]; });
+    GRID_STRIDE(c, g.n) y[c] = g19_row<double, false>(0.0, g, (int)c, [&](long q) { return x[q]; });
 }
 
 // ---- setup ----------------------------------------------------------------
@@ -323,8 +329,7 @@ k_g19_spmv(G19v<double> g, const double *__restrict__ x, double *__restrict__ y)
 // a_{c,c+e} == a_{c+e,c} for the three + directions
 __global__ void k_g7_extract(int nx, int ny, int nz, const int *__restrict__ rowptr,
                              const int *__restrict__ col, const double *__restrict__ val,
-                             double *c, double *px, double *py, double *pz, float *c32,
-                             float *px32, float *py32, float *pz32, int *bad)
+                             double *cf, float *cf32, int *bad)
 {
     const long nxy = (long)nx * ny, n = nxy * nz;
     GRID_STRIDE(s, n) {
@@ -359,8 +364,12 @@ __global__ void k_g7_extract(int nx, int ny, int nz, const int *__restrict__ row
             ok = ok && col[pt] == (int)q && col[oq] == (int)s &&
                  __double_as_longlong(val[oq]) == __double_as_longlong(vt);
         }
-        c[s] = vc; px[s] = vr; py[s] = vu; pz[s] = vt;
-        if (c32) { c32[s] = (float)vc; px32[s] = (float)vr; py32[s] = (float)vu; pz32[s] = (float)vt; }
+        const double v4[4] = {vc, vr, vu, vt};
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            cf[slice_at(s, a, 4)] = v4[a];
+            if (cf32) cf32[slice_at(s, a, 4)] = (float)v4[a];
+        }
         if (!ok) atomicOr(bad, 1);
     }
 }
@@ -382,19 +391,13 @@ int nb(long n)
 }
 
 template <class V> G7v<V> g7v(const Grid7 &g);
-template <> G7v<double> g7v<double>(const Grid7 &g)
-{
-    return {g.c, g.px, g.py, g.pz, g.nx, g.ny, g.nz};
-}
-template <> G7v<float> g7v<float>(const Grid7 &g)
-{
-    return {g.c32, g.px32, g.py32, g.pz32, g.nx, g.ny, g.nz};
-}
+template <> G7v<double> g7v<double>(const Grid7 &g) { return {g.cf, g.nx, g.ny, g.nz}; }
+template <> G7v<float> g7v<float>(const Grid7 &g) { return {g.cf32, g.nx, g.ny, g.nz}; }
 
-template <class V> G19v<V> g19v(const Grid19 &g, long n);
-template <> G19v<double> g19v<double>(const Grid19 &g, long n) { return {g.v, n, g.nx, g.ny, g.nz}; }
-template <> G19v<float> g19v<float>(const Grid19 &g, long n) { return {g.v32, n, g.nx, g.ny, g.nz}; }
-template <> G19v<__nv_bfloat16> g19v<__nv_bfloat16>(const Grid19 &g, long n)
+template <class V> G19v<V> g19v(const Grid19 &g, int n);
+template <> G19v<double> g19v<double>(const Grid19 &g, int n) { return {g.v, n, g.nx, g.ny, g.nz}; }
+template <> G19v<float> g19v<float>(const Grid19 &g, int n) { return {g.v32, n, g.nx, g.ny, g.nz}; }
+template <> G19v<__nv_bfloat16> g19v<__nv_bfloat16>(const Grid19 &g, int n)
 {
     return {g.v16, n, g.nx, g.ny, g.nz};
 }
@@ -409,8 +412,8 @@ bool g19_applies(int nx, int ny, int nz)
 
 void g7_free(Grid7 &g)
 {
-    dfree(g.c); dfree(g.px); dfree(g.py); dfree(g.pz);
-    dfree(g.c32); dfree(g.px32); dfree(g.py32); dfree(g.pz32);
+    dfree(g.cf);
+    dfree(g.cf32);
     g = Grid7();
 }
 
@@ -427,16 +430,15 @@ int g7_build(Level &L, int nx, int ny, int nz, bool f32, cudaStream_t st, int *d
     if (n != L.A.n || n <= 0) return HMFEM_OK;
     Grid7 g;
     g.nx = nx; g.ny = ny; g.nz = nz;
-    double **d64[4] = {&g.c, &g.px, &g.py, &g.pz};
-    float **d32[4] = {&g.c32, &g.px32, &g.py32, &g.pz32};
-    for (int a = 0; a < 4; a++) {
-        *d64[a] = (double *)dalloc(sizeof(double) * n);
-        if (f32) *d32[a] = (float *)dalloc(sizeof(float) * n);
-        if (!*d64[a] || (f32 && !*d32[a])) { g7_free(g); return HMFEM_E_CUDA; }
-    }
+    const long long m = slice_len(n, 4);
+    g.cf = (double *)dalloc(sizeof(double) * m);
+    if (f32) g.cf32 = (float *)dalloc(sizeof(float) * m);
+    if (!g.cf || (f32 && !g.cf32)) { g7_free(g); return HMFEM_E_CUDA; }
+    HM_CUDA(cudaMemsetAsync(g.cf, 0, sizeof(double) * m, st));  // tail of the last slice
+    if (f32) HM_CUDA(cudaMemsetAsync(g.cf32, 0, sizeof(float) * m, st));
     HM_CUDA(cudaMemsetAsync(dwork, 0, sizeof(int), st));
-    k_g7_extract<<<nb(n), 256, 0, st>>>(nx, ny, nz, L.A.rowptr, L.A.col, L.A.val, g.c, g.px,
-                                        g.py, g.pz, g.c32, g.px32, g.py32, g.pz32, dwork);
+    k_g7_extract<<<nb(n), 256, 0, st>>>(nx, ny, nz, L.A.rowptr, L.A.col, L.A.val, g.cf,
+                                        g.cf32, dwork);
     HM_LAUNCHED();
     int bad = 0;
     HM_CUDA(cudaMemcpyAsync(&bad, dwork, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -448,7 +450,7 @@ int g7_build(Level &L, int nx, int ny, int nz, bool f32, cudaStream_t st, int *d
 
 int g19_lowp(Grid19 &g, int n, bool f32, bool bf16, cudaStream_t st)
 {
-    const long m = (long)kQ19 * n;
+    const long m = (long)slice_len(n, kQ19);
     if (f32 && !g.v32) {
         g.v32 = (float *)dalloc(sizeof(float) * m);
         if (!g.v32) return HMFEM_E_CUDA;
@@ -467,21 +469,23 @@ int g19_lowp(Grid19 &g, int n, bool f32, bool bf16, cudaStream_t st)
 // ---- launchers used by the cycle and the CG --------------------------------
 
 template <class T, class V>
-int g7_pre(const Level &L, const T *f, const T *dinv, T w, T *u, T *rs, const Ctl *ctl,
-            cudaStream_t st)
+int g7_pre(const Level &L, const T *f, const T *u, T *rs, const Ctl *ctl, cudaStream_t st)
 {
     const int n = L.A.n;
-    k_g7_pre<T, V><<<nb(n), 256, 0, st>>>(g7v<V>(L.g7), n, f, dinv, w, u, rs, ctl);
+    const int nblk = occ_blocks((const void *)k_g7_pre<T, V>, n, 256, kRedBlocks);
+    k_g7_pre<T, V><<<nblk, 256, 0, st>>>(g7v<V>(L.g7), n, f, u, rs, ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
 
 template <class T>
-int g7_restrict(const Level &L, const T *rs, T *fc, const Ctl *ctl, cudaStream_t st)
+int g7_restrict(const Level &L, const T *rs, T *fc, Seed<T> sd, const Ctl *ctl,
+                cudaStream_t st)
 {
     const Grid7 &g = L.g7;
     const long m = (long)((g.nx + 1) >> 1) * g.ny * g.nz;
-    k_g7_restrict<T><<<nb(m), 256, 0, st>>>(g.nx, g.ny, g.nz, L.cid, rs, fc, ctl);
+    const int nblk = occ_blocks((const void *)k_g7_restrict<T>, m, 256, kRedBlocks);
+    k_g7_restrict<T><<<nblk, 256, 0, st>>>(g.nx, g.ny, g.nz, L.cid, rs, fc, sd, ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -490,7 +494,8 @@ template <class T>
 int g7_prolong(const Level &L, const T *uc, T *u, const Ctl *ctl, cudaStream_t st)
 {
     const Grid7 &g = L.g7;
-    k_g7_prolong<T><<<nb(L.A.n), 256, 0, st>>>(g.nx, g.ny, g.nz, L.cid, uc, u, ctl);
+    const int nblk = occ_blocks((const void *)k_g7_prolong<T>, L.A.n, 256, kRedBlocks);
+    k_g7_prolong<T><<<nblk, 256, 0, st>>>(g.nx, g.ny, g.nz, L.cid, uc, u, ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -500,7 +505,8 @@ int g7_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo, C
              double *part, int first, cudaStream_t st)
 {
     const int n = L.A.n;
-    k_g7_post<T, V, DOT><<<nb(n), 256, 0, st>>>(g7v<V>(L.g7), n, f, dinv, w, u, uo, ctl,
+    const int nblk = occ_blocks((const void *)k_g7_post<T, V, DOT>, n, 256, kRedBlocks);
+    k_g7_post<T, V, DOT><<<nblk, 256, 0, st>>>(g7v<V>(L.g7), n, f, dinv, w, u, uo, ctl,
                                                 part, first);
     HM_LAUNCHED();
     return HMFEM_OK;
@@ -510,16 +516,18 @@ int g7_spmv_dot(const Level &L, const double *x, double *y, Ctl *ctl, double *pa
                  cudaStream_t st)
 {
     const int n = L.A.n;
-    k_g7_spmv_dot<<<nb(n), 256, 0, st>>>(g7v<double>(L.g7), n, x, y, ctl, part);
+    const int nblk = occ_blocks((const void *)k_g7_spmv_dot, n, 256, kRedBlocks);
+    k_g7_spmv_dot<<<nblk, 256, 0, st>>>(g7v<double>(L.g7), n, x, y, ctl, part);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
 
 int g7_resid(const Level &L, const double *b, const double *x, double *r, Ctl *ctl,
-              double *part, int init, cudaStream_t st)
+             double *part, int init, Seed<double> sd, cudaStream_t st)
 {
     const int n = L.A.n;
-    k_g7_resid<<<nb(n), 256, 0, st>>>(g7v<double>(L.g7), n, b, x, r, ctl, part, init);
+    const int nblk = occ_blocks((const void *)k_g7_resid, n, 256, kRedBlocks);
+    k_g7_resid<<<nblk, 256, 0, st>>>(g7v<double>(L.g7), n, b, x, r, ctl, part, init, sd);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -527,17 +535,18 @@ int g7_resid(const Level &L, const double *b, const double *x, double *r, Ctl *c
 int g7_spmv(const Level &L, const double *x, double *y, cudaStream_t st)
 {
     const int n = L.A.n;
-    k_g7_spmv<<<nb(n), 256, 0, st>>>(g7v<double>(L.g7), n, x, y);
+    const int nblk = occ_blocks((const void *)k_g7_spmv, n, 256, kRedBlocks);
+    k_g7_spmv<<<nblk, 256, 0, st>>>(g7v<double>(L.g7), n, x, y);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
 
 template <class T, class V>
-int g19_pre(const Level &L, const T *f, const T *dinv, T w, T *u, T *rs, const Ctl *ctl,
-             cudaStream_t st)
+int g19_pre(const Level &L, const T *f, const T *u, T *rs, const Ctl *ctl, cudaStream_t st)
 {
     const G19v<V> g = g19v<V>(L.g19, L.A.n);
-    k_g19_pre<T, V><<<nb(g.n), 256, 0, st>>>(g, f, dinv, w, L.P.rowptr, u, rs, ctl);
+    const int nblk = occ_blocks((const void *)k_g19_pre<T, V>, g.n, 256, kRedBlocks);
+    k_g19_pre<T, V><<<nblk, 256, 0, st>>>(g, f, u, L.P.rowptr, rs, ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -547,7 +556,8 @@ int g19_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo,
               const Ctl *ctl, cudaStream_t st)
 {
     const G19v<V> g = g19v<V>(L.g19, L.A.n);
-    k_g19_post<T, V><<<nb(g.n), 256, 0, st>>>(g, f, dinv, w, u, uo, ctl);
+    const int nblk = occ_blocks((const void *)k_g19_post<T, V>, g.n, 256, kRedBlocks);
+    k_g19_post<T, V><<<nblk, 256, 0, st>>>(g, f, dinv, w, u, uo, ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -555,46 +565,46 @@ int g19_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo,
 int g19_spmv(const Level &L, const double *x, double *y, cudaStream_t st)
 {
     const G19v<double> g = g19v<double>(L.g19, L.A.n);
-    k_g19_spmv<<<nb(g.n), 256, 0, st>>>(g, x, y);
+    const int nblk = occ_blocks((const void *)k_g19_spmv, g.n, 256, kRedBlocks);
+    k_g19_spmv<<<nblk, 256, 0, st>>>(g, x, y);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
 
-template int g7_pre<double, double>(const Level &, const double *, const double *, double,
-                                     double *, double *, const Ctl *, cudaStream_t);
-template int g7_pre<float, float>(const Level &, const float *, const float *, float,
-                                   float *, float *, const Ctl *, cudaStream_t);
-template int g7_restrict<double>(const Level &, const double *, double *, const Ctl *,
-                                  cudaStream_t);
-template int g7_restrict<float>(const Level &, const float *, float *, const Ctl *,
-                                 cudaStream_t);
+template int g7_pre<double, double>(const Level &, const double *, const double *, double *,
+                                    const Ctl *, cudaStream_t);
+template int g7_pre<float, float>(const Level &, const float *, const float *, float *,
+                                  const Ctl *, cudaStream_t);
+template int g7_restrict<double>(const Level &, const double *, double *, Seed<double>,
+                                 const Ctl *, cudaStream_t);
+template int g7_restrict<float>(const Level &, const float *, float *, Seed<float>,
+                                const Ctl *, cudaStream_t);
 template int g7_prolong<double>(const Level &, const double *, double *, const Ctl *,
-                                 cudaStream_t);
-template int g7_prolong<float>(const Level &, const float *, float *, const Ctl *,
                                 cudaStream_t);
+template int g7_prolong<float>(const Level &, const float *, float *, const Ctl *,
+                               cudaStream_t);
 template int g7_post<double, double, true>(const Level &, const double *, const double *,
+                                           double, const double *, double *, Ctl *,
+                                           double *, int, cudaStream_t);
+template int g7_post<double, double, false>(const Level &, const double *, const double *,
                                             double, const double *, double *, Ctl *,
                                             double *, int, cudaStream_t);
-template int g7_post<double, double, false>(const Level &, const double *, const double *,
-                                             double, const double *, double *, Ctl *,
-                                             double *, int, cudaStream_t);
 template int g7_post<float, float, false>(const Level &, const float *, const float *,
-                                           float, const float *, float *, Ctl *, double *,
-                                           int, cudaStream_t);
-template int g19_pre<double, double>(const Level &, const double *, const double *, double,
-                                      double *, double *, const Ctl *, cudaStream_t);
-template int g19_pre<float, float>(const Level &, const float *, const float *, float,
-                                    float *, float *, const Ctl *, cudaStream_t);
+                                          float, const float *, float *, Ctl *, double *,
+                                          int, cudaStream_t);
+template int g19_pre<double, double>(const Level &, const double *, const double *, double *,
+                                     const Ctl *, cudaStream_t);
+template int g19_pre<float, float>(const Level &, const float *, const float *, float *,
+                                   const Ctl *, cudaStream_t);
 template int g19_pre<float, __nv_bfloat16>(const Level &, const float *, const float *,
-                                            float, float *, float *, const Ctl *,
-                                            cudaStream_t);
+                                           float *, const Ctl *, cudaStream_t);
 template int g19_post<double, double>(const Level &, const double *, const double *,
-                                       double, const double *, double *, const Ctl *,
-                                       cudaStream_t);
+                                      double, const double *, double *, const Ctl *,
+                                      cudaStream_t);
 template int g19_post<float, float>(const Level &, const float *, const float *, float,
-                                     const float *, float *, const Ctl *, cudaStream_t);
+                                    const float *, float *, const Ctl *, cudaStream_t);
 template int g19_post<float, __nv_bfloat16>(const Level &, const float *, const float *,
-                                             float, const float *, float *, const Ctl *,
-                                             cudaStream_t);
+                                            float, const float *, float *, const Ctl *,
+                                            cudaStream_t);
 
 }  // namespace hm
