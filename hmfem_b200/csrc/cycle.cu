@@ -6,9 +6,16 @@
 // precision preconditioner) use FMA.  Every kernel takes the CG control
 // block and returns at once when the solve is already finished, so a
 // captured iteration can be replayed past convergence at no cost.
+#include <cstdlib>
+
 #include "cycle.cuh"
 
 namespace hm {
+
+int g_pdl = [] {
+    const char *e = getenv("HMFEM_PDL");
+    return e ? atoi(e) : 1;
+}();
 
 // t - sum_k a_k x(c_k) (SUB) or t + sum_k a_k x(c_k) over one SELL-32 row
 // (entries at o, o+32, ...), in stored order.  Column indices, values and
@@ -55,6 +62,7 @@ k_pre(const long long *__restrict__ sptr, const int *__restrict__ scol,
       const T *__restrict__ u, const int *__restrict__ prow, T *__restrict__ rs,
       const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     GRID_STRIDE(r, n) {
@@ -74,6 +82,7 @@ k_pre(const long long *__restrict__ sptr, const int *__restrict__ scol,
 template <class T>
 __global__ void k_seed(int n, const T *__restrict__ f, Seed<T> sd)
 {
+    PDL_ENTRY();
     GRID_STRIDE(i, n) sd.put(i, f[i]);
 }
 
@@ -84,6 +93,7 @@ __global__ void __launch_bounds__(256)
 k_restrict(const int *__restrict__ rrow, const int *__restrict__ rcol, int nc,
            const T *__restrict__ rs, T *__restrict__ fc, Seed<T> sd, const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     GRID_STRIDE(e, nc) {
@@ -100,6 +110,7 @@ __global__ void __launch_bounds__(256)
 k_prolong_add(const int *__restrict__ prow, const int *__restrict__ pcol, int n,
               const T *__restrict__ uc, T *__restrict__ u, const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     GRID_STRIDE(i, n) {
@@ -126,6 +137,7 @@ k_post(const long long *__restrict__ sptr, const int *__restrict__ scol,
        const T *__restrict__ dinv, T w, const T *__restrict__ u,
        T *__restrict__ uo, Ctl *ctl, double *part, int first)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     double dot = 0.0;
@@ -156,6 +168,7 @@ __global__ void __launch_bounds__(256)
 k_gs_init(int n, const signed char *__restrict__ color, const T *__restrict__ f,
           const T *__restrict__ dinv, T *__restrict__ u, const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     GRID_STRIDE(i, n) u[i] = color[i] == 0 ? A::mul(f[i], dinv[i]) : (T)0;
@@ -168,10 +181,12 @@ k_gs_init(int n, const signed char *__restrict__ color, const T *__restrict__ f,
 // returned to the group -- the order the oracle's row_dot8 reproduces.
 // Every thread of the warp must call this (a group with no row passes
 // a = e = 0).
-template <class T, class M>
+// CG: load x through L2 only (ld.global.cg) -- for a kernel that also
+// writes x from other blocks between grid barriers, where the read-only and
+// L1 paths could return stale values.
+template <class T, class M, bool CG = false>
 __device__ __forceinline__ T row_dot8(int a, int e, const int *__restrict__ col,
-                                      const M *__restrict__ val,
-                                      const T *__restrict__ x, int g)
+                                      const M *__restrict__ val, const T *x, int g)
 {
     using A = Ar<T>;
     T p = (T)0;
@@ -185,7 +200,8 @@ __device__ __forceinline__ T row_dot8(int a, int e, const int *__restrict__ col,
             v[q] = k < e ? (T)ld(val, k) : (T)0;
         }
 #pragma unroll
-        for (int q = 0; q < 4; q++) xv[q] = k0 + 8 * q < e ? x[c[q]] : (T)0;
+        for (int q = 0; q < 4; q++)
+            xv[q] = k0 + 8 * q < e ? (CG ? __ldcg(x + c[q]) : x[c[q]]) : (T)0;
 #pragma unroll
         for (int q = 0; q < 4; q++)
             if (k0 + 8 * q < e) p = A::add(p, A::mul(v[q], xv[q]));
@@ -204,6 +220,7 @@ k_gs_sweep(const int *__restrict__ rowptr, const int *__restrict__ col,
            long r1, const T *__restrict__ f, const T *__restrict__ dinv,
            T *__restrict__ u, const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     const int g = threadIdx.x & 7;
@@ -228,6 +245,7 @@ k_resid_rs(const int *__restrict__ rowptr, const int *__restrict__ col,
            const T *__restrict__ u, const int *__restrict__ prow,
            T *__restrict__ rs, const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     const int g = threadIdx.x & 7;
@@ -246,12 +264,126 @@ k_resid_rs(const int *__restrict__ rowptr, const int *__restrict__ col,
     }
 }
 
+// ---- one launch per Gauss-Seidel sweep -----------------------------------
+//
+// The colours of a sweep run in one cooperative launch (every block
+// resident), separated by a grid barrier, instead of one launch per colour.
+// Row work and arithmetic are those of k_gs_init / k_gs_sweep / k_resid_rs,
+// so results are bit-identical to them.
+
+// Grid barrier over bar = {arrivals, generation, error}.  The wait is
+// bounded: after kBarrierPolls polls the block flags bar[2] (and the CG
+// control block, which then reports HMFEM_E_TIMEOUT); every block that sees
+// the flag leaves, so a failed barrier never hangs the grid.
+constexpr unsigned kBarrierPolls = 1u << 24;
+
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, Ctl *ctl)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *vb = bar;
+        const unsigned gen = vb[1];
+        __threadfence();
+        if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        } else {
+            unsigned polls = 0;
+            while (vb[1] == gen && vb[2] == 0u) {
+                if (++polls > kBarrierPolls) {
+                    atomicExch(&bar[2], 1u);
+                    if (ctl) { ctl->status = HMFEM_E_TIMEOUT; ctl->done = 1; }
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ((volatile unsigned *)bar)[2] == 0u;
+}
+
+// rows [r0, r1) of crows, four per warp, eight threads per row
+template <class T, class M>
+__device__ __forceinline__ void gs_colour(const int *__restrict__ rowptr,
+                                          const int *__restrict__ col,
+                                          const M *__restrict__ val,
+                                          const int *__restrict__ crows, int r0, int r1,
+                                          const T *__restrict__ f,
+                                          const T *__restrict__ dinv, T *u)
+{
+    using A = Ar<T>;
+    const int g = threadIdx.x & 7;
+    const long nw = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long w = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; r0 + 4 * w < r1;
+         w += nw) {
+        const long t = r0 + 4 * w + ((threadIdx.x & 31) >> 3);
+        const bool on = t < r1;
+        const int row = on ? crows[t] : 0;
+        const int a = on ? rowptr[row] : 0, e = on ? rowptr[row + 1] : 0;
+        const T sum = row_dot8<T, M, true>(a, e, col, val, u, g);
+        if (on && g == 0)
+            u[row] = A::add(__ldcg(u + row), A::mul(A::sub(f[row], sum), dinv[row]));
+    }
+}
+
+// Pre-smoothing of a Gauss-Seidel level: forward sweep from zero (colour 0
+// = D^-1 f, then colours 1..nc-1), then rs = (f - A u) / |P row|.
+template <class T, class M>
+__global__ void __launch_bounds__(512)
+k_gs_pre_fused(const int *__restrict__ rowptr, const int *__restrict__ col,
+               const M *__restrict__ val, int n, const signed char *__restrict__ color,
+               const int *__restrict__ crows, const int *__restrict__ cslot, int ncolors,
+               const T *__restrict__ f, const T *__restrict__ dinv, T *u,
+               const int *__restrict__ prow, T *__restrict__ rs, unsigned *bar, Ctl *ctl)
+{
+    if (finished(ctl) || ((volatile unsigned *)bar)[2]) return;
+    using A = Ar<T>;
+    GRID_STRIDE(i, n) u[i] = color[i] == 0 ? A::mul(f[i], dinv[i]) : (T)0;
+    for (int c = 1; c < ncolors; c++) {
+        if (!grid_barrier(bar, ctl)) return;
+        gs_colour<T>(rowptr, col, val, crows, cslot[c], cslot[c + 1], f, dinv, u);
+    }
+    if (!grid_barrier(bar, ctl)) return;
+    const int g = threadIdx.x & 7;
+    const long nw = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long w = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; 4 * w < n; w += nw) {
+        const long r = 4 * w + ((threadIdx.x & 31) >> 3);
+        const bool on = r < n;
+        const int a = on ? rowptr[r] : 0, e = on ? rowptr[r + 1] : 0;
+        const T sum = row_dot8<T, M, true>(a, e, col, val, u, g);
+        if (on && g == 0) {
+            const T t = A::sub(f[r], sum);
+            const int pc = prow[r + 1] - prow[r];
+            rs[r] = pc == 1 ? t : A::div(t, (T)pc);
+        }
+    }
+}
+
+// Post-smoothing of a Gauss-Seidel level: backward sweep, colours nc-1..0.
+template <class T, class M>
+__global__ void __launch_bounds__(512)
+k_gs_post_fused(const int *__restrict__ rowptr, const int *__restrict__ col,
+                const M *__restrict__ val, const int *__restrict__ crows,
+                const int *__restrict__ cslot, int ncolors, const T *__restrict__ f,
+                const T *__restrict__ dinv, T *u, unsigned *bar, Ctl *ctl)
+{
+    if (finished(ctl) || ((volatile unsigned *)bar)[2]) return;
+    for (int c = ncolors - 1; c >= 0; c--) {
+        gs_colour<T>(rowptr, col, val, crows, cslot[c], cslot[c + 1], f, dinv, u);
+        if (c > 0 && !grid_barrier(bar, ctl)) return;
+    }
+}
+
 // coarsest level: v = D^-1 f (diagonal_solver, amg.h:1074-1097)
 template <class T>
 __global__ void k_diag_solve(int n, const T *__restrict__ dinv,
                              const T *__restrict__ f, T *__restrict__ u,
                              const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     GRID_STRIDE(i, n) u[i] = A::mul(dinv[i], f[i]);
@@ -264,6 +396,7 @@ __global__ void __launch_bounds__(256)
 k_dense_solve(int n, const double *__restrict__ Minv, const T *__restrict__ f,
               T *__restrict__ u, const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     const int lane = threadIdx.x & 31;
     for (long i = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; i < n;
@@ -285,6 +418,7 @@ k_resid(const long long *__restrict__ sptr, const int *__restrict__ scol,
         const double *__restrict__ x, double *__restrict__ r, Ctl *ctl,
         double *part, int init, Seed<double> sd)
 {
+    PDL_ENTRY();
     // init: 1 = start of the solve, 0 = convergence check (residual
     // replacement), 2 = report only
     if (init == 0 && (finished(ctl) || !ctl->check)) return;
@@ -317,6 +451,7 @@ k_spmv_dot(const long long *__restrict__ sptr, const int *__restrict__ scol,
            const double *__restrict__ sval, int n, const double *__restrict__ s,
            double *__restrict__ v, Ctl *ctl, double *part)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     double d = 0.0;
     GRID_STRIDE(i, n) {
@@ -339,6 +474,7 @@ k_update(int n, double *__restrict__ x, double *__restrict__ r,
          const double *__restrict__ s, const double *__restrict__ v, Ctl *ctl,
          double *part, Seed<double> sd)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     const double al = ctl->alpha;
     double rr = 0.0;
@@ -361,6 +497,7 @@ k_update(int n, double *__restrict__ x, double *__restrict__ r,
 __global__ void __launch_bounds__(256)
 k_sdir(int n, double *__restrict__ s, const double *__restrict__ z, Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     const double be = ctl->beta;
     GRID_STRIDE(i, n) s[i] = dadd(dmul(s[i], be), z[i]);
@@ -377,6 +514,7 @@ k_finish_z(int n, const T *__restrict__ src, const double *__restrict__ r,
            const double *__restrict__ v, double *__restrict__ z, Ctl *ctl,
            double *part, int first, int flexible)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     double d1 = 0.0, d2 = 0.0;
     GRID_STRIDE(i, n) {
@@ -408,6 +546,7 @@ k_finish_z(int n, const T *__restrict__ src, const double *__restrict__ r,
 __global__ void k_demote(int n, const double *__restrict__ r, float *__restrict__ f,
                          Seed<float> sd, const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     GRID_STRIDE(i, n) {
         const float fi = (float)r[i];
@@ -433,6 +572,40 @@ static T *cycle_out(Solver &s, int l)
     const int last = s.nlevels - 1;
     if (l == last || l == s.direct_level || s.lv[l].gs) return s.vec_ua<T>(l);
     return s.vec_ub<T>(l);
+}
+
+// Cooperative launch (all blocks co-resident, as the fused sweeps' grid
+// barrier needs), capturable into the CG iteration's graph.
+template <class... KArgs, class... Args>
+static cudaError_t coop_launch(void (*kernel)(KArgs...), int grid, int block,
+                               cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// Blocks of a fused sweep: at most two 512-thread blocks per SM (fewer
+// arrivals per barrier), at most one 32-row pass over n rows, never more
+// than can be co-resident.
+static int gs_blocks(const void *kernel, long n)
+{
+    int nsm = 0, dev = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 512, 0);
+    if (per_sm > 2) per_sm = 2;
+    long b = ceil_div(n, 64);
+    const long full = (long)nsm * (per_sm > 0 ? per_sm : 1);
+    if (b > full) b = full;
+    return (int)(b < 1 ? 1 : b);
 }
 
 // The seed (first Jacobi iterate) a producer of level l's right-hand side
@@ -466,19 +639,19 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
     Ctl *ctl = s.ctl_active ? s.ctl : nullptr;
     T *f = s.vec_f<T>(l), *ua = s.vec_ua<T>(l), *ub = s.vec_ub<T>(l);
     if (l == s.direct_level) {
-        k_dense_solve<T><<<(int)ceil_div((long)n * 32, 256), 256, 0, st>>>(n, s.dense_L, f, ua,
+        launch_pdl(k_dense_solve<T>, (int)ceil_div((long)n * 32, 256), 256, st, n, s.dense_L, f, ua,
                                                                          ctl);
         HM_LAUNCHED();
         return HMFEM_OK;
     }
     if (l == last) {
-        k_diag_solve<T><<<nb(n), 256, 0, st>>>(n, s.vec_dtrue<T>(l), f, ua, ctl);
+        launch_pdl(k_diag_solve<T>, nb(n), 256, st, n, s.vec_dtrue<T>(l), f, ua, ctl);
         HM_LAUNCHED();
         return HMFEM_OK;
     }
     const T w = (T)s.opt.omega;
     if (!seeded && seed_of<T>(s, l).u) {
-        k_seed<T><<<nb(n), 256, 0, st>>>(n, f, seed_of<T>(s, l));
+        launch_pdl(k_seed<T>, nb(n), 256, st, n, f, seed_of<T>(s, l));
         HM_LAUNCHED();
     }
     const bool g7 = s.use_g7(l), g19 = s.use_g19(l);
@@ -494,18 +667,36 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
     auto sweep = [&](int c) {
         const long r0 = L.color_slot[c], r1 = L.color_slot[c + 1];
         csr_vals([&](auto vals) {
-            k_gs_sweep<T><<<nb(ceil_div(r1 - r0, 4) * 32), 256, 0, st>>>(
+            using M = typename std::remove_const<
+                typename std::remove_pointer<decltype(vals)>::type>::type;
+            launch_pdl(k_gs_sweep<T, M>, nb(ceil_div(r1 - r0, 4) * 32), 256, st,
                 L.A.rowptr, L.A.col, vals, L.crows, r0, r1, f, dt, ua, ctl);
             HM_COUNT();
         });
     };
     // ---- pre-smoothing + residual (scaled for the restriction)
-    if (L.gs) {
-        k_gs_init<T><<<nb(n), 256, 0, st>>>(n, L.color, f, dt, ua, ctl);
+    if (L.gs && s.opt.gs_fused) {
+        Ctl *cw = s.ctl_active ? s.ctl : nullptr;
+        cudaError_t le = cudaSuccess;
+        csr_vals([&](auto vals) {
+            using M = typename std::remove_const<
+                typename std::remove_pointer<decltype(vals)>::type>::type;
+            auto kern = k_gs_pre_fused<T, M>;
+            le = coop_launch(kern, gs_blocks((const void *)kern, n), 512, st, L.A.rowptr,
+                             L.A.col, vals, n, (const signed char *)L.color,
+                             (const int *)L.crows, (const int *)L.cslot, L.ncolors,
+                             (const T *)f, dt, ua, (const int *)L.P.rowptr, rs, s.gsbar, cw);
+            HM_COUNT();
+        });
+        HM_CUDA(le);
+    } else if (L.gs) {
+        launch_pdl(k_gs_init<T>, nb(n), 256, st, n, L.color, f, dt, ua, ctl);
         HM_COUNT();
         for (int c = 1; c < L.ncolors; c++) sweep(c);
         csr_vals([&](auto vals) {
-            k_resid_rs<T><<<nb(ceil_div(n, 4) * 32), 256, 0, st>>>(
+            using M = typename std::remove_const<
+                typename std::remove_pointer<decltype(vals)>::type>::type;
+            launch_pdl(k_resid_rs<T, M>, nb(ceil_div(n, 4) * 32), 256, st,
                 L.A.rowptr, L.A.col, vals, n, f, ua, L.P.rowptr, rs, ctl);
             HM_COUNT();
         });
@@ -516,7 +707,9 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
         else HM_CHECK((g19_pre<T, T>(L, f, ua, rs, ctl, st)));
     } else {
         with_vals<T>(s, L.S, l, [&](auto vals) {
-            k_pre<T><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, vals, n, f, ua,
+            using M = typename std::remove_const<
+                typename std::remove_pointer<decltype(vals)>::type>::type;
+            launch_pdl(k_pre<T, M>, nb(n), 256, st, L.S.sptr, L.S.col, vals, n, f, ua,
                                            L.P.rowptr, rs, ctl);
             HM_COUNT();
         });
@@ -525,7 +718,7 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
     if (g7) {
         HM_CHECK((g7_restrict<T>(L, rs, s.vec_f<T>(l + 1), seed_of<T>(s, l + 1), ctl, st)));
     } else {
-        k_restrict<T><<<nb(L.nc), 256, 0, st>>>(L.R.rowptr, L.R.col, L.nc, rs,
+        launch_pdl(k_restrict<T>, nb(L.nc), 256, st, L.R.rowptr, L.R.col, L.nc, rs,
                                                 s.vec_f<T>(l + 1), seed_of<T>(s, l + 1),
                                                 ctl);
         HM_LAUNCHED();
@@ -534,12 +727,25 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
     if (g7) {
         HM_CHECK((g7_prolong<T>(L, cycle_out<T>(s, l + 1), ua, ctl, st)));
     } else {
-        k_prolong_add<T><<<nb(n), 256, 0, st>>>(L.P.rowptr, L.P.col, n,
+        launch_pdl(k_prolong_add<T>, nb(n), 256, st, L.P.rowptr, L.P.col, n,
                                                 cycle_out<T>(s, l + 1), ua, ctl);
         HM_LAUNCHED();
     }
     // ---- post-smoothing
-    if (L.gs) {
+    if (L.gs && s.opt.gs_fused) {
+        Ctl *cw = s.ctl_active ? s.ctl : nullptr;
+        cudaError_t le = cudaSuccess;
+        csr_vals([&](auto vals) {
+            using M = typename std::remove_const<
+                typename std::remove_pointer<decltype(vals)>::type>::type;
+            auto kern = k_gs_post_fused<T, M>;
+            le = coop_launch(kern, gs_blocks((const void *)kern, n), 512, st, L.A.rowptr,
+                             L.A.col, vals, (const int *)L.crows, (const int *)L.cslot,
+                             L.ncolors, (const T *)f, dt, ua, s.gsbar, cw);
+            HM_COUNT();
+        });
+        HM_CUDA(le);
+    } else if (L.gs) {
         for (int c = L.ncolors - 1; c >= 0; c--) sweep(c);
     } else if (g7) {
         if constexpr (std::is_same<T, double>::value) {
@@ -552,16 +758,16 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
         if (bf16) HM_CHECK((g19_post<T, __nv_bfloat16>(L, f, dv, w, ua, ub, ctl, st)));
         else HM_CHECK((g19_post<T, T>(L, f, dv, w, ua, ub, ctl, st)));
     } else if (dot) {
-        k_post<T, T, true><<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, s.sval<T>(l), n,
+        launch_pdl(k_post<T, T, true>, nb(n), 256, st, L.S.sptr, L.S.col, s.sval<T>(l), n,
                                                    f, dv, w, ua, ub, s.ctl, s.part,
                                                    s.first_sigma);
         HM_COUNT();
     } else {
         with_vals<T>(s, L.S, l, [&](auto vals) {
-            k_post<T, typename std::remove_const<typename std::remove_pointer<
-                          decltype(vals)>::type>::type, false>
-                <<<nb(n), 256, 0, st>>>(L.S.sptr, L.S.col, vals, n, f, dv, w, ua, ub,
-                                        ctl, nullptr, 0);
+            using M = typename std::remove_const<
+                typename std::remove_pointer<decltype(vals)>::type>::type;
+            launch_pdl(k_post<T, M, false>, nb(n), 256, st, L.S.sptr, L.S.col, vals, n, f,
+                       dv, w, ua, ub, ctl, nullptr, 0);
             HM_COUNT();
         });
     }
@@ -600,18 +806,18 @@ int cg_precondition(Solver &s, cudaStream_t st)
         // the V-cycle reads f[0] = r in place; z lands in ub[0] = s.z
         HM_CHECK(cycle_fp64(s, 0, st, !top_is_coarse, true));
         if (top_is_coarse) {
-            k_finish_z<double><<<nb(n), 256, 0, st>>>(n, L0.ua, s.r, s.v, s.z,
+            launch_pdl(k_finish_z<double>, nb(n), 256, st, n, L0.ua, s.r, s.v, s.z,
                                                       s.ctl, s.part,
                                                       s.first_sigma, 0);
             HM_LAUNCHED();
         }
         return HMFEM_OK;
     }
-    k_demote<<<nb(n), 256, 0, st>>>(n, s.r, L0.f32, seed_of<float>(s, 0), s.ctl);
+    launch_pdl(k_demote, nb(n), 256, st, n, s.r, L0.f32, seed_of<float>(s, 0), s.ctl);
     HM_LAUNCHED();
     HM_CHECK(cycle_fp32(s, 0, st, false, true));
     const float *z32 = top_is_coarse ? L0.ua32 : L0.ub32;
-    k_finish_z<float><<<nb(n), 256, 0, st>>>(n, z32, s.r, s.v, s.z, s.ctl,
+    launch_pdl(k_finish_z<float>, nb(n), 256, st, n, z32, s.r, s.v, s.z, s.ctl,
                                              s.part, s.first_sigma, 1);
     HM_LAUNCHED();
     return HMFEM_OK;
@@ -624,14 +830,14 @@ int cg_init(Solver &s, cudaStream_t st)
     if (s.use_g7(0)) {
         HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 1, cg_seed(s), st));
     } else {
-        k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
+        launch_pdl(k_resid, nb(n), 256, st, L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
                                        s.r, s.ctl, s.part, 1, cg_seed(s));
         HM_LAUNCHED();
     }
     s.first_sigma = 1;
     HM_CHECK(cg_precondition(s, st));
     s.first_sigma = 0;
-    k_sdir<<<nb(n), 256, 0, st>>>(n, s.s, s.z, s.ctl);
+    launch_pdl(k_sdir, nb(n), 256, st, n, s.s, s.z, s.ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -644,21 +850,21 @@ int cg_iteration(Solver &s, cudaStream_t st)
     if (g7) {
         HM_CHECK(g7_spmv_dot(L0, s.s, s.v, s.ctl, s.part, st));
     } else {
-        k_spmv_dot<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.s,
+        launch_pdl(k_spmv_dot, nb(n), 256, st, L0.S.sptr, L0.S.col, L0.S.val, n, s.s,
                                           s.v, s.ctl, s.part);
         HM_LAUNCHED();
     }
-    k_update<<<nb(n), 256, 0, st>>>(n, s.x, s.r, s.s, s.v, s.ctl, s.part, cg_seed(s));
+    launch_pdl(k_update, nb(n), 256, st, n, s.x, s.r, s.s, s.v, s.ctl, s.part, cg_seed(s));
     HM_LAUNCHED();
     if (g7) {
         HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 0, cg_seed(s), st));
     } else {
-        k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
+        launch_pdl(k_resid, nb(n), 256, st, L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
                                        s.r, s.ctl, s.part, 0, cg_seed(s));
         HM_LAUNCHED();
     }
     HM_CHECK(cg_precondition(s, st));
-    k_sdir<<<nb(n), 256, 0, st>>>(n, s.s, s.z, s.ctl);
+    launch_pdl(k_sdir, nb(n), 256, st, n, s.s, s.z, s.ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -671,7 +877,7 @@ int cg_final_residual(Solver &s, cudaStream_t st)
     if (s.use_g7(0)) {
         HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 2, Seed<double>{}, st));
     } else {
-        k_resid<<<nb(n), 256, 0, st>>>(L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
+        launch_pdl(k_resid, nb(n), 256, st, L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
                                        s.r, s.ctl, s.part, 2, Seed<double>{});
         HM_LAUNCHED();
     }
@@ -710,8 +916,34 @@ __global__ void k_fill_one(double *x, int n)
 //   7 post-smoother FP32 (level 0)  n*4*4 + n*4*4
 //   8 pre-smoother FP32 (level 1)   nnz*4 + n*(4 f + 4 u + 4 P-row + 4 rs)
 //   9 post-smoother FP32 (level 1)  nnz*4 + n*4*4
+// and 12: one whole V-cycle from level l in the solver's precision (bytes
+// reported 0); the difference between levels l and l+1 is level l's share.
 int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
 {
+    if (which == 12) {
+        if (l < 0 || l >= s.nlevels || reps < 1) return HMFEM_E_ARG;
+        cudaStream_t st = s.st;
+        s.ctl_active = false;
+        auto one = [&]() {
+            return s.opt.precision == 1 ? cycle_t<float>(s, l, st, false, false)
+                                        : cycle_t<double>(s, l, st, false, false);
+        };
+        HM_CHECK(one());
+        cudaEvent_t e0, e1;
+        HM_CUDA(cudaEventCreate(&e0));
+        HM_CUDA(cudaEventCreate(&e1));
+        HM_CUDA(cudaEventRecord(e0, st));
+        for (int i = 0; i < reps; i++) HM_CHECK(one());
+        HM_CUDA(cudaEventRecord(e1, st));
+        HM_CUDA(cudaEventSynchronize(e1));
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms = t / reps;
+        *bytes = 0;
+        return HMFEM_OK;
+    }
     if (l < 0 || l >= s.nlevels || reps < 1 || which < 0 || which > 9) return HMFEM_E_ARG;
     if (which >= 1 && l == s.nlevels - 1) return HMFEM_E_ARG;
     if (((which >= 3 && which <= 4) || which >= 6) && s.opt.precision != 1) return HMFEM_E_ARG;

@@ -1,5 +1,7 @@
 // cycle.cuh -- arithmetic helpers shared by the V-cycle translation units.
 #pragma once
+#include <utility>
+
 #include "solver.cuh"
 
 namespace hm {
@@ -23,6 +25,38 @@ __device__ __forceinline__ float ld(const float *p, long long i) { return __ldg(
 __device__ __forceinline__ float ld(const __nv_bfloat16 *p, long long i) { return __bfloat162float(p[i]); }
 
 __device__ __forceinline__ bool finished(const Ctl *c) { return c && *(volatile const int *)&c->done; }
+
+// Programmatic dependent launch: every solve-phase kernel is launched with
+// launch_pdl, so the next kernel in the stream can be scheduled while this
+// one drains; each such kernel calls pdl_wait() before touching memory its
+// predecessors wrote (griddepcontrol.wait returns once they completed and
+// their writes are visible; it returns at once for a plain launch), then
+// pdl_trigger() to let its own successor be scheduled early.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;"); }
+#define PDL_ENTRY()   \
+    do {              \
+        pdl_wait();   \
+        pdl_trigger(); \
+    } while (0)
+
+extern int g_pdl;  // 0: plain stream order (HMFEM_PDL=0)
+
+template <class... KArgs, class... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), int grid, int block, cudaStream_t st,
+                       Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = g_pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);  // error: cudaGetLastError
+}
 
 #define GRID_STRIDE(r, n)                                                     \
     for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < (n);       \

@@ -97,6 +97,7 @@ struct Level {
     signed char *color = nullptr;     // Jones-Plassmann colouring
     int *crows = nullptr;             // rows grouped by colour
     std::vector<long> color_slot;     // first row of each colour in crows
+    int *cslot = nullptr;             // the same offsets on the device
     float *aval32 = nullptr;          // CSR values in FP32 / BF16 (GS levels)
     __nv_bfloat16 *aval16 = nullptr;
 };

@@ -140,6 +140,12 @@ int color_level(Level &L, cudaStream_t st, int *dwork)
     off[0] = 0;
     for (int c = 0; c < nc; c++) off[c + 1] = off[c] + hh[c];
     dfree(key); dfree(row); dfree(skey); dfree(hist);
+    std::vector<int> off32(off.begin(), off.end());
+    L.cslot = (int *)dalloc(sizeof(int) * (nc + 1));
+    if (!L.cslot) return HMFEM_E_CUDA;
+    HM_CUDA(cudaMemcpyAsync(L.cslot, off32.data(), sizeof(int) * (nc + 1),
+                            cudaMemcpyHostToDevice, st));
+    HM_CUDA(cudaStreamSynchronize(st));
     L.crows = srow;          // rows by colour, ascending within a colour
     L.ncolors = nc;
     L.color_slot = off;      // first row of each colour in crows (+ end)

@@ -118,7 +118,7 @@ static void free_level_setup(Level &L, bool keep_matrix)
     free_csr(L.P); free_csr(L.R);
     dfree(L.f); dfree(L.ua); dfree(L.ub); dfree(L.rs);
     dfree(L.f32); dfree(L.ua32); dfree(L.ub32); dfree(L.rs32);
-    dfree(L.color); dfree(L.crows); dfree(L.aval32); dfree(L.aval16);
+    dfree(L.color); dfree(L.crows); dfree(L.cslot); dfree(L.aval32); dfree(L.aval16);
     g7_free(L.g7);
     g19_free(L.g19);
     Csr a = L.A;
@@ -358,6 +358,7 @@ int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out)
     c0.max_iter = s.opt.max_iter;
     c0.stop_rule = s.opt.stop_rule;
     HM_CUDA(cudaMemcpyAsync(s.ctl, &c0, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+    HM_CUDA(cudaMemsetAsync(s.gsbar, 0, sizeof(unsigned) * 4, st));
     cudaEvent_t e0, e1;
     HM_CUDA(cudaEventCreate(&e0));
     HM_CUDA(cudaEventCreate(&e1));
@@ -445,6 +446,7 @@ void hmfem_default_options(hmfem_options *o)
     o->min_coarse = 1;
     o->coarse_direct = 512;
     o->check_every = 2;
+    o->gs_fused = 0;
     o->verbose = 0;
 }
 
@@ -476,13 +478,15 @@ int hmfem_create(hmfem_solver **out, const hmfem_options *opt)
     s.part = (double *)hm::dalloc(sizeof(double) * hm::kRedBlocks * 2);
     s.dwork = (int *)hm::dalloc(sizeof(int) * 64);
     s.mm = (double *)hm::dalloc(sizeof(double) * 2);
+    s.gsbar = (unsigned *)hm::dalloc(sizeof(unsigned) * 4);
     if (cudaMallocHost(&s.ctl_host, 2 * sizeof(hm::Ctl)) != cudaSuccess ||
-        !s.ctl || !s.part || !s.dwork || !s.mm) {
+        !s.ctl || !s.part || !s.dwork || !s.mm || !s.gsbar) {
         hm::set_last_error("out of memory", __FILE__, __LINE__);
         hmfem_destroy(h);
         return HMFEM_E_CUDA;
     }
     cudaMemset(s.ctl, 0, sizeof(hm::Ctl));
+    cudaMemset(s.gsbar, 0, sizeof(unsigned) * 4);
     cudaDeviceSynchronize();
     *out = h;
     return HMFEM_OK;
@@ -499,6 +503,7 @@ int hmfem_destroy(hmfem_solver *h)
     for (int i = 0; i < 3; i++) hm::dfree(s.Kown[i]);
     for (int f = 0; f < 6; f++) hm::dfree(s.face[f]);
     hm::dfree(s.ctl); hm::dfree(s.part); hm::dfree(s.dwork); hm::dfree(s.mm);
+    hm::dfree(s.gsbar);
     hm::alloc_cache_release(s.cache);
     s.cache = nullptr;
     hm::set_alloc_context(s.st, nullptr);
@@ -807,9 +812,16 @@ int hmfem_vcycle(hmfem_solver *h, const double *f, double *u, int mem)
     HM_CHECK(hm::upload(s.r, f, n, mem, st));
     s.ctl_active = false;
     const bool top_coarse = s.nlevels == 1 || s.direct_level == 0;
+    HM_CUDA(cudaMemsetAsync(s.gsbar, 0, sizeof(unsigned) * 4, st));
     HM_CHECK(hm::cycle_fp64(s, 0, st, false, false));
     HM_CHECK(hm::download(u, (const double *)(top_coarse ? s.lv[0].ua : s.z), n, mem, st));
+    unsigned bar[4];
+    HM_CUDA(cudaMemcpyAsync(bar, s.gsbar, sizeof(bar), cudaMemcpyDeviceToHost, st));
     HM_CUDA(cudaStreamSynchronize(st));
+    if (bar[2]) {
+        hm::set_last_error("Gauss-Seidel grid barrier timed out", __FILE__, __LINE__);
+        return HMFEM_E_TIMEOUT;
+    }
     return HMFEM_OK;
 }
 

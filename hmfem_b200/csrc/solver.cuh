@@ -39,6 +39,7 @@ struct Solver {
     Ctl *ctl_host = nullptr;  // pinned, 2 slots
     double *part = nullptr;
     int *dwork = nullptr;
+    unsigned *gsbar = nullptr;  // grid barrier of the fused Gauss-Seidel sweeps
     bool ctl_active = false;
     int first_sigma = 0;
     cudaGraph_t graph = nullptr;

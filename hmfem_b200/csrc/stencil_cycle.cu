@@ -130,6 +130,7 @@ __global__ void __launch_bounds__(256)
 k_g7_pre(G7v<V> g, int n, const T *__restrict__ f, const T *__restrict__ u,
          T *__restrict__ rs, const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     GRID_STRIDE(s, n) {
@@ -147,6 +148,7 @@ __global__ void __launch_bounds__(256)
 k_g7_restrict(int nx, int ny, int nz, const int *__restrict__ cid,
               const T *__restrict__ rs, T *__restrict__ fc, Seed<T> sd, const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     const unsigned hx = (unsigned)(nx + 1) >> 1;
@@ -182,6 +184,7 @@ __global__ void __launch_bounds__(256)
 k_g7_prolong(int nx, int ny, int nz, const int *__restrict__ cid,
              const T *__restrict__ uc, T *__restrict__ u, const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     const long nxy = (long)nx * ny, n = nxy * nz;
@@ -217,6 +220,7 @@ __global__ void __launch_bounds__(256)
 k_g7_post(G7v<V> g, int n, const T *__restrict__ f, const T *__restrict__ dinv, T w,
           const T *__restrict__ u, T *__restrict__ uo, Ctl *ctl, double *part, int first)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     double dot = 0.0;
@@ -239,6 +243,7 @@ __global__ void __launch_bounds__(256)
 k_g7_spmv_dot(G7v<double> g, int n, const double *__restrict__ x, double *__restrict__ y,
               Ctl *ctl, double *part)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     double d = 0.0;
     GRID_STRIDE(s, n) {
@@ -255,6 +260,7 @@ k_g7_spmv_dot(G7v<double> g, int n, const double *__restrict__ x, double *__rest
 __global__ void __launch_bounds__(256)
 k_g7_spmv(G7v<double> g, int n, const double *__restrict__ x, double *__restrict__ y)
 {
+    PDL_ENTRY();
     GRID_STRIDE(s, n) {
         int i, j, k;
         cell_ijk((unsigned)s, g.nx, g.ny, i, j, k);
@@ -267,6 +273,7 @@ __global__ void __launch_bounds__(256)
 k_g7_resid(G7v<double> g, int n, const double *__restrict__ b, const double *__restrict__ x,
            double *__restrict__ r, Ctl *ctl, double *part, int init, Seed<double> sd)
 {
+    PDL_ENTRY();
     if (init == 0 && (finished(ctl) || !ctl->check)) return;
     double rr = 0.0, bb = 0.0;
     GRID_STRIDE(s, n) {
@@ -293,6 +300,7 @@ __global__ void __launch_bounds__(256)
 k_g19_pre(G19v<V> g, const T *__restrict__ f, const T *__restrict__ u,
           const int *__restrict__ prow, T *__restrict__ rs, const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     GRID_STRIDE(c, g.n) {
@@ -307,6 +315,7 @@ __global__ void __launch_bounds__(256)
 k_g19_post(G19v<V> g, const T *__restrict__ f, const T *__restrict__ dinv, T w,
            const T *__restrict__ u, T *__restrict__ uo, const Ctl *ctl)
 {
+    PDL_ENTRY();
     if (finished(ctl)) return;
     using A = Ar<T>;
     GRID_STRIDE(c, g.n) {
@@ -319,6 +328,7 @@ k_g19_post(G19v<V> g, const T *__restrict__ f, const T *__restrict__ dinv, T w,
 __global__ void __launch_bounds__(256)
 k_g19_spmv(G19v<double> g, const double *__restrict__ x, double *__restrict__ y)
 {
+    PDL_ENTRY();
     GRID_STRIDE(c, g.n) y[c] = g19_row<double, false>(0.0, g, (int)c, [&](long q) { return x[q]; });
 }
 
@@ -473,7 +483,7 @@ int g7_pre(const Level &L, const T *f, const T *u, T *rs, const Ctl *ctl, cudaSt
 {
     const int n = L.A.n;
     const int nblk = occ_blocks((const void *)k_g7_pre<T, V>, n, 256, kRedBlocks);
-    k_g7_pre<T, V><<<nblk, 256, 0, st>>>(g7v<V>(L.g7), n, f, u, rs, ctl);
+    launch_pdl(k_g7_pre<T, V>, nblk, 256, st, g7v<V>(L.g7), n, f, u, rs, ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -485,7 +495,7 @@ int g7_restrict(const Level &L, const T *rs, T *fc, Seed<T> sd, const Ctl *ctl,
     const Grid7 &g = L.g7;
     const long m = (long)((g.nx + 1) >> 1) * g.ny * g.nz;
     const int nblk = occ_blocks((const void *)k_g7_restrict<T>, m, 256, kRedBlocks);
-    k_g7_restrict<T><<<nblk, 256, 0, st>>>(g.nx, g.ny, g.nz, L.cid, rs, fc, sd, ctl);
+    launch_pdl(k_g7_restrict<T>, nblk, 256, st, g.nx, g.ny, g.nz, L.cid, rs, fc, sd, ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -495,7 +505,7 @@ int g7_prolong(const Level &L, const T *uc, T *u, const Ctl *ctl, cudaStream_t s
 {
     const Grid7 &g = L.g7;
     const int nblk = occ_blocks((const void *)k_g7_prolong<T>, L.A.n, 256, kRedBlocks);
-    k_g7_prolong<T><<<nblk, 256, 0, st>>>(g.nx, g.ny, g.nz, L.cid, uc, u, ctl);
+    launch_pdl(k_g7_prolong<T>, nblk, 256, st, g.nx, g.ny, g.nz, L.cid, uc, u, ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -506,7 +516,7 @@ int g7_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo, C
 {
     const int n = L.A.n;
     const int nblk = occ_blocks((const void *)k_g7_post<T, V, DOT>, n, 256, kRedBlocks);
-    k_g7_post<T, V, DOT><<<nblk, 256, 0, st>>>(g7v<V>(L.g7), n, f, dinv, w, u, uo, ctl,
+    launch_pdl(k_g7_post<T, V, DOT>, nblk, 256, st, g7v<V>(L.g7), n, f, dinv, w, u, uo, ctl,
                                                 part, first);
     HM_LAUNCHED();
     return HMFEM_OK;
@@ -517,7 +527,7 @@ int g7_spmv_dot(const Level &L, const double *x, double *y, Ctl *ctl, double *pa
 {
     const int n = L.A.n;
     const int nblk = occ_blocks((const void *)k_g7_spmv_dot, n, 256, kRedBlocks);
-    k_g7_spmv_dot<<<nblk, 256, 0, st>>>(g7v<double>(L.g7), n, x, y, ctl, part);
+    launch_pdl(k_g7_spmv_dot, nblk, 256, st, g7v<double>(L.g7), n, x, y, ctl, part);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -527,7 +537,7 @@ int g7_resid(const Level &L, const double *b, const double *x, double *r, Ctl *c
 {
     const int n = L.A.n;
     const int nblk = occ_blocks((const void *)k_g7_resid, n, 256, kRedBlocks);
-    k_g7_resid<<<nblk, 256, 0, st>>>(g7v<double>(L.g7), n, b, x, r, ctl, part, init, sd);
+    launch_pdl(k_g7_resid, nblk, 256, st, g7v<double>(L.g7), n, b, x, r, ctl, part, init, sd);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -536,7 +546,7 @@ int g7_spmv(const Level &L, const double *x, double *y, cudaStream_t st)
 {
     const int n = L.A.n;
     const int nblk = occ_blocks((const void *)k_g7_spmv, n, 256, kRedBlocks);
-    k_g7_spmv<<<nblk, 256, 0, st>>>(g7v<double>(L.g7), n, x, y);
+    launch_pdl(k_g7_spmv, nblk, 256, st, g7v<double>(L.g7), n, x, y);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -546,7 +556,7 @@ int g19_pre(const Level &L, const T *f, const T *u, T *rs, const Ctl *ctl, cudaS
 {
     const G19v<V> g = g19v<V>(L.g19, L.A.n);
     const int nblk = occ_blocks((const void *)k_g19_pre<T, V>, g.n, 256, kRedBlocks);
-    k_g19_pre<T, V><<<nblk, 256, 0, st>>>(g, f, u, L.P.rowptr, rs, ctl);
+    launch_pdl(k_g19_pre<T, V>, nblk, 256, st, g, f, u, L.P.rowptr, rs, ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -557,7 +567,7 @@ int g19_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo,
 {
     const G19v<V> g = g19v<V>(L.g19, L.A.n);
     const int nblk = occ_blocks((const void *)k_g19_post<T, V>, g.n, 256, kRedBlocks);
-    k_g19_post<T, V><<<nblk, 256, 0, st>>>(g, f, dinv, w, u, uo, ctl);
+    launch_pdl(k_g19_post<T, V>, nblk, 256, st, g, f, dinv, w, u, uo, ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -566,7 +576,7 @@ int g19_spmv(const Level &L, const double *x, double *y, cudaStream_t st)
 {
     const G19v<double> g = g19v<double>(L.g19, L.A.n);
     const int nblk = occ_blocks((const void *)k_g19_spmv, g.n, 256, kRedBlocks);
-    k_g19_spmv<<<nblk, 256, 0, st>>>(g, x, y);
+    launch_pdl(k_g19_spmv, nblk, 256, st, g, x, y);
     HM_LAUNCHED();
     return HMFEM_OK;
 }

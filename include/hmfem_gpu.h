@@ -103,7 +103,7 @@ typedef struct {
                           SPD preconditioner for any SPD matrix) */
     int gs_from;       /* levels >= gs_from (below the coarse solve) use a
                           multicolour Gauss-Seidel smoother instead: forward
-                          sweep over greedy natural-order colours before the
+                          sweep over Jones-Plassmann colours before the
                           restriction, backward sweep after the
                           prolongation; < 0 disables (default 2) */
     double omega;      /* Jacobi weight (compute.cpp:35 passes 1.0) */
@@ -119,8 +119,12 @@ typedef struct {
                           level (amg.h:1353-1364) */
     int check_every;   /* host polls convergence every k iterations */
     int generic_setup; /* 1: coarsen an assembled level 0 with the generic
-                          kernels too (default 0: from its 7-point
-                          structure; both give the identical hierarchy) */
+                          kernels and solve every level on SELL-32 (default
+                          0: level 0 from its 7-point structure, levels 0-1
+                          solved in structured forms; identical results) */
+    int gs_fused;      /* 1: one cooperative launch per Gauss-Seidel sweep
+                          (grid barrier between colours); 0 (default): one
+                          launch per colour (identical results) */
     int verbose;
 } hmfem_options;
 

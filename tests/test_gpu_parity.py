@@ -116,6 +116,19 @@ def test_vcycle_bit_exact(case, smoother, gs_from, oracle_smoother, omega,
     np.testing.assert_array_equal(s.vcycle(f), H.vcycle(f, oracle_smoother, omega))
 
 
+@pytest.mark.parametrize("gs_from,oracle_smoother", [(2, 12), (1, 11)])
+def test_vcycle_gs_fused_sweeps(case, gs_from, oracle_smoother):
+    """gs_fused=1: each Gauss-Seidel sweep as one cooperative launch with
+    grid barriers between colours instead of one launch per colour; the
+    same bits either way."""
+    name, p, (perm, ind, b, csr, H) = case
+    s = gpu.Solver(smoother=1, gs_from=gs_from, coarse_direct=0, gs_fused=1)
+    s.assemble(p)
+    s.setup()
+    f = np.random.default_rng(11).standard_normal(p.n)
+    np.testing.assert_array_equal(s.vcycle(f), H.vcycle(f, oracle_smoother, 1.0))
+
+
 @pytest.mark.parametrize("generic_setup", [0, 1])
 def test_spmv_bit_exact(case, port, generic_setup):
     name, p, (perm, ind, b, csr, H) = case
