@@ -159,6 +159,72 @@ k_post(const long long *__restrict__ sptr, const int *__restrict__ scol,
     }
 }
 
+// ---- Chebyshev smoothing (coarse levels) ---------------------------------
+//
+// K steps of the Chebyshev iteration on D^-1 A (D the l1 diagonal) over
+// [1/30, 1]; the oracle's cheb_steps restates the same operations.  The
+// first direction d0 = (1/theta * t) D^-1 (t = f from zero, seeded by the
+// producer of f; t = f - A u after the prolongation, k_cheb0); then per
+// step, in one pass: q = A d (row order, from 0), r = r - D^-1 q,
+// d' = c1 d + c2 r, u = u + d' (first step: d0 + d' from zero, (u + d0) + d'
+// otherwise).  d ping-pongs between two vectors because every row gathers
+// it; r and u are only read at their own row.
+
+// post-smoother, step 0: t = f - A u;  r = D^-1 t;  d0 = (ith t) D^-1
+template <class T, class M>
+__global__ void __launch_bounds__(256, 6)
+k_cheb0(const long long *__restrict__ sptr, const int *__restrict__ scol,
+        const M *__restrict__ sval, int n, const T *__restrict__ f,
+        const T *__restrict__ dinv, T ith, const T *__restrict__ u, T *__restrict__ r,
+        T *__restrict__ d, const Ctl *ctl)
+{
+    PDL_ENTRY();
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    GRID_STRIDE(i, n) {
+        const long q = i >> 5;
+        const long long base = sptr[q];
+        const int wd = (int)((sptr[q + 1] - base) >> 5);
+        const T t = row_acc<T, true>(f[i], scol, sval, base + (i & 31), wd,
+                                     [&](int c) { return u[c]; });
+        const T di = dinv[i];
+        r[i] = A::mul(di, t);
+        d[i] = A::mul(A::mul(ith, t), di);
+    }
+}
+
+// one Chebyshev step; MODE 0: first step from zero, 1: first step after the
+// prolongation, 2: later steps.  last: r and d' are not needed afterwards.
+template <class T, class M, int MODE>
+__global__ void __launch_bounds__(256, 6)
+k_cheb_step(const long long *__restrict__ sptr, const int *__restrict__ scol,
+            const M *__restrict__ sval, int n, const T *__restrict__ f,
+            const T *__restrict__ dinv, T c1, T c2, const T *__restrict__ din,
+            T *__restrict__ dout, T *__restrict__ r, T *__restrict__ u, int last,
+            const Ctl *ctl)
+{
+    PDL_ENTRY();
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    GRID_STRIDE(i, n) {
+        const long q = i >> 5;
+        const long long base = sptr[q];
+        const int wd = (int)((sptr[q + 1] - base) >> 5);
+        const T ad = row_acc<T, false>((T)0, scol, sval, base + (i & 31), wd,
+                                       [&](int c) { return din[c]; });
+        const T di = dinv[i], dold = din[i];
+        const T rp = MODE == 0 ? A::mul(di, f[i]) : r[i];
+        const T rn = A::sub(rp, A::mul(di, ad));
+        const T dn = A::add(A::mul(c1, dold), A::mul(c2, rn));
+        u[i] = MODE == 0 ? A::add(dold, dn)
+             : MODE == 1 ? A::add(A::add(u[i], dold), dn) : A::add(u[i], dn);
+        if (!last) {
+            r[i] = rn;
+            dout[i] = dn;
+        }
+    }
+}
+
 // ---- multicolour Gauss-Seidel (coarse levels) ---------------------------
 
 // Forward sweep from zero, first colour: u_i = f_i / a_ii on colour 0,
@@ -570,8 +636,31 @@ template <class T>
 static T *cycle_out(Solver &s, int l)
 {
     const int last = s.nlevels - 1;
-    if (l == last || l == s.direct_level || s.lv[l].gs) return s.vec_ua<T>(l);
+    if (l == last || l == s.direct_level || s.lv[l].gs || s.lv[l].cheb) return s.vec_ua<T>(l);
     return s.vec_ub<T>(l);
+}
+
+// Chebyshev coefficients on [1/30, 1] (the oracle's cheb_coeffs, same
+// expressions, same doubles): 1/theta and, for steps k >= 1, c1_k, c2_k
+struct ChebCoef {
+    double ith, c1[10], c2[10];
+};
+
+static ChebCoef cheb_coef(int K)
+{
+    const double lo = 1.0 / 30.0, hi = 1.0;
+    const double th = (hi + lo) / 2, de = (hi - lo) / 2;
+    const double sg = th / de;
+    ChebCoef c{};
+    double rho = 1.0 / sg;
+    c.ith = 1.0 / th;
+    for (int k = 1; k < K && k < 10; k++) {
+        const double rn = 1.0 / (2.0 * sg - rho);
+        c.c1[k] = rn * rho;
+        c.c2[k] = 2.0 * rn / de;
+        rho = rn;
+    }
+    return c;
 }
 
 // Cooperative launch (all blocks co-resident, as the fused sweeps' grid
@@ -615,8 +704,15 @@ static Seed<T> seed_of(Solver &s, int l)
 {
     const int last = s.nlevels - 1;
     if (l >= last || l == s.direct_level || s.lv[l].gs) return {nullptr, nullptr, (T)0};
+    // Chebyshev: the first direction d0 = (1/theta f) D^-1, kept in ub
+    if (s.lv[l].cheb)
+        return {s.vec_ub<T>(l), s.vec_dinv<T>(l), (T)cheb_coef(s.opt.cheb_degree).ith};
     return {s.vec_ua<T>(l), s.vec_dinv<T>(l), (T)s.opt.omega};
 }
+
+template <class T> static T *vec_dx(Solver &s, int l);
+template <> double *vec_dx<double>(Solver &s, int l) { return s.lv[l].dx; }
+template <> float *vec_dx<float>(Solver &s, int l) { return s.lv[l].dx32; }
 
 // Launches fn(values) with the level's matrix values in the cycle's
 // storage type: FP64, FP32, or BF16 on levels >= bf16_from.
@@ -700,6 +796,26 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
                 L.A.rowptr, L.A.col, vals, n, f, ua, L.P.rowptr, rs, ctl);
             HM_COUNT();
         });
+    } else if (L.cheb) {
+        // d0 was seeded into ub by the producer of f; K-1 steps, then the
+        // residual for the restriction (r lives in rs until then)
+        const int K = s.opt.cheb_degree;
+        const ChebCoef cc = cheb_coef(K);
+        T *dbuf[2] = {ub, vec_dx<T>(s, l)};
+        with_vals<T>(s, L.S, l, [&](auto vals) {
+            using M = typename std::remove_const<
+                typename std::remove_pointer<decltype(vals)>::type>::type;
+            for (int k = 1; k < K; k++) {
+                auto kern = k == 1 ? k_cheb_step<T, M, 0> : k_cheb_step<T, M, 2>;
+                launch_pdl(kern, nb(n), 256, st, L.S.sptr, L.S.col, vals, n, f, dv,
+                           (T)cc.c1[k], (T)cc.c2[k], dbuf[(k - 1) & 1], dbuf[k & 1], rs, ua,
+                           (int)(k == K - 1), ctl);
+                HM_COUNT();
+            }
+            launch_pdl(k_pre<T, M>, nb(n), 256, st, L.S.sptr, L.S.col, vals, n, f, ua,
+                       L.P.rowptr, rs, ctl);
+            HM_COUNT();
+        });
     } else if (g7) {
         HM_CHECK((g7_pre<T, T>(L, f, ua, rs, ctl, st)));
     } else if (g19) {
@@ -747,6 +863,24 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
         HM_CUDA(le);
     } else if (L.gs) {
         for (int c = L.ncolors - 1; c >= 0; c--) sweep(c);
+    } else if (L.cheb) {
+        const int K = s.opt.cheb_degree;
+        const ChebCoef cc = cheb_coef(K);
+        T *dbuf[2] = {ub, vec_dx<T>(s, l)};
+        with_vals<T>(s, L.S, l, [&](auto vals) {
+            using M = typename std::remove_const<
+                typename std::remove_pointer<decltype(vals)>::type>::type;
+            launch_pdl(k_cheb0<T, M>, nb(n), 256, st, L.S.sptr, L.S.col, vals, n, f, dv,
+                       (T)cc.ith, ua, rs, dbuf[0], ctl);
+            HM_COUNT();
+            for (int k = 1; k < K; k++) {
+                auto kern = k == 1 ? k_cheb_step<T, M, 1> : k_cheb_step<T, M, 2>;
+                launch_pdl(kern, nb(n), 256, st, L.S.sptr, L.S.col, vals, n, f, dv,
+                           (T)cc.c1[k], (T)cc.c2[k], dbuf[(k - 1) & 1], dbuf[k & 1], rs, ua,
+                           (int)(k == K - 1), ctl);
+                HM_COUNT();
+            }
+        });
     } else if (g7) {
         if constexpr (std::is_same<T, double>::value) {
             if (dot) HM_CHECK((g7_post<T, T, true>(L, f, dv, w, ua, ub, s.ctl, s.part, s.first_sigma, st)));

@@ -91,6 +91,10 @@ struct Level {
     // V-cycle vectors (FP64 and FP32 sets)
     double *f = nullptr, *ua = nullptr, *ub = nullptr, *rs = nullptr;
     float *f32 = nullptr, *ua32 = nullptr, *ub32 = nullptr, *rs32 = nullptr;
+    // Chebyshev smoother (levels >= cheb_from): second search direction
+    bool cheb = false;
+    double *dx = nullptr;
+    float *dx32 = nullptr;
     // multicolour Gauss-Seidel smoother (levels >= gs_from)
     bool gs = false;
     int ncolors = 0;

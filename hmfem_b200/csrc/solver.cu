@@ -118,6 +118,7 @@ static void free_level_setup(Level &L, bool keep_matrix)
     free_csr(L.P); free_csr(L.R);
     dfree(L.f); dfree(L.ua); dfree(L.ub); dfree(L.rs);
     dfree(L.f32); dfree(L.ua32); dfree(L.ub32); dfree(L.rs32);
+    dfree(L.dx); dfree(L.dx32);
     dfree(L.color); dfree(L.crows); dfree(L.cslot); dfree(L.aval32); dfree(L.aval16);
     g7_free(L.g7);
     g19_free(L.g19);
@@ -262,8 +263,11 @@ int setup(Solver &s)
     const bool low = s.opt.precision == 1;
     if (s.have_grid && s.opt.generic_setup == 0)
         HM_CHECK(g7_build(s.lv[0], s.nx, s.ny, s.nz, low, st, s.dwork));
+    // Chebyshev levels: cheb_from and below, above the coarsest
+    for (int k = 0; k < s.nlevels; k++)
+        s.lv[k].cheb = s.opt.cheb_from >= 1 && k >= s.opt.cheb_from && k < s.nlevels - 1;
     if (s.nlevels > 1 && s.lv[1].g19.v) {
-        const bool smoothed = 1 < s.nlevels - 1 && !(s.opt.gs_from >= 1 && s.opt.gs_from <= 1);
+        const bool smoothed = 1 < s.nlevels - 1 && s.opt.gs_from != 1 && !s.lv[1].cheb;
         if (s.use_g7(0) && smoothed)
             HM_CHECK(g19_lowp(s.lv[1].g19, s.lv[1].A.n, low && !s.use_bf16(1),
                               low && s.use_bf16(1), st));
@@ -279,8 +283,14 @@ int setup(Solver &s)
         }
         HM_ALLOC(L.dsm, double, L.A.n);
         HM_ALLOC(L.dsm32, float, L.A.n);
-        HM_CHECK(launch_smoother_diag(L.A, s.opt.smoother, L.dsm, L.dsm32, st));
+        // Chebyshev levels always use the l1 diagonal (its bound 1 on the
+        // spectrum of D^-1 A fixes the Chebyshev interval)
+        HM_CHECK(launch_smoother_diag(L.A, L.cheb ? 1 : s.opt.smoother, L.dsm, L.dsm32, st));
         HM_CHECK(alloc_level_vectors(s, L));
+        if (L.cheb) {
+            HM_ALLOC(L.dx, double, L.A.n);
+            if (low) HM_ALLOC(L.dx32, float, L.A.n);
+        }
     }
     HM_PHASE("setup: SELL + vectors", st);
     // dense coarse solve on the first level small enough
@@ -309,6 +319,7 @@ int setup(Solver &s)
     if (s.opt.gs_from >= 1) {
         const int stop = s.direct_level >= 0 ? s.direct_level : s.nlevels - 1;
         for (int k = s.opt.gs_from; k < stop; k++) {
+            if (s.lv[k].cheb) continue;
             HM_CHECK(color_level(s.lv[k], st, s.dwork));
             if (s.lv[k].gs && s.opt.precision == 1)
                 HM_CHECK(csr_fill_lowp(s.lv[k], s.use_bf16(k), st));
@@ -447,6 +458,8 @@ void hmfem_default_options(hmfem_options *o)
     o->coarse_direct = 512;
     o->check_every = 2;
     o->gs_fused = 0;
+    o->cheb_from = 2;
+    o->cheb_degree = 4;
     o->verbose = 0;
 }
 
@@ -458,7 +471,8 @@ int hmfem_create(hmfem_solver **out, const hmfem_options *opt)
     hm::set_alloc_context(s.st, s.cache);
     if (opt) s.opt = *opt;
     else hmfem_default_options(&s.opt);
-    if (s.opt.max_levels < 1 || s.opt.max_levels > 64 || s.opt.tol < 0) {
+    if (s.opt.max_levels < 1 || s.opt.max_levels > 64 || s.opt.tol < 0 ||
+        (s.opt.cheb_from >= 1 && (s.opt.cheb_degree < 2 || s.opt.cheb_degree > 9))) {
         delete h;
         hm::set_last_error("invalid options", __FILE__, __LINE__);
         return HMFEM_E_ARG;

@@ -51,7 +51,8 @@ class Options(C.Structure):
                 ("max_iter", C.c_int), ("max_levels", C.c_int),
                 ("min_coarse", C.c_int), ("coarse_direct", C.c_int),
                 ("check_every", C.c_int), ("generic_setup", C.c_int),
-                ("gs_fused", C.c_int), ("verbose", C.c_int)]
+                ("gs_fused", C.c_int), ("cheb_from", C.c_int),
+                ("cheb_degree", C.c_int), ("verbose", C.c_int)]
 
 
 class Stats(C.Structure):

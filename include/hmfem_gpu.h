@@ -125,6 +125,11 @@ typedef struct {
     int gs_fused;      /* 1: one cooperative launch per Gauss-Seidel sweep
                           (grid barrier between colours); 0 (default): one
                           launch per colour (identical results) */
+    int cheb_from;     /* levels >= cheb_from (below the coarse solve) are
+                          smoothed by `cheb_degree` Chebyshev steps in
+                          D_l1^-1 A over [1/30, 1] instead (takes precedence
+                          over gs_from; default 2; < 1 disables) */
+    int cheb_degree;   /* 2..9 (default 4) */
     int verbose;
 } hmfem_options;
 

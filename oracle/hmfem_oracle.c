@@ -594,6 +594,59 @@ static void gs_colour(const or_level *A, int c, const double *f, double *u)
     }
 }
 
+/* Chebyshev smoothing (project smoother for the coarse levels, no
+ * reference counterpart): K steps of the Chebyshev iteration (Saad,
+ * Iterative Methods for Sparse Linear Systems, alg. 12.1) on D^-1 A with D
+ * the l1 diagonal, over the interval [1/30, 1] -- 1 bounds the spectrum of
+ * D^-1 A by Gershgorin (d_i = a_ii + sum_j!=i |a_ij|).  Coefficients:
+ * theta = (hi+lo)/2, delta = (hi-lo)/2, sigma = theta/delta, rho_0 =
+ * 1/sigma, rho_k = 1/(2 sigma - rho_{k-1}), c1_k = rho_k rho_{k-1}, c2_k =
+ * 2 rho_k / delta.  The GPU computes the same doubles on its host. */
+#define OR_CHEB_LO (1.0 / 30.0)
+#define OR_CHEB_HI 1.0
+
+static void cheb_coeffs(int K, double *ith, double *c1, double *c2)
+{
+    const double th = (OR_CHEB_HI + OR_CHEB_LO) / 2, de = (OR_CHEB_HI - OR_CHEB_LO) / 2;
+    const double sg = th / de;
+    double rho = 1.0 / sg;
+    *ith = 1.0 / th;
+    for (int k = 1; k < K; k++) {
+        const double rn = 1.0 / (2.0 * sg - rho);
+        c1[k] = rn * rho;
+        c2[k] = 2.0 * rn / de;
+        rho = rn;
+    }
+}
+
+/* Steps k = 1..K-1 after the first direction d (= d0) is formed: per step
+ * q = sum_j a_ij d_j (row order, from 0); r = r - D^-1 q; d' = c1 d + c2 r;
+ * u = u + d' (first step: u = d0 + d' from zero, (u + d0) + d' otherwise).
+ * first_r0: the pre-smoother forms r0 = D^-1 f inside its first step. */
+static void cheb_steps(const or_level *A, int K, int from_zero, const double *f,
+                       double *u, double *r, double *d, double *dn)
+{
+    double ith, c1[10], c2[10];
+    cheb_coeffs(K, &ith, c1, c2);
+    const int n = A->n;
+    const double *dv = A->dl1inv;
+    for (int k = 1; k < K; k++) {
+        long m = 0;
+        for (int i = 0; i < n; i++) {
+            double q = 0.0;
+            for (int j = 0; j < A->cnt[i]; j++, m++) q += A->ele[m] * d[A->col[m]];
+            const double rp = (k == 1 && from_zero) ? dv[i] * f[i] : r[i];
+            const double rn = rp - dv[i] * q;
+            const double dd = c1[k] * d[i] + c2[k] * rn;
+            if (k == 1) u[i] = from_zero ? d[i] + dd : (u[i] + d[i]) + dd;
+            else u[i] = u[i] + dd;
+            r[i] = rn;
+            dn[i] = dd;
+        }
+        memcpy(d, dn, sizeof(double) * n);
+    }
+}
+
 static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
                double omega)
 {
@@ -609,8 +662,28 @@ static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
     const int gs_from = smoother >= 100 ? (smoother / 10) % 10
                         : smoother >= 10 ? smoother - 10 : 1 << 30;
     const int gs_to = smoother >= 100 ? smoother % 10 : 1 << 30;
-    const int use_gs = l >= gs_from && l < gs_to;
-    if (use_gs) {
+    const int use_gs = l >= gs_from && l < gs_to && smoother < 200;
+    /* smoother 200+10c+K: Chebyshev of degree K on levels >= c, l1-Jacobi
+     * below */
+    const int use_cheb = smoother >= 200 && smoother < 300 && l >= (smoother / 10) % 10;
+    const int cheb_k = smoother % 10;
+    double *cd = NULL, *cdn = NULL;
+    if (use_cheb) {
+        cd = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+        cdn = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+    }
+    if (use_cheb) {
+        double ith, c1[10], c2[10];
+        cheb_coeffs(cheb_k, &ith, c1, c2);
+        for (int i = 0; i < n; i++) cd[i] = ith * f[i] * A->dl1inv[i];
+        cheb_steps(A, cheb_k, 1, f, u, r, cd, cdn);
+        long m = 0;
+        for (int i = 0; i < n; i++) {
+            double t = f[i];
+            for (int j = 0; j < A->cnt[i]; j++, m++) t -= A->ele[m] * u[A->col[m]];
+            r[i] = t;
+        }
+    } else if (use_gs) {
         /* multicolour Gauss-Seidel, forward over colours from zero, then the
          * residual (the GPU smoother on coarse levels; no reference
          * counterpart -- the reference's own GS is lexicographic) */
@@ -644,7 +717,21 @@ static void mg(const or_hierarchy *H, or_work *W, int l, int smoother,
     restrict_simple(A, H->lv[l + 1].n, r, W[l + 1].f);
     mg(H, W, l + 1, smoother, omega);
     prolong_simple(A, W[l + 1].u, s);
-    if (use_gs) {
+    if (use_cheb) {
+        double ith, c1[10], c2[10];
+        cheb_coeffs(cheb_k, &ith, c1, c2);
+        for (int i = 0; i < n; i++) u[i] += s[i];
+        long m = 0;
+        for (int i = 0; i < n; i++) {
+            double t = f[i];
+            for (int j = 0; j < A->cnt[i]; j++, m++) t -= A->ele[m] * u[A->col[m]];
+            r[i] = A->dl1inv[i] * t;
+            cd[i] = ith * t * A->dl1inv[i];
+        }
+        cheb_steps(A, cheb_k, 0, f, u, r, cd, cdn);
+        free(cd);
+        free(cdn);
+    } else if (use_gs) {
         for (int i = 0; i < n; i++) u[i] += s[i];
         for (int c = A->ncolors - 1; c >= 0; c--) gs_colour(A, c, f, u);
     } else if (smoother == 0) {

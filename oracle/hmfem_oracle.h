@@ -95,7 +95,11 @@ void or_amg_free(or_hierarchy *H);
  *             preconditioner for any SPD matrix.
  * smoother 10+g: l1-Jacobi on levels < g, multicolour Gauss-Seidel (forward
  *             pre-sweep over colours 0..C-1 from zero, backward post-sweep)
- *             on levels >= g -- the GPU solver's default with g = 2. */
+ *             on levels >= g;
+ * smoother 100+10g+t: as 10+g on levels [g, t) only;
+ * smoother 200+10c+K: l1-Jacobi on levels < c, Chebyshev of degree K
+ *             (2..9) in D_l1^-1 A over [1/30, 1] on levels >= c -- the GPU
+ *             solver's default with c = 2, K = 3. */
 void or_vcycle(const or_hierarchy *H, int smoother, double omega,
                const double *f, double *u);
 

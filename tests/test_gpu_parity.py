@@ -97,19 +97,24 @@ def test_hierarchy_bit_exact(case, generic_setup):
             np.testing.assert_array_equal(g[k], o[k], err_msg=f"L{l} {k}")
 
 
-@pytest.mark.parametrize("smoother,gs_from,oracle_smoother,omega",
-                         [(0, -1, 1, 1.0), (0, -1, 1, 0.6), (1, -1, 2, 1.0),
-                          (1, 2, 12, 1.0), (1, 1, 11, 1.0)])
+@pytest.mark.parametrize("smoother,gs_from,cheb,oracle_smoother,omega",
+                         [(0, -1, None, 1, 1.0), (0, -1, None, 1, 0.6),
+                          (1, -1, None, 2, 1.0), (1, 2, None, 12, 1.0),
+                          (1, 1, None, 11, 1.0), (1, 2, (2, 3), 223, 1.0),
+                          (1, 2, (1, 2), 212, 1.0), (1, 2, (2, 4), 224, 1.0)])
 @pytest.mark.parametrize("generic_setup", [0, 1])
-def test_vcycle_bit_exact(case, smoother, gs_from, oracle_smoother, omega,
+def test_vcycle_bit_exact(case, smoother, gs_from, cheb, oracle_smoother, omega,
                           generic_setup):
     """generic_setup=0 runs the two finest levels of an assembled grid in
     their structured forms (7-point stencil, 19-offset level 1),
-    generic_setup=1 everything on SELL-32; both equal the oracle's cycle."""
+    generic_setup=1 everything on SELL-32; both equal the oracle's cycle.
+    cheb = (first level, degree) of the Chebyshev coarse smoother."""
     name, p, (perm, ind, b, csr, H) = case
+    cheb_from, cheb_degree = cheb if cheb else (-1, 3)
     # coarse_direct=0: the reference's diagonal solve on the coarsest level
     s = gpu.Solver(smoother=smoother, gs_from=gs_from, omega=omega,
-                   coarse_direct=0, generic_setup=generic_setup)
+                   coarse_direct=0, generic_setup=generic_setup,
+                   cheb_from=cheb_from, cheb_degree=cheb_degree)
     s.assemble(p)
     s.setup()
     f = np.random.default_rng(11).standard_normal(p.n)
@@ -122,7 +127,8 @@ def test_vcycle_gs_fused_sweeps(case, gs_from, oracle_smoother):
     grid barriers between colours instead of one launch per colour; the
     same bits either way."""
     name, p, (perm, ind, b, csr, H) = case
-    s = gpu.Solver(smoother=1, gs_from=gs_from, coarse_direct=0, gs_fused=1)
+    s = gpu.Solver(smoother=1, gs_from=gs_from, coarse_direct=0, gs_fused=1,
+                   cheb_from=-1)
     s.assemble(p)
     s.setup()
     f = np.random.default_rng(11).standard_normal(p.n)
