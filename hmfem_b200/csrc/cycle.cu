@@ -1050,6 +1050,9 @@ __global__ void k_fill_one(double *x, int n)
 //   7 post-smoother FP32 (level 0)  n*4*4 + n*4*4
 //   8 pre-smoother FP32 (level 1)   nnz*4 + n*(4 f + 4 u + 4 P-row + 4 rs)
 //   9 post-smoother FP32 (level 1)  nnz*4 + n*4*4
+//  10 Chebyshev step FP32 (coarse level, SELL)  nnz*(4+4) + n*4*7
+//  11 Chebyshev step FP64 (coarse level, SELL)  nnz*(8+4) + n*8*7
+//     (d gathered, D^-1, r and u read and written, d' written)
 // and 12: one whole V-cycle from level l in the solver's precision (bytes
 // reported 0); the difference between levels l and l+1 is level l's share.
 int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
@@ -1078,11 +1081,13 @@ int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
         *bytes = 0;
         return HMFEM_OK;
     }
-    if (l < 0 || l >= s.nlevels || reps < 1 || which < 0 || which > 9) return HMFEM_E_ARG;
+    if (l < 0 || l >= s.nlevels || reps < 1 || which < 0 || which > 11) return HMFEM_E_ARG;
     if (which >= 1 && l == s.nlevels - 1) return HMFEM_E_ARG;
-    if (((which >= 3 && which <= 4) || which >= 6) && s.opt.precision != 1) return HMFEM_E_ARG;
+    if (((which >= 3 && which <= 4) || (which >= 6 && which <= 10)) && s.opt.precision != 1)
+        return HMFEM_E_ARG;
     if (which >= 5 && which <= 7 && !s.use_g7(l)) return HMFEM_E_ARG;
-    if (which >= 8 && (!s.use_g19(l) || s.use_bf16(l))) return HMFEM_E_ARG;
+    if (which >= 8 && which <= 9 && (!s.use_g19(l) || s.use_bf16(l))) return HMFEM_E_ARG;
+    if (which >= 10 && (!s.lv[l].cheb || s.use_bf16(l))) return HMFEM_E_ARG;
     Level &L = s.lv[l];
     cudaStream_t st = s.st;
     if (which <= 4 && !L.S.sptr) {
@@ -1129,6 +1134,16 @@ int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
             break;
         case 8: g19_pre<float, float>(L, xf, L.ua32, yf, nullptr, st); break;
         case 9: g19_post<float, float>(L, xf, L.dsm32, (float)w, L.ua32, yf, nullptr, st); break;
+        case 10:
+            k_cheb_step<float, float, 2><<<nb(n), 256, 0, st>>>(
+                L.S.sptr, L.S.col, L.S.val32, n, L.f32, L.dsm32, 0.5f, 0.25f, xf, yf,
+                L.rs32, L.ua32, 0, nullptr);
+            break;
+        case 11:
+            k_cheb_step<double, double, 2><<<nb(n), 256, 0, st>>>(
+                L.S.sptr, L.S.col, L.S.val, n, L.f, L.dsm, 0.5, 0.25, x, y, L.rs, L.ua, 0,
+                nullptr);
+            break;
         default:
             if (vb16 == 2)
                 k_post<float, __nv_bfloat16, false><<<nb(n), 256, 0, st>>>(
@@ -1170,7 +1185,9 @@ int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
     case 6: *bytes = (double)n * 28; break;
     case 7: *bytes = (double)n * 32; break;
     case 8: *bytes = nnz * 4 + (double)n * 16; break;
-    default: *bytes = nnz * 4 + (double)n * 16; break;
+    case 9: *bytes = nnz * 4 + (double)n * 16; break;
+    case 10: *bytes = nnz * 8 + (double)n * 4 * 7; break;
+    default: *bytes = nnz * 12 + (double)n * 8 * 7; break;
     }
     return HMFEM_OK;
 }
