@@ -32,6 +32,11 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# DRAM bytes (read + write) per cell of one k_g7_spmv_dot launch, from an
+# ncu --set full capture of the same kernel on config 2 at 192^3 (7.08M
+# cells, 328 MB): the launch is linear in cells, so bench scales it.
+SPMV_TRAFFIC_B_PER_CELL = 46.4
+
 METRIC = "cells/s to ||r||/||b||<=1e-10 (256^3 lognormal+conduits), chosen=FP32 V-cycle in FP64 FCG"
 
 
@@ -284,7 +289,10 @@ def run_ours(args):
                          "achieved": round(achieved, 1), "peak": peak,
                          "peak_source": peak_src, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
-                         "algorithmic_bytes": by0, "ms": ms0, "traffic": None},
+                         "algorithmic_bytes": by0, "ms": ms0,
+                         "traffic": round(SPMV_TRAFFIC_B_PER_CELL * n),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                           "of one launch at 192^3, scaled by cells"},
             "kernels_gbs": kernels_gbs,
             "gpu_launches": launches["chosen"],
             "gpu_launches_per_step": launches["chosen"] / args.steps,
