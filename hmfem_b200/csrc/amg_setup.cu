@@ -292,7 +292,10 @@ k_union_warp(UnionArgs A, const int *rows, const int *nrows_dev, int tier)
 // are grouped (match_any) and the group's lowest lane adds their values to
 // the column's slot in lane (= generation) order, so every sum keeps the
 // reference's order.  Only the distinct columns are sorted at the end.
-// Rows with more than HCAP/2 candidates go to list[tier].
+// The table is sized for distinct columns, not candidates: a row whose
+// distinct count passes HCAP/2 is abandoned (nothing written yet) and goes
+// to list[tier]; as at most 32 keys enter per chunk, the load stays below
+// HCAP - 32 and every probe sequence ends.
 template <int STAGE, int HCAP>
 __global__ void __launch_bounds__(128)
 k_union_hash(UnionArgs A, const int *rows, const int *nrows_dev, int tier)
@@ -314,15 +317,12 @@ k_union_hash(UnionArgs A, const int *rows, const int *nrows_dev, int tier)
          t += ((long)gridDim.x * blockDim.x) >> 5) {
         const int r = rows ? rows[t] : (int)t;
         const long long o = A.cptr[r];
-        const int m = (int)(A.cptr[r + 1] - o);
-        if (m > HCAP / 2) {
-            if (lane == 0) A.list[tier][atomicAdd(A.nlist[tier], 1)] = r;
-            continue;
-        }
         for (int q = lane; q < HCAP; q += 32) M.key[q] = -1;
         __syncwarp();
         const int ob = A.orow[r], oe = A.orow[r + 1];
-        for (int c0 = ob; c0 < oe; c0 += 32) {
+        int ndist = 0;
+        bool full = false;
+        for (int c0 = ob; c0 < oe && !full; c0 += 32) {
             // this group's outer entries: inner row start, length, scale
             const int k = c0 + lane;
             const bool ok = k < oe;
@@ -342,7 +342,7 @@ k_union_hash(UnionArgs A, const int *rows, const int *nrows_dev, int tier)
             const int tot = __shfl_sync(0xffffffffu, x, 31);
             const int nk = min(32, oe - c0);
             __syncwarp();
-            for (int g0 = 0; g0 < tot; g0 += 32) {
+            for (int g0 = 0; g0 < tot && !full; g0 += 32) {
                 const int g = g0 + lane;
                 const bool on = g < tot;
                 int col = -1;
@@ -361,9 +361,9 @@ k_union_hash(UnionArgs A, const int *rows, const int *nrows_dev, int tier)
                 M.cv[lane] = tv;
                 const unsigned grp = __match_any_sync(0xffffffffu, col);
                 __syncwarp();
+                bool fresh = false;
                 if (on && lane == __ffs(grp) - 1) {
                     unsigned h = ((unsigned)col * 2654435761u) & (HCAP - 1);
-                    bool fresh = false;
                     for (;;) {
                         int prev = atomicCAS(&M.key[h], -1, col);
                         if (prev == -1) { fresh = true; break; }
@@ -379,8 +379,14 @@ k_union_hash(UnionArgs A, const int *rows, const int *nrows_dev, int tier)
                     }
                     M.val[h] = acc;
                 }
+                ndist += __popc(__ballot_sync(0xffffffffu, fresh));
+                full = ndist > HCAP / 2;
                 __syncwarp();
             }
+        }
+        if (full) {  // too many distinct columns for this tier
+            if (lane == 0) A.list[tier][atomicAdd(A.nlist[tier], 1)] = r;
+            continue;
         }
         // distinct columns, sorted
         int u = 0;
@@ -514,11 +520,12 @@ int run_union(UnionArgs A, Csr &out, int *dwork, cudaStream_t st)
     A.nlist[1] = dwork + 1;
     A.err = dwork + 2;
     HM_CUDA(cudaMemsetAsync(dwork, 0, 3 * sizeof(int), st));
-    // pass B: three tiers (<= 64 candidates, <= 1024, <= 4096)
+    // pass B: three tiers (<= 64 distinct columns, <= 512, <= 4096
+    // candidates)
     {
         auto k0 = k_union_hash<STAGE, 128>;
-        auto k1 = k_union_hash<STAGE, 2048>;
-        const size_t m0 = hash_smem<STAGE, 128>(), m1 = hash_smem<STAGE, 2048>();
+        auto k1 = k_union_hash<STAGE, 1024>;
+        const size_t m0 = hash_smem<STAGE, 128>(), m1 = hash_smem<STAGE, 1024>();
         HM_CUDA(cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m0));
         HM_CUDA(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m1));
         k0<<<nblk((long)n * 32, 128, 148L * 64), 128, m0, st>>>(A, nullptr, nullptr, 0);
@@ -569,6 +576,8 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
     HM_CUDA(cudaMemsetAsync(dwork, 0, 4 * sizeof(int), st));
     if (grid3) {
         HM_CHECK(stencil_parity_split(grid3[0], grid3[1], grid3[2], L.sel, st));
+    } else if (L.g19.nx > 0) {
+        HM_CHECK(stencil19_split(L.g19.nx, L.g19.ny, L.g19.nz, L.sel, st));
     } else if (n > 0) {
         k_lfmis<<<(int)ceil_div(n, kMisTile), kMisTile, 0, st>>>(
             L.A.rowptr, L.A.col, n, L.sel, (unsigned *)(dwork + 2), dwork);

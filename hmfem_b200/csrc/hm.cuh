@@ -153,6 +153,9 @@ int launch_spmv(const Sell &S, const double *x, double *y, cudaStream_t st);
 int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *err_dev,
                 const int *grid3 = nullptr);
 int stencil_parity_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st);
+// level 1 of a parity split (nx even, nx, ny >= 4): its greedy C/F split
+// from the 19-offset structure, one launch per x-row wavefront
+int stencil19_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st);
 int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
                      double *g19v, cudaStream_t st);
 // colouring + rows grouped by colour; returns HMFEM_OK with L.gs = false

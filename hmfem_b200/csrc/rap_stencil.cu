@@ -265,7 +265,71 @@ int nbk(long n)
     return (int)(b < 148L * 16 ? b : 148L * 16);
 }
 
+// ---- the C/F split of level 1 from its 19-offset structure ---------------
+//
+// The reference's greedy split (amg.h:1-32, node_selection in natural
+// order, strength all-true at eps = 0) makes a node C iff none of its
+// lower-numbered neighbours is C.  On level 1 (even cells, coarse id
+// s >> 1 for nx even) the lower neighbours of the even cell (i,j,k) are the
+// offsets q19 = 0..8: (0,0,-2), (0,-1,-1), (-1,0,-1), (1,0,-1), (0,1,-1),
+// (0,-2,0), (-1,-1,0), (1,-1,0) -- in the x-rows (j,k-2), (j-1,k-1),
+// (j,k-1), (j+1,k-1), (j-2,k), (j-1,k) -- and (-2,0,0), the previous cell of
+// the same x-row.  So an x-row depends only on rows with a smaller
+// t = j + 2k, and the rows of one t are independent: one launch per t,
+// one warp per row.  Inside a row, with "blocked" = some lower neighbour in
+// another row is C, the row recurrence C_b = !blocked_b && !C_{b-1} makes
+// every run of unblocked cells alternate C, F, C, ... from its first cell
+// (or from the carried state of the previous 32-cell chunk).
+__global__ void __launch_bounds__(128)
+k_mis19_front(SG g, int t, int kmin, int rows, signed char *sel)
+{
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= rows) return;  // whole warps leave together
+    const int k = kmin + w, j = t - 2 * k;
+    const int p = (j + k) & 1, m = (g.nx - p + 1) >> 1;
+    const long rowbase = (long)j * g.nx + (long)k * g.nxy;
+    bool prev_c = false;
+    for (int b0 = 0; b0 < m; b0 += 32) {
+        const int b = b0 + lane;
+        const bool valid = b < m;
+        const int i = p + 2 * b;
+        const long s = rowbase + i;
+        bool blocked = !valid;
+        if (valid) {
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int a = i + q19x(q), bb = j + q19y(q), c = k + q19z(q);
+                if (a >= 0 && a < g.nx && bb >= 0 && bb < g.ny && c >= 0 && c < g.nz &&
+                    sel[(s + q19x(q) + q19y(q) * (long)g.nx + q19z(q) * g.nxy) >> 1] == 1)
+                    blocked = true;
+            }
+        }
+        const unsigned B = __ballot_sync(0xffffffffu, blocked);
+        const unsigned lower = B & ((1u << lane) - 1u);
+        bool is_c;
+        if (lower) is_c = !blocked && (((lane - (31 - __clz(lower)) - 1) & 1) == 0);
+        else is_c = !blocked && ((lane & 1) == (prev_c ? 1 : 0));
+        if (valid) sel[s >> 1] = is_c ? 1 : 2;
+        prev_c = __shfl_sync(0xffffffffu, is_c, 31);
+    }
+}
+
 }  // namespace
+
+int stencil19_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st)
+{
+    SG g{nx, ny, nz, (long)nx * ny};
+    const int tmax = (ny - 1) + 2 * (nz - 1);
+    for (int t = 0; t <= tmax; t++) {
+        const int kmin = t - (ny - 1) > 0 ? (t - (ny - 1) + 1) / 2 : 0;
+        const int kmax = t / 2 < nz - 1 ? t / 2 : nz - 1;
+        const int rows = kmax - kmin + 1;
+        if (rows <= 0) continue;
+        k_mis19_front<<<(rows + 3) / 4, 128, 0, st>>>(g, t, kmin, rows, sel);
+        HM_LAUNCHED();
+    }
+    return HMFEM_OK;
+}
 
 int stencil_parity_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st)
 {

@@ -42,48 +42,60 @@ int launch_smoother_diag(const Csr &A, int kind, double *dsm, float *dsm32,
     return HMFEM_OK;
 }
 
-// Explicit FP64 inverse of a small SPD level by in-place Gauss-Jordan
-// elimination (one block; SPD, so no pivoting): the coarse solve then is a
-// single dense mat-vec.  err = 1 on a non-positive pivot.
-__global__ void k_dense_factor(int n, const int *__restrict__ rowptr,
-                               const int *__restrict__ col,
-                               const double *__restrict__ val, double *M,
-                               int *err)
+// Explicit FP64 inverse of a small SPD level by Gauss-Jordan elimination
+// (SPD, so no pivoting): the coarse solve then is a single dense mat-vec.
+// One launch per pivot k over the whole matrix, reading one buffer and
+// writing the other (every element reads the old pivot row and column, so
+// no ordering inside a step is needed); err = 1 on a non-positive pivot.
+constexpr int kDenseMax = 512;
+
+__global__ void k_dense_load(int n, const int *__restrict__ rowptr,
+                             const int *__restrict__ col, const double *__restrict__ val,
+                             double *M)
 {
-    const long nn = (long)n * n;
-    for (long q = threadIdx.x; q < nn; q += blockDim.x) M[q] = 0.0;
+    const int i = blockIdx.y;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) M[(long)i * n + j] = 0.0;
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    if (threadIdx.x == 0)
         for (int k = rowptr[i]; k < rowptr[i + 1]; k++) M[(long)i * n + col[k]] += val[k];
-    __syncthreads();
-    __shared__ double s_pinv;
-    for (int k = 0; k < n; k++) {
-        if (threadIdx.x == 0) {
-            double p = M[(long)k * n + k];
-            if (!(p > 0.0)) { *err = 1; p = 1.0; }
-            s_pinv = 1.0 / p;
-        }
-        __syncthreads();
-        const double pinv = s_pinv;
-        for (int j = threadIdx.x; j < n; j += blockDim.x)
-            if (j != k) M[(long)k * n + j] *= pinv;
-        __syncthreads();
-        for (long q = threadIdx.x; q < nn; q += blockDim.x) {
-            const int i = (int)(q / n), j = (int)(q % n);
-            if (i != k && j != k) M[q] -= M[(long)i * n + k] * M[(long)k * n + j];
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += blockDim.x)
-            if (i != k) M[(long)i * n + k] *= -pinv;
-        if (threadIdx.x == 0) M[(long)k * n + k] = pinv;
-        __syncthreads();
+}
+
+__global__ void k_gj_step(int n, int k, const double *__restrict__ src, double *__restrict__ dst,
+                          int *err)
+{
+    const int i = blockIdx.y;
+    const double p = src[(long)k * n + k];
+    const double pinv = 1.0 / (p > 0.0 ? p : 1.0);
+    if (i == 0 && threadIdx.x == 0 && !(p > 0.0)) *err = 1;
+    const double *rk = src + (long)k * n, *ri = src + (long)i * n;
+    const double cik = ri[k];
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double v;
+        if (i == k) v = j == k ? pinv : rk[j] * pinv;
+        else if (j == k) v = cik * -pinv;
+        else v = ri[j] - cik * (rk[j] * pinv);
+        dst[(long)i * n + j] = v;
     }
 }
 
 int dense_factor(const Csr &A, double *Lf, int *err, cudaStream_t st)
 {
-    k_dense_factor<<<1, 1024, 0, st>>>(A.n, A.rowptr, A.col, A.val, Lf, err);
+    const int n = A.n;
+    if (n <= 0) return HMFEM_OK;
+    double *tmp = (double *)dalloc(sizeof(double) * (size_t)n * n);
+    if (!tmp) return HMFEM_E_CUDA;
+    const int th = n < 128 ? 32 * (int)ceil_div(n, 32) : 128;
+    // after n steps the inverse must land in Lf: start in the other buffer
+    double *a = (n & 1) ? tmp : Lf, *b = (n & 1) ? Lf : tmp;
+    k_dense_load<<<dim3(1, n), th, 0, st>>>(n, A.rowptr, A.col, A.val, a);
     HM_LAUNCHED();
+    for (int k = 0; k < n; k++) {
+        k_gj_step<<<dim3(1, n), th, 0, st>>>(n, k, a, b, err);
+        HM_LAUNCHED();
+        double *t = a; a = b; b = t;
+    }
+    HM_CUDA(cudaStreamSynchronize(st));
+    dfree(tmp);
     return HMFEM_OK;
 }
 
@@ -297,7 +309,7 @@ int setup(Solver &s)
     s.direct_level = -1;
     if (s.opt.coarse_direct > 0) {
         for (int k = 0; k < s.nlevels; k++) {
-            if (s.lv[k].A.n <= s.opt.coarse_direct) {
+            if (s.lv[k].A.n <= s.opt.coarse_direct && s.lv[k].A.n <= kDenseMax) {
                 const long n = s.lv[k].A.n;
                 HM_ALLOC(s.dense_L, double, n * n);
                 HM_CUDA(cudaMemsetAsync(s.dwork, 0, sizeof(int), st));

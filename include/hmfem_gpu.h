@@ -114,7 +114,8 @@ typedef struct {
     int max_levels;    /* compute.cpp:36: 16 */
     int min_coarse;    /* compute.cpp:37: 1 */
     int coarse_direct; /* solve the first level with <= this many rows
-                          exactly (explicit FP64 inverse, default 512); 0 =
+                          (at most 512) exactly (explicit FP64 inverse,
+                          default 512); 0 =
                           the reference's diagonal solve on the coarsest
                           level (amg.h:1353-1364) */
     int check_every;   /* host polls convergence every k iterations */
