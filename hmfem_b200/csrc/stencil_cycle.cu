@@ -171,7 +171,7 @@ k_g7_restrict(int nx, int ny, int nz, const int *__restrict__ cid,
         if (i < nx - 1) acc = A::add(acc, vr);
         if (j < ny - 1) acc = A::add(acc, vu);
         if (k < nz - 1) acc = A::add(acc, vt);
-        const int e = cid[s];
+        const int e = cid ? cid[s] : (int)(s >> 1);
         fc[e] = acc;
         sd.put(e, acc);
     }
@@ -211,6 +211,46 @@ k_g7_prolong(int nx, int ny, int nz, const int *__restrict__ cid,
             add = c == 1 ? t : A::div(t, (T)c);
         }
         u[s] = A::add(u[s], add);
+    }
+}
+
+// The same for nx even, a thread per x-neighbour pair (2t, 2t+1): one of
+// the two is a C cell, the other an F cell, so no warp diverges on the
+// cell type; coarse ids are s >> 1 (no index array) and every load of a
+// thread is independent.
+template <class T>
+__global__ void __launch_bounds__(256)
+k_g7_prolong2(int nx, int ny, int nz, const T *__restrict__ uc, T *__restrict__ u,
+              const Ctl *ctl)
+{
+    PDL_ENTRY();
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    const long nxy = (long)nx * ny, npair = nxy * nz / 2;
+    GRID_STRIDE(t, npair) {
+        const long s0 = 2 * t;
+        int i0, j, k;
+        cell_ijk((unsigned)s0, nx, ny, i0, j, k);
+        const bool c_first = ((j + k) & 1) == 0;  // i0 is even
+        const long sc = c_first ? s0 : s0 + 1, sf = c_first ? s0 + 1 : s0;
+        const int fi = c_first ? i0 + 1 : i0;
+        const T vc = uc[sc >> 1];
+        const bool h[6] = {j > 0, fi > 0, fi < nx - 1, j < ny - 1, k < nz - 1, k > 0};
+        const long o[6] = {-nx, -1, 1, nx, nxy, -nxy};
+        T v[6];
+#pragma unroll
+        for (int d = 0; d < 6; d++) v[d] = h[d] ? uc[(sf + o[d]) >> 1] : (T)0;
+        T acc = (T)0;
+        int c = 0;
+#pragma unroll
+        for (int d = 0; d < 6; d++) {
+            if (!h[d]) continue;
+            acc = c == 0 ? v[d] : A::add(acc, v[d]);
+            c++;
+        }
+        const T vf = c == 1 ? acc : A::div(acc, (T)c);
+        u[sc] = A::add(u[sc], vc);
+        u[sf] = A::add(u[sf], vf);
     }
 }
 
@@ -495,7 +535,9 @@ int g7_restrict(const Level &L, const T *rs, T *fc, Seed<T> sd, const Ctl *ctl,
     const Grid7 &g = L.g7;
     const long m = (long)((g.nx + 1) >> 1) * g.ny * g.nz;
     const int nblk = occ_blocks((const void *)k_g7_restrict<T>, m, 256, kRedBlocks);
-    launch_pdl(k_g7_restrict<T>, nblk, 256, st, g.nx, g.ny, g.nz, L.cid, rs, fc, sd, ctl);
+    // nx even: the C cell s has coarse id s >> 1, no index array needed
+    const int *cid = g.nx % 2 ? L.cid : nullptr;
+    launch_pdl(k_g7_restrict<T>, nblk, 256, st, g.nx, g.ny, g.nz, cid, rs, fc, sd, ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -504,6 +546,13 @@ template <class T>
 int g7_prolong(const Level &L, const T *uc, T *u, const Ctl *ctl, cudaStream_t st)
 {
     const Grid7 &g = L.g7;
+    if (g.nx % 2 == 0) {
+        const long npair = (long)L.A.n / 2;
+        const int nblk = occ_blocks((const void *)k_g7_prolong2<T>, npair, 256, kRedBlocks);
+        launch_pdl(k_g7_prolong2<T>, nblk, 256, st, g.nx, g.ny, g.nz, uc, u, ctl);
+        HM_LAUNCHED();
+        return HMFEM_OK;
+    }
     const int nblk = occ_blocks((const void *)k_g7_prolong<T>, L.A.n, 256, kRedBlocks);
     launch_pdl(k_g7_prolong<T>, nblk, 256, st, g.nx, g.ny, g.nz, L.cid, uc, u, ctl);
     HM_LAUNCHED();
