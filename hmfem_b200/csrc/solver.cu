@@ -201,8 +201,53 @@ static int download(T *dst, const T *src, long n, int mem, cudaStream_t st)
     return HMFEM_OK;
 }
 
+// flag = 1 if the m 32-bit words at a and b differ anywhere
+__global__ void k_words_differ(const unsigned *__restrict__ a, const unsigned *__restrict__ b,
+                               long m, int *flag)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < m;
+         i += (long)gridDim.x * blockDim.x)
+        if (a[i] != b[i]) { *flag = 1; return; }
+}
+
+static int words_differ(const void *a, const void *b, long bytes, int *flag, cudaStream_t st)
+{
+    const long m = bytes / 4;
+    if (m <= 0) return HMFEM_OK;
+    long nb = ceil_div(m, 256);
+    if (nb > 148L * 8) nb = 148L * 8;
+    k_words_differ<<<(int)nb, 256, 0, st>>>((const unsigned *)a, (const unsigned *)b, m, flag);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+// Setup reuse: compare a candidate level-0 CSR (device arrays) with the
+// one the hierarchy was built from; *same = bitwise identical.
+static int same_level0(Solver &s, const int *rowptr, const int *col, const double *val,
+                       bool *same)
+{
+    const Csr &A = s.lv[0].A;
+    cudaStream_t st = s.st;
+    HM_CUDA(cudaMemsetAsync(s.dwork, 0, sizeof(int), st));
+    HM_CHECK(words_differ(rowptr, A.rowptr, sizeof(int) * ((long)A.n + 1), s.dwork, st));
+    HM_CHECK(words_differ(col, A.col, sizeof(int) * A.nnz, s.dwork, st));
+    HM_CHECK(words_differ(val, A.val, sizeof(double) * A.nnz, s.dwork, st));
+    int flag = 1;
+    HM_CUDA(cudaMemcpyAsync(&flag, s.dwork, sizeof(int), cudaMemcpyDeviceToHost, st));
+    HM_CUDA(cudaStreamSynchronize(st));
+    *same = flag == 0;
+    return HMFEM_OK;
+}
+
+static bool can_reuse(const Solver &s, long n, long nnz)
+{
+    return s.opt.reuse_setup && s.setup_done && !s.have_grid && !s.lv.empty() &&
+           s.lv[0].A.n == n && (nnz < 0 || s.lv[0].A.nnz == nnz);
+}
+
 static int new_level0(Solver &s, int n)
 {
+    s.l0_same = false;
     free_hierarchy(s, false);
     free_vectors(s);
     s.lv.resize(1);
@@ -244,6 +289,12 @@ int setup(Solver &s)
                        __FILE__, __LINE__);
         return HMFEM_E_ARG;
     }
+    if (s.opt.reuse_setup && s.setup_done && s.l0_same) {
+        s.l0_same = false;  // one reuse per matrix set
+        s.last.setup_reused = 1;
+        return HMFEM_OK;
+    }
+    s.last.setup_reused = 0;
     cudaStream_t st = s.st;
     HM_PHASE(nullptr, st);
     free_hierarchy(s, true);
@@ -650,6 +701,30 @@ int hmfem_set_matrix(hmfem_solver *h, int n, long nnz, const int *cnt,
     Solver &s = h->s;
     hm::set_alloc_context(s.st, s.cache);
     cudaStream_t st = s.st;
+    if (hm::can_reuse(s, n, nnz)) {
+        int *rp = nullptr, *cl = nullptr;
+        double *vl = nullptr;
+        HM_ALLOC(rp, int, (long)n + 1);
+        HM_ALLOC(cl, int, nnz);
+        HM_ALLOC(vl, double, nnz);
+        HM_CHECK(hm::upload(rp, cnt, n, mem, st));
+        long tot = 0;
+        HM_CHECK(hm::rowptr_from_counts(rp, n, st, &tot));
+        bool same = false;
+        if (tot == nnz) {
+            HM_CHECK(hm::upload(cl, col, nnz, mem, st));
+            HM_CHECK(hm::upload(vl, ele, nnz, mem, st));
+            HM_CHECK(hm::same_level0(s, rp, cl, vl, &same));
+        }
+        hm::dfree(rp); hm::dfree(cl); hm::dfree(vl);
+        if (same) {
+            if (b) HM_CHECK(hm::upload(s.b, b, n, mem, st));
+            else HM_CUDA(cudaMemsetAsync(s.b, 0, sizeof(double) * n, st));
+            HM_CUDA(cudaStreamSynchronize(st));
+            s.l0_same = true;
+            return HMFEM_OK;
+        }
+    }
     HM_CHECK(hm::new_level0(s, n));
     s.have_grid = false;
     hm::Level &L = s.lv[0];
@@ -680,6 +755,44 @@ int hmfem_set_stencil(hmfem_solver *h, int nx, int ny, int nz,
     Solver &s = h->s;
     hm::set_alloc_context(s.st, s.cache);
     cudaStream_t st = s.st;
+    if (hm::can_reuse(s, n, -1)) {
+        // pack into scratch and compare with the matrix setup used
+        const hmfem_ele *cp = perm;
+        const hmfem_ind *ci = indcol;
+        hmfem_ele *tp = nullptr;
+        hmfem_ind *ti = nullptr;
+        if (!mem) {
+            HM_ALLOC(tp, hmfem_ele, n);
+            HM_ALLOC(ti, hmfem_ind, n);
+            HM_CHECK(hm::upload(tp, perm, n, 0, st));
+            HM_CHECK(hm::upload(ti, indcol, n, 0, st));
+            cp = tp;
+            ci = ti;
+        }
+        int *rp = nullptr;
+        HM_ALLOC(rp, int, n + 1);
+        HM_CHECK(hm::launch_pack_stencil((int)n, cp, ci, rp, nullptr, nullptr, nullptr, 0, st));
+        long nnz = 0;
+        HM_CHECK(hm::rowptr_from_counts(rp, (int)n, st, &nnz));
+        bool same = false;
+        if (nnz == s.lv[0].A.nnz && nnz > 0) {
+            int *cl = nullptr;
+            double *vl = nullptr;
+            HM_ALLOC(cl, int, nnz);
+            HM_ALLOC(vl, double, nnz);
+            HM_CHECK(hm::launch_pack_stencil((int)n, cp, ci, nullptr, rp, cl, vl, 1, st));
+            HM_CHECK(hm::same_level0(s, rp, cl, vl, &same));
+            hm::dfree(cl); hm::dfree(vl);
+        }
+        hm::dfree(rp); hm::dfree(tp); hm::dfree(ti);
+        if (same) {
+            if (b) HM_CHECK(hm::upload(s.b, b, n, mem, st));
+            else HM_CUDA(cudaMemsetAsync(s.b, 0, sizeof(double) * n, st));
+            HM_CUDA(cudaStreamSynchronize(st));
+            s.l0_same = true;
+            return HMFEM_OK;
+        }
+    }
     HM_CHECK(hm::new_level0(s, (int)n));
     s.have_grid = false;
     const hmfem_ele *dp = perm;
@@ -911,6 +1024,9 @@ static void bridge_options(hmfem_options *o)
     // compute.cpp:41-42: PCG eps 1e-8 on the preconditioned residual
     o->tol = 1e-8;
     o->stop_rule = 1;
+    // the reservoir loop hands the same matrix again on every Picard
+    // iteration (main.c:457-514): keep the hierarchy when it is unchanged
+    o->reuse_setup = 1;
     const char *t = getenv("HMFEM_TOL");
     if (t) o->tol = atof(t);
     const char *r = getenv("HMFEM_STOP");

@@ -30,6 +30,7 @@ struct Solver {
     std::vector<Level> lv;
     int nlevels = 0;
     bool setup_done = false;
+    bool l0_same = false;  // the last matrix set equals the one setup used
     int direct_level = -1;
     double *dense_L = nullptr;
 

@@ -52,7 +52,8 @@ class Options(C.Structure):
                 ("min_coarse", C.c_int), ("coarse_direct", C.c_int),
                 ("check_every", C.c_int), ("generic_setup", C.c_int),
                 ("gs_fused", C.c_int), ("cheb_from", C.c_int),
-                ("cheb_degree", C.c_int), ("verbose", C.c_int)]
+                ("cheb_degree", C.c_int), ("reuse_setup", C.c_int),
+                ("verbose", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -60,7 +61,8 @@ class Stats(C.Structure):
                 ("status", C.c_int), ("relres", C.c_double),
                 ("t_assemble_ms", C.c_double), ("t_setup_ms", C.c_double),
                 ("t_solve_ms", C.c_double), ("t_flux_ms", C.c_double),
-                ("divmin", C.c_double), ("divmax", C.c_double)]
+                ("divmin", C.c_double), ("divmax", C.c_double),
+                ("setup_reused", C.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -131,6 +131,14 @@ typedef struct {
                           D_l1^-1 A over [1/30, 1] instead (takes precedence
                           over gs_from; default 2; < 1 disables) */
     int cheb_degree;   /* 2..9 (default 4) */
+    int reuse_setup;   /* 1: hmfem_set_matrix / hmfem_set_stencil compare
+                          the new level-0 matrix with the current one on
+                          the device and, when it is bitwise identical,
+                          keep the whole hierarchy (the next hmfem_setup is
+                          a no-op) -- the reference's Picard loop re-runs
+                          the AMG setup on an unchanged matrix (main.c:
+                          457-514).  Default 0; compute / solve_linsys set
+                          it. */
     int verbose;
 } hmfem_options;
 
@@ -141,6 +149,7 @@ typedef struct {
     double relres;        /* final true ||b - A x|| / ||b|| (FP64) */
     double t_assemble_ms, t_setup_ms, t_solve_ms, t_flux_ms;
     double divmin, divmax; /* divvel_pontual min/max |div u| */
+    int setup_reused;      /* 1: the last hmfem_setup kept the hierarchy */
 } hmfem_stats;
 
 void hmfem_default_options(hmfem_options *opt);

@@ -212,6 +212,57 @@ def test_solve_linsys_dropin_warm_start(port):
     assert _rel(x, xo) < 1e-6
 
 
+def test_setup_reuse_keeps_hierarchy_for_unchanged_matrix(port):
+    """reuse_setup=1 (the reference bridge's setting): handing the same
+    matrix again keeps the hierarchy -- the solve with a new right-hand side
+    is bit-identical to a fresh solver's -- and any changed value rebuilds
+    it."""
+    p = config_problem(2, size=24)
+    perm, ind, b, (cnt, col, ele), H = _oracle(port, p)
+    s = gpu.Solver(tol=1e-10, reuse_setup=1)
+    s.set_matrix(cnt, col, ele, b)
+    s.setup()
+    x1, st1 = s.solve()
+    assert st1["setup_reused"] == 0
+    b2 = np.random.default_rng(8).standard_normal(p.n)
+    s.set_matrix(cnt, col, ele.copy(), b2)
+    s.setup()
+    x2, st2 = s.solve()
+    assert st2["setup_reused"] == 1
+    fresh = gpu.Solver(tol=1e-10)
+    fresh.set_matrix(cnt, col, ele, b2)
+    fresh.setup()
+    x3, st3 = fresh.solve()
+    np.testing.assert_array_equal(x2, x3)
+    # one changed value (a larger diagonal keeps it SPD): rebuilt
+    ele4 = ele.copy()
+    rp = np.concatenate([[0], np.cumsum(cnt)])
+    d0 = rp[0] + int(np.nonzero(col[rp[0]:rp[1]] == 0)[0][0])
+    ele4[d0] *= 1.5
+    s.set_matrix(cnt, col, ele4, b)
+    s.setup()
+    x4, st4 = s.solve()
+    assert st4["setup_reused"] == 0
+    H4 = port.amg(cnt, col, ele4)
+    xo, _, _ = H4.pcg(b, eps=1e-12, stop=1)
+    assert _rel(x4, xo) < 1e-8
+
+
+def test_compute_bridge_repeated_calls(port):
+    """The reservoir loop calls compute with the same matrix each Picard
+    iteration; the second call reuses the setup and returns the same x."""
+    p = config_problem(1, size=16)
+    perm, ind, b, (cnt, col, ele), H = _oracle(port, p)
+    hdr = np.array([p.n, len(col)], np.int32)
+    xa = np.zeros(p.n)
+    xb = np.zeros(p.n)
+    assert gpu.compute(hdr, cnt, col, ele, b.copy(), xa) == 0
+    ia = gpu.iter_amg()
+    assert gpu.compute(hdr, cnt, col, ele, b.copy(), xb) == 0
+    np.testing.assert_array_equal(xa, xb)
+    assert gpu.iter_amg() == ia
+
+
 def test_device_pointers_in_place():
     p = config_problem(2, size=24)
     s = gpu.Solver(tol=1e-10)
