@@ -1,5 +1,6 @@
 // common.cuh -- shared device helpers for the hmfem B200 kernels (sm_100a).
 #pragma once
+#include <atomic>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -30,8 +31,11 @@ void set_last_error(const char *msg, const char *file, int line);
 
 // Number of this library's kernels launched (captured launches count once
 // at capture; graph replays add the captured count).
-extern unsigned long long g_nlaunch;
-#define HM_COUNT() (++hm::g_nlaunch)
+// g_nlaunch counts every thread's launches; t_nlaunch the calling host
+// thread's (what a graph capture on this thread recorded)
+extern std::atomic<unsigned long long> g_nlaunch;
+extern thread_local unsigned long long t_nlaunch;
+#define HM_COUNT() (++hm::g_nlaunch, ++hm::t_nlaunch)
 #define HM_LAUNCHED()                                                         \
     do {                                                                      \
         HM_COUNT();                                                           \

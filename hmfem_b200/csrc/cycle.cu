@@ -482,7 +482,7 @@ __global__ void __launch_bounds__(256, 6)
 k_resid(const long long *__restrict__ sptr, const int *__restrict__ scol,
         const double *__restrict__ sval, int n, const double *__restrict__ b,
         const double *__restrict__ x, double *__restrict__ r, Ctl *ctl,
-        double *part, int init, Seed<double> sd)
+        double *part, int init, Seed<double> sd, Demote dm)
 {
     PDL_ENTRY();
     // init: 1 = start of the solve, 0 = convergence check (residual
@@ -499,7 +499,10 @@ k_resid(const long long *__restrict__ sptr, const int *__restrict__ scol,
         double bi = b[i];
         double ri = dsub(bi, s);
         r[i] = ri;
-        if (init != 2) sd.put(i, ri);
+        if (init != 2) {
+            sd.put(i, ri);
+            dm.put(i, ri);
+        }
         rr += ri * ri;
         bb += bi * bi;
     }
@@ -538,7 +541,7 @@ k_spmv_dot(const long long *__restrict__ sptr, const int *__restrict__ scol,
 __global__ void __launch_bounds__(256)
 k_update(int n, double *__restrict__ x, double *__restrict__ r,
          const double *__restrict__ s, const double *__restrict__ v, Ctl *ctl,
-         double *part, Seed<double> sd)
+         double *part, Seed<double> sd, Demote dm)
 {
     PDL_ENTRY();
     if (finished(ctl)) return;
@@ -549,6 +552,7 @@ k_update(int n, double *__restrict__ x, double *__restrict__ r,
         double ri = dsub(r[i], dmul(v[i], al));
         r[i] = ri;
         sd.put(i, ri);
+        dm.put(i, ri);
         rr += ri * ri;
     }
     grid_reduce_sum(rr, part, &ctl->tickets[RED_RR], [&](double t) {
@@ -560,13 +564,14 @@ k_update(int n, double *__restrict__ x, double *__restrict__ r,
 }
 
 // s = s * beta + z  (scale_add, pcg.h:69); sigma_last = sigma (pcg.h:70)
+template <class T>
 __global__ void __launch_bounds__(256)
-k_sdir(int n, double *__restrict__ s, const double *__restrict__ z, Ctl *ctl)
+k_sdir(int n, double *__restrict__ s, const T *__restrict__ z, Ctl *ctl)
 {
     PDL_ENTRY();
     if (finished(ctl)) return;
     const double be = ctl->beta;
-    GRID_STRIDE(i, n) s[i] = dadd(dmul(s[i], be), z[i]);
+    GRID_STRIDE(i, n) s[i] = dadd(dmul(s[i], be), (double)z[i]);
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->sigma_last = ctl->sigma;
 }
 
@@ -585,7 +590,7 @@ k_finish_z(int n, const T *__restrict__ src, const double *__restrict__ r,
     double d1 = 0.0, d2 = 0.0;
     GRID_STRIDE(i, n) {
         double zi = (double)src[i];
-        z[i] = zi;
+        if (z) z[i] = zi;
         d1 += zi * r[i];
         if (flexible && !first) d2 += zi * v[i];
     }
@@ -929,6 +934,18 @@ static Seed<double> cg_seed(Solver &s)
     return seed_of<double>(s, 0);
 }
 
+static Demote cg_demote(Solver &s)
+{
+    if (s.opt.precision != 1) return {nullptr, {nullptr, nullptr, 0.f}};
+    return {s.lv[0].f32, seed_of<float>(s, 0)};
+}
+
+static const float *cg_z32(Solver &s)
+{
+    const bool top_is_coarse = s.nlevels == 1 || s.direct_level == 0;
+    return top_is_coarse ? s.lv[0].ua32 : s.lv[0].ub32;
+}
+
 // z = C r, sigma = (z, r), beta (fused into the last V-cycle kernel where
 // the V-cycle is FP64 and has a coarse level)
 int cg_precondition(Solver &s, cudaStream_t st)
@@ -947,12 +964,21 @@ int cg_precondition(Solver &s, cudaStream_t st)
         }
         return HMFEM_OK;
     }
-    launch_pdl(k_demote, nb(n), 256, st, n, s.r, L0.f32, seed_of<float>(s, 0), s.ctl);
-    HM_LAUNCHED();
+    // f32 and its seed were written by the kernel that produced r
     HM_CHECK(cycle_fp32(s, 0, st, false, true));
-    const float *z32 = top_is_coarse ? L0.ua32 : L0.ub32;
-    launch_pdl(k_finish_z<float>, nb(n), 256, st, n, z32, s.r, s.v, s.z, s.ctl,
-                                             s.part, s.first_sigma, 1);
+    launch_pdl(k_finish_z<float>, nb(n), 256, st, n, cg_z32(s), s.r, s.v,
+               (double *)nullptr, s.ctl, s.part, s.first_sigma, 1);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+// s = s beta + z with z the preconditioned residual (FP32 cycle: read as
+// FP32 straight from the cycle's output, never stored in FP64)
+static int cg_sdir(Solver &s, cudaStream_t st)
+{
+    const int n = s.lv[0].A.n;
+    if (s.opt.precision == 1) launch_pdl(k_sdir<float>, nb(n), 256, st, n, s.s, cg_z32(s), s.ctl);
+    else launch_pdl(k_sdir<double>, nb(n), 256, st, n, s.s, (const double *)s.z, s.ctl);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -962,17 +988,16 @@ int cg_init(Solver &s, cudaStream_t st)
     Level &L0 = s.lv[0];
     const int n = L0.A.n;
     if (s.use_g7(0)) {
-        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 1, cg_seed(s), st));
+        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 1, cg_seed(s), cg_demote(s), st));
     } else {
         launch_pdl(k_resid, nb(n), 256, st, L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
-                                       s.r, s.ctl, s.part, 1, cg_seed(s));
+                                       s.r, s.ctl, s.part, 1, cg_seed(s), cg_demote(s));
         HM_LAUNCHED();
     }
     s.first_sigma = 1;
     HM_CHECK(cg_precondition(s, st));
     s.first_sigma = 0;
-    launch_pdl(k_sdir, nb(n), 256, st, n, s.s, s.z, s.ctl);
-    HM_LAUNCHED();
+    HM_CHECK(cg_sdir(s, st));
     return HMFEM_OK;
 }
 
@@ -988,18 +1013,18 @@ int cg_iteration(Solver &s, cudaStream_t st)
                                           s.v, s.ctl, s.part);
         HM_LAUNCHED();
     }
-    launch_pdl(k_update, nb(n), 256, st, n, s.x, s.r, s.s, s.v, s.ctl, s.part, cg_seed(s));
+    launch_pdl(k_update, nb(n), 256, st, n, s.x, s.r, s.s, s.v, s.ctl, s.part, cg_seed(s),
+               cg_demote(s));
     HM_LAUNCHED();
     if (g7) {
-        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 0, cg_seed(s), st));
+        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 0, cg_seed(s), cg_demote(s), st));
     } else {
         launch_pdl(k_resid, nb(n), 256, st, L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
-                                       s.r, s.ctl, s.part, 0, cg_seed(s));
+                                       s.r, s.ctl, s.part, 0, cg_seed(s), cg_demote(s));
         HM_LAUNCHED();
     }
     HM_CHECK(cg_precondition(s, st));
-    launch_pdl(k_sdir, nb(n), 256, st, n, s.s, s.z, s.ctl);
-    HM_LAUNCHED();
+    HM_CHECK(cg_sdir(s, st));
     return HMFEM_OK;
 }
 
@@ -1009,10 +1034,10 @@ int cg_final_residual(Solver &s, cudaStream_t st)
     Level &L0 = s.lv[0];
     const int n = L0.A.n;
     if (s.use_g7(0)) {
-        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 2, Seed<double>{}, st));
+        HM_CHECK(g7_resid(L0, s.b, s.x, s.r, s.ctl, s.part, 2, Seed<double>{}, Demote{}, st));
     } else {
         launch_pdl(k_resid, nb(n), 256, st, L0.S.sptr, L0.S.col, L0.S.val, n, s.b, s.x,
-                                       s.r, s.ctl, s.part, 2, Seed<double>{});
+                                       s.r, s.ctl, s.part, 2, Seed<double>{}, Demote{});
         HM_LAUNCHED();
     }
     return HMFEM_OK;

@@ -77,6 +77,21 @@ template <class T> struct Seed {
     }
 };
 
+// The FP32 cycle's right-hand side: the CG kernels that write r also write
+// f = (float) r and its seed (f == nullptr: FP64 cycle, nothing to do).
+struct Demote {
+    float *f;
+    Seed<float> sd;
+    __device__ __forceinline__ void put(long i, double r) const
+    {
+        if (f) {
+            const float fi = (float)r;
+            f[i] = fi;
+            sd.put(i, fi);
+        }
+    }
+};
+
 // sigma = (C r, r) once the preconditioner is applied (pcg.h:66-67, and
 // 46-47 on the first application); run by the last block of the fused
 // reduction.

@@ -402,9 +402,9 @@ static int capture_iteration(Solver &s)
     cudaStream_t cs;
     HM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     HM_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    const unsigned long long before = g_nlaunch;
+    const unsigned long long before = t_nlaunch;
     int rc = cg_iteration(s, cs);
-    s.graph_kernels = g_nlaunch - before;
+    s.graph_kernels = t_nlaunch - before;
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);
@@ -1101,4 +1101,4 @@ void solve_linsys_cxx(hmfem_ele *perm, hmfem_ind *indcol, double *b, double *x,
     solve_linsys(perm, indcol, b, x, N);
 }
 
-extern "C" unsigned long long hmfem_launch_count(void) { return hm::g_nlaunch; }
+extern "C" unsigned long long hmfem_launch_count(void) { return hm::g_nlaunch.load(); }

@@ -8,6 +8,7 @@
 namespace hm {
 
 template <class T> struct Seed;  // cycle.cuh
+struct Demote;                     // cycle.cuh
 
 struct Solver {
     hmfem_options opt;
@@ -105,7 +106,7 @@ int g7_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo, C
 int g7_spmv_dot(const Level &L, const double *x, double *y, Ctl *ctl, double *part,
                  cudaStream_t st);
 int g7_resid(const Level &L, const double *b, const double *x, double *r, Ctl *ctl,
-             double *part, int init, Seed<double> sd, cudaStream_t st);
+             double *part, int init, Seed<double> sd, Demote dm, cudaStream_t st);
 int g7_spmv(const Level &L, const double *x, double *y, cudaStream_t st);
 template <class T, class V>
 int g19_pre(const Level &L, const T *f, const T *u, T *rs, const Ctl *ctl, cudaStream_t st);

@@ -1,6 +1,7 @@
 // sparse.cu -- scans, CSR -> SELL-32 conversion, diagonal extraction and the
 // FP64 SELL SpMV.
 #include <cub/device/device_scan.cuh>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <unordered_map>
@@ -9,7 +10,8 @@
 
 namespace hm {
 
-static char g_err[512];
+// per host thread: solvers driven from several threads report their own
+static thread_local char g_err[512];
 
 void set_last_error(const char *msg, const char *file, int line)
 {
@@ -17,7 +19,8 @@ void set_last_error(const char *msg, const char *file, int line)
 }
 
 int g_verbose = 0;
-unsigned long long g_nlaunch = 0;
+std::atomic<unsigned long long> g_nlaunch{0};
+thread_local unsigned long long t_nlaunch = 0;
 
 void phase_mark(const char *label, cudaStream_t st)
 {
@@ -39,8 +42,9 @@ namespace hm {
 // Device memory comes from the stream-ordered pool of the current device
 // with its release threshold raised, so the buffers a setup frees are handed
 // back to the next setup without synchronising cudaMalloc / cudaFree calls.
-static cudaStream_t g_astream = nullptr;
-static unsigned g_pool_ready = 0;  // bit per device
+// the allocation context is per host thread (one solver per thread)
+static thread_local cudaStream_t g_astream = nullptr;
+static std::atomic<unsigned> g_pool_ready{0};  // bit per device
 
 // Per-solver cache of freed blocks keyed by exact size: a solver that sets
 // up the same grid again gets every buffer back without touching the pool.
@@ -48,7 +52,7 @@ struct AllocCache {
     std::unordered_map<void *, size_t> live;
     std::multimap<size_t, void *> idle;
 };
-static AllocCache *g_cache = nullptr;
+static thread_local AllocCache *g_cache = nullptr;
 
 void set_alloc_stream(cudaStream_t st) { g_astream = st; }
 

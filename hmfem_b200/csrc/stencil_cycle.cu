@@ -311,7 +311,8 @@ k_g7_spmv(G7v<double> g, int n, const double *__restrict__ x, double *__restrict
 // r = b - A x; (r, r); (b, b)   (k_resid on the stencil)
 __global__ void __launch_bounds__(256)
 k_g7_resid(G7v<double> g, int n, const double *__restrict__ b, const double *__restrict__ x,
-           double *__restrict__ r, Ctl *ctl, double *part, int init, Seed<double> sd)
+           double *__restrict__ r, Ctl *ctl, double *part, int init, Seed<double> sd,
+           Demote dm)
 {
     PDL_ENTRY();
     if (init == 0 && (finished(ctl) || !ctl->check)) return;
@@ -323,7 +324,10 @@ k_g7_resid(G7v<double> g, int n, const double *__restrict__ b, const double *__r
         const double bi = b[s];
         const double ri = dsub(bi, a);
         r[s] = ri;
-        if (init != 2) sd.put(s, ri);
+        if (init != 2) {
+            sd.put(s, ri);
+            dm.put(s, ri);
+        }
         rr += ri * ri;
         bb += bi * bi;
     }
@@ -582,11 +586,12 @@ int g7_spmv_dot(const Level &L, const double *x, double *y, Ctl *ctl, double *pa
 }
 
 int g7_resid(const Level &L, const double *b, const double *x, double *r, Ctl *ctl,
-             double *part, int init, Seed<double> sd, cudaStream_t st)
+             double *part, int init, Seed<double> sd, Demote dm, cudaStream_t st)
 {
     const int n = L.A.n;
     const int nblk = occ_blocks((const void *)k_g7_resid, n, 256, kRedBlocks);
-    launch_pdl(k_g7_resid, nblk, 256, st, g7v<double>(L.g7), n, b, x, r, ctl, part, init, sd);
+    launch_pdl(k_g7_resid, nblk, 256, st, g7v<double>(L.g7), n, b, x, r, ctl, part, init, sd,
+               dm);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
