@@ -1,0 +1,216 @@
+"""The learned initial guess: a 3-level 3-D U-Net (16/32/64 channels, 3x3x3
+kernels) that maps log K, the conduit mask and the Dirichlet mask of a grid
+to a pressure guess for the CG.  No counterpart in the reference.
+
+Every 3x3x3 convolution -- forward, data gradient and weight gradient --
+runs on this library's tcgen05 tensor-core kernels (`hmfem_conv3d_fwd`,
+`hmfem_conv3d_wgrad`: BF16 operands, FP32 accumulation).  PyTorch is the
+training driver around them: autograd bookkeeping, the 2x average pooling,
+nearest upsampling and channel concatenation (pure data movement), the 1x1
+head and the Adam update of the FP32 master weights.
+
+Activations are channels-last: a grid of n = nx*ny*nz cells is an (n, C)
+BF16 tensor, cell s = x + nx (y + ny z).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+
+from . import gpu
+
+CH = (16, 32, 64)
+IN_CH = 16          # 3 input features, zero-padded to the kernels' K step
+_SHAPES = {(16, 16), (16, 32), (32, 16), (32, 32), (32, 64), (64, 32), (64, 64),
+           (96, 32), (32, 96), (48, 16), (16, 48)}
+
+
+def _lib():
+    L = gpu.lib()
+    if not getattr(L, "_guess_bound", False):
+        vp, i = C.c_void_p, C.c_int
+        L.hmfem_conv3d_fwd.argtypes = [vp, vp, vp, vp, i, i, i, i, i, i, vp, vp]
+        L.hmfem_conv3d_wgrad.argtypes = [vp, vp, vp, i, i, i, i, i, vp, vp]
+        L._guess_bound = True
+    return L
+
+
+_ERR = {}
+
+
+def _err_buf(dev):
+    if dev not in _ERR:
+        _ERR[dev] = torch.zeros(1, dtype=torch.int32, device=dev)
+    return _ERR[dev]
+
+
+def check_errors(dev=None):
+    """Raises if a tensor-core kernel reported a timed-out wait."""
+    dev = dev or torch.device("cuda", torch.cuda.current_device())
+    e = _err_buf(dev)
+    if int(e.item()) != 0:
+        e.zero_()
+        raise RuntimeError("conv3d: a bounded tensor-core wait gave up")
+
+
+def conv3d_raw(x, w, bias, dims, relu):
+    """out = relu?(conv(x, w) + bias): x (n, cin) bf16, w (27, cout, cin) bf16."""
+    nx, ny, nz = dims
+    n, cin = x.shape
+    cout = w.shape[1]
+    assert (cin, cout) in _SHAPES, (cin, cout)
+    assert x.dtype == torch.bfloat16 and w.dtype == torch.bfloat16
+    x = x.contiguous()
+    w = w.contiguous()
+    out = torch.empty(n, cout, dtype=torch.bfloat16, device=x.device)
+    st = torch.cuda.current_stream(x.device).cuda_stream
+    rc = _lib().hmfem_conv3d_fwd(x.data_ptr(), w.data_ptr(),
+                                 bias.data_ptr() if bias is not None else None,
+                                 out.data_ptr(), nx, ny, nz, cin, cout, int(relu),
+                                 _err_buf(x.device).data_ptr(), st)
+    if rc != 0:
+        raise gpu.HmfemError(rc, gpu.last_error())
+    return out
+
+
+def conv3d_wgrad_raw(x, dy, dims):
+    """dw (27, cout, cin) fp32 = sum over cells dy[cell][co] x[cell + tap][ci]."""
+    nx, ny, nz = dims
+    cin, cout = x.shape[1], dy.shape[1]
+    dw = torch.zeros(27, cout, cin, dtype=torch.float32, device=x.device)
+    st = torch.cuda.current_stream(x.device).cuda_stream
+    rc = _lib().hmfem_conv3d_wgrad(x.contiguous().data_ptr(), dy.contiguous().data_ptr(),
+                                   dw.data_ptr(), nx, ny, nz, cin, cout,
+                                   _err_buf(x.device).data_ptr(), st)
+    if rc != 0:
+        raise gpu.HmfemError(rc, gpu.last_error())
+    return dw
+
+
+def flip_transpose(w):
+    """Weights of the data gradient: w_t[t][ci][co] = w[26 - t][co][ci]."""
+    return w.flip(0).transpose(1, 2).contiguous()
+
+
+class Conv3x3x3(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, w, bias, dims, relu):
+        wb = w.to(torch.bfloat16)
+        out = conv3d_raw(x, wb, bias, dims, relu)
+        ctx.save_for_backward(x, wb, out)
+        ctx.dims, ctx.relu = dims, relu
+        return out
+
+    @staticmethod
+    def backward(ctx, gout):
+        x, wb, out = ctx.saved_tensors
+        g = gout.to(torch.bfloat16)
+        if ctx.relu:
+            g = g * (out > 0).to(g.dtype)
+        gx = conv3d_raw(g, flip_transpose(wb), None, ctx.dims, False)
+        gw = conv3d_wgrad_raw(x, g, ctx.dims)
+        gb = g.float().sum(0)
+        return gx, gw, gb, None, None
+
+
+def conv(x, w, b, dims, relu=True):
+    return Conv3x3x3.apply(x, w, b, dims, relu)
+
+
+# ---- grid data movement (channels-last, dims (nx, ny, nz)) -----------------
+
+def pool2(x, dims):
+    nx, ny, nz = dims
+    c = x.shape[1]
+    v = x.view(nz // 2, 2, ny // 2, 2, nx // 2, 2, c).float().mean(dim=(1, 3, 5))
+    return v.reshape(-1, c).to(x.dtype), (nx // 2, ny // 2, nz // 2)
+
+
+def up2(x, dims):
+    nx, ny, nz = dims
+    c = x.shape[1]
+    v = x.view(nz, 1, ny, 1, nx, 1, c).expand(nz, 2, ny, 2, nx, 2, c)
+    return v.reshape(-1, c), (2 * nx, 2 * ny, 2 * nz)
+
+
+class UNet(torch.nn.Module):
+    """enc 16 -> pool -> enc 32 -> pool -> 64 -> up + skip -> 32 -> up + skip
+    -> 16 -> 1x1 head; two 3x3x3 convolutions (ReLU) per stage."""
+
+    SPEC = [("e0a", IN_CH, 16), ("e0b", 16, 16), ("e1a", 16, 32), ("e1b", 32, 32),
+            ("bna", 32, 64), ("bnb", 64, 64), ("d1a", 96, 32), ("d1b", 32, 32),
+            ("d0a", 48, 16), ("d0b", 16, 16)]
+
+    def __init__(self, seed=0):
+        super().__init__()
+        g = torch.Generator().manual_seed(seed)
+        self.w = torch.nn.ParameterDict()
+        self.b = torch.nn.ParameterDict()
+        for name, cin, cout in self.SPEC:
+            std = math.sqrt(2.0 / (27 * cin))
+            self.w[name] = torch.nn.Parameter(torch.randn(27, cout, cin, generator=g) * std)
+            self.b[name] = torch.nn.Parameter(torch.zeros(cout))
+        self.head = torch.nn.Parameter(torch.randn(16, generator=g) * 0.01)
+        self.head_b = torch.nn.Parameter(torch.zeros(1))
+
+    def n_params(self):
+        return sum(p.numel() for p in self.parameters())
+
+    def forward(self, feats, dims):
+        """feats (n, IN_CH) bf16 -> (n,) fp32 pressure correction."""
+        def block(x, a, b_, d):
+            x = conv(x, self.w[a], self.b[a], d)
+            return conv(x, self.w[b_], self.b[b_], d)
+        d0 = dims
+        e0 = block(feats, "e0a", "e0b", d0)
+        x, d1 = pool2(e0, d0)
+        e1 = block(x, "e1a", "e1b", d1)
+        x, d2 = pool2(e1, d1)
+        x = block(x, "bna", "bnb", d2)
+        x, _ = up2(x, d2)
+        x = block(torch.cat([x, e1], 1), "d1a", "d1b", d1)
+        x, _ = up2(x, d1)
+        x = block(torch.cat([x, e0], 1), "d0a", "d0b", d0)
+        return x.float() @ self.head + self.head_b
+
+
+# ---- inputs and targets ------------------------------------------------------
+
+def features(prob, device="cuda"):
+    """(n, IN_CH) bf16: (log10 K + 14) / 2, conduit mask, Dirichlet face mask
+    (+1 at x = 0, -1 at x = 1), zero padding channels."""
+    nx, ny, nz = prob.nx, prob.ny, prob.nz
+    f = torch.zeros(prob.n, IN_CH, dtype=torch.float32, device=device)
+    f[:, 0] = (torch.log10(torch.as_tensor(prob.KX, device=device)) + 14.0) / 2.0
+    if getattr(prob, "conduit_mask", None) is not None:
+        f[:, 1] = torch.as_tensor(prob.conduit_mask, device=device).float()
+    i = torch.arange(prob.n, device=device) % nx
+    f[:, 2] = (i == 0).float() - (i == nx - 1).float()
+    return f.to(torch.bfloat16)
+
+
+def linear_profile(prob, device="cuda"):
+    """The homogeneous solution p = 1 - (i + 1/2) / nx the net corrects."""
+    i = (torch.arange(prob.n, device=device) % prob.nx).double()
+    return 1.0 - (i + 0.5) / prob.nx
+
+
+def guess(model, prob, device="cuda"):
+    """FP64 pressure guess on the device."""
+    with torch.no_grad():
+        corr = model(features(prob, device), (prob.nx, prob.ny, prob.nz))
+    return linear_profile(prob, device) + corr.double()
+
+
+def save(model, path):
+    np.savez(path, **{k: v.detach().cpu().float().numpy() for k, v in model.state_dict().items()})
+
+
+def load(path, device="cuda"):
+    m = UNet()
+    d = np.load(path)
+    m.load_state_dict({k: torch.tensor(d[k]) for k in d.files})
+    return m.to(device)

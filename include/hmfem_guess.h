@@ -1,0 +1,35 @@
+/* hmfem_guess.h -- kernels of the learned initial guess (a 3-level 3-D
+ * U-Net mapping log K, the conduit mask and the Dirichlet mask to a pressure
+ * guess).  No counterpart in the reference: the reference always starts its
+ * CG from the previous pressure or zero.
+ *
+ * Tensors are device pointers.  Activations are channels-last BF16: cell
+ * s = x + nx (y + ny z) holds C consecutive values.  3x3x3 weights are BF16
+ * [27][Cout][Cin] with tap t = 9 (dz+1) + 3 (dy+1) + (dx+1) (cross-
+ * correlation, zero padding).  Supported (Cin, Cout): (16,16) (16,32)
+ * (32,16) (32,32) (32,64) (64,32) (64,64) (96,32) (32,96) (48,16) (16,48).
+ * `stream` is a cudaStream_t (NULL: legacy default stream); `err` a device
+ * int the kernels set to 1 if a bounded tensor-core wait gave up. */
+#ifndef HMFEM_GUESS_H
+#define HMFEM_GUESS_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* out = relu?(conv3x3x3(in, w) + bias) on the tcgen05 tensor cores (BF16
+ * operands, FP32 accumulation in tensor memory); bias may be NULL.  With
+ * weights flipped in the taps and transposed in the channels this is also
+ * the data gradient of a convolution. */
+int hmfem_conv3d_fwd(const void *in, const void *w, const float *bias, void *out, int nx,
+                     int ny, int nz, int cin, int cout, int relu, int *err, void *stream);
+
+/* dw[27][cout][cin] += sum over cells of dy[cell][co] x[cell + tap][ci] (the
+ * weight gradient), FP32, on the tensor cores. */
+int hmfem_conv3d_wgrad(const void *x, const void *dy, float *dw, int nx, int ny, int nz,
+                       int cin, int cout, int *err, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
