@@ -179,30 +179,33 @@ class UNet(torch.nn.Module):
 
 # ---- inputs and targets ------------------------------------------------------
 
-def features(prob, device="cuda"):
-    """(n, IN_CH) bf16: (log10 K + 14) / 2, conduit mask, Dirichlet face mask
-    (+1 at x = 0, -1 at x = 1), zero padding channels."""
-    nx, ny, nz = prob.nx, prob.ny, prob.nz
-    f = torch.zeros(prob.n, IN_CH, dtype=torch.float32, device=device)
-    f[:, 0] = (torch.log10(torch.as_tensor(prob.KX, device=device)) + 14.0) / 2.0
-    if getattr(prob, "conduit_mask", None) is not None:
-        f[:, 1] = torch.as_tensor(prob.conduit_mask, device=device).float()
-    i = torch.arange(prob.n, device=device) % nx
+def features(K, mask, dims):
+    """(n, IN_CH) bf16 from device K (n,) and conduit mask (n,):
+    (log10 K + 14) / 2, the mask, the Dirichlet face mask (+1 at x = 0,
+    -1 at x = 1) and zero channels up to IN_CH."""
+    nx = dims[0]
+    n = K.numel()
+    f = torch.zeros(n, IN_CH, dtype=torch.float32, device=K.device)
+    f[:, 0] = (torch.log10(K) + 14.0) / 2.0
+    if mask is not None:
+        f[:, 1] = mask.float()
+    i = torch.arange(n, device=K.device) % nx
     f[:, 2] = (i == 0).float() - (i == nx - 1).float()
     return f.to(torch.bfloat16)
 
 
-def linear_profile(prob, device="cuda"):
+def linear_profile(dims, device="cuda"):
     """The homogeneous solution p = 1 - (i + 1/2) / nx the net corrects."""
-    i = (torch.arange(prob.n, device=device) % prob.nx).double()
-    return 1.0 - (i + 0.5) / prob.nx
+    nx, ny, nz = dims
+    i = (torch.arange(nx * ny * nz, device=device) % nx).double()
+    return 1.0 - (i + 0.5) / nx
 
 
-def guess(model, prob, device="cuda"):
+def predict(model, K, mask, dims):
     """FP64 pressure guess on the device."""
     with torch.no_grad():
-        corr = model(features(prob, device), (prob.nx, prob.ny, prob.nz))
-    return linear_profile(prob, device) + corr.double()
+        corr = model(features(K, mask, dims), dims)
+    return linear_profile(dims, K.device) + corr.double()
 
 
 def save(model, path):
