@@ -88,7 +88,7 @@ def _feats(f3):
     return f
 
 
-def train(model, data, size, epochs, lr=2e-3, log_every=0):
+def train(model, data, size, epochs, lr=1e-3, log_every=0):
     dims = (size, size, size)
     opt = torch.optim.Adam(model.parameters(), lr=lr)
     steps = epochs * len(data)
@@ -103,11 +103,12 @@ def train(model, data, size, epochs, lr=2e-3, log_every=0):
             loss = (pred - target).norm() / pnorm
             opt.zero_grad(set_to_none=True)
             loss.backward()
+            torch.nn.utils.clip_grad_norm_(model.parameters(), 1.0)
             opt.step()
             sched.step()
             k += 1
             if log_every and k % log_every == 0:
-                hist.append((k, float(loss)))
+                hist.append((k, float(loss.detach())))
     guess.check_errors()
     return hist
 
@@ -146,7 +147,7 @@ def main():
     ap.add_argument("--train", type=int, default=2048)
     ap.add_argument("--eval", type=int, default=256)
     ap.add_argument("--epochs", type=int, default=4)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default="unet_guess.npz")
     args = ap.parse_args()
     torch.manual_seed(0)

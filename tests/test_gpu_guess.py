@@ -79,10 +79,12 @@ def _ref_forward_with_grad(model, feats, dims):
 
 def test_short_training_guess_beats_zero_guess():
     size = 32
-    data = train_guess.make_dataset(range(32), size)
+    data = train_guess.make_dataset(range(16), size)
     model = guess.UNet().cuda()
-    hist = train_guess.train(model, data, size, epochs=3, log_every=8)
-    assert hist[-1][1] < hist[0][1]  # the loss went down
+    hist = train_guess.train(model, data, size, epochs=6, log_every=1)
+    first = np.mean([h[1] for h in hist[:16]])
+    last = np.mean([h[1] for h in hist[-16:]])
+    assert last < first  # the mean loss over an epoch went down
     rows = train_guess.evaluate(model, range(32, 36), size)
     assert all(r["relres_net"] <= 1e-10 for r in rows)
     assert np.mean([r["it_net"] for r in rows]) <= np.mean([r["it_zero"] for r in rows])
