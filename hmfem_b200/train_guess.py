@@ -141,6 +141,21 @@ def evaluate(model, seeds, size, device="cuda", tol=1e-10):
     return rows
 
 
+def infer_once(size=128, seed=5000, path=None):
+    """One guess inference on a config-4 grid (the command the conv3d ncu
+    summary profiles); returns its wall time in ms."""
+    model = guess.load(path) if path else guess.UNet().cuda()
+    prob, K, mask = sample(seed, size)
+    dims = (size, size, size)
+    guess.predict(model, K, mask, dims)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    guess.predict(model, K, mask, dims)
+    torch.cuda.synchronize()
+    guess.check_errors()
+    return 1e3 * (time.perf_counter() - t0)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--size", type=int, default=128)
@@ -149,7 +164,12 @@ def main():
     ap.add_argument("--epochs", type=int, default=4)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default="unet_guess.npz")
+    ap.add_argument("--infer-only", action="store_true",
+                    help="time one inference at --size (no training) and exit")
     args = ap.parse_args()
+    if args.infer_only:
+        print(json.dumps({"size": args.size, "inference_ms": infer_once(args.size)}))
+        return
     torch.manual_seed(0)
     t0 = time.perf_counter()
     data = make_dataset(range(args.train), args.size)
