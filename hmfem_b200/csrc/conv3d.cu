@@ -157,12 +157,34 @@ __host__ __device__ constexpr int tmem_cols(int n)
 
 // ---- forward / data gradient ----------------------------------------------
 
+// Taps gathered per stage (one barrier and one commit per stage) and
+// whether all 27 taps of the weights stay resident in shared memory.
 template <int CIN, int COUT>
 struct FwdSmem {
-    static constexpr int kA = CIN * 256;       // 128 rows x CIN x 2 B
-    static constexpr int kB = COUT * CIN * 2;  // COUT rows x CIN x 2 B
-    static constexpr int kBytes = 2 * kA + 2 * kB + 64;
+    static constexpr int kStage = (24 * 1024) / (CIN * 256) < 1 ? 1
+                                : (24 * 1024) / (CIN * 256) > 9 ? 9
+                                : (24 * 1024) / (CIN * 256);
+    static constexpr bool kWRes = 27 * COUT * CIN * 2 <= 56 * 1024;
+    static constexpr int kATap = CIN * 256;       // 128 rows x CIN x 2 B
+    static constexpr int kBTap = COUT * CIN * 2;  // COUT rows x CIN x 2 B
+    static constexpr int kA = kStage * kATap;     // one A buffer
+    static constexpr int kB = kWRes ? 27 * kBTap : kStage * kBTap;
+    static constexpr int kBBufs = kWRes ? 1 : 2;
+    static constexpr int kBytes = 2 * kA + kBBufs * kB + 64;
 };
+
+// B tile of one tap into shared memory (K-major: row n = output channel)
+template <int CIN, int COUT>
+__device__ __forceinline__ void stage_weights(const __nv_bfloat16 *__restrict__ w, int tap,
+                                              unsigned char *dst, int tid)
+{
+    constexpr int ACH = CIN / 8;
+    const uint4 *wt = (const uint4 *)(w + (long)tap * COUT * CIN);
+    for (int i = tid; i < COUT * ACH; i += 128) {
+        const int row = i / ACH, c = i % ACH;
+        *(uint4 *)(dst + c * (COUT * 16) + row * 16) = wt[row * ACH + c];
+    }
+}
 
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(128)
@@ -173,8 +195,9 @@ k_conv3d(const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 256, "channel counts");
     extern __shared__ __align__(128) unsigned char smem[];
     using S = FwdSmem<CIN, COUT>;
+    constexpr int ST = S::kStage;
     unsigned char *abuf = smem, *bbuf = smem + 2 * S::kA;
-    uint64_t *mbar = (uint64_t *)(smem + 2 * S::kA + 2 * S::kB);
+    uint64_t *mbar = (uint64_t *)(smem + 2 * S::kA + S::kBBufs * S::kB);
     uint32_t *tslot = (uint32_t *)(mbar + 2);
     constexpr int NCOL = tmem_cols(COUT);
     constexpr uint32_t IDESC = idesc_bf16(128, COUT);
@@ -188,6 +211,8 @@ k_conv3d(const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__
         mbar_init(&mbar[1]);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    if (S::kWRes)  // all taps' weights, once per CTA
+        for (int t = 0; t < 27; t++) stage_weights<CIN, COUT>(w, t, bbuf + t * S::kBTap, tid);
     if (warp == 0) tmem_alloc(tslot, NCOL);
     tc_before_sync();
     __syncthreads();
@@ -202,8 +227,10 @@ k_conv3d(const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__
         const bool valid = m < n;
         const int x = valid ? (int)(m % nx) : 0, y = valid ? (int)((m / nx) % ny) : 0,
                   z = valid ? (int)(m / nxy) : 0;
-        for (int tap = 0; tap < 27 && ok; tap++) {
-            const int b = tap & 1;
+        int stage = 0;
+        for (int t0 = 0; t0 < 27 && ok; t0 += ST, stage++) {
+            const int b = stage & 1;
+            const int nt = 27 - t0 < ST ? 27 - t0 : ST;
             if (pending[b]) {  // the MMAs that read buffer b are done
                 ok = mbar_wait(&mbar[b], parity[b]);
                 parity[b] ^= 1u;
@@ -211,33 +238,39 @@ k_conv3d(const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__
                 ok = __syncthreads_and(ok);
                 if (!ok) break;
             }
-            const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
-            const int xx = x + dx, yy = y + dy, zz = z + dz;
-            const bool in_grid = valid && xx >= 0 && xx < nx && yy >= 0 && yy < ny && zz >= 0 &&
-                                 zz < nz;
-            const uint4 *src = (const uint4 *)(in + (xx + (long)yy * nx + (long)zz * nxy) * CIN);
             unsigned char *a = abuf + b * S::kA;
+            for (int j = 0; j < nt; j++) {
+                const int tap = t0 + j;
+                const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+                const int xx = x + dx, yy = y + dy, zz = z + dz;
+                const bool in_grid = valid && xx >= 0 && xx < nx && yy >= 0 && yy < ny &&
+                                     zz >= 0 && zz < nz;
+                const uint4 *src =
+                    (const uint4 *)(in + (xx + (long)yy * nx + (long)zz * nxy) * CIN);
 #pragma unroll
-            for (int c = 0; c < ACH; c++) {
-                const uint4 v = in_grid ? src[c] : make_uint4(0, 0, 0, 0);
-                *(uint4 *)(a + c * 2048 + tid * 16) = v;
-            }
-            unsigned char *bb = bbuf + b * S::kB;
-            const uint4 *wt = (const uint4 *)(w + (long)tap * COUT * CIN);
-            for (int i = tid; i < COUT * ACH; i += 128) {
-                const int row = i / ACH, c = i % ACH;
-                *(uint4 *)(bb + c * (COUT * 16) + row * 16) = wt[row * ACH + c];
+                for (int c = 0; c < ACH; c++) {
+                    const uint4 v = in_grid ? src[c] : make_uint4(0, 0, 0, 0);
+                    *(uint4 *)(a + j * S::kATap + c * 2048 + tid * 16) = v;
+                }
+                if (!S::kWRes)
+                    stage_weights<CIN, COUT>(w, tap, bbuf + b * S::kB + j * S::kBTap, tid);
             }
             fence_async_smem();
             __syncthreads();
             if (tid == 0) {
                 tc_after_sync();
-                const uint32_t sa = smem_u32(a), sb = smem_u32(bb);
+                for (int j = 0; j < nt; j++) {
+                    const int tap = t0 + j;
+                    const uint32_t sa = smem_u32(a + j * S::kATap);
+                    const uint32_t sb = smem_u32(S::kWRes ? bbuf + tap * S::kBTap
+                                                          : bbuf + b * S::kB + j * S::kBTap);
 #pragma unroll
-                for (int kk = 0; kk < CIN / 16; kk++) {
-                    const uint64_t da = kmajor_desc(sa + kk * 2 * 2048, 2048, 128);
-                    const uint64_t db = kmajor_desc(sb + kk * 2 * (COUT * 16), COUT * 16, 128);
-                    umma_bf16(tmem, da, db, IDESC, (tap | kk) != 0);
+                    for (int kk = 0; kk < CIN / 16; kk++) {
+                        const uint64_t da = kmajor_desc(sa + kk * 2 * 2048, 2048, 128);
+                        const uint64_t db =
+                            kmajor_desc(sb + kk * 2 * (COUT * 16), COUT * 16, 128);
+                        umma_bf16(tmem, da, db, IDESC, (tap | kk) != 0);
+                    }
                 }
                 umma_commit(&mbar[b]);
             }
