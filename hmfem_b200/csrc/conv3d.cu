@@ -474,11 +474,17 @@ int launch_fwd(const void *in, const void *w, const float *bias, void *out, int 
     using S = FwdSmem<CIN, COUT>;
     auto k = k_conv3d<CIN, COUT>;
     HM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kBytes));
+    HM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     const long n = (long)nx * ny * nz, ntiles = (n + 127) / 128;
-    int per_sm = 0, dev = 0, nsm = 0;
+    int per_sm = 0, dev = 0, nsm = 0, smem_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 128, S::kBytes);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 128, S::kBytes) != cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        per_sm = smem_sm / (S::kBytes + 1024);  // 1 KB reserved per CTA
+    }
     // resident CTAs must also fit the SM's 512 TMEM columns
     const int tmem_fit = 512 / tmem_cols(COUT);
     if (per_sm > tmem_fit) per_sm = tmem_fit;
@@ -497,6 +503,7 @@ int launch_wgrad(const void *x, const void *dy, float *dw, int nx, int ny, int n
     using S = WgSmem<CIN, COUT>;
     auto k = k_conv3d_wgrad<CIN, COUT>;
     HM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kBytes));
+    HM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     const long n = (long)nx * ny * nz;
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
