@@ -480,11 +480,9 @@ int launch_fwd(const void *in, const void *w, const float *bias, void *out, int 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 128, S::kBytes) != cudaSuccess ||
-        per_sm < 1) {
-        cudaGetLastError();
-        per_sm = smem_sm / (S::kBytes + 1024);  // 1 KB reserved per CTA
-    }
+    // resident CTAs: shared memory (1 KB reserved per CTA), 16 per SM at most
+    per_sm = smem_sm / (S::kBytes + 1024);
+    if (per_sm > 16) per_sm = 16;
     // resident CTAs must also fit the SM's 512 TMEM columns
     const int tmem_fit = 512 / tmem_cols(COUT);
     if (per_sm > tmem_fit) per_sm = tmem_fit;
