@@ -316,18 +316,72 @@ k_mis19_front(SG g, int t, int kmin, int rows, signed char *sel)
 
 }  // namespace
 
-int stencil19_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st)
+static int mis19_enqueue(const SG &g, signed char *sel, cudaStream_t st)
 {
-    SG g{nx, ny, nz, (long)nx * ny};
-    const int tmax = (ny - 1) + 2 * (nz - 1);
+    const int tmax = (g.ny - 1) + 2 * (g.nz - 1);
     for (int t = 0; t <= tmax; t++) {
-        const int kmin = t - (ny - 1) > 0 ? (t - (ny - 1) + 1) / 2 : 0;
-        const int kmax = t / 2 < nz - 1 ? t / 2 : nz - 1;
+        const int kmin = t - (g.ny - 1) > 0 ? (t - (g.ny - 1) + 1) / 2 : 0;
+        const int kmax = t / 2 < g.nz - 1 ? t / 2 : g.nz - 1;
         const int rows = kmax - kmin + 1;
         if (rows <= 0) continue;
         k_mis19_front<<<(rows + 3) / 4, 128, 0, st>>>(g, t, kmin, rows, sel);
         HM_LAUNCHED();
     }
+    return HMFEM_OK;
+}
+
+// The wavefront is a few hundred dependent launches; a grid shape seen
+// twice on this host thread (a solver set up again, the same shape of
+// another realisation) has them recorded in a CUDA graph and replayed.
+// The graph holds the sel address, so it is kept per (shape, sel).
+struct Mis19Graph {
+    int nx = 0, ny = 0, nz = 0;
+    signed char *sel = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long kernels = 0;
+};
+static thread_local Mis19Graph t_mis_graph;
+static thread_local int t_mis_seen[3] = {0, 0, 0};
+
+int stencil19_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st)
+{
+    SG g{nx, ny, nz, (long)nx * ny};
+    Mis19Graph &G = t_mis_graph;
+    if (G.exec && G.nx == nx && G.ny == ny && G.nz == nz && G.sel == sel) {
+        HM_CUDA(cudaGraphLaunch(G.exec, st));
+        g_nlaunch += G.kernels;
+        return HMFEM_OK;
+    }
+    const bool seen = t_mis_seen[0] == nx && t_mis_seen[1] == ny && t_mis_seen[2] == nz;
+    t_mis_seen[0] = nx; t_mis_seen[1] = ny; t_mis_seen[2] = nz;
+    if (!seen) return mis19_enqueue(g, sel, st);
+    // record it on a private stream, then replay on st
+    cudaStream_t cs;
+    HM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    HM_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    const unsigned long long before = t_nlaunch;
+    int rc = mis19_enqueue(g, sel, cs);
+    const unsigned long long k = t_nlaunch - before;
+    g_nlaunch -= k;  // counted when replayed
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(cs, &graph);
+    cudaStreamDestroy(cs);
+    if (rc != HMFEM_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return rc != HMFEM_OK ? rc : mis19_enqueue(g, sel, st);
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return mis19_enqueue(g, sel, st);
+    }
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    G.nx = nx; G.ny = ny; G.nz = nz; G.sel = sel; G.exec = ex; G.kernels = k;
+    HM_CUDA(cudaGraphLaunch(ex, st));
+    g_nlaunch += k;
     return HMFEM_OK;
 }
 
