@@ -649,19 +649,32 @@ int hmfem_assemble(hmfem_solver *h, int nx, int ny, int nz, double hx,
     s.hx = hx; s.hy = hy; s.hz = hz; s.visc = visc;
     for (int f = 0; f < 6; f++) s.bc[f] = bc_type[f];
     // permeabilities: device pointers are used in place, host arrays copied
+    // -- once when the caller passes the same array for several directions
+    // (isotropic K, as the reference's Perm fields usually are)
     const double *K[3] = {KX, KY, KZ};
+    const double *dK[3] = {KX, KY, KZ};
     for (int i = 0; i < 3; i++) {
         if (mem) {
             hm::dfree(s.Kown[i]);
             s.Kown[i] = nullptr;
-        } else {
-            if (!s.Kown[i]) HM_ALLOC(s.Kown[i], double, n);
-            HM_CHECK(hm::upload(s.Kown[i], K[i], n, 0, st));
+            continue;
         }
+        int same = -1;
+        for (int j = 0; j < i; j++)
+            if (K[j] == K[i]) same = j;
+        if (same >= 0) {
+            hm::dfree(s.Kown[i]);
+            s.Kown[i] = nullptr;
+            dK[i] = dK[same];
+            continue;
+        }
+        if (!s.Kown[i]) HM_ALLOC(s.Kown[i], double, n);
+        HM_CHECK(hm::upload(s.Kown[i], K[i], n, 0, st));
+        dK[i] = s.Kown[i];
     }
-    s.KX = mem ? KX : s.Kown[0];
-    s.KY = mem ? KY : s.Kown[1];
-    s.KZ = mem ? KZ : s.Kown[2];
+    s.KX = dK[0];
+    s.KY = dK[1];
+    s.KZ = dK[2];
     // face values in the Bound layout (l,r: ny*nz; u,d: nx*nz; t,b: nx*ny)
     const long fsz[6] = {(long)ny * nz, (long)ny * nz, (long)nx * nz,
                          (long)nx * nz, (long)nx * ny, (long)nx * ny};
