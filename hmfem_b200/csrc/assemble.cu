@@ -90,6 +90,49 @@ __global__ void k_l0_rowcounts(int nx, int ny, int nz, int *cnt)
     }
 }
 
+// Right-hand side of cell s (source_term, set_source_term.c:23-220; faces in
+// the reference's interface order L,R,D,U,T,B, then the karst and well
+// exchange terms of :206-220).
+__device__ __forceinline__ double cell_rhs(const Grid &g, const FacePtrs &fv, int i,
+                                           int j, int k, long s, const Faces &F,
+                                           double ki, double wi, double pcs, double pws)
+{
+    double r = 0.0;
+    if (i == 0) {
+        double gv = fv.l[(long)k * g.ny + j];
+        if (g.bc[0] == 0) r = dadd(r, dmul(F.l, gv));
+        if (g.bc[0] == 1) r = dadd(r, gv / g.hx);
+    }
+    if (g.allneu && s == g.spec) r = dadd(r, dmul(F.l, 1.0));
+    if (i == g.nx - 1) {
+        double gv = fv.r[(long)k * g.ny + j];
+        if (g.bc[1] == 0) r = dadd(r, dmul(F.r, gv));
+        if (g.bc[1] == 1) r = dsub(r, gv / g.hx);
+    }
+    if (j == 0) {
+        double gv = fv.d[(long)k * g.nx + i];
+        if (g.bc[3] == 0) r = dadd(r, dmul(F.d, gv));
+        if (g.bc[3] == 1) r = dadd(r, gv / g.hy);
+    }
+    if (j == g.ny - 1) {
+        double gv = fv.u[(long)k * g.nx + i];
+        if (g.bc[2] == 0) r = dadd(r, dmul(F.u, gv));
+        if (g.bc[2] == 1) r = dsub(r, gv / g.hy);
+    }
+    if (k == g.nz - 1) {
+        double gv = fv.t[(long)j * g.nx + i];
+        if (g.bc[4] == 0) r = dadd(r, dmul(F.t, gv));
+        if (g.bc[4] == 1) r = dsub(r, gv / g.hz);
+    }
+    if (k == 0) {
+        double gv = fv.b[(long)j * g.nx + i];
+        if (g.bc[5] == 0) r = dadd(r, dmul(F.b, gv));
+        if (g.bc[5] == 1) r = dadd(r, gv / g.hz);
+    }
+    r = dadd(dadd(r, dmul(ki, pcs) / g.vve), dmul(wi, pws) / g.vve);
+    return r;
+}
+
 // One thread per cell: faces, diagonal, CSR row (d,l,c,r,u,t,b as
 // solve_linearsystem_AMG.c:103-139 packs it) and right-hand side.
 __global__ void __launch_bounds__(256)
@@ -117,42 +160,31 @@ k_assemble(Grid g, const double *__restrict__ KX, const double *__restrict__ KY,
         if (j < g.ny - 1)   { col[q] = (int)(s + nx);  val[q] = -F.u; q++; }
         if (k < g.nz - 1)   { col[q] = (int)(s + nxy); val[q] = -F.t; q++; }
         if (k > 0)          { col[q] = (int)(s - nxy); val[q] = -F.b; q++; }
-        // source_term, set_source_term.c:23-220, faces in order L,R,D,U,T,B
-        double r = 0.0;
-        if (i == 0) {
-            double gv = fv.l[(long)k * g.ny + j];
-            if (g.bc[0] == 0) r = dadd(r, dmul(F.l, gv));
-            if (g.bc[0] == 1) r = dadd(r, gv / g.hx);
-        }
-        if (g.allneu && s == g.spec) r = dadd(r, dmul(F.l, 1.0));
-        if (i == g.nx - 1) {
-            double gv = fv.r[(long)k * g.ny + j];
-            if (g.bc[1] == 0) r = dadd(r, dmul(F.r, gv));
-            if (g.bc[1] == 1) r = dsub(r, gv / g.hx);
-        }
-        if (j == 0) {
-            double gv = fv.d[(long)k * g.nx + i];
-            if (g.bc[3] == 0) r = dadd(r, dmul(F.d, gv));
-            if (g.bc[3] == 1) r = dadd(r, gv / g.hy);
-        }
-        if (j == g.ny - 1) {
-            double gv = fv.u[(long)k * g.nx + i];
-            if (g.bc[2] == 0) r = dadd(r, dmul(F.u, gv));
-            if (g.bc[2] == 1) r = dsub(r, gv / g.hy);
-        }
-        if (k == g.nz - 1) {
-            double gv = fv.t[(long)j * g.nx + i];
-            if (g.bc[4] == 0) r = dadd(r, dmul(F.t, gv));
-            if (g.bc[4] == 1) r = dsub(r, gv / g.hz);
-        }
-        if (k == 0) {
-            double gv = fv.b[(long)j * g.nx + i];
-            if (g.bc[5] == 0) r = dadd(r, dmul(F.b, gv));
-            if (g.bc[5] == 1) r = dadd(r, gv / g.hz);
-        }
-        double pcs = PC ? PC[s] : 0.0, pws = PW ? PW[s] : 0.0;
-        r = dadd(dadd(r, dmul(ki, pcs) / g.vve), dmul(wi, pws) / g.vve);
-        b[s] = r;
+        b[s] = cell_rhs(g, fv, i, j, k, s, F, ki, wi, PC ? PC[s] : 0.0, PW ? PW[s] : 0.0);
+    }
+}
+
+// The Picard loop's right-hand side patch (reservoir.c:19-52 /
+// set_source_term.c:206-220): only the cells a conduit element exchanges
+// with change between iterations.  Element e = own[t] owns reservoir cell
+// ecell[e] (the last conduit element mapped to it, as pc_aux is filled) and
+// brings its conduit pressure pc[e].
+__global__ void k_exchange_rhs(Grid g, const double *__restrict__ KX,
+                               const double *__restrict__ KY,
+                               const double *__restrict__ KZ, FacePtrs fv, int m,
+                               const int *__restrict__ own, const int *__restrict__ ecell,
+                               const double *__restrict__ pc, const double *__restrict__ KI,
+                               const double *__restrict__ WI, const double *__restrict__ PW,
+                               double *__restrict__ b)
+{
+    const long nx = g.nx, nxy = (long)g.nx * g.ny;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        int e = own[t];
+        long s = ecell[e];
+        int i = (int)(s % nx), j = (int)((s / nx) % g.ny), k = (int)(s / nxy);
+        Faces F = cell_faces(g, i, j, k, s, KX, KY, KZ);
+        b[s] = cell_rhs(g, fv, i, j, k, s, F, KI[s], WI ? WI[s] : 0.0, pc[e],
+                        PW ? PW[s] : 0.0);
     }
 }
 
@@ -263,6 +295,22 @@ int launch_assemble(int nx, int ny, int nz, double hx, double hy, double hz,
     long n = (long)nx * ny * nz;
     k_assemble<<<grid_for(n, 256), 256, 0, st>>>(g, KX, KY, KZ, fv, KI, WI, pc,
                                                  pw, rowptr, col, val, b);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+int launch_exchange_rhs(int nx, int ny, int nz, double hx, double hy, double hz,
+                        double visc, const double *KX, const double *KY,
+                        const double *KZ, const int bc[6], double *const face[6],
+                        int m, const int *own, const int *ecell, const double *pc,
+                        const double *KI, const double *WI, const double *pw,
+                        double *b, cudaStream_t st)
+{
+    if (m <= 0) return HMFEM_OK;
+    Grid g = make_grid(nx, ny, nz, hx, hy, hz, visc, bc);
+    FacePtrs fv{face[0], face[1], face[2], face[3], face[4], face[5]};
+    k_exchange_rhs<<<grid_for(m, 128), 128, 0, st>>>(g, KX, KY, KZ, fv, m, own, ecell, pc,
+                                                     KI, WI, pw, b);
     HM_LAUNCHED();
     return HMFEM_OK;
 }

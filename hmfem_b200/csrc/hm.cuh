@@ -128,6 +128,12 @@ int launch_assemble(int nx, int ny, int nz, double hx, double hy, double hz,
                     const double *KI, const double *WI, const double *pc,
                     const double *pw, const int *rowptr, int *col, double *val,
                     double *b, cudaStream_t st);
+int launch_exchange_rhs(int nx, int ny, int nz, double hx, double hy, double hz,
+                        double visc, const double *KX, const double *KY,
+                        const double *KZ, const int bc[6], double *const face[6],
+                        int m, const int *own, const int *ecell, const double *pc,
+                        const double *KI, const double *WI, const double *pw,
+                        double *b, cudaStream_t st);
 int launch_pack_stencil(int n, const hmfem_ele *perm, const hmfem_ind *ind,
                         int *cnt, const int *rowptr, int *col, double *val,
                         int pass, cudaStream_t st);

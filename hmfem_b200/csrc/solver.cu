@@ -492,6 +492,25 @@ int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out)
     return s.last.status;
 }
 
+int assemble_coupled(Solver &s, const double *KI, const double *WI, const double *pw)
+{
+    if (!s.have_grid || s.lv.empty() || !s.lv[0].A.val) {
+        set_last_error("the coupled matrix needs an assembled grid (hmfem_assemble)",
+                       __FILE__, __LINE__);
+        return HMFEM_E_ARG;
+    }
+    free_hierarchy(s, true);
+    Level &L = s.lv[0];
+    // same sparsity (the exchange terms only touch the centre): row pointers
+    // and columns stay, values and right-hand side are rewritten
+    HM_CHECK(launch_assemble(s.nx, s.ny, s.nz, s.hx, s.hy, s.hz, s.visc, s.KX, s.KY,
+                             s.KZ, s.bc, s.face, KI, WI, nullptr, pw, L.A.rowptr,
+                             L.A.col, L.A.val, s.b, s.st));
+    s.setup_done = false;
+    s.l0_same = false;
+    return HMFEM_OK;
+}
+
 }  // namespace hm
 
 using hm::Solver;
@@ -499,10 +518,6 @@ using hm::Solver;
 // ============================================================================
 // C-ABI
 // ============================================================================
-struct hmfem_solver {
-    Solver s;
-};
-
 extern "C" {
 
 void hmfem_default_options(hmfem_options *o)
@@ -575,6 +590,7 @@ int hmfem_destroy(hmfem_solver *h)
     Solver &s = h->s;
     hm::set_alloc_context(s.st, s.cache);
     if (s.st) cudaStreamSynchronize(s.st);
+    hm::karst_release(s);
     hm::free_hierarchy(s, false);
     hm::free_vectors(s);
     for (int i = 0; i < 3; i++) hm::dfree(s.Kown[i]);

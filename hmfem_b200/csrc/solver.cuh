@@ -49,6 +49,9 @@ struct Solver {
     unsigned long long graph_kernels = 0;  // kernels in one captured iteration
     hmfem_stats last{};
 
+    // the coupled reservoir / conduit run (karst.cu), when one was made
+    struct KarstRun *karst = nullptr;
+
     bool use_bf16(int l) const
     {
         return opt.precision == 1 && opt.bf16_from >= 0 && l >= opt.bf16_from;
@@ -115,4 +118,18 @@ int g19_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo,
               const Ctl *ctl, cudaStream_t st);
 int g19_spmv(const Level &L, const double *x, double *y, cudaStream_t st);
 
+// solver.cu entry points the coupled driver (karst.cu) builds on
+int setup(Solver &s);
+int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out);
+// Rebuilds level 0 of the last hmfem_assemble grid (same K, faces and
+// boundary types) with the karst / well exchange terms: KI, WI in the
+// diagonal, WI*pw in the right-hand side (device arrays, nullable).  The
+// hierarchy is dropped; the next solve sets up again.
+int assemble_coupled(Solver &s, const double *KI, const double *WI, const double *pw);
+void karst_release(Solver &s);  // karst.cu
+
 }  // namespace hm
+
+struct hmfem_solver {
+    hm::Solver s;
+};

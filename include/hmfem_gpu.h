@@ -165,8 +165,8 @@ const char *hmfem_last_error(void);
  * set_source_term.c:9-223 on the device).  K arrays are n = nx*ny*nz cells,
  * s = i + j nx + k nx ny.  Faces l,r,u,d,t,b; bc_type 0 Dirichlet, 1
  * Neumann; face_vals[f] (nullable) are per-face arrays in the Bound layout,
- * else bc_value[f] everywhere.  KI/WI (nullable) are the well/karst indices
- * of the diagonal and pc/pw the pressures they multiply in the RHS. */
+ * else bc_value[f] everywhere.  No well or conduit exchange terms: the
+ * coupled reservoir / conduit run adds them (hmfem_picard, hmfem_karst.h). */
 int hmfem_assemble(hmfem_solver *s, int nx, int ny, int nz, double hx,
                    double hy, double hz, double visc, const double *KX,
                    const double *KY, const double *KZ, const int bc_type[6],

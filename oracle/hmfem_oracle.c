@@ -932,3 +932,441 @@ void or_fluxes(int nx, int ny, int nz, double hx, double hy, double hz,
     if (divmin) *divmin = mn;
     if (divmax) *divmax = mx;
 }
+
+/* ==== the coupled conduit model ========================================== */
+
+/* main.c:416-448: element i of conduit j steps along its axis from
+ * (sxi, syi, szi). */
+int or_karst_cell(const or_karst *K, int j, int i, int nx, int ny)
+{
+    int x = K->sxi[j], y = K->syi[j], z = K->szi[j];
+    if (K->pos[j] == 1) x += i;
+    else if (K->pos[j] == 2) y += i;
+    else z += i;
+    return x + y * nx + z * nx * ny;
+}
+
+int or_karst_check(const or_karst *K, int nx, int ny, int nz)
+{
+    for (int j = 0; j < K->nk; j++) {
+        int m = K->len[j], p = K->pos[j];
+        int x = K->sxi[j], y = K->syi[j], z = K->szi[j];
+        if (p < 1 || p > 3 || m < 1) return -1;
+        int n_ax = p == 1 ? nx : p == 2 ? ny : nz;
+        int a0 = p == 1 ? x : p == 2 ? y : z;
+        if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return -1;
+        if (a0 + m > n_ax) return -1;
+        for (int f = 0; f < 2; f++) {
+            int bt = f ? K->bound_r[j] : K->bound_l[j];
+            if (bt != 0 && bt != 1 && bt != 3) return -1;
+            if (bt != 3) continue;
+            if (f == 0 && a0 < 1) return -1;
+            if (f == 1 && (a0 + m >= n_ax || p == 3)) return -1;
+        }
+        if (K->n_brechas[j] < 0 || K->n_brechas[j] > K->max_brechas) return -1;
+        for (int b = 0; b < K->n_brechas[j]; b++) {
+            int s = K->brechas[b * K->nk + j];
+            if (s < 0 || s + 1 >= m) return -1;
+        }
+    }
+    return 0;
+}
+
+#define KM(a, i, j) ((a)[(i) * nk + (j)])
+
+/* permeabilities.c:795-867 */
+void or_karst_keff(const or_karst *K, const or_kgrid *G, or_kstate *S, int j)
+{
+    const int nk = K->nk, m = K->len[j];
+    const double hs = K->pos[j] == 1 ? G->hx : K->pos[j] == 2 ? G->hy : G->hz;
+    const double ks = K->Kc[j], visc = G->visc;
+    int i;
+    for (i = 0; i < m - 1; i++) {
+        KM(S->kr, i, j) = or_hm(ks, ks);
+        KM(S->kr, i, j) = KM(S->kr, i, j) / (hs * hs * visc);
+    }
+    for (i = 1; i < m; i++) {
+        KM(S->kl, i, j) = or_hm(ks, ks);
+        KM(S->kl, i, j) = KM(S->kl, i, j) / (hs * hs * visc);
+    }
+    if (K->bound_l[j] == 0) KM(S->kl, 0, j) = 2 * (ks) / (hs * hs * visc);
+    if (K->bound_l[j] == 1) KM(S->kl, 0, j) = 0;
+    if (K->bound_l[j] == 3) KM(S->kl, 0, j) = 2 * ks / (visc * hs * hs);
+    if (K->bound_r[j] == 0) KM(S->kr, m - 1, j) = 2 * (ks) / (hs * hs * visc);
+    if (K->bound_r[j] == 1) KM(S->kr, m - 1, j) = 0;
+    if (K->bound_r[j] == 3) KM(S->kr, m - 1, j) = 2 * ks / (visc * hs * hs);
+    for (i = 0; i < m; i++)
+        KM(S->kc, i, j) = KM(S->kl, i, j) + KM(S->kr, i, j) + KM(S->kic, i, j) / visc;
+}
+
+/* The nonlinear Robin end term of set_source_term.c:298-404 and
+ * flux_reconstruction.c:398-486: the reservoir flux u through the face
+ * between the cell beyond the end (s) and the end cell (saux), and the
+ * K-weighted mean pressure lm of the two. */
+static void robin_end(const or_karst *K, const or_kgrid *G, int j, int right,
+                      double *u, double *lm)
+{
+    const int nx = G->nx, ny = G->ny, nxy = nx * ny, m = K->len[j];
+    int x = K->sxi[j], y = K->syi[j], z = K->szi[j], s, saux;
+    const double *p = G->p_old;
+    const double *KK;
+    double face, hh;
+    if (K->pos[j] == 1) {
+        s = right ? IDX(x + m, y, z) : IDX(x - 1, y, z);
+        saux = right ? IDX(x + m - 1, y, z) : IDX(x, y, z);
+        face = right ? G->perm[s].l : G->perm[s].r;
+        KK = G->KX; hh = G->hx;
+    } else if (K->pos[j] == 2) {
+        s = right ? IDX(x, y + m, z) : IDX(x, y - 1, z);
+        saux = right ? IDX(x, y + m - 1, z) : IDX(x, y, z);
+        face = right ? G->perm[s].d : G->perm[s].u;
+        KK = G->KY; hh = G->hy;
+    } else {
+        s = right ? IDX(x, y, z + m) : IDX(x, y, z - 1);
+        saux = right ? IDX(x, y, z + m - 1) : IDX(x, y, z);
+        face = right ? G->perm[s].b : G->perm[s].t;
+        KK = G->KZ; hh = G->hz;
+    }
+    (void)ny;
+    *u = hh * face * (p[s] - p[saux]);
+    *lm = (KK[s] * p[s] + KK[saux] * p[saux]) / (KK[s] + KK[saux]);
+}
+
+/* set_source_term.c:256-414 */
+void or_source_term1d(const or_karst *K, const or_kgrid *G, or_kstate *S,
+                      int j, double *f)
+{
+    const int nk = K->nk, m = K->len[j];
+    const double hs = K->pos[j] == 1 ? G->hx : K->pos[j] == 2 ? G->hy : G->hz;
+    const double visc = G->visc, rho = G->rho, ks = K->Kc[j];
+    int i;
+    for (i = 0; i < m; i++)
+        f[i] = (KM(S->kic, i, j) * KM(S->paux, i, j)) / visc;
+    /* fractures (set_source_term.c:272-295) */
+    for (i = 0; i < K->n_brechas[j]; i++) {
+        int s = K->brechas[i * nk + j];
+        double cR = or_hm(ks, ks), R;
+        double *ucr = &S->ucR[i * nk + j], *ucl = &S->ucL[i * nk + j];
+        double cb = K->cb[i * nk + j], be = K->beta[i * nk + j];
+        if (*ucr < 0) R = -cb * be;
+        else R = cb * be;
+        double uR = (cR / (visc * hs)) *
+                    (KM(S->pc_old, s, j) - KM(S->pc_old, s + 1, j) - rho * *ucr * *ucr * R);
+        double uL = (cR / (visc * hs)) *
+                    (KM(S->pc_old, s + 1, j) - KM(S->pc_old, s, j) + rho * *ucl * *ucl * R);
+        *ucr = uR;
+        *ucl = uL;
+        f[s] = f[s] + (cR / (visc * hs)) * (rho * uR * uR * R);
+        f[s + 1] = f[s + 1] - (cR / (visc * hs)) * (rho * uL * uL * R);
+    }
+    const double c0 = K->cont[j], c1 = K->cont[nk + j];
+    /* left end (set_source_term.c:302-366) */
+    if (K->bound_l[j] == 0) f[0] = f[0] + (KM(S->kl, 0, j)) * c0;
+    if (K->bound_l[j] == 1) f[0] = f[0] + c0 / (hs);
+    if (K->bound_l[j] == 3) {
+        double u, lm, c;
+        robin_end(K, G, j, 0, &u, &lm);
+        if (u < 0) c = -K->ccont[j] * (c0 - 1);
+        else c = K->ccont[j] * (c0 - 1);
+        double font = -lm + rho * u * u * c;
+        f[0] = f[0] - 2 * ks / (visc * hs * hs) * font;
+    }
+    /* right end (set_source_term.c:368-410) */
+    if (K->bound_r[j] == 0) f[m - 1] = f[m - 1] + KM(S->kr, m - 1, j) * c1;
+    if (K->bound_r[j] == 1) f[m - 1] = f[m - 1] - c1 / (hs);
+    if (K->bound_r[j] == 3) {
+        double u, lm, c;
+        robin_end(K, G, j, 1, &u, &lm);
+        if (u < 0) c = -K->ccont[nk + j] * (c1 - 1);
+        else c = K->ccont[nk + j] * (c1 - 1);
+        double font = -lm + rho * u * u * c;
+        f[m - 1] = f[m - 1] - font * 2 * ks / (visc * hs * hs);
+    }
+}
+
+void or_thomas(int m, const double *kl, const double *kc, const double *kr,
+               int stride, const double *f, double *x)
+{
+    /* forward sweep: q[i] = r[i] / w[i] kept in x[], g[i] in a scratch;
+     * w[i] = c[i] - l[i] q[i-1], g[i] = (f[i] + l[i] g[i-1]) / w[i] */
+    double *g = (double *)malloc(sizeof(double) * (m > 0 ? m : 1));
+    double w = kc[0];
+    g[0] = f[0] / w;
+    for (int i = 1; i < m; i++) {
+        double q = kr[(i - 1) * stride] / w;
+        x[i - 1] = q;
+        double l = kl[i * stride];
+        w = kc[i * stride] - l * q;
+        g[i] = (f[i] + l * g[i - 1]) / w;
+    }
+    /* back substitution: x[i] = g[i] + q[i] x[i+1] */
+    double nxt = g[m - 1];
+    x[m - 1] = nxt;
+    for (int i = m - 2; i >= 0; i--) {
+        nxt = g[i] + x[i] * nxt;
+        x[i] = nxt;
+    }
+    free(g);
+}
+
+/* solve_linearsystem_AMG.c:200-294: the conduit system in count/col/ele
+ * form (l, c, r per row) handed to compute(). */
+static void conduit_compute(const or_karst *K, const or_kstate *S, int j,
+                            const double *f, double *x)
+{
+    const int nk = K->nk, m = K->len[j];
+    int *cnt = (int *)malloc(sizeof(int) * m);
+    int *col = (int *)malloc(sizeof(int) * 3 * m);
+    double *ele = (double *)malloc(sizeof(double) * 3 * m);
+    int l = 0;
+    for (int s = 0; s < m; s++) {
+        cnt[s] = 1 + (s > 0) + (s < m - 1);
+        if (s > 0) { col[l] = s - 1; ele[l] = -KM(S->kl, s, j); l++; }
+        col[l] = s; ele[l] = KM(S->kc, s, j); l++;
+        if (s < m - 1) { col[l] = s + 1; ele[l] = -KM(S->kr, s, j); l++; }
+    }
+    int hdr[2] = {m, l};
+    for (int s = 0; s < m; s++) x[s] = 0.0;
+    or_compute(hdr, cnt, col, ele, f, x, 1e-8, 0, NULL, NULL);
+    free(cnt); free(col); free(ele);
+}
+
+/* karst.c:8-40 */
+void or_conduit(const or_karst *K, const or_kgrid *G, or_kstate *S,
+                int solver)
+{
+    const int nk = K->nk;
+    double *f = (double *)malloc(sizeof(double) * (S->mmax + 1));
+    double *x = (double *)malloc(sizeof(double) * (S->mmax + 1));
+    for (int j = 0; j < nk; j++) {
+        const int m = K->len[j];
+        or_karst_keff(K, G, S, j);
+        or_source_term1d(K, G, S, j, f);
+        if (solver == 1) conduit_compute(K, S, j, f, x);
+        else or_thomas(m, &S->kl[j], &S->kc[j], &S->kr[j], nk, f, x);
+        for (int i = 0; i < m; i++) KM(S->pc, i, j) = x[i];
+    }
+    free(f);
+    free(x);
+}
+
+/* flux_reconstruction.c:322-496 */
+void or_fluxo1d(const or_karst *K, const or_kgrid *G, const or_kstate *S,
+                double *ucl, double *ucr)
+{
+    const int nk = K->nk;
+    const double visc = G->visc, rho = G->rho;
+    for (int j = 0; j < nk; j++) {
+        const int m = K->len[j];
+        const double hs = K->pos[j] == 1 ? G->hx : K->pos[j] == 2 ? G->hy : G->hz;
+        const double ks = K->Kc[j];
+        const double *x = S->pc;
+        int i;
+        for (i = 0; i < m - 1; i++)
+            KM(ucr, i, j) = hs * KM(S->kr, i, j) * (KM(x, i, j) - KM(x, i + 1, j));
+        for (i = 1; i < m; i++)
+            KM(ucl, i, j) = hs * KM(S->kl, i, j) * (KM(x, i, j) - KM(x, i - 1, j));
+        for (i = 0; i < K->n_brechas[j]; i++) {
+            double c, cb = K->cb[i * nk + j], be = K->beta[i * nk + j];
+            double ur = S->ucR[i * nk + j], ul = S->ucL[i * nk + j];
+            if (ur < 0) c = -cb * be;
+            else c = cb * be;
+            int s = K->brechas[i * nk + j];
+            double cR = or_hm(ks, ks);
+            KM(ucr, s, j) = (cR / (visc * hs)) *
+                            (KM(x, s, j) - KM(x, s + 1, j) - 0.5 * rho * ur * ur * c);
+            KM(ucl, s + 1, j) = (cR / (visc * hs)) *
+                                (KM(x, s + 1, j) - KM(x, s, j) + 0.5 * rho * ul * ul * c);
+        }
+        const double c0 = K->cont[j], c1 = K->cont[nk + j];
+        if (K->bound_l[j] == 0) KM(ucl, 0, j) = hs * KM(S->kl, 0, j) * (KM(x, 0, j) - c0);
+        /* the Neumann left end takes cont_karst[1] (flux_reconstruction.c:372-376) */
+        if (K->bound_l[j] == 1) KM(ucl, 0, j) = -c1;
+        if (K->bound_l[j] == 3) {
+            double u, lm, c;
+            robin_end(K, G, j, 0, &u, &lm);
+            if (u < 0) c = -K->ccont[j] * (c0 - 1);
+            else c = K->ccont[j] * (c0 - 1);
+            KM(ucl, 0, j) = (2 * ks) / (visc * hs) * (KM(x, 0, j) - lm + rho * u * u * c);
+        }
+        if (K->bound_r[j] == 0)
+            KM(ucr, m - 1, j) = hs * KM(S->kr, m - 1, j) * (KM(x, m - 1, j) - c1);
+        if (K->bound_r[j] == 1) KM(ucr, m - 1, j) = c1;
+        if (K->bound_r[j] == 3) {
+            double u, lm, c;
+            robin_end(K, G, j, 1, &u, &lm);
+            if (u < 0) c = -K->ccont[nk + j] * (c1 - 1);
+            else c = K->ccont[nk + j] * (c1 - 1);
+            KM(ucr, m - 1, j) = (2 * ks) / (visc * hs) * (KM(x, m - 1, j) - lm + rho * u * u * c);
+        }
+    }
+}
+
+/* main.c:102-113 (erro_relativo) */
+static double rel_change(int n, const double *y, const double *y_old)
+{
+    double s1 = 0, s2 = 0;
+    for (int i = 0; i < n; i++) {
+        s1 = s1 + (y[i] - y_old[i]) * (y[i] - y_old[i]);
+        s2 = s2 + y[i] * y[i];
+    }
+    return sqrt(s1) / sqrt(s2);
+}
+
+/* reservoir.c:8-57 with the hierarchy kept: the matrix of the coupled
+ * system does not change between Picard iterations, only pc_aux in the
+ * right-hand side (set_source_term.c:206-220). */
+static void reservoir_rhs(const or_karst *K, int nx, int ny, int nz, double hx,
+                          double hy, double hz, double visc, const or_bound *B,
+                          const int bc[6], const or_ele *perm, const double *KI,
+                          const double *WI, const double *pw,
+                          const double *pc_old, double *pcaux, double *b)
+{
+    const int n = nx * ny * nz, nk = K->nk;
+    for (int s = 0; s < n; s++) pcaux[s] = 0.0;
+    for (int j = 0; j < nk; j++)
+        for (int i = 0; i < K->len[j]; i++)
+            pcaux[or_karst_cell(K, j, i, nx, ny)] = KM(pc_old, i, j);
+    for (int s = 0; s < n; s++) b[s] = 0.0;
+    or_source_term(nx, ny, nz, hx, hy, hz, visc, B, bc, perm, KI, WI, pcaux,
+                   pw, b);
+}
+
+int or_picard(const or_karst *K, int nx, int ny, int nz, double hx, double hy,
+              double hz, double visc, double rho, const double *KX,
+              const double *KY, const double *KZ, const int bc_type[6],
+              const double val6[6], const double *WI, const double *pw,
+              double tol, int iter_max, double solve_eps, int solve_stop,
+              int conduit_solver, double *p, double *pc, double *ucl,
+              double *ucr, or_ele *v, double *out, double *qk)
+{
+    if (or_karst_check(K, nx, ny, nz) != 0) return -1;
+    const int n = nx * ny * nz, nk = K->nk;
+    int mmax = 0;
+    for (int j = 0; j < nk; j++) if (K->len[j] > mmax) mmax = K->len[j];
+    const long mm = (long)mmax * nk;
+    const long bb = (long)(K->max_brechas > 0 ? K->max_brechas : 1) * nk;
+    or_kstate S;
+    S.mmax = mmax;
+    S.kl = (double *)calloc(mm, sizeof(double));
+    S.kr = (double *)calloc(mm, sizeof(double));
+    S.kc = (double *)calloc(mm, sizeof(double));
+    S.kic = (double *)calloc(mm, sizeof(double));
+    S.paux = (double *)calloc(mm, sizeof(double));
+    S.pc = pc;
+    S.pc_old = (double *)calloc(mm, sizeof(double));
+    S.ucR = (double *)calloc(bb, sizeof(double));
+    S.ucL = (double *)calloc(bb, sizeof(double));
+    for (long q = 0; q < mm; q++) pc[q] = 0.0;
+    /* constant boundary values (main.c:140-152, set_boundaries.c) */
+    double *fv[6];
+    const long fsz[6] = {(long)ny * nz, (long)ny * nz, (long)nx * nz,
+                         (long)nx * nz, (long)nx * ny, (long)nx * ny};
+    for (int f = 0; f < 6; f++) {
+        fv[f] = (double *)malloc(sizeof(double) * fsz[f]);
+        for (long q = 0; q < fsz[f]; q++) fv[f][q] = val6[f];
+    }
+    or_bound B = {fv[0], fv[1], fv[2], fv[3], fv[4], fv[5]};
+    or_ele *perm = (or_ele *)calloc(n, sizeof(or_ele));
+    or_ind *ind = (or_ind *)malloc(sizeof(or_ind) * n);
+    double *b = (double *)malloc(sizeof(double) * n);
+    double *pcaux = (double *)malloc(sizeof(double) * n);
+    double *p_old = (double *)malloc(sizeof(double) * n);
+    double *KI = (double *)calloc(n, sizeof(double));
+    int *cnt = (int *)malloc(sizeof(int) * n);
+    int *col = (int *)malloc(sizeof(int) * 7L * n);
+    double *ele = (double *)malloc(sizeof(double) * 7L * n);
+    or_hierarchy H;
+    double rr;
+
+    /* first reservoir solve: no well, no conduit exchange (main.c:393) */
+    or_assemble(nx, ny, nz, hx, hy, hz, visc, KX, KY, KZ, bc_type, NULL, NULL,
+                perm, ind);
+    reservoir_rhs(K, nx, ny, nz, hx, hy, hz, visc, &B, bc_type, perm, NULL,
+                  NULL, pw, S.pc_old, pcaux, b);
+    or_pack_csr(n, perm, ind, cnt, col, ele);
+    for (int s = 0; s < n; s++) p[s] = 0.0;
+    or_amg_setup(n, cnt, col, ele, 16, 1, 0.0, &H);
+    or_pcg(&H, 0, 1.0, b, p, solve_eps, 10000, solve_stop, &rr);
+    or_amg_free(&H);
+    memcpy(p_old, p, sizeof(double) * n);
+
+    /* karst index, KI_c, p_aux (main.c:410-449) */
+    for (int j = 0; j < nk; j++) {
+        const double hs = K->pos[j] == 1 ? hx : K->pos[j] == 2 ? hy : hz;
+        for (int i = 0; i < K->len[j]; i++) {
+            int c = or_karst_cell(K, j, i, nx, ny);
+            KI[c] = K->kindex[j];
+            KM(S.kic, i, j) = K->kindex[j] / (K->area[j] * hs);
+            KM(S.paux, i, j) = p_old[c];
+        }
+    }
+    /* the coupled matrix (reservoir.c:51 with KI and WI) */
+    or_assemble(nx, ny, nz, hx, hy, hz, visc, KX, KY, KZ, bc_type, KI, WI,
+                perm, ind);
+    or_pack_csr(n, perm, ind, cnt, col, ele);
+    or_amg_setup(n, cnt, col, ele, 16, 1, 0.0, &H);
+    or_kgrid G = {nx, ny, nz, hx, hy, hz, visc, rho, KX, KY, KZ, perm, p_old};
+    /* conduit() before the loop (main.c:452) reads the matrix faces of the
+     * first (uncoupled) call, which equal the coupled ones: KI and WI only
+     * enter the centre */
+    or_conduit(K, &G, &S, conduit_solver);
+
+    double error = 1.0;
+    int iter = 0;
+    while (iter < iter_max && error > tol) {
+        memcpy(S.pc_old, pc, sizeof(double) * mm);
+        reservoir_rhs(K, nx, ny, nz, hx, hy, hz, visc, &B, bc_type, perm, KI,
+                      WI, pw, S.pc_old, pcaux, b);
+        or_pcg(&H, 0, 1.0, b, p, solve_eps, 10000, solve_stop, &rr);
+        /* main.c:480-486 keeps the last entry, the reservoir change */
+        error = rel_change(n, p, p_old);
+        memcpy(p_old, p, sizeof(double) * n);
+        for (int j = 0; j < nk; j++)
+            for (int i = 0; i < K->len[j]; i++)
+                KM(S.paux, i, j) = p_old[or_karst_cell(K, j, i, nx, ny)];
+        or_conduit(K, &G, &S, conduit_solver);
+        iter++;
+    }
+    or_amg_free(&H);
+
+    double *ul = ucl ? ucl : (double *)calloc(mm, sizeof(double));
+    double *ur = ucr ? ucr : (double *)calloc(mm, sizeof(double));
+    for (long q = 0; q < mm; q++) { ul[q] = 0.0; ur[q] = 0.0; }
+    or_fluxo1d(K, &G, &S, ul, ur);
+    if (v) or_fluxes(nx, ny, nz, hx, hy, hz, p, perm, &B, bc_type, v, NULL, NULL);
+    /* balances (main.c:523-529, 566-593) */
+    if (out) {
+        double Q = 0.0, pm = 0.0;
+        for (int s = 0; s < n; s++) {
+            double wi = WI ? WI[s] : 0.0, pws = pw ? pw[s] : 0.0;
+            Q = Q + (wi / visc) * (pws - p[s]);
+            pm = pm + p[s];
+        }
+        out[0] = error;
+        out[1] = Q;
+        out[2] = pm / n;
+    }
+    if (qk)
+        for (int j = 0; j < nk; j++) {
+            const double hs = K->pos[j] == 1 ? hx : K->pos[j] == 2 ? hy : hz;
+            double qc = 0.0, q3 = 0.0;
+            for (int i = 0; i < K->len[j]; i++) {
+                int c = or_karst_cell(K, j, i, nx, ny);
+                qc = qc + (-KI[c] / visc) * (KM(pc, i, j) - p[c]) * hs;
+                q3 = q3 + (KI[c] / visc) * (KM(pc, i, j) - p[c]);
+            }
+            qk[j] = qc;
+            qk[nk + j] = q3;
+            qk[2 * nk + j] = KM(ul, 0, j) * K->area[j] + KM(ur, K->len[j] - 1, j) * K->area[j];
+        }
+    if (!ucl) free(ul);
+    if (!ucr) free(ur);
+    for (int f = 0; f < 6; f++) free(fv[f]);
+    free(S.kl); free(S.kr); free(S.kc); free(S.kic); free(S.paux);
+    free(S.pc_old); free(S.ucR); free(S.ucL);
+    free(perm); free(ind); free(b); free(pcaux); free(p_old); free(KI);
+    free(cnt); free(col); free(ele);
+    return iter;
+}
+#undef KM

@@ -141,6 +141,86 @@ int or_level_copy(const or_hierarchy *H, int l, int *cnt, int *col,
                   double *ele, double *dinv, char *sel, int *pcnt, int *pcol,
                   double *pele);
 
+/* ---- the coupled conduit model (karst.c, main.c:383-557) --------------- */
+
+/* A conduit set as main.c:197-280 reads it from data_<nk>_<type>.dat.
+ * Per-conduit arrays have nk entries; the per-end tables cont/ccont are
+ * [f*nk + j] (f = 0 left end, 1 right end); the per-fracture tables are
+ * [b*nk + j] for b < max_brechas, beta already R^4 - 1 (main.c:256).
+ * pos: 1 = conduit along x, 2 = along y, 3 = along z.  bound: 0 Dirichlet,
+ * 1 Neumann, 3 nonlinear Robin (permeabilities.c:826-858).  Same layout as
+ * hmfem_karst in include/hmfem_karst.h. */
+typedef struct {
+    int nk, max_brechas;
+    const int *len, *sxi, *syi, *szi, *pos;
+    const double *Kc;
+    const int *bound_l, *bound_r;
+    const double *cont, *ccont;
+    const double *kindex, *area;
+    const int *n_brechas;
+    const double *beta, *cb;
+    const int *brechas;
+} or_karst;
+
+/* The 3-D side the conduit terms read (the matrix faces of the coupled
+ * system, K and the last reservoir pressure). */
+typedef struct {
+    int nx, ny, nz;
+    double hx, hy, hz, visc, rho;
+    const double *KX, *KY, *KZ;
+    const or_ele *perm;
+    const double *p_old;
+} or_kgrid;
+
+/* Conduit state; matrices are [i*nk + j] with mmax rows (pc[i][j] of
+ * main.c), ucR/ucL are [b*nk + j]. */
+typedef struct {
+    int mmax;
+    double *kl, *kr, *kc, *kic, *paux, *pc, *pc_old, *ucR, *ucL;
+} or_kstate;
+
+/* 0 when the set is usable on an nx x ny x nz grid, else -1: a conduit
+ * leaves the grid, a fracture sits on the last element, a Robin end has no
+ * reservoir cell beyond it, or a Robin right end of a z conduit (the
+ * reference leaves its source term undefined, set_source_term.c:368-404). */
+int or_karst_check(const or_karst *K, int nx, int ny, int nz);
+/* 3-D cell of conduit j, element i (main.c:416-448). */
+int or_karst_cell(const or_karst *K, int j, int i, int nx, int ny);
+/* permeabilities.c:795-867 (permeabilidade_karst) for conduit j. */
+void or_karst_keff(const or_karst *K, const or_kgrid *G, or_kstate *S, int j);
+/* set_source_term.c:256-414 (source_term1d) for conduit j into f (len). */
+void or_source_term1d(const or_karst *K, const or_kgrid *G, or_kstate *S,
+                      int j, double *f);
+/* The tridiagonal conduit system solve_linearsystem_AMG.c:200-294 builds
+ * (row i: -kl[i] x[i-1] + kc[i] x[i] - kr[i] x[i+1] = f[i]) solved by the
+ * Thomas algorithm; kl/kc/kr are read with stride `stride`. */
+void or_thomas(int m, const double *kl, const double *kc, const double *kr,
+               int stride, const double *f, double *x);
+/* karst.c:8-40 (conduit): keff, source term and solve of every conduit.
+ * solver 0: Thomas; 1: compute() (AMG-PCG, 1e-8, pcg.h rule) as the
+ * reference does (compute.cpp:40-45). */
+void or_conduit(const or_karst *K, const or_kgrid *G, or_kstate *S,
+                int solver);
+/* flux_reconstruction.c:322-496 (fluxo1d) into ucl/ucr ([i*nk + j]). */
+void or_fluxo1d(const or_karst *K, const or_kgrid *G, const or_kstate *S,
+                double *ucl, double *ucr);
+
+/* The coupled Picard loop of main.c:383-489 and the conduit/well balances
+ * of main.c:523-593.  The 3-D solves run this oracle's AMG-PCG (compute.cpp
+ * settings) to solve_eps with stop rule solve_stop (or_pcg); conduit_solver
+ * as or_conduit.  WI/pw (nullable) are the well index and well pressure.
+ * Outputs: p (n), pc (mmax*nk), and when non-NULL ucl/ucr (mmax*nk), v (n
+ * 3-D face fluxes), out[0..2] = {error, Q well, mean p} and
+ * qk[3*nk] = {Qc1d, Qc3d, Qcb} per conduit.  Returns the Picard iteration
+ * count, or -1 when or_karst_check fails. */
+int or_picard(const or_karst *K, int nx, int ny, int nz, double hx, double hy,
+              double hz, double visc, double rho, const double *KX,
+              const double *KY, const double *KZ, const int bc_type[6],
+              const double val6[6], const double *WI, const double *pw,
+              double tol, int iter_max, double solve_eps, int solve_stop,
+              int conduit_solver, double *p, double *pc, double *ucl,
+              double *ucr, or_ele *v, double *out, double *qk);
+
 #ifdef __cplusplus
 }
 #endif

@@ -279,3 +279,189 @@ class Ref:
                                   np.asarray(p.bc_value, np.float64), eps, x,
                                   _ptr(v), times, C.byref(rr))
         return x, v, it, rr.value, times
+
+
+# ---- the coupled conduit model (karst.c, main.c:383-557) ----------------------
+
+class _KGrid(C.Structure):      # or_kgrid
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double),
+                ("visc", C.c_double), ("rho", C.c_double),
+                ("KX", C.c_void_p), ("KY", C.c_void_p), ("KZ", C.c_void_p),
+                ("perm", C.c_void_p), ("p_old", C.c_void_p)]
+
+
+class _KState(C.Structure):     # or_kstate
+    _fields_ = [("mmax", C.c_int)] + [(f, C.c_void_p) for f in (
+        "kl", "kr", "kc", "kic", "paux", "pc", "pc_old", "ucR", "ucL")]
+
+
+def _vp(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _picard_out(k, n):
+    mm = (k.mmax, k.nk)
+    return dict(p=np.zeros(n), pc=np.zeros(mm), ucl=np.zeros(mm), ucr=np.zeros(mm),
+                v=np.zeros((n, 7)), out=np.zeros(3), qk=np.zeros((3, k.nk)))
+
+
+def karst_state_inputs(k, prob, p_old):
+    """paux and KI_c of main.c:410-449 for a conduit set (matrices
+    [i, j] with max(len) rows)."""
+    paux = np.zeros((k.mmax, k.nk))
+    kic = np.zeros((k.mmax, k.nk))
+    hs = k.hs(prob.hx, prob.hy, prob.hz)
+    for j, c in enumerate(k.cells(prob.nx, prob.ny)):
+        paux[:len(c), j] = p_old[c]
+        kic[:len(c), j] = k.kindex[j] / (k.area[j] * hs[j])
+    return paux, kic
+
+
+def _port_bind(L):
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    L.or_karst_check.argtypes = [vp, i, i, i]
+    L.or_karst_keff.argtypes = [vp, vp, vp, i]
+    L.or_source_term1d.argtypes = [vp, vp, vp, i, vp]
+    L.or_conduit.argtypes = [vp, vp, vp, i]
+    L.or_fluxo1d.argtypes = [vp, vp, vp, vp, vp]
+    L.or_picard.argtypes = ([vp, i, i, i, d, d, d, d, d, vp, vp, vp, vp, vp, vp, vp,
+                             d, i, d, i, i] + [vp] * 7)
+
+
+def _port_karst_check(self, k, nx, ny, nz):
+    _port_bind(self.L)
+    ks = k.struct()
+    return self.L.or_karst_check(C.addressof(ks), nx, ny, nz)
+
+
+def _port_conduit_step(self, k, prob, perm, p_old, pc_old, ucR, ucL, rho=1000.0,
+                       solver=0):
+    """karst.c:8-40 from given state; also the source term f of each conduit
+    (from the same starting fracture state)."""
+    _port_bind(self.L)
+    ks = k.struct()
+    p_old = _f64(p_old)
+    perm = np.ascontiguousarray(perm, dtype=np.float64)
+    KX, KY, KZ = _f64(prob.KX), _f64(prob.KY), _f64(prob.KZ)
+    G = _KGrid(prob.nx, prob.ny, prob.nz, prob.hx, prob.hy, prob.hz, prob.visc, rho,
+               KX.ctypes.data, KY.ctypes.data, KZ.ctypes.data, perm.ctypes.data,
+               p_old.ctypes.data)
+    paux, kic = karst_state_inputs(k, prob, p_old)
+    mm = (k.mmax, k.nk)
+    arr = dict(kl=np.zeros(mm), kr=np.zeros(mm), kc=np.zeros(mm), kic=kic, paux=paux,
+               pc=np.zeros(mm), pc_old=_f64(pc_old).copy(),
+               ucR=_f64(ucR).copy().reshape(-1) if k.max_brechas else np.zeros(1),
+               ucL=_f64(ucL).copy().reshape(-1) if k.max_brechas else np.zeros(1))
+
+    def state(a):
+        return _KState(k.mmax, *[a[f].ctypes.data for f in (
+            "kl", "kr", "kc", "kic", "paux", "pc", "pc_old", "ucR", "ucL")])
+
+    # source terms on a copy of the fracture state
+    a2 = {f: v.copy() for f, v in arr.items()}
+    S2 = state(a2)
+    f = np.zeros(mm)
+    for j in range(k.nk):
+        fj = np.zeros(k.mmax + 1)
+        self.L.or_karst_keff(C.addressof(ks), C.addressof(G), C.addressof(S2), j)
+        self.L.or_source_term1d(C.addressof(ks), C.addressof(G), C.addressof(S2), j,
+                                _vp(fj))
+        f[:k.len[j], j] = fj[:k.len[j]]
+    S = state(arr)
+    self.L.or_conduit(C.addressof(ks), C.addressof(G), C.addressof(S), solver)
+    out = {x: arr[x] for x in ("kl", "kr", "kc", "pc")}
+    out["ucR"] = arr["ucR"][:k.max_brechas * k.nk].reshape(k.max_brechas, k.nk)
+    out["ucL"] = arr["ucL"][:k.max_brechas * k.nk].reshape(k.max_brechas, k.nk)
+    out["f"] = f
+    return out
+
+
+def _port_picard(self, k, prob, WI=None, pw=None, rho=1000.0, tol=1e-8, iter_max=1000,
+                 solve_eps=1e-10, solve_stop=1, conduit_solver=0):
+    """main.c:383-557 on this oracle (or_picard)."""
+    _port_bind(self.L)
+    ks = k.struct()
+    n = prob.n
+    o = _picard_out(k, n)
+    KX, KY, KZ = _f64(prob.KX), _f64(prob.KY), _f64(prob.KZ)
+    bct = np.asarray(prob.bc_type, np.int32)
+    bcv = np.asarray(prob.bc_value, np.float64)
+    WI, pw = _f64(WI), _f64(pw)
+    it = self.L.or_picard(C.addressof(ks), prob.nx, prob.ny, prob.nz, prob.hx, prob.hy,
+                          prob.hz, prob.visc, rho, _vp(KX), _vp(KY), _vp(KZ), _vp(bct),
+                          _vp(bcv), _vp(WI), _vp(pw), tol, iter_max, solve_eps,
+                          solve_stop, conduit_solver, _vp(o["p"]), _vp(o["pc"]),
+                          _vp(o["ucl"]), _vp(o["ucr"]), _vp(o["v"]), _vp(o["out"]),
+                          _vp(o["qk"]))
+    if it < 0:
+        raise ValueError("conduit set does not fit the grid")
+    o["iterations"] = it
+    return o
+
+
+Port.karst_check = _port_karst_check
+Port.conduit_step = _port_conduit_step
+Port.picard = _port_picard
+
+
+def _ref_bind(L):
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    L.ref_conduit_step.argtypes = [vp, i, i, i, d, d, d, d, d] + [vp] * 15 + [d]
+    L.ref_picard.argtypes = ([vp, i, i, i, d, d, d, d, d, vp, vp, vp, vp, vp, vp, vp,
+                              d, i, d] + [vp] * 8)
+
+
+def _ref_conduit_step(self, k, prob, perm, p_old, pc_old, ucR, ucL, rho=1000.0, eps=1e-8):
+    """The reference's conduit() (and source_term1d alone for f) on given
+    state; 1-D solves through compute() at eps with the pcg.h rule."""
+    _ref_bind(self.L)
+    ks = k.struct()
+    p_old = _f64(p_old)
+    perm = np.ascontiguousarray(perm, dtype=np.float64)
+    paux, kic = karst_state_inputs(k, prob, p_old)
+    mm = (k.mmax, k.nk)
+    kl, kr, kc, f, pc = (np.zeros(mm) for _ in range(5))
+    uR = _f64(ucR).copy().reshape(-1) if k.max_brechas else np.zeros(1)
+    uL = _f64(ucL).copy().reshape(-1) if k.max_brechas else np.zeros(1)
+    KX, KY, KZ = _f64(prob.KX), _f64(prob.KY), _f64(prob.KZ)
+    pco = _f64(pc_old)
+    self.L.ref_conduit_step(C.addressof(ks), prob.nx, prob.ny, prob.nz, prob.hx, prob.hy,
+                            prob.hz, prob.visc, rho, _vp(KX), _vp(KY), _vp(KZ), _vp(perm),
+                            _vp(p_old), _vp(paux), _vp(kic), _vp(pco), _vp(uR), _vp(uL),
+                            _vp(kl), _vp(kr), _vp(kc), _vp(f), _vp(pc), eps)
+    mb = k.max_brechas
+    return dict(kl=kl, kr=kr, kc=kc, f=f, pc=pc,
+                ucR=uR[:mb * k.nk].reshape(mb, k.nk), ucL=uL[:mb * k.nk].reshape(mb, k.nk))
+
+
+def _ref_picard(self, k, prob, WI=None, pw=None, rho=1000.0, tol=1e-8, iter_max=1000,
+                eps=1e-8):
+    """The reference's coupled run (its reservoir(), conduit(), fluxo1d(),
+    fluxos()) with every solve through compute() at eps (pcg.h rule)."""
+    _ref_bind(self.L)
+    ks = k.struct()
+    n = prob.n
+    o = _picard_out(k, n)
+    times = np.zeros(2)
+    KX, KY, KZ = _f64(prob.KX), _f64(prob.KY), _f64(prob.KZ)
+    bct = np.asarray(prob.bc_type, np.int32)
+    bcv = np.asarray(prob.bc_value, np.float64)
+    WI, pw = _f64(WI), _f64(pw)
+    it = self.L.ref_picard(C.addressof(ks), prob.nx, prob.ny, prob.nz, prob.hx, prob.hy,
+                           prob.hz, prob.visc, rho, _vp(KX), _vp(KY), _vp(KZ), _vp(bct),
+                           _vp(bcv), _vp(WI), _vp(pw), tol, iter_max, eps, _vp(o["p"]),
+                           _vp(o["pc"]), _vp(o["ucl"]), _vp(o["ucr"]), _vp(o["v"]),
+                           _vp(o["out"]), _vp(o["qk"]), _vp(times))
+    o["iterations"] = it
+    o["seconds"] = float(times[0])
+    o["computes"] = int(times[1])
+    return o
+
+
+Ref.conduit_step = _ref_conduit_step
+Ref.picard = _ref_picard

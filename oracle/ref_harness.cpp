@@ -31,6 +31,7 @@
 #undef private
 #include "structs.h"
 #include "functions.h"
+#include "hmfem_oracle.h"
 
 /* ---- globals normally defined by the application's main.c (variables.h) */
 Dim N;
@@ -381,6 +382,270 @@ int ref_solve_all(int nx, int ny, int nz, double hx, double hy, double hz,
     if (relres) *relres = g_relres;
     free(pm); free(ic); free(b);
     return iter_amg;
+}
+
+}  // extern "C"
+
+/* ---- the coupled conduit model ------------------------------------------ */
+/* Sets the conduit globals that main.c:197-307 would read from the data file
+ * (an or_karst has the data file's layout, see hmfem_oracle.h). */
+static void karst_globals(const or_karst *k)
+{
+    const int nk = k->nk;
+    number_karst = nk;
+    M = (DimK *)malloc((nk + 1) * sizeof(DimK));
+    Mmax = 0;
+    for (int j = 0; j < nk; j++) {
+        M[j].s = k->len[j]; M[j].sxi = k->sxi[j]; M[j].syi = k->syi[j];
+        M[j].szi = k->szi[j]; M[j].pos = k->pos[j];
+        if (M[j].s > Mmax) Mmax = M[j].s;
+    }
+    Kc = create_vector(nk);
+    BoundKarst = (FACEK *)malloc(sizeof(FACEK));
+    BoundKarst->l = create_int(nk);
+    BoundKarst->r = create_int(nk);
+    cont_karst = create_matrix(2, nk);
+    C_contorno = create_matrix(2, nk);
+    n_brechas = create_int(nk);
+    hs = create_vector(nk);
+    for (int j = 0; j < nk; j++) {
+        Kc[j] = k->Kc[j];
+        BoundKarst->l[j] = k->bound_l[j];
+        BoundKarst->r[j] = k->bound_r[j];
+        for (int f = 0; f < 2; f++) {
+            cont_karst[f][j] = k->cont[f * nk + j];
+            C_contorno[f][j] = k->ccont[f * nk + j];
+        }
+        n_brechas[j] = k->n_brechas[j];
+        hs[j] = M[j].pos == 1 ? h.x : M[j].pos == 2 ? h.y : h.z;
+    }
+    const int mb = k->max_brechas;
+    ::beta = create_matrix(mb, nk);
+    C = create_matrix(mb, nk);
+    brechas = create_matrix_int(mb, nk);
+    for (int b = 0; b < mb; b++)
+        for (int j = 0; j < nk; j++) {
+            ::beta[b][j] = k->beta[b * nk + j];
+            C[b][j] = k->cb[b * nk + j];
+            brechas[b][j] = k->brechas[b * nk + j];
+        }
+    ucL_old = create_matrix(mb, nk);
+    ucR_old = create_matrix(mb, nk);
+    pc = create_matrix(Mmax, nk);
+    pc_old = create_matrix(Mmax, nk);
+    indcol1 = (IND *)malloc((Mmax + 1) * sizeof(IND));
+    uc = (ELEK *)malloc((Mmax + 1) * sizeof(ELEK));
+    uc->l = create_matrix(Mmax, nk);
+    uc->r = create_matrix(Mmax, nk);
+    uc->c = create_matrix(Mmax, nk);
+}
+
+static int karst_cell(int j, int i)
+{
+    int x = M[j].sxi, y = M[j].syi, z = M[j].szi;
+    if (M[j].pos == 1) x += i;
+    else if (M[j].pos == 2) y += i;
+    else z += i;
+    return pindex(x, y, z, N);
+}
+
+/* main.c:102-113 */
+static double rel_change(const double *y, const double *y_old, int n)
+{
+    double s1 = 0, s2 = 0;
+    for (int i = 0; i < n; i++) {
+        s1 = s1 + (y[i] - y_old[i]) * (y[i] - y_old[i]);
+        s2 = s2 + y[i] * y[i];
+    }
+    return sqrt(s1) / sqrt(s2);
+}
+
+extern "C" {
+
+/* One conduit() call of the reference (karst.c:8-40 through
+ * permeabilidade_karst, source_term1d and solve_linsys_1d) on given state:
+ * p_old / perm / K of the 3-D side, paux, KI_c, pc_old and the fracture
+ * velocities ucR/ucL (in: previous, out: updated).  Matrices [i*nk + j]
+ * (mmax rows), fracture tables [b*nk + j].  Outputs keff (kl, kr, kc), the
+ * source term f of each conduit ([i*nk + j]) and pc.  The 1-D solves go
+ * through compute() with the pcg.h rule at eps. */
+int ref_conduit_step(const or_karst *k, int nx, int ny, int nz, double hx,
+                     double hy, double hz, double visc, double rho_,
+                     const double *KX, const double *KY, const double *KZ,
+                     ELE *perm_in, const double *p_old, const double *paux,
+                     const double *kic, const double *pcold_in, double *ucR_io,
+                     double *ucL_io, double *kl, double *kr, double *kc,
+                     double *f_out, double *pc_out, double eps)
+{
+    N.x = nx; N.y = ny; N.z = nz; N.xy = nx * ny; N.t = nx * ny * nz;
+    h.x = hx; h.y = hy; h.z = hz;
+    viscosidade = visc;
+    rho = rho_;
+    karst_globals(k);
+    const int nk = k->nk, mb = k->max_brechas;
+    Perm Kp;
+    Kp.X = (double *)KX; Kp.Y = (double *)KY; Kp.Z = (double *)KZ;
+    Kp.S = create_matrix(Mmax, nk);
+    double **KI_c = create_matrix(Mmax, nk), **p_aux = create_matrix(Mmax, nk);
+    for (int j = 0; j < nk; j++)
+        for (int i = 0; i < Mmax; i++) {
+            Kp.S[i][j] = Kc[j];
+            KI_c[i][j] = kic[i * nk + j];
+            p_aux[i][j] = paux[i * nk + j];
+            pc_old[i][j] = pcold_in[i * nk + j];
+        }
+    for (int b = 0; b < mb; b++)
+        for (int j = 0; j < nk; j++) {
+            ucR_old[b][j] = ucR_io[b * nk + j];
+            ucL_old[b][j] = ucL_io[b * nk + j];
+        }
+    ELEK keff;
+    keff.l = create_matrix(Mmax, nk);
+    keff.r = create_matrix(Mmax, nk);
+    keff.c = create_matrix(Mmax, nk);
+    g_mode = 1;
+    g_eps = eps;
+    /* the source terms by themselves first (they update the fracture
+     * velocities), then conduit() from the same starting state */
+    for (int j = 0; j < nk; j++) {
+        std::vector<double> f(M[j].s + 2, 0.0);
+        permeabilidade_karst(&Kp, &keff, indcol1, hs, M, BoundKarst, viscosidade, KI_c, j);
+        source_term1d(&keff, hs, M, BoundKarst, cont_karst, KI_c, p_aux, &Kp,
+                      perm_in, (double *)p_old, j, f.data());
+        for (int i = 0; i < M[j].s; i++) f_out[i * nk + j] = f[i];
+    }
+    for (int b = 0; b < mb; b++)
+        for (int j = 0; j < nk; j++) {
+            ucR_old[b][j] = ucR_io[b * nk + j];
+            ucL_old[b][j] = ucL_io[b * nk + j];
+        }
+    conduit(p_aux, cont_karst, KI_c, viscosidade, M, hs, indcol1, BoundKarst,
+            &keff, &Kp, perm_in, (double *)p_old, pc);
+    for (int j = 0; j < nk; j++)
+        for (int i = 0; i < M[j].s; i++) {
+            kl[i * nk + j] = keff.l[i][j];
+            kr[i * nk + j] = keff.r[i][j];
+            kc[i * nk + j] = keff.c[i][j];
+            pc_out[i * nk + j] = pc[i][j];
+        }
+    for (int b = 0; b < mb; b++)
+        for (int j = 0; j < nk; j++) {
+            ucR_io[b * nk + j] = ucR_old[b][j];
+            ucL_io[b * nk + j] = ucL_old[b][j];
+        }
+    return 0;
+}
+
+/* The reference's coupled run: main.c:383-489 (restated loop around the
+ * reference's own reservoir() and conduit()), then fluxo1d / fluxos and the
+ * balances of main.c:523-593.  Every solve goes through compute() with the
+ * pcg.h stop rule at eps (compute.cpp uses 1e-8).  Same outputs as
+ * or_picard; times[0] = the run (s), times[1] = compute() calls. */
+int ref_picard(const or_karst *k, int nx, int ny, int nz, double hx, double hy,
+               double hz, double visc, double rho_, const double *KX,
+               const double *KY, const double *KZ, const int *bc,
+               const double *val6, const double *WI_in, const double *pw_in,
+               double tol, int iter_max, double eps, double *p_out,
+               double *pc_out, double *ucl, double *ucr, ELE *v_out,
+               double *out, double *qk, double *times)
+{
+    double t0 = now();
+    set_grid(nx, ny, nz, hx, hy, hz, bc, visc);
+    rho = rho_;
+    karst_globals(k);
+    const int nk = k->nk;
+    Perm Kp;
+    Kp.X = create_vector(N.t); Kp.Y = create_vector(N.t); Kp.Z = create_vector(N.t);
+    for (int s = 0; s < N.t; s++) { Kp.X[s] = KX[s]; Kp.Y[s] = KY[s]; Kp.Z[s] = KZ[s]; }
+    Kp.S = create_matrix(Mmax, nk);
+    for (int j = 0; j < nk; j++)
+        for (int i = 0; i < Mmax; i++) Kp.S[i][j] = Kc[j];   /* permeabilities.c:46-51 */
+    double *WI = create_vector(N.t), *KI = create_vector(N.t), *pw = create_vector(N.t);
+    if (pw_in) for (int s = 0; s < N.t; s++) pw[s] = pw_in[s];
+    Bound *Bd = make_bound(val6);
+    ELE *pm = (ELE *)calloc(N.t + 1, sizeof(ELE));
+    IND *ic = (IND *)malloc((N.t + 1) * sizeof(IND));
+    for (int s = 0; s < N.t; s++) {
+        ic[s].c = ic[s].u = ic[s].d = ic[s].l = -1;
+        ic[s].r = ic[s].t = ic[s].b = -1;
+    }
+    double *p = create_vector(N.t), *p_old = create_vector(N.t);
+    g_mode = 1;
+    g_eps = eps;
+    int ncompute = 0;
+    reservoir(N, &Kp, WI, KI, pc_old, ic, Bd, pm, h, boundary, viscosidade, pw, M, p);
+    ncompute++;
+    for (int s = 0; s < N.t; s++) p_old[s] = p[s];
+    if (WI_in) for (int s = 0; s < N.t; s++) WI[s] = WI_in[s];
+    double **KI_c = create_matrix(Mmax, nk), **p_aux = create_matrix(Mmax, nk);
+    for (int j = 0; j < nk; j++)
+        for (int i = 0; i < M[j].s; i++) {
+            int aux = karst_cell(j, i);
+            KI[aux] = k->kindex[j];
+            KI_c[i][j] = k->kindex[j] / (k->area[j] * hs[j]);
+            p_aux[i][j] = p_old[aux];
+            Kp.S[i][j] = Kc[j];
+        }
+    ELEK keff;
+    keff.l = create_matrix(Mmax, nk);
+    keff.r = create_matrix(Mmax, nk);
+    keff.c = create_matrix(Mmax, nk);
+    conduit(p_aux, cont_karst, KI_c, viscosidade, M, hs, indcol1, BoundKarst,
+            &keff, &Kp, pm, p_old, pc);
+    ncompute += nk;
+    double error = 1;
+    int iter = 0;
+    while (iter < iter_max && error > tol) {
+        for (int i = 0; i < Mmax; i++)
+            for (int j = 0; j < nk; j++) pc_old[i][j] = pc[i][j];
+        reservoir(N, &Kp, WI, KI, pc_old, ic, Bd, pm, h, boundary, viscosidade, pw, M, p);
+        error = rel_change(p, p_old, N.t);
+        for (int s = 0; s < N.t; s++) p_old[s] = p[s];
+        for (int j = 0; j < nk; j++)
+            for (int i = 0; i < M[j].s; i++) p_aux[i][j] = p_old[karst_cell(j, i)];
+        conduit(p_aux, cont_karst, KI_c, viscosidade, M, hs, indcol1, BoundKarst,
+                &keff, &Kp, pm, p_old, pc);
+        ncompute += 1 + nk;
+        iter++;
+    }
+    double t1 = now();
+    fluxo1d(pc, &keff, uc, hs, M, cont_karst, BoundKarst, &Kp, pm, p_old);
+    if (v_out) fluxos(p, pm, v_out, Bd, h, N);
+    for (int s = 0; s < N.t; s++) p_out[s] = p[s];
+    for (int i = 0; i < Mmax; i++)
+        for (int j = 0; j < nk; j++) {
+            bool in = i < M[j].s;
+            pc_out[i * nk + j] = in ? pc[i][j] : 0.0;
+            if (ucl) ucl[i * nk + j] = in ? uc->l[i][j] : 0.0;
+            if (ucr) ucr[i * nk + j] = in ? uc->r[i][j] : 0.0;
+        }
+    if (out) {
+        double Q = 0.0, pm_ = 0.0;
+        for (int s = 0; s < N.t; s++) {
+            Q = Q + (WI[s] / viscosidade) * (pw[s] - p[s]);
+            pm_ = pm_ + p[s];
+        }
+        out[0] = error;
+        out[1] = Q;
+        out[2] = pm_ / N.t;
+    }
+    if (qk)
+        for (int j = 0; j < nk; j++) {
+            double qc = 0.0, q3 = 0.0;
+            for (int i = 0; i < M[j].s; i++) {
+                int aux = karst_cell(j, i);
+                qc = qc + (-KI[aux] / viscosidade) * (pc[i][j] - p[aux]) * hs[j];
+                q3 = q3 + (KI[aux] / viscosidade) * (pc[i][j] - p[aux]);
+            }
+            qk[j] = qc;
+            qk[nk + j] = q3;
+            qk[2 * nk + j] = uc->l[0][j] * k->area[j] + uc->r[M[j].s - 1][j] * k->area[j];
+        }
+    if (times) { times[0] = t1 - t0; times[1] = ncompute; }
+    free_bound(Bd);
+    free(pm); free(ic); free(p); free(p_old); free(WI); free(KI); free(pw);
+    free(Kp.X); free(Kp.Y); free(Kp.Z);
+    return iter;
 }
 
 }  // extern "C"

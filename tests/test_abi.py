@@ -1,5 +1,5 @@
-"""The C-ABI library loads and exports every symbol include/hmfem_gpu.h
-declares (no compute calls: runs without a GPU)."""
+"""The C-ABI library loads and exports every symbol the headers in include/
+declare (no compute calls: runs without a GPU)."""
 import os
 import re
 import subprocess
@@ -10,7 +10,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    src = open(os.path.join(ROOT, "include", "hmfem_gpu.h")).read()
+    inc = os.path.join(ROOT, "include")
+    src = "".join(open(os.path.join(inc, f)).read()
+                  for f in sorted(os.listdir(inc)) if f.endswith(".h"))
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     names = set(re.findall(r"\b([A-Za-z_]\w*)\s*\(", src))
     names -= {"if", "for", "while", "return", "sizeof"}
