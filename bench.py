@@ -58,6 +58,8 @@ def parse():
                     help="report the learned-guess variant as the headline")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched uneven-instance measurement (config 3)")
+    ap.add_argument("--no-coupled", action="store_true",
+                    help="skip the coupled reservoir/conduit (Picard) workload")
     ap.add_argument("--cpu-sample", type=int, default=96)
     ap.add_argument("--profile-step", type=int, default=-1, metavar="PRECISION",
                     help="run one untimed step (assembly + setup + solve) of "
@@ -301,6 +303,7 @@ def run_ours(args):
            "h2d_bytes_per_step": nk * n * 8 + n * 8, "d2h_bytes_per_step": n * 8}
 
     batched = None if args.no_batch else run_batch(args, world)
+    coupled = None if args.no_coupled else run_coupled(args, world, rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -337,6 +340,7 @@ def run_ours(args):
             "gpu_launches": launches["chosen"],
             "gpu_launches_per_step": launches["chosen"] / args.steps,
             "batched": batched,
+            "coupled": coupled,
             "cpu_baseline": cpu,
             "clocks": ch["clocks"],
         }
@@ -357,7 +361,8 @@ def _ref_worker(args_tuple):
     from oracle.oracle import Ref
     p = config_problem(2, realisation=seed_off, size=size)
     t0 = time.perf_counter()
-    x, v, it, rel, times = Ref().solve_all(p, eps=tol)
+    with _QuietStdout():
+        x, v, it, rel, times = Ref().solve_all(p, eps=tol)
     dt = time.perf_counter() - t0
     return p.n, dt, it, rel, list(times)
 
@@ -367,14 +372,17 @@ def run_batch(args, world, n_inst=96):
     log10 std ~ U[1,2], correlation 4 cells, 0-4 conduits at 1e-10), FP32
     V-cycle in FP64 flexible CG to 1e-10, several solvers on their own
     streams (worker count tuned once per GPU).  Every rank solves the same
-    batch (replicas); wall clock around the whole batch, max over ranks."""
+    batch (replicas); one untimed pass, then wall clock around the whole
+    batch, max over ranks."""
     import torch
 
     from hmfem_b200 import batch as hb
     from hmfem_b200.problem import config_problem
     probs = [config_problem(3, realisation=r) for r in range(n_inst)]
     workers, tune = hb.tune_workers(probs[:16], precision=1, tol=args.tol)
-    hb.solve_batch(probs[:4], 1, args.tol, workers=workers)  # warm-up
+    # warm-up: one untimed pass over the whole batch, so the device memory
+    # pool has grown to the batch's working set before the timed pass
+    hb.solve_batch(probs, 1, args.tol, workers=workers)
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()
@@ -392,6 +400,95 @@ def run_batch(args, world, n_inst=96):
             "max_relres": float(max(r[1]["relres"] for r in res)),
             "timing": "host wall clock around the batch (host K in, pressure out)",
             "tuning": tune}
+
+
+class _QuietStdout:
+    """Sends file descriptor 1 to /dev/null while the reference's own C code
+    runs (fluxos prints its divergence bounds), so stdout keeps one JSON
+    line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
+def coupled_case():
+    """The reference's own coupled run (roda.sh: 210 x 42 x 20 cells on
+    210 x 210 x 100 m, homogeneous K = 1e-13, conduit file data_1_2.dat,
+    well column (105, 21, z >= 10) at 10 MPa, main.c constants)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import karst_cases as KC
+
+    from hmfem_b200.karst import Karst
+    prob = KC.reservoir(210, 42, 20, 1.0, 5.0, 5.0)
+    WI, pw = KC.well(prob, 105, 21, 10)
+    k = Karst.read(os.path.join(ROOT, "tests", "golden", "karst_data_1_2.dat"), 1)
+    return prob, k, WI, pw, KC.RHO
+
+
+def run_coupled(args, world, rank, reps=3):
+    """The Picard loop of main.c:383-489 through hmfem_picard (host K, WI,
+    pw in; reservoir and conduit pressures out), FP64 V-cycle PCG to
+    ||r||/||b|| <= 1e-10 per reservoir solve, Picard tolerance 1e-8; wall
+    clock per run (1 warm-up, median of `reps`), max over ranks."""
+    import torch
+
+    from hmfem_b200 import gpu, karst
+    prob, k, WI, pw, rho = coupled_case()
+    s = gpu.Solver(precision=0, tol=1e-10, stop_rule=0)
+    karst.picard(s, k, prob, WI, pw, rho=rho, fluxes=False)  # warm-up
+    torch.cuda.synchronize()
+    barrier(world)
+    walls, r = [], None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        r = karst.picard(s, k, prob, WI, pw, rho=rho, fluxes=False)
+        walls.append(time.perf_counter() - t0)
+    s.close()
+    wall = max_over_ranks(float(np.median(walls)), world)
+    st = r["stats"]
+    out = {"workload": "reference run script case: 210x42x20 reservoir + 1 conduit "
+                       "(data_1_2.dat: 123 elements, nonlinear Robin ends, 2 fractures) "
+                       "+ well column",
+           "cells": prob.n, "picard_iterations": st["iterations"],
+           "picard_error": st["error"], "cg_iterations": st["cg_iterations"],
+           "amg_setups": st["setups"], "wall_ms": 1e3 * wall,
+           "device_setup_ms": st["t_setup_ms"], "device_loop_ms": st["t_loop_ms"],
+           "timing": "host wall clock around hmfem_picard, host arrays in and out"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_reference"] = coupled_cpu_sample(prob, k, WI, pw, rho)
+        per = out["cpu_reference"].get("s_per_iteration")
+        if per:
+            est = out["cpu_reference"]["first_solve_s"] + per * st["iterations"]
+            out["cpu_reference"]["full_run_estimate_s"] = est
+            out["speedup_vs_reference_estimate"] = est / wall
+    return out
+
+
+def coupled_cpu_sample(prob, k, WI, pw, rho, iters=2):
+    """The reference's own coupled loop (oracle/_ref: its reservoir(),
+    conduit(), compute()) for the first `iters` Picard iterations, 1 core."""
+    try:
+        from oracle.oracle import Ref
+        R = Ref()
+        with _QuietStdout():
+            r0 = R.picard(k, prob, WI, pw, rho=rho, iter_max=0)
+            r2 = R.picard(k, prob, WI, pw, rho=rho, iter_max=iters)
+    except Exception as e:  # reference build missing
+        return {"unavailable": str(e)}
+    per = (r2["seconds"] - r0["seconds"]) / iters
+    return {"kind": "reference", "cores": 1, "first_solve_s": r0["seconds"],
+            "s_per_iteration": per,
+            "sample": f"first reservoir solve + {iters} Picard iterations of the "
+                      f"reference's loop ({r2['seconds']:.1f} s)"}
 
 
 def cpu_baseline_sample(size, cores=1, tol=1e-10):

@@ -263,13 +263,15 @@ __global__ void k_ref_to_elem(KDev d, int mmax, const double *__restrict__ in, d
     if (i < d.len[j]) e[d.off[j] + i] = in[t];
 }
 
-// fracture arrays <-> the reference's [b * nk + j] tables
+// fracture arrays <-> the reference's [b * nk + j] tables (entries past a
+// conduit's fracture count are left as they are, as the reference leaves
+// ucR_old / ucL_old there)
 __global__ void k_frac_to_ref(KDev d, int mb, const double *__restrict__ e, double *out)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= mb * d.nk) return;
     const int b = t / d.nk, j = t % d.nk;
-    out[t] = b < d.nb[j] ? e[d.boff[j] + b] : 0.0;
+    if (b < d.nb[j]) out[t] = e[d.boff[j] + b];
 }
 
 __global__ void k_ref_to_frac(KDev d, int mb, const double *__restrict__ in, double *e)
@@ -950,6 +952,7 @@ int hmfem_conduit_step(const hmfem_karst *k, int nx, int ny, int nz, double hx, 
                 double *const fo[2] = {ucR, ucL};
                 double *const fe[2] = {d.ucR, d.ucL};
                 for (int a = 0; a < 2; a++) {
+                    cudaMemcpyAsync(fstage, fo[a], sizeof(double) * mb, in, st);
                     hm::k_frac_to_ref<<<hm::grid1(mb, 128), 128, 0, st>>>(d, H.mbt, fe[a], fstage);
                     HM_COUNT();
                     cudaMemcpyAsync(fo[a], fstage, sizeof(double) * mb, outk, st);

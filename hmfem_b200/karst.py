@@ -232,7 +232,7 @@ def picard(solver, k: Karst, prob, WI=None, pw=None, rho=1000.0, tol=1e-8,
         rc2 = L.hmfem_picard_fluxes(solver.h, _p(ucl), _p(ucr), _p(qk), 0)
         if rc2 != 0:
             raise gpu.HmfemError(rc2, gpu.last_error())
-        out.update(ucl=ucl, ucr=ucr, qk=qk, v=solver.fluxes(p)[0])
+        out.update(ucl=ucl, ucr=ucr, qk=qk, v=solver.fluxes(p, np.zeros((n, 7)))[0])
     return out
 
 
