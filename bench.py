@@ -60,6 +60,8 @@ def parse():
                     help="skip the batched uneven-instance measurement (config 3)")
     ap.add_argument("--no-coupled", action="store_true",
                     help="skip the coupled reservoir/conduit (Picard) workload")
+    ap.add_argument("--no-output", action="store_true",
+                    help="skip the result-file writers")
     ap.add_argument("--cpu-sample", type=int, default=96)
     ap.add_argument("--profile-step", type=int, default=-1, metavar="PRECISION",
                     help="run one untimed step (assembly + setup + solve) of "
@@ -304,6 +306,9 @@ def run_ours(args):
 
     batched = None if args.no_batch else run_batch(args, world)
     coupled = None if args.no_coupled else run_coupled(args, world, rank)
+    output = None
+    if not args.no_output and rank == 0:
+        output = run_output(args, prob, s_e2e, xh, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -341,6 +346,7 @@ def run_ours(args):
             "gpu_launches_per_step": launches["chosen"] / args.steps,
             "batched": batched,
             "coupled": coupled,
+            "output": output,
             "cpu_baseline": cpu,
             "clocks": ch["clocks"],
         }
@@ -471,6 +477,83 @@ def run_coupled(args, world, rank, reps=3):
             out["cpu_reference"]["full_run_estimate_s"] = est
             out["speedup_vs_reference_estimate"] = est / wall
     return out
+
+
+def run_output(args, prob, solver, p, world):
+    """The reference's result files of this solve (save_pressure,
+    save_flux, vts_StructuredGrid_file) written by the GPU writers
+    (include/hmfem_textio.h) to a scratch directory, one file at a time
+    (host pressure and fluxes in, file on disk out; wall clock per file);
+    beside them the reference's own writers (oracle/_ref) on a 64^3 sample,
+    scaled per byte."""
+    import ctypes as C
+    import shutil
+    import tempfile
+
+    from hmfem_b200 import gpu
+    L = gpu.lib()
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    L.hmfem_save_pressure.argtypes = [C.c_char_p, i, i, i, d, d, d, vp, i]
+    L.hmfem_save_flux.argtypes = [C.c_char_p, i, i, i, d, d, d, vp, i]
+    L.hmfem_save_vts.argtypes = [C.c_char_p, i, i, i, d, d, d, vp, vp, i]
+    v, _, _ = solver.fluxes(p, np.zeros((prob.n, 7)))
+    g = (prob.nx, prob.ny, prob.nz, prob.hx, prob.hy, prob.hz)
+    pp, pv = C.c_void_p(p.ctypes.data), C.c_void_p(v.ctypes.data)
+    calls = {"pressure_reservoir.dat": lambda f: L.hmfem_save_pressure(f, *g, pp, 0),
+             "flux_reservoir.dat": lambda f: L.hmfem_save_flux(f, *g, pv, 0),
+             "campos.vts": lambda f: L.hmfem_save_vts(f, *g, pv, pp, 0)}
+    d_out = tempfile.mkdtemp(prefix="hmfem_out_")
+    res = {}
+    try:
+        calls["pressure_reservoir.dat"](os.devnull.encode())  # warm-up
+        for name, fn in calls.items():
+            path = os.path.join(d_out, name)
+            t0 = time.perf_counter()
+            rc = fn(path.encode())
+            dt = time.perf_counter() - t0
+            size = os.path.getsize(path)
+            os.remove(path)
+            res[name] = {"rc": rc, "s": dt, "bytes": size, "MB_per_s": size / dt / 1e6}
+    finally:
+        shutil.rmtree(d_out, ignore_errors=True)
+    out = {"workload": f"result files of the {prob.nx}^3 solve, written to a scratch "
+                       f"directory (host arrays in)", "files": res,
+           "timing": "host wall clock per file, format + copies + file write"}
+    if not args.no_cpu_baseline:
+        out["cpu_reference"] = output_cpu_sample()
+        tot_gpu = sum(r["s"] for r in res.values())
+        tot_bytes = sum(r["bytes"] for r in res.values())
+        per = out["cpu_reference"].get("s_per_byte")
+        if per:
+            out["cpu_reference"]["estimate_s"] = per * tot_bytes
+            out["speedup_vs_reference_estimate"] = per * tot_bytes / tot_gpu
+    return out
+
+
+def output_cpu_sample(size=64):
+    """The reference's save_pressure + save_flux + vts_StructuredGrid_file
+    (oracle/_ref) on a size^3 field, one core."""
+    import ctypes as C
+    import tempfile
+    try:
+        from oracle.oracle import REF_SO
+        L = C.CDLL(REF_SO)
+        L.ref_save_grid.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_double,
+                                    C.c_double, C.c_double, C.c_void_p, C.c_void_p]
+    except Exception as e:  # reference build missing
+        return {"unavailable": str(e)}
+    n = size ** 3
+    rng = np.random.default_rng(0)
+    p = 6e7 * (1 + 0.01 * rng.standard_normal(n))
+    v = rng.standard_normal((n, 7)) * 1e-7
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        L.ref_save_grid(d.encode(), size, size, size, 1.0 / size, 1.0 / size, 1.0 / size,
+                        p.ctypes.data, v.ctypes.data)
+        dt = time.perf_counter() - t0
+        nbytes = sum(os.path.getsize(os.path.join(d, f)) for f in os.listdir(d))
+    return {"kind": "reference", "cores": 1, "s": dt, "bytes": nbytes, "s_per_byte": dt / nbytes,
+            "sample": f"save_pressure + save_flux + vts_StructuredGrid_file at {size}^3"}
 
 
 def coupled_cpu_sample(prob, k, WI, pw, rho, iters=2):

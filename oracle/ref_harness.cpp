@@ -649,3 +649,44 @@ int ref_picard(const or_karst *k, int nx, int ny, int nz, double hx, double hy,
 }
 
 }  // extern "C"
+
+/* ---- the reference's result writers (posprocessing_output.c, vtk.c) ------ */
+extern "C" {
+
+/* save_pressure / save_flux / vts_StructuredGrid_file into directory dir
+ * (the reference's dirname): pressure_reservoir.dat, flux_reservoir.dat,
+ * campos.vts. */
+int ref_save_grid(const char *dir, int nx, int ny, int nz, double hx, double hy,
+                  double hz, double *p, ELE *v)
+{
+    N.x = nx; N.y = ny; N.z = nz; N.xy = nx * ny; N.t = nx * ny * nz;
+    h.x = hx; h.y = hy; h.z = hz;
+    dirname = dir;
+    if (p) save_pressure(p, N, h);
+    if (v) save_flux(v, N, h);
+    if (p && v) vts_StructuredGrid_file(v, p, N, h);
+    return 0;
+}
+
+/* save_pressure_1d / save_flux_1d into dir for a conduit set; pc, ucl, ucr
+ * in the [i*nk + j] layout. */
+int ref_save_karst(const char *dir, const or_karst *k, double hx, double hy,
+                   double hz, const double *pcf, const double *ucl,
+                   const double *ucr)
+{
+    h.x = hx; h.y = hy; h.z = hz;
+    dirname = dir;
+    karst_globals(k);
+    const int nk = k->nk;
+    for (int i = 0; i < Mmax; i++)
+        for (int j = 0; j < nk; j++) {
+            pc[i][j] = pcf[i * nk + j];
+            uc->l[i][j] = ucl[i * nk + j];
+            uc->r[i][j] = ucr[i * nk + j];
+        }
+    save_pressure_1d(pc, M, hs, h);
+    save_flux_1d(uc, M, hs, h);
+    return 0;
+}
+
+}  // extern "C"
