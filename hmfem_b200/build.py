@@ -19,7 +19,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=default", "--expt-relaxed-constexpr",
          "--extended-lambda"]
 SOURCES = ["assemble.cu", "sparse.cu", "amg_setup.cu", "rap_stencil.cu", "stencil_cycle.cu", "smoother_setup.cu", "cycle.cu", "solver.cu",
-           "device_abi.cu", "noalloc.cu", "conv3d.cu", "karst.cu", "textio.cu"]
+           "device_abi.cu", "noalloc.cu", "conv3d.cu", "karst.cu", "textio.cu", "permio.cu"]
 
 
 def _deps():
@@ -28,6 +28,7 @@ def _deps():
     hdrs.append(os.path.join(HERE, "..", "include", "hmfem_guess.h"))
     hdrs.append(os.path.join(HERE, "..", "include", "hmfem_karst.h"))
     hdrs.append(os.path.join(HERE, "..", "include", "hmfem_textio.h"))
+    hdrs.append(os.path.join(HERE, "..", "include", "hmfem_permio.h"))
     return max(os.path.getmtime(h) for h in hdrs)
 
 

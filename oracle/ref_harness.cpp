@@ -690,3 +690,29 @@ int ref_save_karst(const char *dir, const or_karst *k, double hx, double hy,
 }
 
 }  // extern "C"
+
+/* ---- the reference's permeability readers (permeabilities.c) ------------- */
+extern "C" {
+
+/* variant 0 read_set_perm_field, 1 read_layer_perm_field (layer), 2
+ * gaussian_permfield (geological grid ngx^3 through nxg/nyg/nzg); the
+ * simulation grid nx*ny*nz on Ix*Iy*Iz with h = I/N as main.c:163-165. */
+int ref_read_perm(int variant, const char *path, int layer_, int ng, int nx, int ny,
+                  int nz, double Ix, double Iy, double Iz, double *KX, double *KY,
+                  double *KZ)
+{
+    N.x = nx; N.y = ny; N.z = nz; N.xy = nx * ny; N.t = nx * ny * nz;
+    I.x = Ix; I.y = Iy; I.z = Iz;
+    h.x = I.x / N.x; h.y = I.y / N.y; h.z = I.z / N.z;
+    fn = path;
+    layer = layer_;
+    nxg = nyg = nzg = ng;
+    Perm K;
+    K.X = KX; K.Y = KY; K.Z = KZ;
+    if (variant == 0) read_set_perm_field(&K, N, h, I);
+    else if (variant == 1) read_layer_perm_field(&K, N, h, I);
+    else gaussian_permfield(&K, N, h, I);
+    return 0;
+}
+
+}  // extern "C"
