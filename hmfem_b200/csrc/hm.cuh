@@ -189,6 +189,7 @@ void dfree(void *p);
 void set_alloc_stream(cudaStream_t st);  // stream that orders dalloc/dfree
 struct AllocCache;                       // per-solver exact-size block cache
 void set_alloc_context(cudaStream_t st, AllocCache *c);
+void get_alloc_context(cudaStream_t *st, AllocCache **c);
 AllocCache *alloc_cache_new();
 void alloc_cache_release(AllocCache *c);
 

@@ -603,6 +603,8 @@ int hmfem_destroy(hmfem_solver *h)
     if (s.ctl_host) cudaFreeHost(s.ctl_host);
     if (s.st) cudaStreamSynchronize(s.st);
     if (s.own_stream && s.st) cudaStreamDestroy(s.st);
+    // the thread's allocation context must not keep naming a dead stream
+    hm::set_alloc_context(nullptr, nullptr);
     delete h;
     return HMFEM_OK;
 }

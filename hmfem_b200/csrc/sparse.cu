@@ -62,6 +62,12 @@ void set_alloc_context(cudaStream_t st, AllocCache *c)
     g_cache = c;
 }
 
+void get_alloc_context(cudaStream_t *st, AllocCache **c)
+{
+    *st = g_astream;
+    *c = g_cache;
+}
+
 AllocCache *alloc_cache_new() { return new AllocCache(); }
 
 void alloc_cache_release(AllocCache *c)

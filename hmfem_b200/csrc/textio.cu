@@ -584,13 +584,28 @@ int device_view(const T *a, long n, int mem, cudaStream_t st, std::vector<void *
     return HMFEM_OK;
 }
 
+// One writer call: its buffers, file and the allocation context of this
+// thread (the scan draws its temporary storage from it: pointed at the
+// writer's stream for the call, restored afterwards).
 struct Scope {
     Writer w;
     std::vector<void *> keep;
     FILE *f = nullptr;
+    cudaStream_t saved_st = nullptr;
+    AllocCache *saved_cache = nullptr;
+    bool ctx = false;
+    int open(long maxrec)
+    {
+        HM_CHECK(w.open(maxrec));
+        get_alloc_context(&saved_st, &saved_cache);
+        set_alloc_context(w.st, nullptr);
+        ctx = true;
+        return HMFEM_OK;
+    }
     ~Scope()
     {
         w.close();
+        if (ctx) set_alloc_context(saved_st, saved_cache);
         for (void *p : keep) cudaFree(p);
         if (f) fclose(f);
     }
@@ -628,7 +643,7 @@ int hmfem_save_pressure(const char *path, int nx, int ny, int nz, double hx, dou
     if (!path || !p || nx < 1 || ny < 1 || nz < 1) return HMFEM_E_ARG;
     hm::Scope S;
     hm::Job J = hm::grid_job(hm::L_PRESSURE, nx, ny, nz, hx, hy, hz);
-    HM_CHECK(S.w.open(J.nrec));
+    HM_CHECK(S.open(J.nrec));
     HM_CHECK(hm::device_view(p, J.nrec, mem, S.w.st, S.keep, &J.p));
     HM_CHECK(hm::open_file(S, path));
     return S.w.run(J, S.f, nullptr);
@@ -640,7 +655,7 @@ int hmfem_save_flux(const char *path, int nx, int ny, int nz, double hx, double 
     if (!path || !v || nx < 1 || ny < 1 || nz < 1) return HMFEM_E_ARG;
     hm::Scope S;
     hm::Job J = hm::grid_job(hm::L_FLUX, nx, ny, nz, hx, hy, hz);
-    HM_CHECK(S.w.open(J.nrec));
+    HM_CHECK(S.open(J.nrec));
     HM_CHECK(hm::device_view(v, J.nrec, mem, S.w.st, S.keep, &J.v));
     HM_CHECK(hm::open_file(S, path));
     return S.w.run(J, S.f, nullptr);
@@ -652,7 +667,7 @@ int hmfem_save_vts(const char *path, int nx, int ny, int nz, double hx, double h
     if (!path || !v || !p || nx < 1 || ny < 1 || nz < 1) return HMFEM_E_ARG;
     hm::Scope S;
     const long n = (long)nx * ny * nz;
-    HM_CHECK(S.w.open(n));
+    HM_CHECK(S.open(n));
     hm::Job J = hm::grid_job(hm::L_VTS_VEL, nx, ny, nz, hx, hy, hz);
     HM_CHECK(hm::device_view(v, n, mem, S.w.st, S.keep, &J.v));
     HM_CHECK(hm::device_view(p, n, mem, S.w.st, S.keep, &J.p));
@@ -703,7 +718,7 @@ int hmfem_save_karst(const char *dir, const hmfem_karst *k, double hx, double hy
     }
     if (nk == 0) return HMFEM_OK;
     hm::Scope S;
-    HM_CHECK(S.w.open(mmax));
+    HM_CHECK(S.open(mmax));
     const long mm = (long)mmax * nk;
     const double *dpc = nullptr, *dl = nullptr, *dr = nullptr;
     HM_CHECK(hm::device_view(pc, mm, mem, S.w.st, S.keep, &dpc));
@@ -755,7 +770,7 @@ int hmfem_format_numbers(const double *x, long n, char conv, int prec, char *out
     J.layout = conv == 'e' ? hm::L_NUM_E : hm::L_NUM_F;
     J.nrec = n;
     J.prec = prec;
-    HM_CHECK(S.w.open(n));
+    HM_CHECK(S.open(n));
     HM_CHECK(hm::device_view(x, n, mem, S.w.st, S.keep, &J.p));
     std::string text;
     if (n > 0) HM_CHECK(S.w.run(J, nullptr, &text));
