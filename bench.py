@@ -646,7 +646,10 @@ def profile_step(args):
     from hmfem_b200.problem import config_problem
     prob = config_problem(2, size=args.size)
     K = torch.tensor(prob.KX, device="cuda")
-    s = gpu.Solver(precision=args.profile_step, tol=args.tol)
+    # the options of the bench's variants: plain FP64, or the chosen FP32
+    # V-cycle with levels >= 1 stored in BF16
+    s = gpu.Solver(precision=args.profile_step, tol=args.tol,
+                   bf16_from=1 if args.profile_step == 1 else -1, check_every=2)
     x = torch.zeros(prob.n, dtype=torch.float64, device="cuda")
     s.assemble(prob, KX=K, KY=K, KZ=K)
     s.setup()

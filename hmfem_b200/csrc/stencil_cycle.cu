@@ -80,6 +80,14 @@ template <class V> struct G19v {
     const V *v;   // slice-interleaved, 19 per row
     int n;        // coarse rows
     int nx, ny, nz;
+    // coarse row c = (x-pair, j, k) by multiplication: c / (nx/2) and
+    // row / ny as __umul64hi(., m) with m = floor(2^64 / d) + 1 (exact for
+    // 32-bit operands and 2 <= d < 2^32)
+    unsigned long long mhx, mny;
+    // coarse id of neighbour q: c + dq[parity][q] (the fine cell of c is
+    // s = 2c + parity, parity = (j + k) & 1, and (s + off_q) >> 1 =
+    // c + ((parity + off_q) >> 1))
+    int dq[2][kQ19];
 };
 
 // t -/+ sum over level-1 row c of a_cq x(q), ascending q.  No bounds test:
@@ -93,10 +101,11 @@ __device__ __forceinline__ T g19_row(T t, const G19v<V> &g, int c, X x)
 {
     using A = Ar<T>;
     constexpr int CH = 5;
-    const unsigned hx = (unsigned)g.nx >> 1, cu = (unsigned)c;
-    const unsigned row = cu / hx, k = row / (unsigned)g.ny, j = row - k * (unsigned)g.ny;
-    const int s = 2 * c + (int)((j + k) & 1);  // fine index (nx even)
-    const int nx = g.nx, nxy = g.nx * g.ny, last = g.n - 1;
+    const unsigned cu = (unsigned)c;
+    const unsigned row = (unsigned)__umul64hi(cu, g.mhx);
+    const unsigned k = (unsigned)__umul64hi(row, g.mny), j = row - k * (unsigned)g.ny;
+    const bool odd = ((j + k) & 1) != 0;
+    const int last = g.n - 1;
 #pragma unroll
     for (int q0 = 0; q0 < kQ19; q0 += CH) {
         T a[CH], xv[CH];
@@ -105,7 +114,7 @@ __device__ __forceinline__ T g19_row(T t, const G19v<V> &g, int c, X x)
             const int q = q0 + d;
             if (q < kQ19) {
                 a[d] = (T)ld(g.v, slice_at(c, q, kQ19));
-                int e = (s + q19x(q) + q19y(q) * nx + q19z(q) * nxy) >> 1;
+                int e = c + (odd ? g.dq[1][q] : g.dq[0][q]);
                 e = e < 0 ? 0 : (e > last ? last : e);
                 xv[d] = x(e);
             }
@@ -448,12 +457,36 @@ template <class V> G7v<V> g7v(const Grid7 &g);
 template <> G7v<double> g7v<double>(const Grid7 &g) { return {g.cf, g.nx, g.ny, g.nz}; }
 template <> G7v<float> g7v<float>(const Grid7 &g) { return {g.cf32, g.nx, g.ny, g.nz}; }
 
+// floor(2^64 / d) + 1 (d >= 2)
+unsigned long long mul_inverse(unsigned d)
+{
+    return (unsigned long long)(~0ull / d) + ((~0ull % d) == d - 1 ? 2ull : 1ull);
+}
+
+template <class V> G19v<V> g19v_of(const V *v, const Grid19 &g, int n)
+{
+    G19v<V> o;
+    o.v = v;
+    o.n = n;
+    o.nx = g.nx; o.ny = g.ny; o.nz = g.nz;
+    o.mhx = mul_inverse((unsigned)g.nx >> 1);
+    o.mny = mul_inverse((unsigned)g.ny);
+    const long nx = g.nx, nxy = (long)g.nx * g.ny;
+    for (int par = 0; par < 2; par++)
+        for (int q = 0; q < kQ19; q++) {
+            const long off = q19x(q) + q19y(q) * nx + q19z(q) * nxy;
+            const long y = par + off;
+            o.dq[par][q] = (int)(y >= 0 ? y / 2 : -((-y + 1) / 2));  // floor(y / 2)
+        }
+    return o;
+}
+
 template <class V> G19v<V> g19v(const Grid19 &g, int n);
-template <> G19v<double> g19v<double>(const Grid19 &g, int n) { return {g.v, n, g.nx, g.ny, g.nz}; }
-template <> G19v<float> g19v<float>(const Grid19 &g, int n) { return {g.v32, n, g.nx, g.ny, g.nz}; }
+template <> G19v<double> g19v<double>(const Grid19 &g, int n) { return g19v_of(g.v, g, n); }
+template <> G19v<float> g19v<float>(const Grid19 &g, int n) { return g19v_of(g.v32, g, n); }
 template <> G19v<__nv_bfloat16> g19v<__nv_bfloat16>(const Grid19 &g, int n)
 {
-    return {g.v16, n, g.nx, g.ny, g.nz};
+    return g19v_of(g.v16, g, n);
 }
 
 }  // namespace
