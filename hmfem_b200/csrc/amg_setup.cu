@@ -567,7 +567,7 @@ int run_union(UnionArgs A, Csr &out, int *dwork, cudaStream_t st)
 }  // namespace
 
 int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
-                const int *grid3)
+                const int *grid3, bool schur)
 {
     const int n = L.A.n;
     // ---- C/F split ----------------------------------------------------
@@ -653,7 +653,7 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
             C.g19.nz = grid3[2];
             C.g19.v = g19v;
         }
-        HM_CHECK(stencil_galerkin(grid3[0], grid3[1], grid3[2], L, C.A, g19v, st));
+        HM_CHECK(stencil_galerkin(grid3[0], grid3[1], grid3[2], L, C.A, g19v, st, schur));
         HM_PHASE("  P^T A P (stencil)", st);
         return HMFEM_OK;
     }

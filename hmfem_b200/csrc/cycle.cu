@@ -709,6 +709,7 @@ static Seed<T> seed_of(Solver &s, int l)
 {
     const int last = s.nlevels - 1;
     if (l >= last || l == s.direct_level || s.lv[l].gs) return {nullptr, nullptr, (T)0};
+    if (l == 0 && s.use_schur0()) return {nullptr, nullptr, (T)0};  // not smoothed
     // Chebyshev: the first direction d0 = (1/theta f) D^-1, kept in ub
     if (s.lv[l].cheb)
         return {s.vec_ub<T>(l), s.vec_dinv<T>(l), (T)cheb_coef(s.opt.cheb_degree).ith};
@@ -748,6 +749,15 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
     if (l == last) {
         launch_pdl(k_diag_solve<T>, nb(n), 256, st, n, s.vec_dtrue<T>(l), f, ua, ctl);
         HM_LAUNCHED();
+        return HMFEM_OK;
+    }
+    if (l == 0 && s.use_schur0()) {
+        // exact red-black reduction: coarse right-hand side, V-cycle on the
+        // Schur complement, F cells solved with its result
+        const T *d0 = s.vec_dtrue<T>(0);
+        HM_CHECK((g7_sred<T>(L, f, d0, s.vec_f<T>(1), seed_of<T>(s, 1), ctl, st)));
+        HM_CHECK(cycle_t<T>(s, 1, st, false, true));
+        HM_CHECK((g7_sprol<T>(L, f, d0, cycle_out<T>(s, 1), ub, ctl, st)));
         return HMFEM_OK;
     }
     const T w = (T)s.opt.omega;

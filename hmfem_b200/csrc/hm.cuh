@@ -157,13 +157,15 @@ int launch_spmv(const Sell &S, const double *x, double *y, cudaStream_t st);
 // split and Galerkin product then come from the 7-point structure
 // (rap_stencil.cu), bit-identical to the generic kernels.
 int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *err_dev,
-                const int *grid3 = nullptr);
+                const int *grid3 = nullptr, bool schur = false);
 int stencil_parity_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st);
 // level 1 of a parity split (nx even, nx, ny >= 4): its greedy C/F split
 // from the 19-offset structure, one launch per x-row wavefront
 int stencil19_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st);
+// schur: the exact red-black reduction's level 1 instead of the Galerkin
+// product with the averaging interpolation (same rows and columns)
 int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
-                     double *g19v, cudaStream_t st);
+                     double *g19v, cudaStream_t st, bool schur = false);
 // colouring + rows grouped by colour; returns HMFEM_OK with L.gs = false
 // when the level needs more than 63 colours
 int color_level(Level &L, cudaStream_t st, int *dwork);

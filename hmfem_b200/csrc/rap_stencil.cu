@@ -250,6 +250,68 @@ k_sg_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
     }
 }
 
+// Level 1 of the exact red-black reduction (hmfem_options.schur0): the
+// Schur complement S = A_CC - A_CF A_FF^-1 A_FC of the parity split, which
+// is P^T A P for the interpolation P_F = -A_FF^-1 A_FC, P_C = I (the F
+// equations solved exactly for given C values).  Same rows, columns and
+// slot layout as k_sg_fill.  Values, evaluated in this order without FMA
+// contraction: diagonal a_cc, minus (a_cf a_cf) / a_ff for each neighbour
+// f of c in row order d,l,r,u,t,b; slot q: minus the sum, in that order of
+// f and then of f's row order, of (a_cf a_fq) / a_ff over the F cells f
+// adjacent to both c and q.
+__global__ void __launch_bounds__(128)
+k_schur_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
+             const double *__restrict__ val, const int *__restrict__ cid,
+             const int *__restrict__ crow, int *ccol, double *cval, double *g19v)
+{
+    const long n = (long)((g.nx + 1) >> 1) * g.ny * g.nz;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+         t += (long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        if (!even_cell(g, t, i, j, k)) continue;
+        const long s = i + (long)j * g.nx + (long)k * g.nxy;
+        const unsigned pmc = present(g, i, j, k);
+        double out[19];
+        unsigned hv = 0;
+        double *acc = out;
+        double dsum = aval(rowptr, val, s, pmc, DC);
+        const int adir[6] = {DD, DL, DR, DU, DT, DB};
+#pragma unroll
+        for (int aa = 0; aa < 6; aa++) {
+            const int e = adir[aa];
+            if (!(pmc & (1u << e))) continue;
+            const double a_ce = aval(rowptr, val, s, pmc, e);
+            const long f = s + DX(e) + (long)DY(e) * g.nx + (long)DZ(e) * g.nxy;
+            const unsigned pmf = present(g, i + DX(e), j + DY(e), k + DZ(e));
+            const double a_ff = aval(rowptr, val, f, pmf, DC);
+            dsum = dsub(dsum, dmul(a_ce, a_ce) / a_ff);
+#pragma unroll
+            for (int b2 = 0; b2 < 7; b2++) {
+                if (b2 == DC || !(pmf & (1u << b2))) continue;
+                const int sl = slot_of(DX(e) + DX(b2), DY(e) + DY(b2), DZ(e) + DZ(b2));
+                if (sl <= 0) continue;  // back to c (its diagonal is above)
+                SG_ADD(sl, dmul(a_ce, aval(rowptr, val, f, pmf, b2)) / a_ff);
+            }
+        }
+        out[0] = dsum;
+        hv |= 1u;
+#pragma unroll
+        for (int sl = 1; sl < 19; sl++) out[sl] = -out[sl];
+        const unsigned in = in_grid(g, i, j, k);
+        const int c = cid[s];
+        const long o = crow[c];
+#pragma unroll
+        for (int sl = 0; sl < 19; sl++) {
+            const bool on = in & (1u << sl);
+            if (g19v) g19v[slice_at(c, q19_of(OX(sl), OY(sl), OZ(sl)), kQ19)] = on ? out[sl] : 0.0;
+            if (!on) continue;
+            const long e = o + __popc(in & tb.less[sl]);
+            ccol[e] = cid[s + tb.lin[sl]];
+            cval[e] = out[sl];
+        }
+    }
+}
+
 constexpr bool slots_consistent()
 {
     for (int t = 0; t < 19; t++)
@@ -394,7 +456,7 @@ int stencil_parity_split(int nx, int ny, int nz, signed char *sel, cudaStream_t 
 }
 
 int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
-                     double *g19v, cudaStream_t st)
+                     double *g19v, cudaStream_t st, bool schur)
 {
     SG g{nx, ny, nz, (long)nx * ny};
     const long n = g.nxy * nz;
@@ -407,9 +469,13 @@ int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
     out.col = (int *)dalloc(sizeof(int) * (out.nnz > 0 ? out.nnz : 1));
     out.val = (double *)dalloc(sizeof(double) * (out.nnz > 0 ? out.nnz : 1));
     if (!out.col || !out.val) return HMFEM_E_CUDA;
-    k_sg_fill<<<nbk(n / 2), 128, 0, st>>>(g, slot_table(g), L.A.rowptr, L.A.val, L.pw,
-                                          L.cid, out.rowptr, out.col, out.val, g19v,
-                                          (long)L.nc);
+    if (schur)
+        k_schur_fill<<<nbk(n / 2), 128, 0, st>>>(g, slot_table(g), L.A.rowptr, L.A.val,
+                                                 L.cid, out.rowptr, out.col, out.val, g19v);
+    else
+        k_sg_fill<<<nbk(n / 2), 128, 0, st>>>(g, slot_table(g), L.A.rowptr, L.A.val, L.pw,
+                                              L.cid, out.rowptr, out.col, out.val, g19v,
+                                              (long)L.nc);
     HM_LAUNCHED();
     return HMFEM_OK;
 }

@@ -158,6 +158,7 @@ static void free_hierarchy(Solver &s, bool keep_l0)
     s.direct_level = -1;
     s.nlevels = s.lv.size();
     s.setup_done = false;
+    s.schur0_built = false;
 }
 
 static void free_vectors(Solver &s)
@@ -313,8 +314,10 @@ int setup(Solver &s)
         s.lv.emplace_back();
         const int grid3[3] = {s.nx, s.ny, s.nz};
         const bool stencil = l == 0 && s.have_grid && s.opt.generic_setup == 0;
+        const bool schur = stencil && s.opt.schur0 && s.opt.precision == 1;
         HM_CHECK(amg_coarsen(s.lv[l], s.lv[l + 1], st, s.dwork,
-                             stencil ? grid3 : nullptr));
+                             stencil ? grid3 : nullptr, schur));
+        if (schur) s.schur0_built = true;
         l++;
         long gold = gcnt;
         gcnt = s.lv[l].A.n;
@@ -326,6 +329,12 @@ int setup(Solver &s)
     const bool low = s.opt.precision == 1;
     if (s.have_grid && s.opt.generic_setup == 0)
         HM_CHECK(g7_build(s.lv[0], s.nx, s.ny, s.nz, low, st, s.dwork));
+    if (s.schur0_built && !s.use_g7(0)) {
+        // the reduction needs the stencil form of level 0 (a bitwise
+        // symmetric 7-point matrix, which hmfem_assemble always produces)
+        set_last_error("schur0: level 0 has no 7-point stencil form", __FILE__, __LINE__);
+        return HMFEM_E_ARG;
+    }
     // Chebyshev levels: cheb_from and below, above the coarsest
     for (int k = 0; k < s.nlevels; k++)
         s.lv[k].cheb = s.opt.cheb_from >= 1 && k >= s.opt.cheb_from && k < s.nlevels - 1;
@@ -538,6 +547,7 @@ void hmfem_default_options(hmfem_options *o)
     o->gs_fused = 0;
     o->cheb_from = 2;
     o->cheb_degree = 4;
+    o->schur0 = 0;
     o->verbose = 0;
 }
 

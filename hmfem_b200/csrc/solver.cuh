@@ -59,6 +59,10 @@ struct Solver {
     // structured solve-phase forms (stencil_cycle.cu), when setup built them
     bool use_g7(int l) const { return l == 0 && !lv.empty() && lv[0].g7.cf; }
     bool use_g19(int l) const { return l == 1 && (int)lv.size() > 1 && lv[1].g19.v; }
+    // level 1 is the Schur complement of level 0's red-black split
+    // (opt.schur0, FP32 cycle): level 0 is then reduced exactly
+    bool schur0_built = false;
+    bool use_schur0() const { return schur0_built && use_g7(0); }
     // level vectors; level 0 of the FP64 cycle works on the CG's r and z
     template <class T> T *vec_f(int l);
     template <class T> T *vec_ua(int l);
@@ -103,6 +107,14 @@ int g7_restrict(const Level &L, const T *rs, T *fc, Seed<T> sd, const Ctl *ctl,
                 cudaStream_t st);
 template <class T>
 int g7_prolong(const Level &L, const T *uc, T *u, const Ctl *ctl, cudaStream_t st);
+// the exact red-black reduction of level 0 (schur0): coarse right-hand side
+// from f, and the level-0 result from the coarse one
+template <class T>
+int g7_sred(const Level &L, const T *f, const T *dinv, T *fc, Seed<T> sd, const Ctl *ctl,
+            cudaStream_t st);
+template <class T>
+int g7_sprol(const Level &L, const T *f, const T *dinv, const T *uc, T *z, const Ctl *ctl,
+             cudaStream_t st);
 template <class T, class V, bool DOT>
 int g7_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo, Ctl *ctl,
              double *part, int first, cudaStream_t st);

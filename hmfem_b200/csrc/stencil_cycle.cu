@@ -263,6 +263,130 @@ k_g7_prolong2(int nx, int ny, int nz, const T *__restrict__ uc, T *__restrict__ 
     }
 }
 
+// ---- level 0, exact red-black reduction (hmfem_options.schur0) -----------
+//
+// With the interpolation P_F = -A_FF^-1 A_FC (level 1 = the Schur
+// complement, k_schur_fill) level 0 needs no smoothing: the F equations are
+// solved exactly.  Restriction: u0 = A_FF^-1 f on F cells, 0 on C cells,
+// leaves a residual that is zero on F cells, so the coarse right-hand side
+// is f_c - sum over c's neighbours f of a_cf f_f / a_ff.  Prolongation: C
+// cells take the coarse value, F cells solve their equation with it,
+// (f_f - sum over f's neighbours c of a_fc u_c) / a_ff.  Neighbours in row
+// order d, l, r, u, t, b; the coupling a_{s,s+e} comes from the stencil form
+// (the +x/+y/+z entry of the lower cell).
+template <class T, class V>
+__device__ __forceinline__ T g7_coupling(const G7v<V> &g, long s, long nx, long nxy, int e)
+{
+    // e: 0 d, 1 l, 2 r, 3 u, 4 t, 5 b
+    switch (e) {
+    case 0: return (T)ld(g.cf, slice_at(s - nx, 2, 4));
+    case 1: return (T)ld(g.cf, slice_at(s - 1, 1, 4));
+    case 2: return (T)ld(g.cf, slice_at(s, 1, 4));
+    case 3: return (T)ld(g.cf, slice_at(s, 2, 4));
+    case 4: return (T)ld(g.cf, slice_at(s, 3, 4));
+    default: return (T)ld(g.cf, slice_at(s - nxy, 3, 4));
+    }
+}
+
+// fc[c] = f_s - sum_f a_sf (f_f dinv_f) over the C cells s (coarse id cid[s],
+// or s >> 1 for nx even)
+template <class T, class V>
+__global__ void __launch_bounds__(256)
+k_g7_sred(G7v<V> g, const T *__restrict__ f, const T *__restrict__ dinv,
+          const int *__restrict__ cid, T *__restrict__ fc, Seed<T> sd, const Ctl *ctl)
+{
+    PDL_ENTRY();
+    if (finished(ctl)) return;
+    using A = Ar<T>;
+    const unsigned hx = (unsigned)(g.nx + 1) >> 1;
+    const long nx = g.nx, nxy = (long)g.nx * g.ny, m = (long)hx * g.ny * g.nz;
+    GRID_STRIDE(t, m) {
+        const unsigned tu = (unsigned)t, r = tu / hx, kk0 = r / (unsigned)g.ny;
+        const int j = (int)(r - kk0 * (unsigned)g.ny), k = (int)kk0;
+        const int i = 2 * (int)(tu - r * hx) + ((j + k) & 1);
+        if (i >= g.nx) continue;
+        const long s = i + (long)r * nx;
+        const bool h[6] = {j > 0, i > 0, i < g.nx - 1, j < g.ny - 1, k < g.nz - 1, k > 0};
+        const long o[6] = {-nx, -1, 1, nx, nxy, -nxy};
+        T a[6], v[6];
+#pragma unroll
+        for (int e = 0; e < 6; e++) {
+            a[e] = h[e] ? g7_coupling<T>(g, s, nx, nxy, e) : (T)0;
+            v[e] = h[e] ? A::mul(f[s + o[e]], dinv[s + o[e]]) : (T)0;
+        }
+        T acc = f[s];
+#pragma unroll
+        for (int e = 0; e < 6; e++)
+            if (h[e]) acc = A::sub(acc, A::mul(a[e], v[e]));
+        const int c = cid ? cid[s] : (int)(s >> 1);
+        fc[c] = acc;
+        sd.put(c, acc);
+    }
+}
+
+// z on one F cell: (f_s - sum_c a_sc uc[c]) dinv_s
+template <class T, class V, class CI>
+__device__ __forceinline__ T g7_fsolve(const G7v<V> &g, long s, int i, int j, int k,
+                                       const T *__restrict__ f, const T *__restrict__ dinv,
+                                       const T *__restrict__ uc, CI coarse_id)
+{
+    using A = Ar<T>;
+    const long nx = g.nx, nxy = (long)g.nx * g.ny;
+    const bool h[6] = {j > 0, i > 0, i < g.nx - 1, j < g.ny - 1, k < g.nz - 1, k > 0};
+    const long o[6] = {-nx, -1, 1, nx, nxy, -nxy};
+    T a[6], v[6];
+#pragma unroll
+    for (int e = 0; e < 6; e++) {
+        a[e] = h[e] ? g7_coupling<T>(g, s, nx, nxy, e) : (T)0;
+        v[e] = h[e] ? uc[coarse_id(s + o[e])] : (T)0;
+    }
+    T acc = f[s];
+#pragma unroll
+    for (int e = 0; e < 6; e++)
+        if (h[e]) acc = A::sub(acc, A::mul(a[e], v[e]));
+    return A::mul(acc, dinv[s]);
+}
+
+// nx even: a thread per x-neighbour pair (one C cell, one F cell), coarse
+// ids s >> 1
+template <class T, class V>
+__global__ void __launch_bounds__(256)
+k_g7_sprol2(G7v<V> g, const T *__restrict__ f, const T *__restrict__ dinv,
+            const T *__restrict__ uc, T *__restrict__ z, const Ctl *ctl)
+{
+    PDL_ENTRY();
+    if (finished(ctl)) return;
+    const long npair = (long)g.nx * g.ny * g.nz / 2;
+    GRID_STRIDE(t, npair) {
+        const long s0 = 2 * t;
+        int i0, j, k;
+        cell_ijk((unsigned)s0, g.nx, g.ny, i0, j, k);
+        const bool c_first = ((j + k) & 1) == 0;
+        const long sc = c_first ? s0 : s0 + 1, sf = c_first ? s0 + 1 : s0;
+        const int fi = c_first ? i0 + 1 : i0;
+        z[sc] = uc[sc >> 1];
+        z[sf] = g7_fsolve<T>(g, sf, fi, j, k, f, dinv, uc, [](long q) { return q >> 1; });
+    }
+}
+
+// any nx: a thread per cell, coarse ids from cid
+template <class T, class V>
+__global__ void __launch_bounds__(256)
+k_g7_sprol(G7v<V> g, const T *__restrict__ f, const T *__restrict__ dinv,
+           const int *__restrict__ cid, const T *__restrict__ uc, T *__restrict__ z,
+           const Ctl *ctl)
+{
+    PDL_ENTRY();
+    if (finished(ctl)) return;
+    const long n = (long)g.nx * g.ny * g.nz;
+    GRID_STRIDE(s, n) {
+        int i, j, k;
+        cell_ijk((unsigned)s, g.nx, g.ny, i, j, k);
+        if (((i + j + k) & 1) == 0) z[s] = uc[cid[s]];
+        else z[s] = g7_fsolve<T>(g, s, i, j, k, f, dinv, uc, [&](long q) { return cid[q]; });
+    }
+}
+
 // v = f - A u;  u_out = u + w v D^-1;  optionally sigma = (u_out, f)
 template <class T, class V, bool DOT>
 __global__ void __launch_bounds__(256)
@@ -580,6 +704,39 @@ int g7_restrict(const Level &L, const T *rs, T *fc, Seed<T> sd, const Ctl *ctl,
 }
 
 template <class T>
+int g7_sred(const Level &L, const T *f, const T *dinv, T *fc, Seed<T> sd, const Ctl *ctl,
+            cudaStream_t st)
+{
+    const Grid7 &g = L.g7;
+    const long m = (long)((g.nx + 1) >> 1) * g.ny * g.nz;
+    const G7v<T> gv = g7v<T>(g);
+    const int nblk = occ_blocks((const void *)k_g7_sred<T, T>, m, 256, kRedBlocks);
+    const int *cid = g.nx % 2 ? L.cid : nullptr;
+    launch_pdl(k_g7_sred<T, T>, nblk, 256, st, gv, f, dinv, cid, fc, sd, ctl);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+template <class T>
+int g7_sprol(const Level &L, const T *f, const T *dinv, const T *uc, T *z, const Ctl *ctl,
+             cudaStream_t st)
+{
+    const Grid7 &g = L.g7;
+    const G7v<T> gv = g7v<T>(g);
+    if (g.nx % 2 == 0) {
+        const long npair = (long)L.A.n / 2;
+        const int nblk = occ_blocks((const void *)k_g7_sprol2<T, T>, npair, 256, kRedBlocks);
+        launch_pdl(k_g7_sprol2<T, T>, nblk, 256, st, gv, f, dinv, uc, z, ctl);
+        HM_LAUNCHED();
+        return HMFEM_OK;
+    }
+    const int nblk = occ_blocks((const void *)k_g7_sprol<T, T>, L.A.n, 256, kRedBlocks);
+    launch_pdl(k_g7_sprol<T, T>, nblk, 256, st, gv, f, dinv, (const int *)L.cid, uc, z, ctl);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+template <class T>
 int g7_prolong(const Level &L, const T *uc, T *u, const Ctl *ctl, cudaStream_t st)
 {
     const Grid7 &g = L.g7;
@@ -680,6 +837,14 @@ template int g7_prolong<double>(const Level &, const double *, double *, const C
                                 cudaStream_t);
 template int g7_prolong<float>(const Level &, const float *, float *, const Ctl *,
                                cudaStream_t);
+template int g7_sred<float>(const Level &, const float *, const float *, float *,
+                            Seed<float>, const Ctl *, cudaStream_t);
+template int g7_sprol<float>(const Level &, const float *, const float *, const float *,
+                             float *, const Ctl *, cudaStream_t);
+template int g7_sred<double>(const Level &, const double *, const double *, double *,
+                             Seed<double>, const Ctl *, cudaStream_t);
+template int g7_sprol<double>(const Level &, const double *, const double *,
+                              const double *, double *, const Ctl *, cudaStream_t);
 template int g7_post<double, double, true>(const Level &, const double *, const double *,
                                            double, const double *, double *, Ctl *,
                                            double *, int, cudaStream_t);

@@ -53,7 +53,7 @@ class Options(C.Structure):
                 ("check_every", C.c_int), ("generic_setup", C.c_int),
                 ("gs_fused", C.c_int), ("cheb_from", C.c_int),
                 ("cheb_degree", C.c_int), ("reuse_setup", C.c_int),
-                ("verbose", C.c_int)]
+                ("schur0", C.c_int), ("verbose", C.c_int)]
 
 
 class Stats(C.Structure):

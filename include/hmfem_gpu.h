@@ -139,6 +139,15 @@ typedef struct {
                           the AMG setup on an unchanged matrix (main.c:
                           457-514).  Default 0; compute / solve_linsys set
                           it. */
+    int schur0;        /* 1 (with precision 1 on an assembled grid): level 1
+                          is the Schur complement A_CC - A_CF A_FF^-1 A_FC
+                          of level 0's red-black split instead of the
+                          Galerkin product with the reference's averaging
+                          interpolation (same rows and columns, so every
+                          coarser level keeps the reference's structure),
+                          and the V-cycle reduces level 0 exactly: no
+                          level-0 smoothing, one restriction and one
+                          prolongation pass.  Default 0. */
     int verbose;
 } hmfem_options;
 

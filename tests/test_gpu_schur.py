@@ -1,0 +1,92 @@
+"""The exact red-black reduction of level 0 (hmfem_options.schur0) on the
+GPU: level 1 bit-exact with the restatement (oracle/schur.py), the
+reference's structure on every level, an exact preconditioner when level 1
+is solved exactly, and solves that land on the FP64 oracle's pressure."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from hmfem_b200 import gpu
+from hmfem_b200.problem import config_problem, make_problem
+from oracle import schur as S
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "mixed_8x6x5": lambda: make_problem(8, 6, 5, log10k=(-14.0, 1.0, 1.5), n_conduits=1, seed=4,
+                                        bc_type=(0, 1, 0, 1, 0, 1),
+                                        bc_value=(1.0, 0.5, 0.0, 0.0, 0.2, 0.0)),
+    "odd_7x6x5": lambda: make_problem(7, 6, 5, log10k=(-14.0, 1.0, 1.5), seed=9),
+    "config1_24": lambda: config_problem(1, size=24),
+    "config2_32": lambda: config_problem(2, size=32),
+}
+
+
+def _solver(**kw):
+    return gpu.Solver(precision=1, schur0=1, **kw)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_level1_is_the_schur_complement_bit_exact(name, port):
+    p = CASES[name]()
+    perm, ind, b = port.assemble(p)
+    s = _solver()
+    s.assemble(p)
+    s.setup()
+    L1 = s.level(1)
+    cnt, col, ele = S.schur_level1(perm, p.nx, p.ny, p.nz)
+    assert np.array_equal(L1["cnt"], cnt) and np.array_equal(L1["col"], col)
+    assert np.array_equal(L1["ele"], ele)
+    # every level keeps the reference's structure
+    r = gpu.Solver(precision=1)
+    r.assemble(p)
+    r.setup()
+    assert s.num_levels() == r.num_levels()
+    for l in range(s.num_levels()):
+        a, c = s.level(l), r.level(l)
+        for key in ("cnt", "col", "sel", "pcnt", "pcol"):
+            assert np.array_equal(a[key], c[key]), (l, key)
+    s.close()
+    r.close()
+
+
+def test_exact_when_level1_is_solved_exactly(port):
+    """8^3 with the dense direct solve from 300 rows down: level 1 (256
+    rows) is solved exactly, so one cycle is A^-1 (to the cycle's rounding)
+    and the flexible CG needs two steps."""
+    p = make_problem(8, 8, 8, log10k=(-14.0, 1.0, 1.0), seed=2)
+    perm, ind, b = port.assemble(p)
+    cnt, col, ele = port.pack(perm, ind)
+    ptr = np.zeros(p.n + 1, np.int64)
+    ptr[1:] = np.cumsum(cnt)
+    A = sp.csr_matrix((ele, col, ptr), shape=(p.n, p.n)).toarray()
+    s = _solver(tol=1e-10, coarse_direct=300)
+    s.assemble(p)
+    s.setup()
+    f = np.random.default_rng(0).standard_normal(p.n)
+    u = s.vcycle(f)  # the FP64 cycle
+    want = np.linalg.solve(A, f)
+    assert np.linalg.norm(u - want) <= 1e-10 * np.linalg.norm(want)
+    x, st = s.solve()
+    assert st["status"] == 0 and st["iterations"] <= 2, st
+    s.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_solve_matches_oracle(name, port):
+    p = CASES[name]()
+    perm, ind, b = port.assemble(p)
+    cnt, col, ele = port.pack(perm, ind)
+    H = port.amg(cnt, col, ele)
+    xo, _, _ = H.pcg(b, eps=1e-12, stop=1)
+    its = {}
+    for schur in (0, 1):
+        s = gpu.Solver(precision=1, schur0=schur, tol=1e-12, bf16_from=1)
+        s.assemble(p)
+        s.setup()
+        x, st = s.solve()
+        s.close()
+        assert st["status"] == 0 and st["relres"] <= 1e-12
+        assert np.linalg.norm(x - xo) <= 1e-9 * np.linalg.norm(xo)
+        its[schur] = st["iterations"]
+    assert its[1] <= its[0], its
