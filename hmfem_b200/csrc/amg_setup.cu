@@ -617,13 +617,17 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
     L.R.nnz = L.P.nnz;
     L.R.rowptr = (int *)dalloc(sizeof(int) * (L.nc + 1));
     L.R.col = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
-    int *keys_out = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
-    HM_CUDA(cudaMemsetAsync(L.R.rowptr, 0, sizeof(int) * (L.nc + 1), st));
-    k_hist<<<nblk(L.P.nnz, 256), 256, 0, st>>>(L.P.col, L.P.nnz, L.R.rowptr);
-    HM_LAUNCHED();
-    long rn = 0;
-    HM_CHECK(rowptr_from_counts(L.R.rowptr, L.nc, st, &rn));
-    {
+    if (grid3) {
+        dfree(pown);
+        HM_CHECK(stencil_parity_R(grid3[0], grid3[1], grid3[2], L.cid, L.nc, L.R, st));
+        HM_PHASE("  P and R", st);
+    } else {
+        int *keys_out = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
+        HM_CUDA(cudaMemsetAsync(L.R.rowptr, 0, sizeof(int) * (L.nc + 1), st));
+        k_hist<<<nblk(L.P.nnz, 256), 256, 0, st>>>(L.P.col, L.P.nnz, L.R.rowptr);
+        HM_LAUNCHED();
+        long rn = 0;
+        HM_CHECK(rowptr_from_counts(L.R.rowptr, L.nc, st, &rn));
         size_t tmp = 0;
         int bits = 1;
         while ((1l << bits) < (long)L.nc + 1) bits++;
@@ -636,10 +640,10 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
                                                 st));
         HM_CUDA(cudaStreamSynchronize(st));
         dfree(t);
+        dfree(keys_out);
+        dfree(pown);
+        HM_PHASE("  P and R", st);
     }
-    dfree(keys_out);
-    dfree(pown);
-    HM_PHASE("  P and R", st);
     // ---- Galerkin product ---------------------------------------------
     if (grid3) {
         double *g19v = nullptr;

@@ -159,6 +159,9 @@ int launch_spmv(const Sell &S, const double *x, double *y, cudaStream_t st);
 int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *err_dev,
                 const int *grid3 = nullptr, bool schur = false);
 int stencil_parity_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st);
+// R = P^T of the parity split (rowptr / col allocated by the caller, R.nnz
+// set to P's nnz)
+int stencil_parity_R(int nx, int ny, int nz, const int *cid, int nc, Csr &R, cudaStream_t st);
 // level 1 of a parity split (nx even, nx, ny >= 4): its greedy C/F split
 // from the 19-offset structure, one launch per x-row wavefront
 int stencil19_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st);

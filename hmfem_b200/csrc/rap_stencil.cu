@@ -312,6 +312,41 @@ k_schur_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
     }
 }
 
+// R = P^T of the parity split in closed form: coarse row c (C cell s) holds
+// s and its in-grid neighbours (all F, all interpolating from s), fine rows
+// ascending -- what the stable sort of P's coarse ids gives.
+__global__ void k_parity_rcount(SG g, const int *__restrict__ cid, int *cnt)
+{
+    const long n = (long)((g.nx + 1) >> 1) * g.ny * g.nz;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+         t += (long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        if (!even_cell(g, t, i, j, k)) continue;
+        cnt[cid[i + (long)j * g.nx + (long)k * g.nxy]] = __popc(present(g, i, j, k));
+    }
+}
+
+__global__ void k_parity_rfill(SG g, const int *__restrict__ cid,
+                               const int *__restrict__ rrow, int *rcol)
+{
+    const long n = (long)((g.nx + 1) >> 1) * g.ny * g.nz;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+         t += (long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        if (!even_cell(g, t, i, j, k)) continue;
+        const long s = i + (long)j * g.nx + (long)k * g.nxy;
+        const unsigned pm = present(g, i, j, k);
+        long o = rrow[cid[s]];
+        // ascending fine index: b, d, l, c, r, u, t
+        const int order[7] = {DB, DD, DL, DC, DR, DU, DT};
+#pragma unroll
+        for (int q = 0; q < 7; q++) {
+            const int d = order[q];
+            if (pm & (1u << d)) rcol[o++] = (int)(s + DX(d) + (long)DY(d) * g.nx + (long)DZ(d) * g.nxy);
+        }
+    }
+}
+
 constexpr bool slots_consistent()
 {
     for (int t = 0; t < 19; t++)
@@ -476,6 +511,25 @@ int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
         k_sg_fill<<<nbk(n / 2), 128, 0, st>>>(g, slot_table(g), L.A.rowptr, L.A.val, L.pw,
                                               L.cid, out.rowptr, out.col, out.val, g19v,
                                               (long)L.nc);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+int stencil_parity_R(int nx, int ny, int nz, const int *cid, int nc, Csr &R, cudaStream_t st)
+{
+    SG g{nx, ny, nz, (long)nx * ny};
+    const long n = g.nxy * nz;
+    R.n = nc;
+    HM_CUDA(cudaMemsetAsync(R.rowptr, 0, sizeof(int) * ((long)nc + 1), st));
+    k_parity_rcount<<<nbk(n / 2), 256, 0, st>>>(g, cid, R.rowptr);
+    HM_LAUNCHED();
+    long nnz = 0;
+    HM_CHECK(rowptr_from_counts(R.rowptr, nc, st, &nnz));
+    if (nnz != R.nnz) {
+        set_last_error("parity split: R size differs from P", __FILE__, __LINE__);
+        return HMFEM_E_CAPACITY;
+    }
+    k_parity_rfill<<<nbk(n / 2), 256, 0, st>>>(g, cid, R.rowptr, R.col);
     HM_LAUNCHED();
     return HMFEM_OK;
 }

@@ -11,9 +11,9 @@
 // format strings: conversions are exact (the decimal digits of the binary
 // value, rounded half to even, from 128-bit integer arithmetic), so the
 // files are identical to the reference's.  A value the exact path does not
-// cover (NaN, infinity, or a magnitude outside the 128-bit range: for
-// %1.9e below ~1e-18 or above ~1e36) sends its line to the host, which
-// formats it with snprintf and the same format string.
+// cover (NaN, infinity, or a magnitude outside the exact range: for %1.9e
+// below ~1e-77 or above ~1e36) sends its line to the host, which formats it
+// with snprintf and the same format string.
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -40,6 +40,96 @@ __constant__ unsigned long long c_pow5[28] = {
     2384185791015625ull, 11920928955078125ull, 59604644775390625ull,
     298023223876953125ull, 1490116119384765625ull, 7450580596923828125ull};
 
+// 5^b, b = 0..86, as four little-endian 64-bit words (5^86 < 2^200)
+__constant__ unsigned long long c_pow5w[87][4] = {
+    {0x0000000000000001ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x0000000000000005ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x0000000000000019ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x000000000000007dull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x0000000000000271ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x0000000000000c35ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x0000000000003d09ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x000000000001312dull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x000000000005f5e1ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x00000000001dcd65ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x00000000009502f9ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x0000000002e90eddull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x000000000e8d4a51ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x0000000048c27395ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x000000016bcc41e9ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x000000071afd498dull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x0000002386f26fc1ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x000000b1a2bc2ec5ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x000003782dace9d9ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x00001158e460913dull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x000056bc75e2d631ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x0001b1ae4d6e2ef5ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x000878678326eac9ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x002a5a058fc295edull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x00d3c21bcecceda1ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x0422ca8b0a00a425ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x14adf4b7320334b9ull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x6765c793fa10079dull, 0x0000000000000000ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x04fce5e3e2502611ull, 0x0000000000000002ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x18f07d736b90be55ull, 0x000000000000000aull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x7cb2734119d3b7a9ull, 0x0000000000000032ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x6f7c40458122964dull, 0x00000000000000fcull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x2d6d415b85acef81ull, 0x00000000000004eeull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xe32246c99c60ad85ull, 0x00000000000018a6ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x6fab61f00de36399ull, 0x0000000000007b42ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x2e58e9b04570f1fdull, 0x000000000002684cull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xe7bc90715b34b9f1ull, 0x00000000000c097cull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x86aed236c807a1b5ull, 0x00000000003c2f70ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xa16a1b11e8262889ull, 0x00000000012ced32ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x2712875988becaadull, 0x0000000005e0a1fdull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xc35ca4bfabb9f561ull, 0x000000001d6329f1ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xd0cf37be5aa1cae5ull, 0x0000000092efd1b8ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x140c16b7c528f679ull, 0x00000002deaf189cull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x643c7196d9ccd05dull, 0x0000000e596b7b0cull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xf52e37f2410011d1ull, 0x00000047bf19673dull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xc9e717bb45005915ull, 0x00000166bb7f0435ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xf18376a85901bd69ull, 0x00000701a97b150cull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xb7915149bd08b30dull, 0x000023084f676940ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x95d69670b12b7f41ull, 0x0000af298d050e43ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xed30f03375d97c45ull, 0x00036bcfc1194751ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xa1f4b1014d3f6d59ull, 0x00111b0ec57e6499ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x29c77506823d22bdull, 0x00558749db77f700ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xd0e549208b31adb1ull, 0x01aba4714957d300ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x147a6da2b7f86475ull, 0x085a36366eb71f04ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0x6664242d97d9f649ull, 0x29c30f1029939b14ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xfff4b4e3f741cf6dull, 0xd0cf4b50cfe20765ull, 0x0000000000000000ull, 0x0000000000000000ull},
+    {0xffc78873d4490d21ull, 0x140c78940f6a24fdull, 0x0000000000000004ull, 0x0000000000000000ull},
+    {0xfee5aa43256d41a5ull, 0x643e5ae44d12b8f5ull, 0x0000000000000014ull, 0x0000000000000000ull},
+    {0xfa7c534fbb224839ull, 0xf537c675815d9ccdull, 0x0000000000000065ull, 0x0000000000000000ull},
+    {0xe46da08ea7ab691dull, 0xca16e04b86d41005ull, 0x00000000000001fdull, 0x0000000000000000ull},
+    {0x762422c946590d91ull, 0xf2726179a224501dull, 0x00000000000009f4ull, 0x0000000000000000ull},
+    {0x4eb4adee5fbd43d5ull, 0xbc3be7602ab59093ull, 0x00000000000031c8ull, 0x0000000000000000ull},
+    {0x898765a7deb25329ull, 0xad2b84e0d58bd2e0ull, 0x000000000000f8ebull, 0x0000000000000000ull},
+    {0xafa4fc47597b9fcdull, 0x61d998642bbb1e62ull, 0x000000000004dc9aull, 0x0000000000000000ull},
+    {0x6e38ed64bf6a1f01ull, 0xe93ff9f4daa797edull, 0x0000000000184f03ull, 0x0000000000000000ull},
+    {0x271ca2f7bd129b05ull, 0x8e3fe1c84545f7a3ull, 0x0000000000798b13ull, 0x0000000000000000ull},
+    {0xc38f2ed6b15d0719ull, 0xc73f68e95a5dd62full, 0x00000000025fb761ull, 0x0000000000000000ull},
+    {0xd1cbea3176d1237dull, 0xe43d0c8ec3d52eeeull, 0x000000000bde94e8ull, 0x0000000000000000ull},
+    {0x18fb92f75215b171ull, 0x75313ec9d329eaaaull, 0x000000003b58e88cull, 0x0000000000000000ull},
+    {0x7ce9ded49a6c7735ull, 0x49f639f11fd19552ull, 0x0000000128bc8abeull, 0x0000000000000000ull},
+    {0x70915a27041e5409ull, 0x71cf21b59f17ea9cull, 0x00000005cbaeb5b7ull, 0x0000000000000000ull},
+    {0x32d6c2c31497a42dull, 0x390ba88c1b77950eull, 0x0000001cfa698c95ull, 0x0000000000000000ull},
+    {0xfe31cdcf66f634e1ull, 0x1d3a4abc8955e946ull, 0x00000090e40fbeeaull, 0x0000000000000000ull},
+    {0xf6f9050d02cf0865ull, 0x922375aeaead8e62ull, 0x000002d4744eba92ull, 0x0000000000000000ull},
+    {0xd2dd19410e0b29f9ull, 0xdab14c696963c7eeull, 0x00000e264589a4dcull, 0x0000000000000000ull},
+    {0x1e517e454637d1ddull, 0x45767e0f0ef2e7aaull, 0x000046bf5bb03850ull, 0x0000000000000000ull},
+    {0x9797775a5f171951ull, 0x5b50764b4abe8652ull, 0x000161bcca711991ull, 0x0000000000000000ull},
+    {0xf5f554c3db737e95ull, 0xc8924f7875b89f9cull, 0x0006e8aff4357fd6ull, 0x0000000000000000ull},
+    {0xcdcaa7d3494178e9ull, 0xeadb8d5a4c9b1e10ull, 0x00228b6fc50b7f31ull, 0x0000000000000000ull},
+    {0x04f547206e475c8dull, 0x9649c2c37f079654ull, 0x00acb92ed9397bf9ull, 0x0000000000000000ull},
+    {0x18ca63a22764cec1ull, 0xef70cdd17b25efa4ull, 0x035f9dea3e1f6bdfull, 0x0000000000000000ull},
+    {0x7bf3f22ac4f809c5ull, 0xad34051767bdae34ull, 0x10de1593369d1b5full, 0x0000000000000000ull},
+    {0x6bc3bad5d8d830d9ull, 0x6204197506b46706ull, 0x54566be0111188deull, 0x0000000000000000ull},
+    {0x1ad2a62d3c38f43dull, 0xea147f4921860320ull, 0xa5b01b605557ac57ull, 0x0000000000000001ull},
+    {0x861d3ee22d1cc531ull, 0x92667c6da79e0fa0ull, 0x3c7088e1aab65db7ull, 0x0000000000000008ull},
+    {0x9e923a6ae18fd9f5ull, 0xdc006e2446164e22ull, 0x2e32ac68558fd495ull, 0x0000000000000029ull},
+    {0x18db241667cf41c9ull, 0x4c0226b55e6f86adull, 0xe6fd5e09abcf26edull, 0x00000000000000cdull}};
+
 __constant__ unsigned long long c_pow10[20] = {
     1ull, 10ull, 100ull, 1000ull, 10000ull, 100000ull, 1000000ull, 10000000ull,
     100000000ull, 1000000000ull, 10000000000ull, 100000000000ull,
@@ -55,6 +145,56 @@ __device__ __forceinline__ void decompose(double x, unsigned long long &m, int &
     const unsigned long long f = b & ((1ull << 52) - 1);
     if (be == 0) { m = f; e2 = -1074; }
     else { m = f | (1ull << 52); e2 = be - 1075; }
+}
+
+// The q < 0 branch for 27 < b = -q <= 86 (small magnitudes): N0 = m 5^b
+// held in four 64-bit words (< 2^253), then T = N0 >> sh with sh = -(e2 + b)
+// and the remainder compared with 2^(sh-1) bit by bit.
+__device__ bool wide_mul_pow5(unsigned long long m, int e2, int b, unsigned long long &T,
+                              int &cmp)
+{
+    if (b > 86) return false;
+    unsigned long long w[4];
+    u128 carry = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const u128 p = (u128)m * c_pow5w[b][k] + carry;
+        w[k] = (unsigned long long)p;
+        carry = p >> 64;
+    }
+    if (carry) return false;
+    const int c = e2 + b;
+    if (c >= 0) return false;  // a large value times 10^b: not reached for %e / %f here
+    const int sh = -c;
+    if (sh > 255) {  // the value is below 2^-2: T = 0, remainder below one half
+        T = 0;
+        cmp = -1;
+        return true;
+    }
+    // T = bits [sh, sh + 64); nothing may be set above them
+    auto bit = [&](int i) -> unsigned long long {
+        return i < 0 || i > 255 ? 0ull : (w[i >> 6] >> (i & 63)) & 1ull;
+    };
+    auto word_at = [&](int i) -> unsigned long long {  // bits [i, i + 64)
+        const int q0 = i >> 6, r0 = i & 63;
+        unsigned long long lo = q0 < 4 ? w[q0] >> r0 : 0ull;
+        unsigned long long hi = (r0 && q0 + 1 < 4) ? w[q0 + 1] << (64 - r0) : 0ull;
+        return lo | hi;
+    };
+    for (int i = sh + 64; i < 256; i += 64)
+        if (word_at(i) != 0ull) return false;
+    T = word_at(sh);
+    // remainder = bits [0, sh): compare with 2^(sh-1)
+    bool low_nonzero = false;
+    for (int i = 0; i < sh - 1; i += 64) {
+        const int len = sh - 1 - i;
+        unsigned long long v = word_at(i);
+        if (len < 64) v &= (1ull << len) - 1;
+        if (v) { low_nonzero = true; break; }
+    }
+    const unsigned long long top = bit(sh - 1);
+    cmp = top ? (low_nonzero ? 1 : 0) : (low_nonzero ? -1 : -2);
+    return true;
 }
 
 // T = floor(m 2^e2 / 10^q) and where the remainder lies: -2 zero, -1 below
@@ -83,7 +223,7 @@ __device__ bool div_pow10(unsigned long long m, int e2, int q, unsigned long lon
         return true;
     }
     const int b = -q;
-    if (b > 27) return false;
+    if (b > 27) return wide_mul_pow5(m, e2, b, T, cmp);
     const u128 N0 = (u128)m * c_pow5[b];  // < 2^116
     const int c = e2 + b;
     if (c >= 0) {

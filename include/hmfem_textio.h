@@ -8,7 +8,7 @@
  * instead of one fprintf per number.  Arrays are host (mem = 0) or device
  * (mem = 1) pointers; grid cell s = i + nx (j + ny k) as everywhere in this
  * library.  Lines holding a value outside the device's exact range (NaN,
- * infinity, or a magnitude beyond ~1e-18 .. 1e36 for %1.9e) are formatted
+ * infinity, or a magnitude beyond ~1e-77 .. 1e36 for %1.9e) are formatted
  * by the host C library with the same format string.  Return HMFEM_OK,
  * HMFEM_E_ARG (bad argument, file not writable) or HMFEM_E_CUDA.
  */

@@ -131,6 +131,9 @@ def adversarial_values(seed=1):
             vals.append(kk / 2.0 ** q)
             vals.append(-kk / 2.0 ** q)
     vals += [1234567890.5, 1234567891.5, 0.0078125, 0.0234375, 0.03125, 0.09375]
+    # the edge of the device's 256-bit range for tiny magnitudes (5^86)
+    for e in range(-90, -40):
+        vals += [1.2345678905 * 10.0 ** e, -7.0 * 10.0 ** e, 2.0 ** (3.32 * e)]
     x = rng.standard_normal(20000) * 10.0 ** rng.integers(-25, 40, 20000)
     return np.concatenate([np.array(vals, dtype=np.float64), x])
 
