@@ -76,10 +76,11 @@ def solve_batch(problems, precision=1, tol=1e-10, workers=4, options=None):
 
 
 def tune_workers(sample, precision=1, tol=1e-10, candidates=(1, 2, 4, 8, 12),
-                 cache=_CACHE, refresh=False):
+                 cache=_CACHE, refresh=False, options=None):
     """Worker count with the highest instance throughput on `sample`
-    (warmed up once), remembered per GPU model and precision in `cache`."""
-    key = _gpu_key(precision)
+    (warmed up once), remembered per GPU model, precision and options in
+    `cache`."""
+    key = _gpu_key(precision) + "".join(f"|{k}={v}" for k, v in sorted((options or {}).items()))
     table = {}
     if cache and os.path.exists(cache):
         try:
@@ -89,11 +90,11 @@ def tune_workers(sample, precision=1, tol=1e-10, candidates=(1, 2, 4, 8, 12),
             table = {}
     if not refresh and key in table:
         return int(table[key]["workers"]), table[key]
-    solve_batch(sample[:2], precision, tol, workers=2)  # warm-up
+    solve_batch(sample[:2], precision, tol, workers=2, options=options)  # warm-up
     rates = {}
     for w in candidates:
         t0 = time.perf_counter()
-        solve_batch(sample, precision, tol, workers=w)
+        solve_batch(sample, precision, tol, workers=w, options=options)
         rates[w] = len(sample) / (time.perf_counter() - t0)
     best = max(rates, key=rates.get)
     entry = {"workers": best, "instances_per_s": rates, "sample": len(sample)}
