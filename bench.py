@@ -448,14 +448,15 @@ def coupled_case():
 
 def run_coupled(args, world, rank, reps=3):
     """The Picard loop of main.c:383-489 through hmfem_picard (host K, WI,
-    pw in; reservoir and conduit pressures out), FP64 V-cycle PCG to
+    pw in; reservoir and conduit pressures out), the chosen solver (FP32
+    V-cycle with the exact level-0 reduction in FP64 flexible CG) to
     ||r||/||b|| <= 1e-10 per reservoir solve, Picard tolerance 1e-8; wall
     clock per run (1 warm-up, median of `reps`), max over ranks."""
     import torch
 
     from hmfem_b200 import gpu, karst
     prob, k, WI, pw, rho = coupled_case()
-    s = gpu.Solver(precision=0, tol=1e-10, stop_rule=0)
+    s = gpu.Solver(precision=1, schur0=1, bf16_from=1, tol=1e-10, stop_rule=0)
     karst.picard(s, k, prob, WI, pw, rho=rho, fluxes=False)  # warm-up
     torch.cuda.synchronize()
     barrier(world)
