@@ -18,7 +18,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=default", "--expt-relaxed-constexpr",
          "--extended-lambda"]
-SOURCES = ["assemble.cu", "sparse.cu", "amg_setup.cu", "rap_stencil.cu", "stencil_cycle.cu", "smoother_setup.cu", "cycle.cu", "solver.cu",
+SOURCES = ["assemble.cu", "sparse.cu", "amg_setup.cu", "rap_stencil.cu", "rap19.cu", "stencil_cycle.cu", "smoother_setup.cu", "cycle.cu", "solver.cu",
            "device_abi.cu", "noalloc.cu", "conv3d.cu", "karst.cu", "textio.cu", "permio.cu"]
 
 

@@ -661,6 +661,14 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
         HM_PHASE("  P^T A P (stencil)", st);
         return HMFEM_OK;
     }
+    if (L.g19.nx > 0) {  // level 1 of a parity split: from its 19-offset structure
+        bool done = false;
+        HM_CHECK(galerkin19(L, C.A, st, &done));
+        if (done) {
+            HM_PHASE("  P^T A P (19-point)", st);
+            return HMFEM_OK;
+        }
+    }
     Csr AP;
     UnionArgs a0{};
     a0.nrows = n;

@@ -169,6 +169,10 @@ int stencil19_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st);
 // product with the averaging interpolation (same rows and columns)
 int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
                      double *g19v, cudaStream_t st, bool schur = false);
+// P^T A P of a level with the 19-offset structure (L.g19 set: level 1 of a
+// parity split) from that structure, bit-identical to the generic product;
+// *done false (and out untouched) when the level does not have it
+int galerkin19(const Level &L, Csr &out, cudaStream_t st, bool *done);
 // colouring + rows grouped by colour; returns HMFEM_OK with L.gs = false
 // when the level needs more than 63 colours
 int color_level(Level &L, cudaStream_t st, int *dwork);

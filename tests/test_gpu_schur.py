@@ -50,6 +50,31 @@ def test_level1_is_the_schur_complement_bit_exact(name, port):
     r.close()
 
 
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_levels_below_the_schur_level_bit_exact(name, port):
+    """Levels >= 2 are the reference's setup (split, P, Galerkin product)
+    applied to the Schur level 1, so the oracle's setup of that matrix gives
+    them bit for bit -- the product from the 19-offset structure (even nx)
+    and the generic one (odd nx) alike."""
+    p = CASES[name]()
+    perm, ind, b = port.assemble(p)
+    cnt, col, ele = S.schur_level1(perm, p.nx, p.ny, p.nz)
+    H = port.amg(cnt, col, ele)
+    s = _solver()
+    s.assemble(p)
+    s.setup()
+    depth = min(H.nlevels, s.num_levels() - 1)
+    assert depth >= 2
+    for l in range(depth):
+        g, o = s.level(l + 1), H.level(l)
+        keys = ("cnt", "col", "ele", "dinv")
+        if l < depth - 1:
+            keys += ("sel", "pcnt", "pcol")
+        for key in keys:
+            assert np.array_equal(g[key], o[key]), (l + 1, key)
+    s.close()
+
+
 def test_exact_when_level1_is_solved_exactly(port):
     """8^3 with the dense direct solve from 300 rows down: level 1 (256
     rows) is solved exactly, so one cycle is A^-1 (to the cycle's rounding)
