@@ -49,6 +49,46 @@ __device__ __forceinline__ T row_acc(T t, const int *__restrict__ scol,
     return t;
 }
 
+// Sell::pk entries: the column is the row plus the high half (int16), the
+// value the BF16 bits of the low half (exactly __bfloat162float of them);
+// same terms, same order as row_acc over col + val16.
+struct Pk16 {
+    unsigned w;
+};
+
+template <class T, bool SUB, int CH = 4, class X>
+__device__ __forceinline__ T row_acc_pk(T t, const Pk16 *__restrict__ pk, long long o, int wd,
+                                        int row, X x)
+{
+    using A = Ar<T>;
+    for (int k0 = 0; k0 < wd; k0 += CH, o += 32 * CH) {
+        unsigned e[CH];
+        T xv[CH];
+#pragma unroll
+        for (int q = 0; q < CH; q++) e[q] = k0 + q < wd ? __ldg(&pk[o + 32 * q].w) : 0u;
+#pragma unroll
+        for (int q = 0; q < CH; q++) xv[q] = k0 + q < wd ? x(row + ((int)e[q] >> 16)) : (T)0;
+#pragma unroll
+        for (int q = 0; q < CH; q++) {
+            if (k0 + q < wd) {
+                const T ax = A::mul((T)__uint_as_float(e[q] << 16), xv[q]);
+                t = SUB ? A::sub(t, ax) : A::add(t, ax);
+            }
+        }
+    }
+    return t;
+}
+
+// row_acc over either storage of a SELL level
+template <class T, bool SUB, class M, class X>
+__device__ __forceinline__ T row_acc_r(T t, const int *__restrict__ scol,
+                                       const M *__restrict__ sval, long long o, int wd,
+                                       int row, X x)
+{
+    if constexpr (std::is_same<M, Pk16>::value) return row_acc_pk<T, SUB>(t, sval, o, wd, row, x);
+    else return row_acc<T, SUB>(t, scol, sval, o, wd, x);
+}
+
 // ---- smoother / transfer kernels --------------------------------------
 
 // Residual after the pre-smoother from zero (device_jacobi 3-arg,
@@ -71,7 +111,8 @@ k_pre(const long long *__restrict__ sptr, const int *__restrict__ scol,
         long long base = sptr[q];
         int wd = (int)((sptr[q + 1] - base) >> 5);
         T t = f[r];
-        t = row_acc<T, true>(t, scol, sval, base + lane, wd, [&](int c) { return u[c]; });
+        t = row_acc_r<T, true>(t, scol, sval, base + lane, wd, (int)r,
+                               [&](int c) { return u[c]; });
         int pc = prow[r + 1] - prow[r];
         rs[r] = pc == 1 ? t : A::div(t, (T)pc);
     }
@@ -148,7 +189,8 @@ k_post(const long long *__restrict__ sptr, const int *__restrict__ scol,
         int wd = (int)((sptr[q + 1] - base) >> 5);
         T fr = f[r];
         T t = fr;
-        t = row_acc<T, true>(t, scol, sval, base + lane, wd, [&](int c) { return u[c]; });
+        t = row_acc_r<T, true>(t, scol, sval, base + lane, wd, (int)r,
+                               [&](int c) { return u[c]; });
         T un = A::add(u[r], A::mul(A::mul(w, t), dinv[r]));
         uo[r] = un;
         if (DOT) dot += (double)un * (double)fr;
@@ -185,8 +227,8 @@ k_cheb0(const long long *__restrict__ sptr, const int *__restrict__ scol,
         const long q = i >> 5;
         const long long base = sptr[q];
         const int wd = (int)((sptr[q + 1] - base) >> 5);
-        const T t = row_acc<T, true>(f[i], scol, sval, base + (i & 31), wd,
-                                     [&](int c) { return u[c]; });
+        const T t = row_acc_r<T, true>(f[i], scol, sval, base + (i & 31), wd, (int)i,
+                                       [&](int c) { return u[c]; });
         const T di = dinv[i];
         r[i] = A::mul(di, t);
         d[i] = A::mul(A::mul(ith, t), di);
@@ -210,8 +252,8 @@ k_cheb_step(const long long *__restrict__ sptr, const int *__restrict__ scol,
         const long q = i >> 5;
         const long long base = sptr[q];
         const int wd = (int)((sptr[q + 1] - base) >> 5);
-        const T ad = row_acc<T, false>((T)0, scol, sval, base + (i & 31), wd,
-                                       [&](int c) { return din[c]; });
+        const T ad = row_acc_r<T, false>((T)0, scol, sval, base + (i & 31), wd, (int)i,
+                                         [&](int c) { return din[c]; });
         const T di = dinv[i], dold = din[i];
         const T rp = MODE == 0 ? A::mul(di, f[i]) : r[i];
         const T rn = A::sub(rp, A::mul(di, ad));
@@ -721,13 +763,16 @@ template <> double *vec_dx<double>(Solver &s, int l) { return s.lv[l].dx; }
 template <> float *vec_dx<float>(Solver &s, int l) { return s.lv[l].dx32; }
 
 // Launches fn(values) with the level's matrix values in the cycle's
-// storage type: FP64, FP32, or BF16 on levels >= bf16_from.
+// storage type: FP64, FP32, or BF16 on levels >= bf16_from (packed with the
+// column offsets, Sell::pk, where they fit).
 template <class T, class F>
 static void with_vals(Solver &s, const Sell &S, int l, F fn)
 {
     if constexpr (std::is_same<T, double>::value) fn(S.val);
-    else if (s.use_bf16(l)) fn(S.val16);
-    else fn(S.val32);
+    else if (s.use_bf16(l)) {
+        if (S.pk) fn((const Pk16 *)S.pk);
+        else fn(S.val16);
+    } else fn(S.val32);
 }
 
 // One V-cycle from level l: f[l] holds the right-hand side, the result is

@@ -33,6 +33,10 @@ struct Sell {
     double *val = nullptr;    // FP64 values
     float *val32 = nullptr;   // FP32 copy (mixed-precision V-cycle)
     __nv_bfloat16 *val16 = nullptr;  // BF16 copy (coarse levels)
+    // BF16 levels whose every column is within +-32767 of its row: one
+    // 32-bit word per entry, the column offset (int16) in the high half and
+    // the BF16 bits in the low half (2/3 of the bytes of col + val16)
+    unsigned *pk = nullptr;
 };
 
 // Solve-phase forms of the two finest levels of a matrix assembled on the

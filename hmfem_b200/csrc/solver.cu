@@ -116,7 +116,7 @@ static void free_csr(Csr &A)
 
 static void free_sell(Sell &S)
 {
-    dfree(S.sptr); dfree(S.col); dfree(S.val); dfree(S.val32); dfree(S.val16);
+    dfree(S.sptr); dfree(S.col); dfree(S.val); dfree(S.val32); dfree(S.val16); dfree(S.pk);
     S = Sell();
 }
 

@@ -1,5 +1,6 @@
 // sparse.cu -- scans, CSR -> SELL-32 conversion, diagonal extraction and the
 // FP64 SELL SpMV.
+#include <cstdlib>
 #include <cub/device/device_scan.cuh>
 #include <atomic>
 #include <map>
@@ -254,6 +255,24 @@ __global__ void k_to_lowp(const double *__restrict__ v, long len, float *f32,
     }
 }
 
+// Packed BF16 entries (Sell::pk); *bad set when an offset does not fit.
+__global__ void k_pack16(const long long *__restrict__ sptr, const int *__restrict__ scol,
+                         const __nv_bfloat16 *__restrict__ v16, long nrows_pad,
+                         unsigned *pk, int *bad)
+{
+    for (long r = blockIdx.x * (long)blockDim.x + threadIdx.x; r < nrows_pad;
+         r += (long)gridDim.x * blockDim.x) {
+        const long long base = sptr[r >> 5];
+        const int w = (int)((sptr[(r >> 5) + 1] - base) >> 5);
+        for (int k = 0; k < w; k++) {
+            const long long o = base + (long long)k * 32 + (r & 31);
+            long d = (long)scol[o] - r;
+            if (d < -32768 || d > 32767) { *bad = 1; d = 0; }
+            pk[o] = ((unsigned)(d & 0xffff) << 16) | (unsigned)__bfloat16_as_ushort(v16[o]);
+        }
+    }
+}
+
 // amg.h:159-166 / 1216-1225: the LAST stored diagonal entry wins.
 __global__ void k_diag_inv(const int *__restrict__ rowptr,
                            const int *__restrict__ col,
@@ -340,6 +359,26 @@ int sell_fill_lowp(Sell &S, bool f32, bool bf16, cudaStream_t st)
                                                    f32 ? S.val32 : nullptr,
                                                    bf16 ? S.val16 : nullptr);
     HM_LAUNCHED();
+    // HMFEM_PACK16=0 keeps the col + val16 form (the packed one computes the
+    // same terms in the same order: a check of the packing)
+    const char *pe = getenv("HMFEM_PACK16");
+    if (bf16 && !S.pk && S.len > 0 && !(pe && atoi(pe) == 0)) {
+        S.pk = (unsigned *)dalloc(sizeof(unsigned) * S.len);
+        int *bad = (int *)dalloc(sizeof(int));
+        if (!S.pk || !bad) { dfree(S.pk); dfree(bad); S.pk = nullptr; return HMFEM_E_CUDA; }
+        HM_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), st));
+        k_pack16<<<nblocks((long)S.nslices * 32, 256), 256, 0, st>>>(
+            S.sptr, S.col, S.val16, (long)S.nslices * 32, S.pk, bad);
+        HM_LAUNCHED();
+        int hb = 0;
+        HM_CUDA(cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+        HM_CUDA(cudaStreamSynchronize(st));
+        dfree(bad);
+        if (hb) {  // columns too far from their rows: the col + val16 form
+            dfree(S.pk);
+            S.pk = nullptr;
+        }
+    }
     return HMFEM_OK;
 }
 

@@ -115,3 +115,21 @@ def test_solve_matches_oracle(name, port):
         assert np.linalg.norm(x - xo) <= 1e-9 * np.linalg.norm(xo)
         its[schur] = st["iterations"]
     assert its[1] <= its[0], its
+
+
+def test_packed_bf16_levels_match_the_unpacked_form(monkeypatch):
+    """BF16 levels stored as one word per entry (int16 column offset + BF16
+    bits) give the very same solve as the column + value arrays."""
+    p = config_problem(2, size=48)
+    out = {}
+    for pack in ("1", "0"):
+        monkeypatch.setenv("HMFEM_PACK16", pack)
+        s = gpu.Solver(precision=1, schur0=1, bf16_from=1, tol=1e-10)
+        s.assemble(p)
+        s.setup()
+        x, st = s.solve()
+        s.close()
+        assert st["status"] == 0
+        out[pack] = (x, st["iterations"])
+    assert out["1"][1] == out["0"][1]
+    assert np.array_equal(out["1"][0], out["0"][0])
