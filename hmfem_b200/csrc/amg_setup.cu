@@ -566,6 +566,44 @@ int run_union(UnionArgs A, Csr &out, int *dwork, cudaStream_t st)
 
 }  // namespace
 
+// P rows (amg.h:332-346), their entries (amg.h:352-380) and weights from
+// the level's split and coarse ids; *pown: the fine row of every entry
+// (for the transpose), freed by the caller, or nullptr not to keep it.
+int build_p(Level &L, cudaStream_t st, int **pown_out)
+{
+    const int n = L.A.n;
+    L.P.n = n;
+    L.P.rowptr = (int *)dalloc(sizeof(int) * (n + 1));
+    if (!L.P.rowptr) return HMFEM_E_CUDA;
+    k_pcount<<<nblk(n, 256), 256, 0, st>>>(L.A.rowptr, L.A.col, L.sel, n, L.P.rowptr);
+    HM_LAUNCHED();
+    HM_CHECK(rowptr_from_counts(L.P.rowptr, n, st, &L.P.nnz));
+    L.P.col = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
+    int *pown = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
+    L.pw = (double *)dalloc(sizeof(double) * (n > 0 ? n : 1));
+    L.pw32 = (float *)dalloc(sizeof(float) * (n > 0 ? n : 1));
+    if (!L.P.col || !pown || !L.pw || !L.pw32) {
+        dfree(pown);
+        set_last_error("out of device memory (P)", __FILE__, __LINE__);
+        return HMFEM_E_CUDA;
+    }
+    k_pfill<<<nblk(n, 256), 256, 0, st>>>(L.A.rowptr, L.A.col, L.sel, L.cid, n,
+                                          L.P.rowptr, L.P.col, pown, L.pw, L.pw32);
+    HM_LAUNCHED();
+    L.p_deferred = false;
+    if (pown_out) *pown_out = pown;
+    else dfree(pown);
+    return HMFEM_OK;
+}
+
+int ensure_p(Level &L, cudaStream_t st)
+{
+    if (!L.p_deferred) return HMFEM_OK;
+    HM_CHECK(build_p(L, st, nullptr));
+    HM_CUDA(cudaStreamSynchronize(st));
+    return HMFEM_OK;
+}
+
 int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
                 const int *grid3, bool schur)
 {
@@ -599,51 +637,48 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
     HM_CHECK(rowptr_from_counts(L.cid, n, st, &nc));
     HM_PHASE("  coarse ids", st);
     L.nc = (int)nc;
-    // ---- P ---------------------------------------------------------------
-    L.P.n = n;
-    L.P.rowptr = (int *)dalloc(sizeof(int) * (n + 1));
-    k_pcount<<<nblk(n, 256), 256, 0, st>>>(L.A.rowptr, L.A.col, L.sel, n, L.P.rowptr);
-    HM_LAUNCHED();
-    HM_CHECK(rowptr_from_counts(L.P.rowptr, n, st, &L.P.nnz));
-    L.P.col = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
-    int *pown = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
-    L.pw = (double *)dalloc(sizeof(double) * (n > 0 ? n : 1));
-    L.pw32 = (float *)dalloc(sizeof(float) * (n > 0 ? n : 1));
-    k_pfill<<<nblk(n, 256), 256, 0, st>>>(L.A.rowptr, L.A.col, L.sel, L.cid, n,
-                                          L.P.rowptr, L.P.col, pown, L.pw, L.pw32);
-    HM_LAUNCHED();
-    // ---- R = P^T, fine rows ascending (stable radix sort on coarse id) -
-    L.R.n = L.nc;
-    L.R.nnz = L.P.nnz;
-    L.R.rowptr = (int *)dalloc(sizeof(int) * (L.nc + 1));
-    L.R.col = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
-    if (grid3) {
-        dfree(pown);
-        HM_CHECK(stencil_parity_R(grid3[0], grid3[1], grid3[2], L.cid, L.nc, L.R, st));
-        HM_PHASE("  P and R", st);
+    // ---- P and R = P^T (fine rows ascending) ----------------------------
+    if (grid3 && schur) {
+        // the exact reduction transfers level 0 without P, R or the P
+        // weights: the reference's P is formed only when it is asked for
+        // (ensure_p: the hierarchy export)
+        L.P = Csr();
+        L.R = Csr();
+        L.p_deferred = true;
     } else {
-        int *keys_out = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
-        HM_CUDA(cudaMemsetAsync(L.R.rowptr, 0, sizeof(int) * (L.nc + 1), st));
-        k_hist<<<nblk(L.P.nnz, 256), 256, 0, st>>>(L.P.col, L.P.nnz, L.R.rowptr);
-        HM_LAUNCHED();
-        long rn = 0;
-        HM_CHECK(rowptr_from_counts(L.R.rowptr, L.nc, st, &rn));
-        size_t tmp = 0;
-        int bits = 1;
-        while ((1l << bits) < (long)L.nc + 1) bits++;
-        HM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, L.P.col, keys_out,
-                                                pown, L.R.col, (int)L.P.nnz, 0,
-                                                bits, st));
-        void *t = dalloc(tmp);
-        HM_CUDA(cub::DeviceRadixSort::SortPairs(t, tmp, L.P.col, keys_out, pown,
-                                                L.R.col, (int)L.P.nnz, 0, bits,
-                                                st));
-        HM_CUDA(cudaStreamSynchronize(st));
-        dfree(t);
-        dfree(keys_out);
-        dfree(pown);
-        HM_PHASE("  P and R", st);
+        int *pown = nullptr;
+        HM_CHECK(build_p(L, st, &pown));
+        L.R.n = L.nc;
+        L.R.nnz = L.P.nnz;
+        L.R.rowptr = (int *)dalloc(sizeof(int) * (L.nc + 1));
+        L.R.col = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
+        if (grid3) {
+            dfree(pown);
+            HM_CHECK(stencil_parity_R(grid3[0], grid3[1], grid3[2], L.cid, L.nc, L.R, st));
+        } else {  // stable radix sort on the coarse id
+            int *keys_out = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
+            HM_CUDA(cudaMemsetAsync(L.R.rowptr, 0, sizeof(int) * (L.nc + 1), st));
+            k_hist<<<nblk(L.P.nnz, 256), 256, 0, st>>>(L.P.col, L.P.nnz, L.R.rowptr);
+            HM_LAUNCHED();
+            long rn = 0;
+            HM_CHECK(rowptr_from_counts(L.R.rowptr, L.nc, st, &rn));
+            size_t tmp = 0;
+            int bits = 1;
+            while ((1l << bits) < (long)L.nc + 1) bits++;
+            HM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, L.P.col, keys_out,
+                                                    pown, L.R.col, (int)L.P.nnz, 0,
+                                                    bits, st));
+            void *t = dalloc(tmp);
+            HM_CUDA(cub::DeviceRadixSort::SortPairs(t, tmp, L.P.col, keys_out, pown,
+                                                    L.R.col, (int)L.P.nnz, 0, bits,
+                                                    st));
+            HM_CUDA(cudaStreamSynchronize(st));
+            dfree(t);
+            dfree(keys_out);
+            dfree(pown);
+        }
     }
+    HM_PHASE("  P and R", st);
     // ---- Galerkin product ---------------------------------------------
     if (grid3) {
         double *g19v = nullptr;

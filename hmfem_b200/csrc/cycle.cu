@@ -1170,6 +1170,7 @@ int time_kernel(Solver &s, int which, int l, int reps, float *ms, double *bytes)
     if (which >= 10 && (!s.lv[l].cheb || s.use_bf16(l))) return HMFEM_E_ARG;
     Level &L = s.lv[l];
     cudaStream_t st = s.st;
+    if (l < s.nlevels - 1) HM_CHECK(ensure_p(L, st));
     if (which <= 4 && !L.S.sptr) {
         HM_CHECK(csr_to_sell(L.A, L.S, st));
         if (s.opt.precision == 1) HM_CHECK(sell_fill_lowp(L.S, true, s.use_bf16(l), st));

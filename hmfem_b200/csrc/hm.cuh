@@ -92,6 +92,7 @@ struct Level {
     double *pw = nullptr;     // 1 / pcnt per fine row (the P weights)
     float *pw32 = nullptr;
     Csr R;                    // P^T rows: fine ids ascending
+    bool p_deferred = false;  // P not formed (level 0 of the exact reduction)
     // V-cycle vectors (FP64 and FP32 sets)
     double *f = nullptr, *ua = nullptr, *ub = nullptr, *rs = nullptr;
     float *f32 = nullptr, *ua32 = nullptr, *ub32 = nullptr, *rs32 = nullptr;
@@ -162,6 +163,8 @@ int launch_spmv(const Sell &S, const double *x, double *y, cudaStream_t st);
 // (rap_stencil.cu), bit-identical to the generic kernels.
 int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *err_dev,
                 const int *grid3 = nullptr, bool schur = false);
+// the reference's P of a level whose setup left it out (p_deferred)
+int ensure_p(Level &L, cudaStream_t st);
 int stencil_parity_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st);
 // R = P^T of the parity split (rowptr / col allocated by the caller, R.nnz
 // set to P's nnz)

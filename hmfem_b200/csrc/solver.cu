@@ -947,6 +947,8 @@ int hmfem_level_info(hmfem_solver *h, int l, int *n, long *nnz, long *pnnz)
 {
     if (!h || l < 0 || l >= h->s.nlevels) return HMFEM_E_ARG;
     hm::Level &L = h->s.lv[l];
+    hm::set_alloc_context(h->s.st, h->s.cache);
+    if (l < h->s.nlevels - 1) HM_CHECK(hm::ensure_p(L, h->s.st));
     *n = L.A.n;
     *nnz = L.A.nnz;
     *pnnz = l < h->s.nlevels - 1 ? L.P.nnz : 0;
@@ -961,6 +963,7 @@ int hmfem_level_copy(hmfem_solver *h, int l, int *cnt, int *col, double *ele,
     hm::set_alloc_context(s.st, s.cache);
     hm::Level &L = s.lv[l];
     cudaStream_t st = s.st;
+    if (l < s.nlevels - 1) HM_CHECK(hm::ensure_p(L, st));
     const int n = L.A.n;
     std::vector<int> rp(n + 1);
     HM_CUDA(cudaMemcpyAsync(rp.data(), L.A.rowptr, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, st));
