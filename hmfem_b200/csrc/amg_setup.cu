@@ -652,9 +652,15 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
         L.R.nnz = L.P.nnz;
         L.R.rowptr = (int *)dalloc(sizeof(int) * (L.nc + 1));
         L.R.col = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
+        bool done = false;
         if (grid3) {
-            dfree(pown);
             HM_CHECK(stencil_parity_R(grid3[0], grid3[1], grid3[2], L.cid, L.nc, L.R, st));
+            done = true;
+        } else if (L.g19.nx > 0) {
+            HM_CHECK(g19_transpose(L, L.R, st, &done));
+        }
+        if (done) {
+            dfree(pown);
         } else {  // stable radix sort on the coarse id
             int *keys_out = (int *)dalloc(sizeof(int) * (L.P.nnz > 0 ? L.P.nnz : 1));
             HM_CUDA(cudaMemsetAsync(L.R.rowptr, 0, sizeof(int) * (L.nc + 1), st));

@@ -180,6 +180,9 @@ int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
 // parity split) from that structure, bit-identical to the generic product;
 // *done false (and out untouched) when the level does not have it
 int galerkin19(const Level &L, Csr &out, cudaStream_t st, bool *done);
+// R = P^T of such a level from its structure (R.rowptr / R.col allocated by
+// the caller, P formed); *done false when the level does not have it
+int g19_transpose(const Level &L, Csr &R, cudaStream_t st, bool *done);
 // colouring + rows grouped by colour; returns HMFEM_OK with L.gs = false
 // when the level needs more than 63 colours
 int color_level(Level &L, cudaStream_t st, int *dwork);

@@ -417,6 +417,48 @@ __global__ void k_compact_rows(const int *__restrict__ rowptr, int n, int stride
     }
 }
 
+// R = P^T of the level: coarse row e lists its C row and that row's F
+// neighbours, ascending (the rows whose P holds e).  A thread per level row;
+// C rows only.
+__global__ void k_g19_rcount(G19L g, int n, const signed char *__restrict__ sel,
+                             const int *__restrict__ cid, int *cnt)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        if (sel[r] != 1) continue;
+        int x, y, z;
+        const int s = row_cell(g, r, x, y, z);
+        int c = 0;
+#pragma unroll
+        for (int q = 0; q < kQ19; q++)
+            if (q == kCentre ||
+                (in_grid3(g, x + q19x(q), y + q19y(q), z + q19z(q)) &&
+                 sel[(s + q19_lin32(q, g.nx, g.nxy)) >> 1] == 2))
+                c++;
+        cnt[cid[r]] = c;
+    }
+}
+
+__global__ void k_g19_rfill(G19L g, int n, const signed char *__restrict__ sel,
+                            const int *__restrict__ cid, const int *__restrict__ rrow, int *rcol)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        if (sel[r] != 1) continue;
+        int x, y, z;
+        const int s = row_cell(g, r, x, y, z);
+        int o = rrow[cid[r]];
+#pragma unroll
+        for (int q = 0; q < kQ19; q++) {
+            if (q == kCentre) {
+                rcol[o++] = r;
+                continue;
+            }
+            if (!in_grid3(g, x + q19x(q), y + q19y(q), z + q19z(q))) continue;
+            const int j = (s + q19_lin32(q, g.nx, g.nxy)) >> 1;
+            if (sel[j] == 2) rcol[o++] = j;
+        }
+    }
+}
+
 T6 make_t6()
 {
     T6 t;
@@ -448,6 +490,30 @@ int blocks_for(long n, int threads, long cap = 148L * 16)
 }
 
 }  // namespace
+
+int g19_transpose(const Level &L, Csr &R, cudaStream_t st, bool *done)
+{
+    *done = false;
+    const Grid19 &gg = L.g19;
+    if (gg.nx <= 0 || (gg.nx & 1) || gg.nx < 4 || gg.ny < 4) return HMFEM_OK;
+    if ((long)gg.nx * gg.ny * gg.nz > (1l << 30)) return HMFEM_OK;
+    const G19L g{gg.nx, gg.ny, gg.nz, gg.nx / 2, gg.nx * gg.ny};
+    const long n = L.A.n;
+    if (n != (long)g.hx * g.ny * g.nz || L.nc < 1) return HMFEM_OK;
+    HM_CUDA(cudaMemsetAsync(R.rowptr, 0, sizeof(int) * ((long)L.nc + 1), st));
+    k_g19_rcount<<<blocks_for(n, 256), 256, 0, st>>>(g, (int)n, L.sel, L.cid, R.rowptr);
+    HM_LAUNCHED();
+    long nnz = 0;
+    HM_CHECK(rowptr_from_counts(R.rowptr, L.nc, st, &nnz));
+    if (nnz != L.P.nnz) {
+        set_last_error("19-offset level: R size differs from P", __FILE__, __LINE__);
+        return HMFEM_E_CAPACITY;
+    }
+    k_g19_rfill<<<blocks_for(n, 256), 256, 0, st>>>(g, (int)n, L.sel, L.cid, R.rowptr, R.col);
+    HM_LAUNCHED();
+    *done = true;
+    return HMFEM_OK;
+}
 
 int galerkin19(const Level &L, Csr &out, cudaStream_t st, bool *done)
 {
