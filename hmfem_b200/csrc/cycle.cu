@@ -605,7 +605,8 @@ k_update(int n, double *__restrict__ x, double *__restrict__ r,
     });
 }
 
-// s = s * beta + z  (scale_add, pcg.h:69); sigma_last = sigma (pcg.h:70)
+// s = s * beta + z  (scale_add, pcg.h:69); sigma_last = sigma (pcg.h:70).
+// beta = 0 (the first direction) reads no s, whose buffer holds nothing yet.
 template <class T>
 __global__ void __launch_bounds__(256)
 k_sdir(int n, double *__restrict__ s, const T *__restrict__ z, Ctl *ctl)
@@ -613,7 +614,11 @@ k_sdir(int n, double *__restrict__ s, const T *__restrict__ z, Ctl *ctl)
     PDL_ENTRY();
     if (finished(ctl)) return;
     const double be = ctl->beta;
-    GRID_STRIDE(i, n) s[i] = dadd(dmul(s[i], be), (double)z[i]);
+    if (be == 0.0) {
+        GRID_STRIDE(i, n) s[i] = (double)z[i];
+    } else {
+        GRID_STRIDE(i, n) s[i] = dadd(dmul(s[i], be), (double)z[i]);
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->sigma_last = ctl->sigma;
 }
 
