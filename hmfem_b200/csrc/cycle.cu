@@ -19,9 +19,9 @@ int g_pdl = [] {
 
 // t - sum_k a_k x(c_k) (SUB) or t + sum_k a_k x(c_k) over one SELL-32 row
 // (entries at o, o+32, ...), in stored order.  Column indices, values and
-// the gathered x are loaded four entries at a time so the dependent gathers
-// overlap; the summation order is unchanged.
-template <class T, bool SUB, int CH = 4, class M, class X>
+// the gathered x are loaded CH entries at a time (four in FP64, eight in
+// FP32) so the dependent gathers overlap; the summation order is unchanged.
+template <class T, bool SUB, int CH = (sizeof(T) == 8 ? 4 : 8), class M, class X>
 __device__ __forceinline__ T row_acc(T t, const int *__restrict__ scol,
                                      const M *__restrict__ sval, long long o,
                                      int wd, X x)
@@ -56,7 +56,7 @@ struct Pk16 {
     unsigned w;
 };
 
-template <class T, bool SUB, int CH = 4, class X>
+template <class T, bool SUB, int CH = (sizeof(T) == 8 ? 4 : 8), class X>
 __device__ __forceinline__ T row_acc_pk(T t, const Pk16 *__restrict__ pk, long long o, int wd,
                                         int row, X x)
 {

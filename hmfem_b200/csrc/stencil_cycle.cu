@@ -94,13 +94,14 @@ template <class V> struct G19v {
 // the coefficient of a neighbour outside the grid is stored as +0, and its
 // x index is clamped into the vector, so it adds t -/+ 0 * x = t (x finite;
 // the SELL kernels' zero padding behaves the same).  Entries are loaded in
-// chunks of five so the gathers overlap without holding all 19 in
-// registers; the summation order is unchanged.
+// chunks (five in FP64, ten in FP32: two rounds of gathers) so the gathers
+// overlap without holding all 19 in registers; the summation order is
+// unchanged.
 template <class T, bool SUB, class V, class X>
 __device__ __forceinline__ T g19_row(T t, const G19v<V> &g, int c, X x)
 {
     using A = Ar<T>;
-    constexpr int CH = 5;
+    constexpr int CH = sizeof(T) == 8 ? 5 : 10;
     const unsigned cu = (unsigned)c;
     const unsigned row = (unsigned)__umul64hi(cu, g.mhx);
     const unsigned k = (unsigned)__umul64hi(row, g.mny), j = row - k * (unsigned)g.ny;
