@@ -684,6 +684,7 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
             dfree(pown);
         }
     }
+    if (L.g19.nx > 0) HM_CHECK(g19_cpts(L, st));  // for the product
     HM_PHASE("  P and R", st);
     // ---- Galerkin product ---------------------------------------------
     if (grid3) {

@@ -93,6 +93,7 @@ struct Level {
     float *pw32 = nullptr;
     Csr R;                    // P^T rows: fine ids ascending
     bool p_deferred = false;  // P not formed (level 0 of the exact reduction)
+    int *cpts = nullptr;      // 19-offset level: the row of each coarse row (setup)
     // V-cycle vectors (FP64 and FP32 sets)
     double *f = nullptr, *ua = nullptr, *ub = nullptr, *rs = nullptr;
     float *f32 = nullptr, *ua32 = nullptr, *ub32 = nullptr, *rs32 = nullptr;
@@ -183,6 +184,8 @@ int galerkin19(const Level &L, Csr &out, cudaStream_t st, bool *done);
 // R = P^T of such a level from its structure (R.rowptr / R.col allocated by
 // the caller, P formed); *done false when the level does not have it
 int g19_transpose(const Level &L, Csr &R, cudaStream_t st, bool *done);
+// L.cpts of such a level (its C rows in coarse-id order, for galerkin19)
+int g19_cpts(Level &L, cudaStream_t st);
 // colouring + rows grouped by colour; returns HMFEM_OK with L.gs = false
 // when the level needs more than 63 colours
 int color_level(Level &L, cudaStream_t st, int *dwork);

@@ -515,6 +515,16 @@ int g19_transpose(const Level &L, Csr &R, cudaStream_t st, bool *done)
     return HMFEM_OK;
 }
 
+int g19_cpts(Level &L, cudaStream_t st)
+{
+    dfree(L.cpts);
+    L.cpts = (int *)dalloc(sizeof(int) * (L.nc > 0 ? L.nc : 1));
+    if (!L.cpts) return HMFEM_E_CUDA;
+    k_cpts<<<blocks_for(L.A.n, 256), 256, 0, st>>>(L.sel, L.cid, L.A.n, L.cpts);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
 int galerkin19(const Level &L, Csr &out, cudaStream_t st, bool *done)
 {
     *done = false;
@@ -523,11 +533,11 @@ int galerkin19(const Level &L, Csr &out, cudaStream_t st, bool *done)
     if ((long)gg.nx * gg.ny * gg.nz > (1l << 30)) return HMFEM_OK;  // 32-bit indices
     const G19L g{gg.nx, gg.ny, gg.nz, gg.nx / 2, gg.nx * gg.ny};
     const long n = L.A.n, nc = L.nc;
-    if (n != (long)g.hx * g.ny * g.nz || nc < 1) return HMFEM_OK;
+    if (n != (long)g.hx * g.ny * g.nz || nc < 1 || !L.cpts) return HMFEM_OK;
     int *ucnt0 = (int *)dalloc(sizeof(int) * n);
     unsigned char *op = (unsigned char *)dalloc((size_t)n * kCap0);
     double *ov = (double *)dalloc(sizeof(double) * n * kCap0);
-    int *cpts = (int *)dalloc(sizeof(int) * nc);
+    const int *cpts = L.cpts;
     int *pcol = (int *)dalloc(sizeof(int) * nc * kCap1);
     double *pval = (double *)dalloc(sizeof(double) * nc * kCap1);
     int *err = (int *)dalloc(sizeof(int));
@@ -536,10 +546,10 @@ int galerkin19(const Level &L, Csr &out, cudaStream_t st, bool *done)
     out.n = (int)nc;
     out.rowptr = (int *)dalloc(sizeof(int) * (nc + 1));
     auto release = [&]() {
-        dfree(ucnt0); dfree(op); dfree(ov); dfree(cpts); dfree(pcol); dfree(pval); dfree(err);
+        dfree(ucnt0); dfree(op); dfree(ov); dfree(pcol); dfree(pval); dfree(err);
         dfree(cb);
     };
-    if (!ucnt0 || !op || !ov || !cpts || !pcol || !pval || !err || !cb || !out.rowptr) {
+    if (!ucnt0 || !op || !ov || !pcol || !pval || !err || !cb || !out.rowptr) {
         release();
         set_last_error("out of device memory (19-point RAP)", __FILE__, __LINE__);
         return HMFEM_E_CUDA;
@@ -552,8 +562,6 @@ int galerkin19(const Level &L, Csr &out, cudaStream_t st, bool *done)
         g, (int)n, L.A.rowptr, L.A.val, cb + 1, L.pw, ucnt0, op, ov, err);
     HM_LAUNCHED();
     HM_PHASE("    (A P) rows", st);
-    k_cpts<<<blocks_for(n, 256), 256, 0, st>>>(L.sel, L.cid, n, cpts);
-    HM_LAUNCHED();
     static const T6 tb = make_t6();
     k_g19_ptap<<<occ_blocks((const void *)k_g19_ptap, nc * 32, 32 * kWarps1, 148 * 8),
                  32 * kWarps1, 0, st>>>(g, tb, cpts, (int)nc, L.cid, ucnt0, op, ov,

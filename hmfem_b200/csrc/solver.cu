@@ -126,7 +126,7 @@ static void free_level_setup(Level &L, bool keep_matrix)
     if (!keep_matrix) free_csr(L.A);
     free_sell(L.S);
     dfree(L.dinv); dfree(L.dinv32); dfree(L.dsm); dfree(L.dsm32);
-    dfree(L.sel); dfree(L.cid); dfree(L.pw); dfree(L.pw32);
+    dfree(L.sel); dfree(L.cid); dfree(L.pw); dfree(L.pw32); dfree(L.cpts);
     free_csr(L.P); free_csr(L.R);
     dfree(L.f); dfree(L.ua); dfree(L.ub); dfree(L.rs);
     dfree(L.f32); dfree(L.ua32); dfree(L.ub32); dfree(L.rs32);
