@@ -604,22 +604,37 @@ int ensure_p(Level &L, cudaStream_t st)
     return HMFEM_OK;
 }
 
+// Per host thread: the stream that forms level 1's split while level 0's
+// Galerkin product runs (the split depends only on the grid's shape).
+static cudaStream_t side_stream()
+{
+    static thread_local cudaStream_t t_side = nullptr;
+    if (!t_side) cudaStreamCreateWithFlags(&t_side, cudaStreamNonBlocking);
+    return t_side;
+}
+
 int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
                 const int *grid3, bool schur)
 {
     const int n = L.A.n;
     // ---- C/F split ----------------------------------------------------
-    L.sel = (signed char *)dalloc(n > 0 ? n : 1);
-    HM_CUDA(cudaMemsetAsync(L.sel, 0, n > 0 ? n : 1, st));
     HM_CUDA(cudaMemsetAsync(dwork, 0, 4 * sizeof(int), st));
-    if (grid3) {
-        HM_CHECK(stencil_parity_split(grid3[0], grid3[1], grid3[2], L.sel, st));
-    } else if (L.g19.nx > 0) {
-        HM_CHECK(stencil19_split(L.g19.nx, L.g19.ny, L.g19.nz, L.sel, st));
-    } else if (n > 0) {
-        k_lfmis<<<(int)ceil_div(n, kMisTile), kMisTile, 0, st>>>(
-            L.A.rowptr, L.A.col, n, L.sel, (unsigned *)(dwork + 2), dwork);
-        HM_LAUNCHED();
+    if (L.sel_split) {  // formed on the side stream while the level above coarsened
+        HM_CUDA(cudaStreamWaitEvent(st, L.sel_ready, 0));
+        cudaEventDestroy(L.sel_ready);
+        L.sel_ready = nullptr;
+    } else {
+        L.sel = (signed char *)dalloc(n > 0 ? n : 1);
+        HM_CUDA(cudaMemsetAsync(L.sel, 0, n > 0 ? n : 1, st));
+        if (grid3) {
+            HM_CHECK(stencil_parity_split(grid3[0], grid3[1], grid3[2], L.sel, st));
+        } else if (L.g19.nx > 0) {
+            HM_CHECK(stencil19_split(L.g19.nx, L.g19.ny, L.g19.nz, L.sel, st));
+        } else if (n > 0) {
+            k_lfmis<<<(int)ceil_div(n, kMisTile), kMisTile, 0, st>>>(
+                L.A.rowptr, L.A.col, n, L.sel, (unsigned *)(dwork + 2), dwork);
+            HM_LAUNCHED();
+        }
     }
     int herr = 0;
     HM_CUDA(cudaMemcpyAsync(&herr, dwork, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -637,6 +652,22 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
     HM_CHECK(rowptr_from_counts(L.cid, n, st, &nc));
     HM_PHASE("  coarse ids", st);
     L.nc = (int)nc;
+    // the next level's split from the 19-offset structure, on the side
+    // stream, overlapping the rest of this level's coarsening
+    if (grid3 && g19_applies(grid3[0], grid3[1], grid3[2]) && nc > 0) {
+        C.sel = (signed char *)dalloc(nc);
+        if (!C.sel) return HMFEM_E_CUDA;
+        cudaEvent_t allocated;
+        HM_CUDA(cudaEventCreateWithFlags(&allocated, cudaEventDisableTiming));
+        HM_CUDA(cudaEventRecord(allocated, st));
+        cudaStream_t side = side_stream();
+        HM_CUDA(cudaStreamWaitEvent(side, allocated, 0));
+        cudaEventDestroy(allocated);
+        HM_CHECK(stencil19_split(grid3[0], grid3[1], grid3[2], C.sel, side));
+        HM_CUDA(cudaEventCreateWithFlags(&C.sel_ready, cudaEventDisableTiming));
+        HM_CUDA(cudaEventRecord(C.sel_ready, side));
+        C.sel_split = true;
+    }
     // ---- P and R = P^T (fine rows ascending) ----------------------------
     if (grid3 && schur) {
         // the exact reduction transfers level 0 without P, R or the P

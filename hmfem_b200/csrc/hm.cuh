@@ -86,6 +86,8 @@ struct Level {
     float *dsm32 = nullptr;
     // transfer to level+1 (absent on the coarsest)
     signed char *sel = nullptr;  // 1 = C, 2 = F
+    bool sel_split = false;           // sel formed early on a side stream,
+    cudaEvent_t sel_ready = nullptr;  // complete once this event is
     int *cid = nullptr;          // coarse id of C rows (prefix count)
     int nc = 0;
     Csr P;                    // P rows: coarse ids in the fine row's order

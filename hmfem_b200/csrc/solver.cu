@@ -123,6 +123,11 @@ static void free_sell(Sell &S)
 // Frees everything built by setup on level l (keeps level 0's matrix).
 static void free_level_setup(Level &L, bool keep_matrix)
 {
+    if (L.sel_ready) {  // a split still running on the side stream
+        cudaEventSynchronize(L.sel_ready);
+        cudaEventDestroy(L.sel_ready);
+        L.sel_ready = nullptr;
+    }
     if (!keep_matrix) free_csr(L.A);
     free_sell(L.S);
     dfree(L.dinv); dfree(L.dinv32); dfree(L.dsm); dfree(L.dsm32);
