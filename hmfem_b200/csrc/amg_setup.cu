@@ -605,11 +605,18 @@ int ensure_p(Level &L, cudaStream_t st)
 }
 
 // Per host thread: the stream that forms level 1's split while level 0's
-// Galerkin product runs (the split depends only on the grid's shape).
+// Galerkin product runs (the split depends only on the grid's shape).  Its
+// kernels are a latency-bound wavefront of small launches, so the stream
+// has the highest priority: their blocks are scheduled between the
+// bandwidth-bound blocks of the main stream instead of after them.
 static cudaStream_t side_stream()
 {
     static thread_local cudaStream_t t_side = nullptr;
-    if (!t_side) cudaStreamCreateWithFlags(&t_side, cudaStreamNonBlocking);
+    if (!t_side) {
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        cudaStreamCreateWithPriority(&t_side, cudaStreamNonBlocking, greatest);
+    }
     return t_side;
 }
 
