@@ -40,7 +40,7 @@ CASES.update({
 })
 
 # Pressure / flux tolerance against the FP64 oracle when both are solved to
-# ||b - A x|| / ||b|| <= 1e-12: 1e-9 relative.
+# ||b - A x|| / ||b|| <= 1e-12: 1e-9 relative (the bar the FP64 path is held to).
 P_RTOL = 1e-9
 
 
