@@ -130,6 +130,8 @@ class Clocks:
 
 
 def dist_init(args):
+    """One process per GPU (torchrun's RANK / WORLD_SIZE / LOCAL_RANK); NCCL
+    on GPUs, gloo where there is none (the host-side tests of this path)."""
     import torch
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -137,9 +139,13 @@ def dist_init(args):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        timeout = datetime.timedelta(seconds=600)
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timeout,
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=timeout)
     return rank, world, local
 
 
@@ -150,11 +156,13 @@ def barrier(world):
 
 
 def max_over_ranks(v, world):
+    """The max of v over the ranks (times are taken as the slowest rank's)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
