@@ -16,8 +16,13 @@
 // and every call uses it: calls that overlap on the GPU (two streams, or two
 // host threads) race on it.  Its device address is looked up the first time
 // the entry point runs on a device (cudaGetSymbolAddress, with that device
-// current); make that first call before any stream capture begins.
+// current, once per device even when several host threads make their first
+// call at the same time); make that first call before any stream capture
+// begins.  Every call reads the divergence bounds back to the host, so it
+// returns only after its work on the stream has finished.
 #include <string.h>
+
+#include <mutex>
 
 #include "hm.cuh"
 
@@ -30,6 +35,8 @@ static __device__ __align__(256) double g_flux_scratch[6 * kFace + 32];
 
 constexpr int kMaxDevices = 64;
 double *g_scratch_addr[kMaxDevices];
+cudaError_t g_scratch_err[kMaxDevices];
+std::once_flag g_scratch_once[kMaxDevices];
 
 struct NaGrid {
     int nx, ny, nz;
@@ -170,12 +177,14 @@ extern "C" int hmfem_fluxes_noalloc(int nx, int ny, int nz, double hx, double hy
         set_last_error("hmfem_fluxes_noalloc: device ordinal out of range", __FILE__, __LINE__);
         return HMFEM_E_ARG;
     }
-    if (!g_scratch_addr[dev]) {
-        // once per device, with that device current
+    // once per device, with that device current; concurrent first calls
+    // wait here for the one that does the lookup
+    std::call_once(g_scratch_once[dev], [dev] {
         void *addr = nullptr;
-        HM_CUDA(cudaGetSymbolAddress(&addr, g_flux_scratch));
-        g_scratch_addr[dev] = (double *)addr;
-    }
+        g_scratch_err[dev] = cudaGetSymbolAddress(&addr, g_flux_scratch);
+        g_scratch_addr[dev] = g_scratch_err[dev] == cudaSuccess ? (double *)addr : nullptr;
+    });
+    HM_CUDA(g_scratch_err[dev]);
     double *scr = g_scratch_addr[dev];
     cudaStream_t st = (cudaStream_t)stream;
     NaGrid g;
@@ -195,12 +204,12 @@ extern "C" int hmfem_fluxes_noalloc(int nx, int ny, int nz, double hx, double hy
     k_na_prepare<<<(int)(pb < 1024 ? pb : 1024), 256, 0, st>>>(
         scr, g, bc_value[0], bc_value[1], bc_value[2], bc_value[3], bc_value[4],
         bc_value[5]);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     const long n = (long)nx * ny * nz;
     long fb = ceil_div(n, 256);
     k_na_flux<<<(int)(fb < 148L * 16 ? fb : 148L * 16), 256, 0, st>>>(scr, g, KX, KY,
                                                                        KZ, p, v);
-    HM_CUDA(cudaGetLastError());
+    HM_LAUNCHED();
     unsigned long long mm[2];
     HM_CUDA(cudaMemcpyAsync(mm, scr + 6 * kFace, sizeof(mm), cudaMemcpyDeviceToHost, st));
     HM_CUDA(cudaStreamSynchronize(st));

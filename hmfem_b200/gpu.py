@@ -348,15 +348,26 @@ def fluxes_noalloc(prob, KX, KY, KZ, p, v, stream=None):
     (n x 7 float64, c untouched) with no device allocation by the library;
     returns (divmin, divmax).  For callers that cannot let the library
     allocate (see include/hmfem_gpu.h)."""
+    import torch
     L = lib()
     bc = (C.c_int * 6)(*prob.bc_type)
     bv = (C.c_double * 6)(*prob.bc_value)
     dmin, dmax = C.c_double(), C.c_double()
+    dev = torch.cuda.current_device()
     ptrs = []
-    for a in (KX, KY, KZ, p, v):
-        pa, mem = _ptr(a)
-        if mem != 1:
-            raise ValueError("fluxes_noalloc takes device arrays only")
+    for name, a, numel in (("KX", KX, prob.n), ("KY", KY, prob.n), ("KZ", KZ, prob.n),
+                           ("p", p, prob.n), ("v", v, 7 * prob.n)):
+        if not (hasattr(a, "is_cuda") and a.is_cuda):
+            raise ValueError(f"fluxes_noalloc: {name} must be a CUDA tensor")
+        if a.dtype != torch.float64:
+            raise ValueError(f"fluxes_noalloc: {name} must be float64, not {a.dtype}")
+        if a.numel() != numel:
+            raise ValueError(f"fluxes_noalloc: {name} has {a.numel()} elements, "
+                             f"the grid needs {numel}")
+        if a.device.index != dev:
+            raise ValueError(f"fluxes_noalloc: {name} is on cuda:{a.device.index}, "
+                             f"the current device is cuda:{dev}")
+        pa, _ = _ptr(a)
         ptrs.append(pa)
     _check(L.hmfem_fluxes_noalloc(prob.nx, prob.ny, prob.nz, prob.hx, prob.hy,
                                   prob.hz, prob.visc, ptrs[0], ptrs[1], ptrs[2],

@@ -231,7 +231,9 @@ unsigned long long hmfem_launch_count(void);
  * have at most HMFEM_NOALLOC_MAX_FACE cells (else HMFEM_E_CAPACITY).  The
  * array is shared by all calls on a device and keeps the last call's
  * contents: calls that overlap on the GPU race.  The first call on a device
- * looks the array's address up; make it before any stream capture.
+ * looks the array's address up (once, also when several host threads call
+ * at the same time); make it before any stream capture.  The call reads the
+ * bounds back to the host, so it returns after its work on the stream is done.
  * stream: cudaStream_t as void*, NULL = the legacy default stream. */
 #define HMFEM_NOALLOC_MAX_FACE 262144
 int hmfem_fluxes_noalloc(int nx, int ny, int nz, double hx, double hy,

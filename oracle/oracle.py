@@ -35,7 +35,8 @@ def build(ref: bool = True) -> None:
     """Compile the restatement (and the reference harness when the tree is
     present) with oracle/Makefile."""
     targets = ["port"] + (["ref"] if ref else [])
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    tree = os.environ.get("HMFEM_REFERENCE", "/root/reference")
+    subprocess.run(["make", "-s", "-C", HERE] + targets + [f"REF={tree}"], check=True)
 
 
 def _ptr(a):
