@@ -21,6 +21,8 @@
 #include <cub/device/device_scan.cuh>
 
 #include "grid19.cuh"
+#include <stdlib.h>
+
 #include "hm.cuh"
 
 namespace hm {
@@ -30,9 +32,20 @@ namespace {
 constexpr int kMisTile = 256;
 constexpr long long kMaxPolls = 1ll << 22;
 
+// The poll limit of the split's bounded wait: kMaxPolls, or lower when the
+// environment sets HMFEM_TEST_POLL_LIMIT (a test makes the wait run out and
+// checks that the call returns HMFEM_E_TIMEOUT and the next one succeeds).
+long long split_poll_limit()
+{
+    const char *e = getenv("HMFEM_TEST_POLL_LIMIT");
+    if (!e || !*e) return kMaxPolls;
+    long long v = atoll(e);
+    return v < 0 ? 0 : (v < kMaxPolls ? v : kMaxPolls);
+}
+
 __global__ void __launch_bounds__(kMisTile)
 k_lfmis(const int *__restrict__ rowptr, const int *__restrict__ col, int n,
-        signed char *sel, unsigned *ticket, int *err)
+        signed char *sel, unsigned *ticket, int *err, long long max_polls)
 {
     __shared__ int s_tile;
     if (threadIdx.x == 0) s_tile = (int)atomicAdd(ticket, 1u);
@@ -54,7 +67,7 @@ k_lfmis(const int *__restrict__ rowptr, const int *__restrict__ col, int n,
         }
         if (anyC) { vs[v] = 2; return; }
         if (allF) { vs[v] = 1; return; }
-        if (++polls > kMaxPolls || *verr) { atomicExch(err, 1); return; }
+        if (++polls > max_polls || *verr) { atomicExch(err, 1); return; }
         if (polls > 32) __nanosleep(64);
     }
 }
@@ -639,7 +652,8 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
             HM_CHECK(stencil19_split(L.g19.nx, L.g19.ny, L.g19.nz, L.sel, st));
         } else if (n > 0) {
             k_lfmis<<<(int)ceil_div(n, kMisTile), kMisTile, 0, st>>>(
-                L.A.rowptr, L.A.col, n, L.sel, (unsigned *)(dwork + 2), dwork);
+                L.A.rowptr, L.A.col, n, L.sel, (unsigned *)(dwork + 2), dwork,
+                split_poll_limit());
             HM_LAUNCHED();
         }
     }

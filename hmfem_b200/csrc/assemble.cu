@@ -141,12 +141,22 @@ k_assemble(Grid g, const double *__restrict__ KX, const double *__restrict__ KY,
            const double *__restrict__ KI, const double *__restrict__ WI,
            const double *__restrict__ PC, const double *__restrict__ PW,
            const int *__restrict__ rowptr, int *__restrict__ col,
-           double *__restrict__ val, double *__restrict__ b)
+           double *__restrict__ val, double *__restrict__ b, int *bad)
 {
     const long nx = g.nx, nxy = (long)g.nx * g.ny, n = nxy * g.nz;
     for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < n;
          s += (long)gridDim.x * blockDim.x) {
         int i = (int)(s % nx), j = (int)((s / nx) % g.ny), k = (int)(s / nxy);
+        // a permeability that is NaN, infinite or negative makes every
+        // coefficient that touches it meaningless (the reference does not
+        // check): flag one such cell as 1 + its index
+        if (bad) {
+            const double kx = KX[s], ky = KY[s], kz = KZ[s];
+            if (!(kx >= 0.0 && kx <= 1.7976931348623157e308) ||
+                !(ky >= 0.0 && ky <= 1.7976931348623157e308) ||
+                !(kz >= 0.0 && kz <= 1.7976931348623157e308))
+                atomicExch(bad, (int)(s + 1));
+        }
         Faces F = cell_faces(g, i, j, k, s, KX, KY, KZ);
         double ki = KI ? KI[s] : 0.0, wi = WI ? WI[s] : 0.0;
         // permeabilities.c:486: l + r + u + d + t + b + KI/(mu V) + WI/(mu V)
@@ -189,15 +199,22 @@ __global__ void k_exchange_rhs(Grid g, const double *__restrict__ KX,
 }
 
 // solve_linearsystem_AMG.c:58-139: count, then fill in d,l,c,r,u,t,b order.
+// Pass 0 also validates the caller's indices: each is -1 (boundary) or a
+// cell in [0, n), otherwise bad = 1 (the reference reads them unchecked).
 __global__ void k_pack_stencil(int n, const hmfem_ele *__restrict__ perm,
                                const hmfem_ind *__restrict__ ind, int *cnt,
                                const int *__restrict__ rowptr, int *col,
-                               double *val, int pass)
+                               double *val, int pass, int *bad)
 {
     for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < n;
          s += (long)gridDim.x * blockDim.x) {
         hmfem_ind I = ind[s];
         if (pass == 0) {
+            if (bad) {
+                const int f[7] = {I.c, I.u, I.d, I.l, I.r, I.t, I.b};
+                for (int q = 0; q < 7; q++)
+                    if (f[q] < -1 || f[q] >= n) atomicExch(bad, 1);
+            }
             cnt[s] = (I.d != -1) + (I.l != -1) + (I.c != -1) + (I.r != -1) +
                      (I.u != -1) + (I.t != -1) + (I.b != -1);
             continue;
@@ -288,13 +305,13 @@ int launch_assemble(int nx, int ny, int nz, double hx, double hy, double hz,
                     const double *KZ, const int bc[6], double *const face[6],
                     const double *KI, const double *WI, const double *pc,
                     const double *pw, const int *rowptr, int *col, double *val,
-                    double *b, cudaStream_t st)
+                    double *b, cudaStream_t st, int *bad)
 {
     Grid g = make_grid(nx, ny, nz, hx, hy, hz, visc, bc);
     FacePtrs fv{face[0], face[1], face[2], face[3], face[4], face[5]};
     long n = (long)nx * ny * nz;
     k_assemble<<<grid_for(n, 256), 256, 0, st>>>(g, KX, KY, KZ, fv, KI, WI, pc,
-                                                 pw, rowptr, col, val, b);
+                                                 pw, rowptr, col, val, b, bad);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -317,10 +334,10 @@ int launch_exchange_rhs(int nx, int ny, int nz, double hx, double hy, double hz,
 
 int launch_pack_stencil(int n, const hmfem_ele *perm, const hmfem_ind *ind,
                         int *cnt, const int *rowptr, int *col, double *val,
-                        int pass, cudaStream_t st)
+                        int pass, cudaStream_t st, int *bad)
 {
     k_pack_stencil<<<grid_for(n, 256), 256, 0, st>>>(n, perm, ind, cnt, rowptr,
-                                                     col, val, pass);
+                                                     col, val, pass, bad);
     HM_LAUNCHED();
     return HMFEM_OK;
 }

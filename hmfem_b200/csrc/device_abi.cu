@@ -4,7 +4,9 @@
 // device_vector / device_amg_solver / device_conjugate_gradient.  Kernels
 // are this project's: grid-stride loops sized to the B200's 148 SMs, no
 // texture references (which CUDA 12 removed), and FP64 arithmetic without
-// FMA contraction so results match the reference's CPU formulas.
+// FMA contraction so results match the reference's CPU formulas.  Like the
+// reference's, these return nothing; every launch is counted in
+// hmfem_launch_count().
 #include "hm.cuh"
 
 namespace {
@@ -112,47 +114,46 @@ __global__ void k_matrix_conversion(const int *acnt, const int *adsp, int *acol,
 extern "C" {
 
 void _device_add_scale(double *x, double *y, double s, unsigned int m)
-{ if (m) k_add_scale<<<grid(m), 256>>>(x, y, s, m); }
+{ if (m) { k_add_scale<<<grid(m), 256>>>(x, y, s, m); HM_COUNT(); } }
 void _device_sub_scale(double *x, double *y, double s, unsigned int m)
-{ if (m) k_sub_scale<<<grid(m), 256>>>(x, y, s, m); }
+{ if (m) { k_sub_scale<<<grid(m), 256>>>(x, y, s, m); HM_COUNT(); } }
 void _device_scale_add(double *x, double *y, double s, unsigned int m)
-{ if (m) k_scale_add<<<grid(m), 256>>>(x, y, s, m); }
+{ if (m) { k_scale_add<<<grid(m), 256>>>(x, y, s, m); HM_COUNT(); } }
 void _device_vector_product(double *x, double *y, double *z, unsigned int n,
                             unsigned int m)
-{ if (m) k_vector_product<<<m, 256>>>(x, y, z, n); }
+{ if (m) { k_vector_product<<<m, 256>>>(x, y, z, n); HM_COUNT(); } }
 void _device_linear_operator(int *cnt, int *dsp, int *col, double *ele, int l,
                              int m, int n, double *u, double *v)
 {
     (void)l; (void)m;
-    if (n > 0) k_linear_operator<<<grid(n), 256>>>(cnt, dsp, col, ele, n, u, v);
+    if (n > 0) { k_linear_operator<<<grid(n), 256>>>(cnt, dsp, col, ele, n, u, v); HM_COUNT(); }
 }
 void _device_jacobi(int *cnt, int *dsp, int *col, double *ele, int l, int n,
                     double *f, double *u, double *v)
 {
     (void)l;
-    if (n > 0) k_jacobi<<<grid(n), 256>>>(cnt, dsp, col, ele, n, f, u, v);
+    if (n > 0) { k_jacobi<<<grid(n), 256>>>(cnt, dsp, col, ele, n, f, u, v); HM_COUNT(); }
 }
 void _device_set_mul(double *x, double *y, double *z, double omega, unsigned int m)
-{ if (m) k_set_mul<<<grid(m), 256>>>(x, y, z, omega, m); }
+{ if (m) { k_set_mul<<<grid(m), 256>>>(x, y, z, omega, m); HM_COUNT(); } }
 void _device_add_mul(double *x, double *y, double *z, double omega, unsigned int m)
-{ if (m) k_add_mul<<<grid(m), 256>>>(x, y, z, omega, m); }
+{ if (m) { k_add_mul<<<grid(m), 256>>>(x, y, z, omega, m); HM_COUNT(); } }
 void _device_diagonal_solver(double *x, double *y, double *z, unsigned int m)
-{ if (m) k_diag<<<grid(m), 256>>>(x, y, z, m); }
+{ if (m) { k_diag<<<grid(m), 256>>>(x, y, z, m); HM_COUNT(); } }
 void _device_com_snd(double *x, double *svec, int *rcom, unsigned int n)
-{ if (n) k_com_snd<<<grid(n), 256>>>(x, svec, rcom, n); }
+{ if (n) { k_com_snd<<<grid(n), 256>>>(x, svec, rcom, n); HM_COUNT(); } }
 void _device_com_rcv(double *x, double *rvec, int *rcom, unsigned int n)
-{ if (n) k_com_rcv<<<grid(n), 256>>>(x, rvec, rcom, n); }
+{ if (n) { k_com_rcv<<<grid(n), 256>>>(x, rvec, rcom, n); HM_COUNT(); } }
 void _device_sub(double *x, double *y, unsigned int m)
-{ if (m) k_sub<<<grid(m), 256>>>(x, y, m); }
+{ if (m) { k_sub<<<grid(m), 256>>>(x, y, m); HM_COUNT(); } }
 void _device_add(double *x, double *y, unsigned int m)
-{ if (m) k_add<<<grid(m), 256>>>(x, y, m); }
+{ if (m) { k_add<<<grid(m), 256>>>(x, y, m); HM_COUNT(); } }
 void _device_rsb(double *x, double *y, unsigned int m)
-{ if (m) k_rsb<<<grid(m), 256>>>(x, y, m); }
+{ if (m) { k_rsb<<<grid(m), 256>>>(x, y, m); HM_COUNT(); } }
 void _device_matrix_conversion(int *acnt, int *adsp, int *acol, double *aele,
                                int *tdsp, int *tcol, double *tele, int n)
 {
-    if (n > 0)
-        k_matrix_conversion<<<grid(n), 256>>>(acnt, adsp, acol, aele, tdsp, tcol, tele, n);
+    if (n > 0) { k_matrix_conversion<<<grid(n), 256>>>(acnt, adsp, acol, aele, tdsp, tcol, tele, n); HM_COUNT(); }
 }
 
 }  // extern "C"

@@ -135,7 +135,7 @@ int launch_assemble(int nx, int ny, int nz, double hx, double hy, double hz,
                     const double *KZ, const int bc[6], double *const face[6],
                     const double *KI, const double *WI, const double *pc,
                     const double *pw, const int *rowptr, int *col, double *val,
-                    double *b, cudaStream_t st);
+                    double *b, cudaStream_t st, int *bad = nullptr);
 int launch_exchange_rhs(int nx, int ny, int nz, double hx, double hy, double hz,
                         double visc, const double *KX, const double *KY,
                         const double *KZ, const int bc[6], double *const face[6],
@@ -144,7 +144,7 @@ int launch_exchange_rhs(int nx, int ny, int nz, double hx, double hy, double hz,
                         double *b, cudaStream_t st);
 int launch_pack_stencil(int n, const hmfem_ele *perm, const hmfem_ind *ind,
                         int *cnt, const int *rowptr, int *col, double *val,
-                        int pass, cudaStream_t st);
+                        int pass, cudaStream_t st, int *bad = nullptr);
 int launch_flux(int nx, int ny, int nz, double hx, double hy, double hz,
                 double visc, const double *KX, const double *KY,
                 const double *KZ, const int bc[6], double *const face[6],
@@ -157,7 +157,10 @@ int csr_to_sell(const Csr &A, Sell &S, cudaStream_t st);
 int sell_fill_lowp(Sell &S, bool f32, bool bf16, cudaStream_t st);
 struct Level;
 int csr_fill_lowp(Level &L, bool bf16, cudaStream_t st);
-int launch_diag_inv(const Csr &A, double *dinv, float *dinv32, cudaStream_t st);
+int launch_diag_inv(const Csr &A, double *dinv, float *dinv32, cudaStream_t st,
+                    int *bad = nullptr);
+int launch_validate_counts(const int *cnt, int n, int *bad, cudaStream_t st);
+int launch_validate_cols(const int *col, long nnz, int n, int *bad, cudaStream_t st);
 int launch_spmv(const Sell &S, const double *x, double *y, cudaStream_t st);
 
 // AMG setup (amg_setup.cu)

@@ -310,11 +310,15 @@ int setup(Solver &s)
     int l = 0;
     long gcnt = s.lv[0].A.n;
     double rel = 0.0;
+    // level 0's diagonal is checked for positivity (flag in dwork[8], read
+    // with the last synchronisation of the setup); the Galerkin levels below
+    // an SPD level 0 are SPD
+    HM_CUDA(cudaMemsetAsync(s.dwork + 8, 0, sizeof(int), st));
     for (;;) {
         Level &L = s.lv[l];
         HM_ALLOC(L.dinv, double, L.A.n);
         HM_ALLOC(L.dinv32, float, L.A.n);
-        HM_CHECK(launch_diag_inv(L.A, L.dinv, L.dinv32, st));
+        HM_CHECK(launch_diag_inv(L.A, L.dinv, L.dinv32, st, l == 0 ? s.dwork + 8 : nullptr));
         if (!(l < s.opt.max_levels - 1 && gcnt > s.opt.min_coarse && rel < 1.0)) break;
         s.lv.emplace_back();
         const int grid3[3] = {s.nx, s.ny, s.nz};
@@ -403,7 +407,16 @@ int setup(Solver &s)
         }
         HM_PHASE("setup: colouring", st);
     }
+    int nonpos = 0;
+    HM_CUDA(cudaMemcpyAsync(&nonpos, s.dwork + 8, sizeof(int), cudaMemcpyDeviceToHost, st));
     HM_CUDA(cudaStreamSynchronize(st));
+    if (nonpos) {
+        char msg[160];
+        snprintf(msg, sizeof(msg),
+                 "matrix is not SPD: diagonal entry of row %d is not positive", nonpos - 1);
+        set_last_error(msg, __FILE__, __LINE__);
+        return HMFEM_E_BREAKDOWN;
+    }
     s.setup_done = true;
     return HMFEM_OK;
 }
@@ -729,12 +742,26 @@ int hmfem_assemble(hmfem_solver *h, int nx, int ny, int nz, double hx,
     HM_ALLOC(L.A.col, int, L.A.nnz);
     HM_ALLOC(L.A.val, double, L.A.nnz);
     HM_PHASE("assemble: row pointers", st);
+    HM_CUDA(cudaMemsetAsync(s.dwork, 0, sizeof(int), st));
     HM_CHECK(hm::launch_assemble(nx, ny, nz, hx, hy, hz, visc, s.KX, s.KY, s.KZ,
                                  s.bc, s.face, nullptr, nullptr, nullptr,
-                                 nullptr, L.A.rowptr, L.A.col, L.A.val, s.b, st));
+                                 nullptr, L.A.rowptr, L.A.col, L.A.val, s.b, st,
+                                 s.dwork));
+    int bad = 0;
+    HM_CUDA(cudaMemcpyAsync(&bad, s.dwork, sizeof(int), cudaMemcpyDeviceToHost, st));
     HM_CUDA(cudaStreamSynchronize(st));
     HM_PHASE("assemble: TPFA kernel", st);
     s.setup_done = false;
+    s.bad_matrix = bad != 0;
+    if (bad) {
+        // the matrix holds garbage: no setup, solve or fluxes until a valid
+        // matrix is set
+        char msg[160];
+        snprintf(msg, sizeof(msg),
+                 "permeability of cell %d is NaN, infinite or negative", bad - 1);
+        hm::set_last_error(msg, __FILE__, __LINE__);
+        return HMFEM_E_ARG;
+    }
     return HMFEM_OK;
 }
 
@@ -745,6 +772,7 @@ int hmfem_set_matrix(hmfem_solver *h, int n, long nnz, const int *cnt,
     if (!h || n < 1 || nnz < 1 || !cnt || !col || !ele) return HMFEM_E_ARG;
     if (nnz > 2147483647L) return HMFEM_E_CAPACITY;
     Solver &s = h->s;
+    s.bad_matrix = false;
     hm::set_alloc_context(s.st, s.cache);
     cudaStream_t st = s.st;
     if (hm::can_reuse(s, n, nnz)) {
@@ -773,10 +801,20 @@ int hmfem_set_matrix(hmfem_solver *h, int n, long nnz, const int *cnt,
     }
     HM_CHECK(hm::new_level0(s, n));
     s.have_grid = false;
+    // until the indices are validated the matrix must not be used
+    s.bad_matrix = true;
     hm::Level &L = s.lv[0];
     HM_CHECK(hm::upload(L.A.rowptr, cnt, n, mem, st));
+    int bad = 0;
+    HM_CUDA(cudaMemsetAsync(s.dwork + 9, 0, sizeof(int), st));
+    HM_CHECK(hm::launch_validate_counts(L.A.rowptr, n, s.dwork + 9, st));
+    HM_CUDA(cudaMemcpyAsync(&bad, s.dwork + 9, sizeof(int), cudaMemcpyDeviceToHost, st));
     long tot = 0;
-    HM_CHECK(hm::rowptr_from_counts(L.A.rowptr, n, st, &tot));
+    HM_CHECK(hm::rowptr_from_counts(L.A.rowptr, n, st, &tot));  // synchronises
+    if (bad) {
+        hm::set_last_error("negative row count", __FILE__, __LINE__);
+        return HMFEM_E_ARG;
+    }
     if (tot != nnz) {
         hm::set_last_error("row counts do not add up to hdr[1]", __FILE__, __LINE__);
         return HMFEM_E_ARG;
@@ -785,10 +823,17 @@ int hmfem_set_matrix(hmfem_solver *h, int n, long nnz, const int *cnt,
     HM_ALLOC(L.A.col, int, nnz);
     HM_ALLOC(L.A.val, double, nnz);
     HM_CHECK(hm::upload(L.A.col, col, nnz, mem, st));
+    HM_CHECK(hm::launch_validate_cols(L.A.col, nnz, n, s.dwork + 9, st));
+    HM_CUDA(cudaMemcpyAsync(&bad, s.dwork + 9, sizeof(int), cudaMemcpyDeviceToHost, st));
     HM_CHECK(hm::upload(L.A.val, ele, nnz, mem, st));
     if (b) HM_CHECK(hm::upload(s.b, b, n, mem, st));
     else HM_CUDA(cudaMemsetAsync(s.b, 0, sizeof(double) * n, st));
     HM_CUDA(cudaStreamSynchronize(st));
+    if (bad) {
+        hm::set_last_error("column index outside [0, n)", __FILE__, __LINE__);
+        return HMFEM_E_ARG;
+    }
+    s.bad_matrix = false;
     return HMFEM_OK;
 }
 
@@ -799,6 +844,7 @@ int hmfem_set_stencil(hmfem_solver *h, int nx, int ny, int nz,
     if (!h || nx < 1 || ny < 1 || nz < 1 || !perm || !indcol) return HMFEM_E_ARG;
     long n = (long)nx * ny * nz;
     Solver &s = h->s;
+    s.bad_matrix = false;
     hm::set_alloc_context(s.st, s.cache);
     cudaStream_t st = s.st;
     if (hm::can_reuse(s, n, -1)) {
@@ -854,9 +900,18 @@ int hmfem_set_stencil(hmfem_solver *h, int nx, int ny, int nz,
         di = ti;
     }
     hm::Level &L = s.lv[0];
+    s.bad_matrix = true;  // until the indices are validated
+    int bad = 0;
+    HM_CUDA(cudaMemsetAsync(s.dwork + 9, 0, sizeof(int), st));
     HM_CHECK(hm::launch_pack_stencil((int)n, dp, di, L.A.rowptr, nullptr, nullptr,
-                                     nullptr, 0, st));
-    HM_CHECK(hm::rowptr_from_counts(L.A.rowptr, (int)n, st, &L.A.nnz));
+                                     nullptr, 0, st, s.dwork + 9));
+    HM_CUDA(cudaMemcpyAsync(&bad, s.dwork + 9, sizeof(int), cudaMemcpyDeviceToHost, st));
+    HM_CHECK(hm::rowptr_from_counts(L.A.rowptr, (int)n, st, &L.A.nnz));  // synchronises
+    if (bad) {
+        hm::dfree(tp); hm::dfree(ti);
+        hm::set_last_error("stencil index outside [-1, n)", __FILE__, __LINE__);
+        return HMFEM_E_ARG;
+    }
     if (L.A.nnz == 0) {
         hm::dfree(tp); hm::dfree(ti);
         hm::set_last_error("no nonzero elements", __FILE__, __LINE__);
@@ -871,12 +926,22 @@ int hmfem_set_stencil(hmfem_solver *h, int nx, int ny, int nz,
     HM_CUDA(cudaStreamSynchronize(st));
     hm::dfree(tp);
     hm::dfree(ti);
+    s.bad_matrix = false;
     return HMFEM_OK;
+}
+
+static int refuse_bad_matrix(const hm::Solver &s)
+{
+    if (!s.bad_matrix) return HMFEM_OK;
+    hm::set_last_error("the last matrix assembled or set was rejected; assemble "
+                       "or set a valid matrix first", __FILE__, __LINE__);
+    return HMFEM_E_ARG;
 }
 
 int hmfem_setup(hmfem_solver *h)
 {
     if (!h) return HMFEM_E_ARG;
+    HM_CHECK(refuse_bad_matrix(h->s));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -898,6 +963,7 @@ int hmfem_solve(hmfem_solver *h, const double *b, double *x, int mem,
 {
     if (!h) return HMFEM_E_ARG;
     if (h->s.lv.empty()) return HMFEM_E_ARG;
+    HM_CHECK(refuse_bad_matrix(h->s));
     hm::set_alloc_context(h->s.st, h->s.cache);
     return hm::solve(h->s, b, x, mem, st);
 }
@@ -907,6 +973,7 @@ int hmfem_fluxes(hmfem_solver *h, const double *p, hmfem_ele *v, int mem,
 {
     if (!h || !p || !v) return HMFEM_E_ARG;
     Solver &s = h->s;
+    HM_CHECK(refuse_bad_matrix(s));
     hm::set_alloc_context(s.st, s.cache);
     if (!s.have_grid) {
         hm::set_last_error("fluxes need the grid problem (hmfem_assemble)", __FILE__, __LINE__);

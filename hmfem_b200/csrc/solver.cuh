@@ -31,6 +31,7 @@ struct Solver {
     std::vector<Level> lv;
     int nlevels = 0;
     bool setup_done = false;
+    bool bad_matrix = false;  // the last assembly met an invalid permeability
     bool l0_same = false;  // the last matrix set equals the one setup used
     int direct_level = -1;
     double *dense_L = nullptr;

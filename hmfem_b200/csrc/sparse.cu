@@ -277,13 +277,16 @@ __global__ void k_pack16(const long long *__restrict__ sptr, const int *__restri
 __global__ void k_diag_inv(const int *__restrict__ rowptr,
                            const int *__restrict__ col,
                            const double *__restrict__ val, int n, double *dinv,
-                           float *dinv32)
+                           float *dinv32, int *bad)
 {
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
          i += (long)gridDim.x * blockDim.x) {
         double d = 0.0;
         for (int k = rowptr[i]; k < rowptr[i + 1]; k++)
             if (col[k] == i) d = val[k];
+        // an SPD matrix has a positive diagonal: flag one row that has not
+        // (zero, negative or NaN) as 1 + its index
+        if (bad && !(d > 0.0)) atomicExch(bad, (int)(i + 1));
         double v = 1.0 / d;
         dinv[i] = v;
         if (dinv32) dinv32[i] = (float)v;
@@ -394,10 +397,44 @@ int csr_fill_lowp(Level &L, bool bf16, cudaStream_t st)
     return HMFEM_OK;
 }
 
-int launch_diag_inv(const Csr &A, double *dinv, float *dinv32, cudaStream_t st)
+// Index validation of a caller's row-by-count matrix before any kernel
+// indexes with it: a negative count flags bad[0] = 1, a column outside
+// [0, n) bad[0] = 2 (the reference reads such indices unchecked).
+__global__ void k_validate_counts(const int *__restrict__ cnt, int n, int *bad)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x)
+        if (cnt[i] < 0) atomicExch(bad, 1);
+}
+
+__global__ void k_validate_cols(const int *__restrict__ col, long nnz, int n, int *bad)
+{
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < nnz;
+         k += (long)gridDim.x * blockDim.x) {
+        const int c = col[k];
+        if (c < 0 || c >= n) atomicExch(bad, 2);
+    }
+}
+
+int launch_validate_counts(const int *cnt, int n, int *bad, cudaStream_t st)
+{
+    k_validate_counts<<<nblocks(n, 256), 256, 0, st>>>(cnt, n, bad);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+int launch_validate_cols(const int *col, long nnz, int n, int *bad, cudaStream_t st)
+{
+    k_validate_cols<<<nblocks(nnz, 256), 256, 0, st>>>(col, nnz, n, bad);
+    HM_LAUNCHED();
+    return HMFEM_OK;
+}
+
+int launch_diag_inv(const Csr &A, double *dinv, float *dinv32, cudaStream_t st,
+                    int *bad)
 {
     k_diag_inv<<<nblocks(A.n, 256), 256, 0, st>>>(A.rowptr, A.col, A.val, A.n,
-                                                   dinv, dinv32);
+                                                   dinv, dinv32, bad);
     HM_LAUNCHED();
     return HMFEM_OK;
 }

@@ -33,51 +33,7 @@
 #include "functions.h"
 #include "hmfem_oracle.h"
 
-/* ---- globals normally defined by the application's main.c (variables.h) */
-Dim N;
-grid I, h;
-Perm *P;
-ELE *perm;
-IND *indcol;
-ELE *v;
-Bound *B;
-FACE boundary;
-FACEK *BoundKarst;
-IND *indcol1;
-ELEK *uc;
-Perm *KI;
-DimK *M;
-double *wi;
-int *IDwi;
-int Nwi;
-int ix0, ixf, jy0, jyf;
-double karst;
-double viscosidade;
-double **beta;
-double rho;
-int *n_brechas;
-int **brechas;
-double **pc_old;
-double **ucL_old;
-double **ucR_old;
-double *hs;
-double *Kc;
-double **cont_karst;
-int number_karst = 0;
-int Mmax;
-double **pc;
-double **C;
-double **C_contorno;
-double nxg, nyg, nzg;
-char fnam[1024];
-const char *fn;
-const char *fnwi;
-const char *dirname = ".";
-double time_total;
-double time_amg;
-int iter_amg;
-int layer;
-int lay;
+#include "app_globals.h"
 
 static double now()
 {
