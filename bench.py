@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--no-output", action="store_true",
                     help="skip the result-file writers")
     ap.add_argument("--cpu-sample", type=int, default=96)
+    ap.add_argument("--no-config1", action="store_true",
+                    help="skip the 128^3 plain-vs-chosen comparison (config 1)")
     ap.add_argument("--profile-step", type=int, default=-1, metavar="PRECISION",
                     help="run one untimed step (assembly + setup + solve) of "
                          "the plain (0) or chosen (1) variant and exit: the "
@@ -71,6 +73,108 @@ def parse():
 
 
 # ---------------------------------------------------------------- helpers --
+
+def _split_kernel(name):
+    """('k_cheb_step', ['float', 'Pk16', '2']) from a demangled kernel name
+    such as 'void hm::(anonymous namespace)::k_cheb_step<float, hm::Pk16, 2>(...)'."""
+    import re
+    m = re.search(r"\b(k_\w+)", name)
+    if not m:
+        return name, []
+    base, i = m.group(1), m.end()
+    args = []
+    if i < len(name) and name[i] == "<":
+        depth, cur = 0, ""
+        for ch in name[i:]:
+            if ch == "<":
+                depth += 1
+                if depth == 1:
+                    continue
+            elif ch == ">":
+                depth -= 1
+                if depth == 0:
+                    args.append(cur.strip())
+                    break
+            elif ch == "," and depth == 1:
+                args.append(cur.strip())
+                cur = ""
+                continue
+            cur += ch
+    return base, [a.split("::")[-1] for a in args]
+
+
+def _tbytes(t):
+    return {"double": 8, "float": 4, "__nv_bfloat16": 2}.get(t, 4)
+
+
+def kernel_bytes(name, level, info, precision):
+    """Algorithmic bytes of one launch (no padding; every vector element and
+    every stored matrix entry once).  `info[l]` = (rows, nonzeros, P
+    nonzeros) of level l; level -1 = the CG's level-0 vectors.  T = vector
+    bytes, vb = matrix value bytes, es = SELL entry bytes (value + 4-byte
+    column; 4 for the packed BF16 word).  Returns None for kernels without
+    a bandwidth model (latency-bound setup work)."""
+    base, targs = _split_kernel(name)
+    l = max(level, 0)
+    n, nnz, pn = info[l]
+    nc = info[l + 1][0] if l + 1 < len(info) else 0
+    T = _tbytes(targs[0]) if targs else 8
+    vb = _tbytes(targs[1]) if len(targs) > 1 else T
+    es = 4 if (len(targs) > 1 and targs[1] == "Pk16") else vb + 4
+    mode = targs[2] if len(targs) > 2 else ""
+    n0 = info[0][0]
+    table = {
+        "k_g7_spmv_dot": 48 * n0,                       # 4 coefficients + s + v
+        "k_update": 48 * n0 + (4 if precision == 1 else 16) * n0,  # x, r, s, v + FP32 r / FP64 seed
+        "k_g7_resid": (56 + (4 if precision == 1 else 16)) * n0,   # runs on check iterations
+        "k_finish_z": (T + 16) * n0,                    # z, r, v
+        "k_sdir": (T + 16) * n0,                        # z, s in/out
+        "k_g7_sred": (T + 3 * vb + T // 2 + T) * n,     # f, couplings, F-half D^-1, fc + seed
+        "k_g7_sprol2": (3 * vb + T + T // 2 + T) * n,   # couplings, F-half f/D^-1, uc, z
+        "k_g7_pre": (4 * vb + 3 * T) * n,
+        "k_g7_post": (4 * vb + 4 * T) * n,
+        "k_g7_restrict": T * n + 3 * T * nc,
+        "k_g7_prolong": T * nc + 2 * T * n,
+        "k_g19_pre": nnz * vb + (3 * T + 4) * n,
+        "k_g19_post": nnz * vb + 4 * T * n,
+        "k_pre": nnz * es + (3 * T + 4) * n,
+        "k_post": nnz * es + 4 * T * n,
+        "k_cheb0": nnz * es + 5 * T * n,
+        "k_cheb_step": nnz * es + {"0": 6, "1": 7}.get(mode, 6) * T * n,
+        "k_restrict": 4 * pn + T * n + (4 + 3 * T) * nc,
+        "k_prolong_add": 4 * n + 4 * pn + T * nc + 2 * T * n,
+        "k_dense_solve": 8 * n * n + 2 * T * n,
+        "k_diag_solve": 3 * T * n,
+    }
+    return table.get(base)
+
+
+def kernel_table(solver, precision, iters, peak):
+    """Every kernel of `iters` CG iterations, timed one launch at a time with
+    CUDA events on the solver stream (hmfem_profile_iteration), with its
+    algorithmic bytes, GB/s and fraction of the HBM peak; sorted by time."""
+    info = []
+    for l in range(solver.num_levels()):
+        info.append(solver.level_info(l))
+    rows = solver.profile_iteration(iters)
+    tot = sum(r["ms"] for r in rows)
+    out = []
+    for r in sorted(rows, key=lambda r: -r["ms"]):
+        base, targs = _split_kernel(r["kernel"])
+        label = base + ("<" + ",".join(targs) + ">" if targs else "")
+        b = kernel_bytes(r["kernel"], r["level"], info, precision)
+        us = 1e3 * r["ms"] / r["launches"]
+        e = {"kernel": label, "level": r["level"], "launches_per_iteration": r["launches"] / iters,
+             "us_per_launch": round(us, 2), "share": round(r["ms"] / tot, 4)}
+        if b is not None:
+            gbs = b / (us * 1e-6) / 1e9
+            e.update(bytes_per_launch=int(b), GBps=round(gbs, 1), frac=round(gbs / peak, 3))
+        out.append(e)
+    return {"iterations_profiled": iters, "sum_ms_per_iteration": round(tot / iters, 4),
+            "kernels": out,
+            "timing": "CUDA events around each launch on the solver stream, launches "
+                      "one at a time (no graph, no programmatic overlap)"}
+
 
 class Clocks:
     """Samples nvidia-smi clocks/throttle reasons during the timed region."""
@@ -176,6 +280,13 @@ def run_ours(args):
     from hmfem_b200.problem import config_problem
 
     rank, world, local = dist_init(args)
+    # the reference's own CPU path on this exact problem, on one host core
+    # in a process of its own while the GPU arms run: the CPU baseline at the
+    # bench's configuration and the FP64 oracle the pressures are checked
+    # against
+    ref_full = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ref_full = start_reference_full(args.size, args.tol)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     prob = config_problem(2, size=args.size)  # same field on every replica
@@ -255,7 +366,7 @@ def run_ours(args):
                              levels=stats[-1]["levels"],
                              setup_ms=stats[-1]["t_setup_ms"],
                              solve_ms=stats[-1]["t_solve_ms"],
-                             clocks=ck.summary(), solver=s, stream=stream)
+                             clocks=ck.summary(), solver=s, stream=stream, x=x)
     # "chosen": the FP32 V-cycle in FP64 flexible CG from the zero guess;
     # the learned guess is measured beside it (--guess-chosen makes it the
     # headline) -- on config-4 data it lowers the initial error but not the
@@ -270,26 +381,17 @@ def run_ours(args):
     s1 = ch["solver"]
     # L0 SpMV of the CG in its 7-point form: 4 coefficients + x + y per cell
     ms0, by0 = s1.time_kernel(5, 0, reps=20)
-    kern = {}
-    for key, sv, w, lvl in (("L0_spmv64_stencil", s0, 5, 0),
-                            ("L0_pre32_stencil", s1, 6, 0),
-                            ("L0_post32_stencil", s1, 7, 0),
-                            ("L1_pre32_19pt", s1, 8, 1),
-                            ("L1_post32_19pt", s1, 9, 1),
-                            ("L2_cheb_step32", s1, 10, 2),
-                            ("L2_cheb_step64", s0, 11, 2)):
-        try:
-            kern[key] = sv.time_kernel(w, lvl, reps=10)
-        except Exception:
-            pass
     peaks = {}
-    try:
+    if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")):
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
-    except Exception:
+    if "hbm_gbs" in peaks:
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    else:
         peak, peak_src = 6650.0, "fallback"
     achieved = by0 / (ms0 / 1e3) / 1e9
-    kernels_gbs = {k: round(b / (m / 1e3) / 1e9, 1) for k, (m, b) in kern.items()}
+    # every kernel of the chosen and the plain CG iteration, timed live
+    kernels = {"chosen": kernel_table(s1, 1, 3, peak),
+               "plain_fp64": kernel_table(s0, 0, 3, peak)}
 
     # ---- e2e through the public API with host buffers (pinned host memory,
     # as an application that streams fields to the GPU keeps them)
@@ -319,6 +421,23 @@ def run_ours(args):
     e2e = {"value": world * n * args.steps / e2e_s, "unit": "cells/s",
            "h2d_bytes_per_step": nk * n * 8 + n * 8, "d2h_bytes_per_step": n * 8}
 
+    # the chosen and plain pressures and fluxes against the reference's
+    # own FP64 solution of the same problem
+    oracle_error, cpu_full = None, None
+    if ref_full is not None:
+        cpu_full, ref_p, ref_v = finish_reference_full(ref_full)
+        if ref_p is not None:
+            oracle_error = {}
+            for name in ("plain_fp64", chosen_name):
+                r = results[name]
+                oracle_error[name] = pressure_flux_error(r["solver"], r["x"], prob, ref_p,
+                                                         ref_v, dev)
+                oracle_error[name]["relres"] = r["relres"]
+            oracle_error["reference_relres"] = cpu_full.get("relres")
+            del ref_p, ref_v
+    config1 = None if args.no_config1 else run_config1(args, dev)
+    config4 = None if (args.no_guess or model is None) else run_config4(args, dev, model)
+
     batched = None if args.no_batch else run_batch(args, world)
     coupled = None if args.no_coupled else run_coupled(args, world, rank)
     output = None
@@ -327,7 +446,8 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(args.cpu_sample, cores=1)
+        cpu = cpu_full if (cpu_full and cpu_full.get("value")) else \
+            cpu_baseline_sample(args.cpu_sample, cores=1)
 
     if rank == 0:
         line = {
@@ -342,7 +462,7 @@ def run_ours(args):
                        "l2": "inputs (K 3x8 B/cell, matrix, hierarchy) larger than L2",
                        "parallelism": f"replicas x{world}"},
             "chosen_variant": chosen_name,
-            **{name: {k: v for k, v in r.items() if k not in ("solver", "stream")}
+            **{name: {k: v for k, v in r.items() if k not in ("solver", "stream", "x")}
                for name, r in results.items()},
             "speedup_chosen_vs_plain": ch["value"] / results["plain_fp64"]["value"],
             "e2e": e2e,
@@ -356,7 +476,10 @@ def run_ours(args):
                          "traffic": round(SPMV_TRAFFIC_B_PER_CELL * n),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
                                            "of one launch at 192^3, scaled by cells"},
-            "kernels_gbs": kernels_gbs,
+            "kernels": kernels,
+            "oracle_error": oracle_error,
+            "config1": config1,
+            "config4": config4,
             "gpu_launches": launches["chosen"],
             "gpu_launches_per_step": launches["chosen"] / args.steps,
             "batched": batched,
@@ -620,38 +743,332 @@ def cpu_baseline_sample(size, cores=1, tol=1e-10):
                                 [round(t, 3) for t in times]))}
 
 
+FACES = [0, 1, 2, 3, 5, 6]   # u, d, l, r, t, b of an ELE row (c unused)
+
+
+def _mem_available_gb():
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 0.0
+
+
+def _ref_full_worker(size, tol, outdir):
+    """The reference's own path (oracle/_ref, the ref_job_* steps of
+    ref_solve_all) on the config-2 problem of this size; writes the
+    pressure, the six face fluxes and the timings to outdir."""
+    from hmfem_b200.problem import config_problem
+    from oracle.oracle import Ref
+    p = config_problem(2, size=size)
+    with _QuietStdout():
+        job = Ref().job(p, eps=tol)
+        job.assemble()
+        job.setup()
+        job.iterate(-1)
+        v = np.zeros((p.n, 7))
+        job.flux(v)
+    x, it, rel, times = job.result()
+    job.close()
+    np.save(os.path.join(outdir, "p.npy"), x)
+    np.save(os.path.join(outdir, "v.npy"), np.ascontiguousarray(v[:, FACES]))
+    json.dump({"n": p.n, "iterations": it, "relres": rel, "times": list(times)},
+              open(os.path.join(outdir, "meta.json"), "w"))
+
+
+def start_reference_full(size, tol, need_gb=24.0):
+    """Starts _ref_full_worker in a spawned process (one host core).  None
+    when the host has too little free memory for it (~13 GB at 256^3)."""
+    import multiprocessing as mp
+    import tempfile
+    if _mem_available_gb() < need_gb * (size / 256.0) ** 3:
+        return {"unavailable": f"host memory: {_mem_available_gb():.0f} GB available"}
+    d = tempfile.mkdtemp(prefix="hmfem_ref_")
+    proc = mp.get_context("spawn").Process(target=_ref_full_worker, args=(size, tol, d),
+                                           daemon=True)
+    t0 = time.perf_counter()
+    proc.start()
+    return {"proc": proc, "dir": d, "t0": t0, "size": size, "tol": tol}
+
+
+def finish_reference_full(ref, timeout=1500):
+    """Waits for start_reference_full's process; returns (cpu_baseline dict,
+    pressure, face fluxes) or (dict with the reason, None, None)."""
+    import shutil
+    if "proc" not in ref:
+        return {"value": None, "unavailable": ref.get("unavailable")}, None, None
+    proc, d = ref["proc"], ref["dir"]
+    proc.join(timeout)
+    try:
+        if proc.is_alive() or proc.exitcode != 0:
+            if proc.is_alive():
+                proc.terminate()
+            return {"value": None, "unavailable": f"reference process exit {proc.exitcode}"}, \
+                None, None
+        meta = json.load(open(os.path.join(d, "meta.json")))
+        p = np.load(os.path.join(d, "p.npy"))
+        v = np.load(os.path.join(d, "v.npy"))
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    t = meta["times"]
+    size = ref["size"]
+    cpu = {"value": meta["n"] / (t[0] + t[1] + t[2]), "unit": "cells/s", "cores": 1,
+           "kind": "reference",
+           "sample": f"the bench's own config2 {size}^3 problem, one full solve: assembly + "
+                     f"CSR + AMG setup + PCG to true relres {ref['tol']} "
+                     f"({meta['iterations']} iterations), the reference's sources "
+                     f"(oracle/_ref), on one host core beside the GPU arms",
+           "split_s": dict(zip(["assemble", "setup", "solve", "flux", "total"],
+                               [round(x, 2) for x in t])),
+           "iterations": meta["iterations"], "relres": meta["relres"]}
+    return cpu, p, v
+
+
+def pressure_flux_error(solver, x, prob, ref_p, ref_v, dev):
+    """Pressure and six face fluxes of a GPU solution against the
+    reference's: relative 2-norm errors, and the divvel_pontual maximum
+    |div u| relative to the largest face flux over h."""
+    import torch
+    p = x.to(torch.float64)
+    v = torch.zeros((prob.n, 7), dtype=torch.float64, device=dev)
+    _, dmin, dmax = solver.fluxes(p, v)
+    ph = p.cpu().numpy()
+    vh = v[:, FACES].cpu().numpy()
+    scale = float(np.abs(ref_v).max()) / min(prob.hx, prob.hy, prob.hz)
+    out = {"p_rel": float(np.linalg.norm(ph - ref_p) / np.linalg.norm(ref_p)),
+           "flux_rel": float(np.linalg.norm(vh - ref_v) / np.linalg.norm(ref_v)),
+           "divmax": dmax, "divmax_rel": dmax / scale if scale > 0 else None}
+    del vh
+    return out
+
+
+def _time_steps(s, prob, K, stream, steps, warmup, x):
+    import torch
+    for _ in range(warmup):
+        s.assemble(prob, KX=K, KY=K, KZ=K)
+        s.setup()
+        x.zero_()
+        s.solve(x=x)
+    times, st = [], None
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.assemble(prob, KX=K, KY=K, KZ=K)
+        s.setup()
+        x.zero_()
+        _, st = s.solve(x=x)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return float(np.mean(times)), st
+
+
+def run_config1(args, dev, steps=5, warmup=3):
+    """Config 1: 128^3, K = 1e-14 + 4 conduits at 1e-10; the plain FP64
+    drop-in against the chosen FP32 V-cycle (level-0 reduction, BF16 levels
+    >= 1) in FP64 flexible CG, both to ||r||/||b|| <= tol; K resident, CUDA
+    events per step (assembly + setup + solve)."""
+    import torch
+
+    from hmfem_b200 import gpu
+    from hmfem_b200.problem import config_problem
+    prob = config_problem(1)
+    K = torch.tensor(prob.KX, device=dev)
+    out = {"workload": "config1 128^3, 4 conduits at 1e-10", "cells": prob.n}
+    for name, prec in (("plain_fp64", 0), ("fp32_chosen", 1)):
+        s = gpu.Solver(precision=prec, tol=args.tol, check_every=2,
+                       bf16_from=1 if prec == 1 else -1, schur0=prec)
+        stream = torch.cuda.ExternalStream(s.stream)
+        x = torch.zeros(prob.n, dtype=torch.float64, device=dev)
+        ms, st = _time_steps(s, prob, K, stream, steps, warmup, x)
+        out[name] = {"ms_per_step": ms, "cells_per_s": prob.n / (ms / 1e3),
+                     "iterations": st["iterations"], "relres": st["relres"],
+                     "setup_ms": st["t_setup_ms"], "solve_ms": st["t_solve_ms"]}
+        s.close()
+    out["speedup_chosen_vs_plain"] = out["plain_fp64"]["ms_per_step"] / out["fp32_chosen"]["ms_per_step"]
+    return out
+
+
+def run_config4(args, dev, model, seeds=range(2048, 2056)):
+    """Config 4 on held-out seeds: 128^3 lognormal (std 1.5, correlation 8)
+    with 0-6 conduits; the chosen solver from the zero guess and from the
+    learned guess (inference inside the timed step), both to tol; CUDA
+    events per solve, K resident."""
+    import torch
+
+    from hmfem_b200 import gpu, guess
+    from hmfem_b200.problem import config_problem
+    s = gpu.Solver(precision=1, tol=args.tol, check_every=2, bf16_from=1, schur0=1)
+    stream = torch.cuda.ExternalStream(s.stream)
+    rows = []
+    for sd in seeds:
+        prob = config_problem(4, realisation=sd)
+        K = torch.tensor(prob.KX, device=dev)
+        mask = torch.as_tensor(prob.conduit_mask, device=dev)
+        dims = (prob.nx, prob.ny, prob.nz)
+        x = torch.zeros(prob.n, dtype=torch.float64, device=dev)
+        r = {}
+        for mode in ("zero", "net", "zero", "net"):   # second pass timed
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s.assemble(prob, KX=K, KY=K, KZ=K)
+            s.setup()
+            if mode == "net":
+                with torch.cuda.stream(stream):
+                    x.copy_(guess.predict(model, K, mask, dims))
+            else:
+                x.zero_()
+            _, st = s.solve(x=x)
+            e1.record(stream)
+            e1.synchronize()
+            r[mode] = (e0.elapsed_time(e1), st["iterations"], st["relres"])
+        rows.append(r)
+    s.close()
+    it_z = [r["zero"][1] for r in rows]
+    it_n = [r["net"][1] for r in rows]
+    return {"workload": f"config4 128^3, held-out seeds {seeds[0]}-{seeds[-1]}",
+            "zero_guess": {"iterations_mean": float(np.mean(it_z)),
+                           "ms_mean": float(np.mean([r["zero"][0] for r in rows]))},
+            "learned_guess": {"iterations_mean": float(np.mean(it_n)),
+                              "ms_mean": float(np.mean([r["net"][0] for r in rows]))},
+            "max_relres": float(max(max(r["zero"][2], r["net"][2]) for r in rows)),
+            "timing": "CUDA events per solve (assembly + setup + [inference] + solve)"}
+
+
+def ref_plan(steps, est_iters=56):
+    """The reference's path for one problem -- what the GPU step times:
+    assembly + CSR, AMG setup + CG start, CG to the tolerance -- split into
+    `steps` parts run in order: the CG in chunks of iterations, the last
+    part finishing it."""
+    if steps <= 1:
+        return [["assemble", "setup", ("iterate", -1)]]
+    if steps == 2:
+        return [["assemble", "setup"], [("iterate", -1)]]
+    if steps == 3:
+        return [["assemble"], ["setup"], [("iterate", -1)]]
+    chunks = steps - 3
+    c = -(-est_iters // (chunks + 1))
+    return [["assemble"], ["setup"]] + [[("iterate", c)] for _ in range(chunks)] + \
+        [[("iterate", -1)]]
+
+
+def _ref_replica(conn, size, tol, plan):
+    """One replica of the reference arm: builds the problem and a reference
+    job, then runs the plan's parts on command ("warm", step index,
+    "result", "quit")."""
+    from hmfem_b200.problem import config_problem
+    from oracle.oracle import Ref
+    R = Ref()
+    p = config_problem(2, size=size)
+    job = R.job(p, eps=tol)
+    conn.send("ready")
+    while True:
+        msg = conn.recv()
+        if msg == "quit":
+            break
+        if msg == "warm":      # pages the library and its code in
+            with _QuietStdout():
+                R.solve_all(config_problem(2, size=24), eps=tol)
+            conn.send("ok")
+        elif msg == "result":
+            _, it, rel, times = job.result(want_p=False)
+            conn.send((it, rel, list(times)))
+        else:
+            with _QuietStdout():
+                for op in plan[msg]:
+                    if op == "assemble":
+                        job.assemble()
+                    elif op == "setup":
+                        job.setup()
+                    elif op == "flux":
+                        job.flux()
+                    else:
+                        job.iterate(op[1])
+            conn.send("ok")
+    job.close()
+
+
 def run_reference(args):
+    """The reference's own CPU path (oracle/_ref) on the bench's own
+    configuration: the config-2 problem of --size (256^3), assembly + CSR +
+    AMG setup + PCG to the true relative residual --tol + fluxes.  The host
+    cores run independent replicas of that solve (the reference is single
+    threaded; as many replicas as cores and free memory allow, ~13 GB
+    each at 256^3), stepped in lockstep: step i runs part i of ref_plan on
+    every replica, so the K timed steps are exactly one full solve per
+    replica.  W warm-up steps run a 24^3 solve per replica.  value = replicas
+    x cells / time of the K steps."""
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
         return
     import multiprocessing as mp
+    size = args.size
+    per_gb = 14.0 * (size / 256.0) ** 3 + 0.5
     cores = os.cpu_count() or 1
-    size = 64
+    reps = max(1, min(cores, 16, int(0.7 * _mem_available_gb() / per_gb)))
+    plan = ref_plan(args.steps)
     ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        for _ in range(args.warmup):
-            pool.map(_ref_worker, [(size, c, args.tol) for c in range(cores)])
-        t0 = time.perf_counter()
-        its = []
-        for _ in range(args.steps):
-            out = pool.map(_ref_worker, [(size, c, args.tol) for c in range(cores)])
-            its.append(out[0][2])
-        dt = time.perf_counter() - t0
-    cells = size ** 3 * cores * args.steps
-    value = cells / dt
+    procs, conns = [], []
+    for _ in range(reps):
+        a, b = ctx.Pipe()
+        pr = ctx.Process(target=_ref_replica, args=(b, size, args.tol, plan), daemon=True)
+        pr.start()
+        procs.append(pr)
+        conns.append(a)
+    for c in conns:
+        c.recv()
+    for _ in range(args.warmup):
+        for c in conns:
+            c.send("warm")
+        for c in conns:
+            c.recv()
+    step_s = []
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        ts = time.perf_counter()
+        for c in conns:
+            c.send(i)
+        for c in conns:
+            c.recv()
+        step_s.append(time.perf_counter() - ts)
+    dt = time.perf_counter() - t0
+    for c in conns:
+        c.send("result")
+    res = [c.recv() for c in conns]
+    for c in conns:
+        c.send("quit")
+    for pr in procs:
+        pr.join(60)
+    n = size ** 3
+    value = reps * n / dt
+    its = sorted({r[0] for r in res})
     line = {"impl": "reference", "metric": METRIC, "value": value,
             "unit": "cells/s", "n_gpus": 0, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"config2 generator at {size}^3 per core "
-                                   f"(bounded sample of the 256^3 workload)",
-                       "tol": args.tol},
-            "cpu_baseline": {"value": value, "unit": "cells/s", "cores": cores,
+            "dtype": "f64", "data": "synthetic (seeded lognormal field + random-walk conduits)",
+            "config": {"workload": f"config2 {size}^3 lognormal+8 conduits",
+                       "cells": n, "tol": args.tol,
+                       "l2": "inputs (K 3x8 B/cell, matrix, hierarchy) larger than L2",
+                       "parallelism": f"replicas x{reps} (host cores)"},
+            "cpu_baseline": {"value": value, "unit": "cells/s", "cores": reps,
                              "kind": "reference",
-                             "sample": f"{cores} independent {size}^3 solves per "
-                                       f"step, one per core, reference sources "
-                                       f"(oracle/_ref), {its[-1]} iterations"},
+                             "sample": f"{reps} independent replicas of the full {size}^3 "
+                                       f"solve, one per host core, in lockstep: the "
+                                       f"{args.steps} steps are one complete solve per "
+                                       f"replica (assembly + CSR + AMG setup + PCG to true "
+                                       f"relres {args.tol}; {its} iterations), "
+                                       f"the reference's sources (oracle/_ref); warm-up: "
+                                       f"a 24^3 solve per replica per warm-up step",
+                             "split_s_replica0": dict(zip(
+                                 ["assemble", "setup", "solve", "flux", "total"],
+                                 [round(x, 2) for x in res[0][2]])),
+                             "step_s": [round(x, 2) for x in step_s],
+                             "max_relres": max(r[1] for r in res)},
             "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

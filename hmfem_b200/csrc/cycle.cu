@@ -12,6 +12,9 @@
 
 namespace hm {
 
+thread_local std::vector<KRec> *t_kprof = nullptr;
+thread_local int t_klevel = -1;
+
 int g_pdl = [] {
     const char *e = getenv("HMFEM_PDL");
     return e ? atoi(e) : 1;
@@ -785,6 +788,7 @@ static void with_vals(Solver &s, const Sell &S, int l, F fn)
 template <class T>
 static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
 {
+    t_klevel = l;
     Level &L = s.lv[l];
     const int last = s.nlevels - 1;
     const int n = L.A.n;
@@ -807,6 +811,7 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
         const T *d0 = s.vec_dtrue<T>(0);
         HM_CHECK((g7_sred<T>(L, f, d0, s.vec_f<T>(1), seed_of<T>(s, 1), ctl, st)));
         HM_CHECK(cycle_t<T>(s, 1, st, false, true));
+        t_klevel = l;
         HM_CHECK((g7_sprol<T>(L, f, d0, cycle_out<T>(s, 1), ub, ctl, st)));
         return HMFEM_OK;
     }
@@ -905,6 +910,7 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
         HM_LAUNCHED();
     }
     HM_CHECK(cycle_t<T>(s, l + 1, st, false, true));
+    t_klevel = l;
     if (g7) {
         HM_CHECK((g7_prolong<T>(L, cycle_out<T>(s, l + 1), ua, ctl, st)));
     } else {
@@ -1016,6 +1022,7 @@ int cg_precondition(Solver &s, cudaStream_t st)
     if (s.opt.precision == 0) {
         // the V-cycle reads f[0] = r in place; z lands in ub[0] = s.z
         HM_CHECK(cycle_fp64(s, 0, st, !top_is_coarse, true));
+        t_klevel = -1;
         if (top_is_coarse) {
             launch_pdl(k_finish_z<double>, nb(n), 256, st, n, L0.ua, s.r, s.v, s.z,
                                                       s.ctl, s.part,
@@ -1026,6 +1033,7 @@ int cg_precondition(Solver &s, cudaStream_t st)
     }
     // f32 and its seed were written by the kernel that produced r
     HM_CHECK(cycle_fp32(s, 0, st, false, true));
+    t_klevel = -1;
     launch_pdl(k_finish_z<float>, nb(n), 256, st, n, cg_z32(s), s.r, s.v,
                (double *)nullptr, s.ctl, s.part, s.first_sigma, 1);
     HM_LAUNCHED();
@@ -1063,6 +1071,7 @@ int cg_init(Solver &s, cudaStream_t st)
 
 int cg_iteration(Solver &s, cudaStream_t st)
 {
+    t_klevel = -1;
     Level &L0 = s.lv[0];
     const int n = L0.A.n;
     const bool g7 = s.use_g7(0);
@@ -1084,6 +1093,7 @@ int cg_iteration(Solver &s, cudaStream_t st)
         HM_LAUNCHED();
     }
     HM_CHECK(cg_precondition(s, st));
+    t_klevel = -1;
     HM_CHECK(cg_sdir(s, st));
     return HMFEM_OK;
 }

@@ -1,6 +1,7 @@
 // cycle.cuh -- arithmetic helpers shared by the V-cycle translation units.
 #pragma once
 #include <utility>
+#include <vector>
 
 #include "solver.cuh"
 
@@ -42,10 +43,28 @@ __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.lau
 
 extern int g_pdl;  // 0: plain stream order (HMFEM_PDL=0)
 
+// Per-launch timing of the solve phase (hmfem_profile_iteration): while
+// t_kprof is set on a host thread, launch_pdl brackets each of its launches
+// with two events and records the kernel and t_klevel (the V-cycle level
+// being worked on, -1 for the CG's level-0 vector work).
+struct KRec {
+    const void *fn;
+    int level;
+    cudaEvent_t e0, e1;
+};
+extern thread_local std::vector<KRec> *t_kprof;
+extern thread_local int t_klevel;
+
 template <class... KArgs, class... Args>
 inline void launch_pdl(void (*kernel)(KArgs...), int grid, int block, cudaStream_t st,
                        Args &&...args)
 {
+    KRec rec{(const void *)kernel, t_klevel, nullptr, nullptr};
+    if (t_kprof) {
+        cudaEventCreate(&rec.e0);
+        cudaEventCreate(&rec.e1);
+        cudaEventRecord(rec.e0, st);
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
@@ -56,6 +75,10 @@ inline void launch_pdl(void (*kernel)(KArgs...), int grid, int block, cudaStream
     cfg.attrs = at;
     cfg.numAttrs = g_pdl ? 1 : 0;
     cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);  // error: cudaGetLastError
+    if (t_kprof) {
+        cudaEventRecord(rec.e1, st);
+        t_kprof->push_back(rec);
+    }
 }
 
 #define GRID_STRIDE(r, n)                                                     \

@@ -5,7 +5,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <cxxabi.h>
+
 #include "solver.cuh"
+#include "cycle.cuh"
 
 namespace hm {
 
@@ -445,6 +448,18 @@ static int capture_iteration(Solver &s)
     return HMFEM_OK;
 }
 
+// the CG control block at the start of a solve
+static int ctl_reset(Solver &s, cudaStream_t st)
+{
+    s.ctl_init = Ctl{};
+    s.ctl_init.tol2 = s.opt.tol * s.opt.tol;
+    s.ctl_init.max_iter = s.opt.max_iter;
+    s.ctl_init.stop_rule = s.opt.stop_rule;
+    HM_CUDA(cudaMemcpyAsync(s.ctl, &s.ctl_init, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+    HM_CUDA(cudaMemsetAsync(s.gsbar, 0, sizeof(unsigned) * 4, st));
+    return HMFEM_OK;
+}
+
 int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out)
 {
     if (!s.setup_done) HM_CHECK(setup(s));
@@ -453,13 +468,7 @@ int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out)
     if (b) HM_CHECK(upload(s.b, b, n, mem, st));
     if (x) HM_CHECK(upload(s.x, (const double *)x, n, mem, st));
     else HM_CUDA(cudaMemsetAsync(s.x, 0, sizeof(double) * n, st));
-    Ctl c0;
-    memset(&c0, 0, sizeof(c0));
-    c0.tol2 = s.opt.tol * s.opt.tol;
-    c0.max_iter = s.opt.max_iter;
-    c0.stop_rule = s.opt.stop_rule;
-    HM_CUDA(cudaMemcpyAsync(s.ctl, &c0, sizeof(Ctl), cudaMemcpyHostToDevice, st));
-    HM_CUDA(cudaMemsetAsync(s.gsbar, 0, sizeof(unsigned) * 4, st));
+    HM_CHECK(ctl_reset(s, st));
     cudaEvent_t e0, e1;
     HM_CUDA(cudaEventCreate(&e0));
     HM_CUDA(cudaEventCreate(&e1));
@@ -515,8 +524,73 @@ int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out)
     if (s.opt.stop_rule == 0 && s.last.status == HMFEM_OK &&
         !(s.last.relres <= s.opt.tol))
         s.last.status = HMFEM_E_NOTCONV;
+    if (s.last.status != HMFEM_OK) {
+        // the device reported the outcome: give it a message of its own
+        char msg[200];
+        if (s.last.status == HMFEM_E_BREAKDOWN)
+            snprintf(msg, sizeof(msg), "CG breakdown after %d iterations: (z, r) or "
+                     "(s, A s) is NaN, infinite or zero", ch.iters);
+        else if (s.last.status == HMFEM_E_TIMEOUT)
+            snprintf(msg, sizeof(msg), "a bounded device wait gave up after %d iterations",
+                     ch.iters);
+        else
+            snprintf(msg, sizeof(msg), "not converged: relres %.3e after %d iterations",
+                     s.last.relres, ch.iters);
+        set_last_error(msg, __FILE__, __LINE__);
+    }
     if (out) *out = s.last;
     return s.last.status;
+}
+
+// `iters` CG iterations from x = 0, launched without the graph, each
+// kernel bracketed by CUDA events on the solver stream; per (kernel,
+// level): launches and summed milliseconds.  The solver's x and r are
+// overwritten (the next hmfem_solve starts from its own x).
+int profile_iteration(Solver &s, int iters, hmfem_kernel_time *out, int cap, int *count)
+{
+    if (!s.setup_done) HM_CHECK(setup(s));
+    cudaStream_t st = s.st;
+    const int n = s.lv[0].A.n;
+    HM_CUDA(cudaMemsetAsync(s.x, 0, sizeof(double) * n, st));
+    HM_CHECK(ctl_reset(s, st));
+    s.ctl_active = true;
+    int rc = cg_init(s, st);
+    std::vector<KRec> recs;
+    recs.reserve(2048);
+    t_kprof = &recs;
+    for (int i = 0; i < iters && rc == HMFEM_OK; i++) rc = cg_iteration(s, st);
+    t_kprof = nullptr;
+    s.ctl_active = false;
+    HM_CUDA(cudaStreamSynchronize(st));
+    struct Agg { const void *fn; int level; int launches; double ms; };
+    std::vector<Agg> agg;
+    for (const KRec &r : recs) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, r.e0, r.e1);
+        cudaEventDestroy(r.e0);
+        cudaEventDestroy(r.e1);
+        size_t q = 0;
+        while (q < agg.size() && !(agg[q].fn == r.fn && agg[q].level == r.level)) q++;
+        if (q == agg.size()) agg.push_back({r.fn, r.level, 0, 0.0});
+        agg[q].launches++;
+        agg[q].ms += ms;
+    }
+    HM_CUDA(cudaGetLastError());
+    if (rc != HMFEM_OK) return rc;
+    const int m = (int)agg.size() < cap ? (int)agg.size() : cap;
+    for (int q = 0; q < m; q++) {
+        const char *name = nullptr;
+        if (cudaFuncGetName(&name, agg[q].fn) != cudaSuccess || !name) name = "?";
+        int dst = 0;
+        char *dem = abi::__cxa_demangle(name, nullptr, nullptr, &dst);
+        snprintf(out[q].name, sizeof(out[q].name), "%s", dem && dst == 0 ? dem : name);
+        free(dem);
+        out[q].level = agg[q].level;
+        out[q].launches = agg[q].launches;
+        out[q].ms = agg[q].ms;
+    }
+    *count = (int)agg.size();
+    return HMFEM_OK;
 }
 
 int assemble_coupled(Solver &s, const double *KI, const double *WI, const double *pw)
@@ -1117,6 +1191,16 @@ int hmfem_last_stats(hmfem_solver *h, hmfem_stats *st)
     if (!h || !st) return HMFEM_E_ARG;
     *st = h->s.last;
     return HMFEM_OK;
+}
+
+int hmfem_profile_iteration(hmfem_solver *h, int iters, hmfem_kernel_time *out, int cap,
+                            int *count)
+{
+    if (!h || iters < 1 || !out || cap < 0 || !count) return HMFEM_E_ARG;
+    HM_CHECK(refuse_bad_matrix(h->s));
+    if (h->s.lv.empty()) return HMFEM_E_ARG;
+    hm::set_alloc_context(h->s.st, h->s.cache);
+    return hm::profile_iteration(h->s, iters, out, cap, count);
 }
 
 int hmfem_time_kernel(hmfem_solver *h, int which, int level, int reps,

@@ -39,6 +39,7 @@ struct Solver {
     // CG state
     double *x = nullptr, *r = nullptr, *s = nullptr, *v = nullptr, *z = nullptr;
     Ctl *ctl = nullptr;
+    Ctl ctl_init{};  // host copy of the control block a solve starts from
     Ctl *ctl_host = nullptr;  // pinned, 2 slots
     double *part = nullptr;
     int *dwork = nullptr;
@@ -134,6 +135,7 @@ int g19_spmv(const Level &L, const double *x, double *y, cudaStream_t st);
 // solver.cu entry points the coupled driver (karst.cu) builds on
 int setup(Solver &s);
 int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out);
+int profile_iteration(Solver &s, int iters, hmfem_kernel_time *out, int cap, int *count);
 // Rebuilds level 0 of the last hmfem_assemble grid (same K, faces and
 // boundary types) with the karst / well exchange terms: KI, WI in the
 // diagonal, WI*pw in the right-hand side (device arrays, nullable).  The

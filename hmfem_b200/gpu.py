@@ -83,8 +83,14 @@ EXPORTS = [
     "hmfem_solve", "hmfem_fluxes", "hmfem_num_levels", "hmfem_level_info",
     "hmfem_level_copy", "hmfem_vcycle", "hmfem_spmv", "hmfem_rhs",
     "hmfem_last_stats", "hmfem_time_kernel", "hmfem_fluxes_noalloc",
-    "hmfem_launch_count",
+    "hmfem_launch_count", "hmfem_profile_iteration",
 ]
+
+
+class KernelTime(C.Structure):
+    """hmfem_kernel_time"""
+    _fields_ = [("name", C.c_char * 96), ("level", C.c_int), ("launches", C.c_int),
+                ("ms", C.c_double)]
 
 NOALLOC_MAX_FACE = 262144  # HMFEM_NOALLOC_MAX_FACE in include/hmfem_gpu.h
 
@@ -127,6 +133,8 @@ def lib():
                                            C.POINTER(C.c_double),
                                            C.POINTER(C.c_double), vp]
         L.hmfem_launch_count.restype = C.c_ulonglong
+        L.hmfem_profile_iteration.argtypes = [vp, ip, C.POINTER(KernelTime), ip,
+                                              C.POINTER(ip)]
         L.compute.argtypes = [vp] * 6
         L.solve_linsys.argtypes = [vp, vp, vp, vp, Dim]
         L.solve_linsys.restype = None
@@ -267,9 +275,28 @@ class Solver:
         _check(self.L.hmfem_last_stats(self.h, C.byref(st)))
         return st.as_dict()
 
+    def profile_iteration(self, iters=3):
+        """Per (kernel, level) launches and summed milliseconds of `iters`
+        CG iterations launched one kernel at a time (hmfem_profile_iteration;
+        level -1 = the CG's level-0 vector work)."""
+        cap = 512
+        buf = (KernelTime * cap)()
+        cnt = C.c_int()
+        _check(self.L.hmfem_profile_iteration(self.h, iters, buf, cap, C.byref(cnt)))
+        return [dict(kernel=buf[i].name.decode(), level=buf[i].level,
+                     launches=buf[i].launches, ms=buf[i].ms)
+                for i in range(min(cnt.value, cap))]
+
     # -- inspection ------------------------------------------------------
     def num_levels(self):
         return self.L.hmfem_num_levels(self.h)
+
+    def level_info(self, l):
+        """(rows, nonzeros, P nonzeros) of level l, without copying it."""
+        n, nnz, pnnz = C.c_int(), C.c_long(), C.c_long()
+        _check(self.L.hmfem_level_info(self.h, l, C.byref(n), C.byref(nnz),
+                                       C.byref(pnnz)))
+        return n.value, nnz.value, pnnz.value
 
     def level(self, l):
         n, nnz, pnnz = C.c_int(), C.c_long(), C.c_long()

@@ -191,8 +191,9 @@ int hmfem_set_stencil(hmfem_solver *s, int nx, int ny, int nz,
                       const double *b, int mem);
 /* AMG hierarchy on the device (structure bit-exact with amg.h). */
 int hmfem_setup(hmfem_solver *s);
-/* Solve A x = b (b NULL: the assembled right-hand side); x = initial guess
- * in, solution out. */
+/* Solve A x = b; x = initial guess in, solution out.  A b passed here
+ * replaces the solver's right-hand side; b NULL solves with the current one
+ * (the assembled or set right-hand side, or the last b passed here). */
 int hmfem_solve(hmfem_solver *s, const double *b, double *x, int mem,
                 hmfem_stats *st);
 /* Face fluxes (flux_reconstruction.c:9-279) into n ELE (c untouched) and the
@@ -215,6 +216,20 @@ int hmfem_last_stats(hmfem_solver *s, hmfem_stats *st);
  * algorithmic bytes per launch. */
 int hmfem_time_kernel(hmfem_solver *s, int which, int level, int reps,
                       float *ms, double *bytes);
+
+/* Measurement: `iters` CG iterations from x = 0 launched one kernel at a
+ * time (no graph), each bracketed by CUDA events on the solver stream;
+ * out[0..min(count, cap)) gets, per kernel and level (-1 = the CG's
+ * level-0 vector work), the launches and their summed duration.  *count =
+ * the number of (kernel, level) pairs.  Overwrites the solver's x. */
+typedef struct {
+    char name[96];
+    int level;
+    int launches;
+    double ms;
+} hmfem_kernel_time;
+int hmfem_profile_iteration(hmfem_solver *s, int iters, hmfem_kernel_time *out,
+                            int cap, int *count);
 
 /* Number of this library's kernels launched so far in the process
  * (graph replays included): a measurement aid. */

@@ -281,6 +281,66 @@ class Ref:
                                   _ptr(v), times, C.byref(rr))
         return x, v, it, rr.value, times
 
+    def job(self, p, eps=1e-10):
+        """The path of solve_all in steps (ref_job_*): assemble() -> setup()
+        -> iterate(k)... -> flux(); one job per process."""
+        return RefJob(self, p, eps)
+
+
+class RefJob:
+    """ref_solve_all's work split into callable parts (for timing the
+    reference in steps).  Keeps the problem's arrays alive."""
+
+    def __init__(self, ref, p, eps):
+        L = ref.L
+        vp = C.c_void_p
+        L.ref_job_new.restype = vp
+        L.ref_job_new.argtypes = [C.c_int] * 3 + [C.c_double] * 4 + [
+            _dp, _dp, _dp, _ip, _dp, C.c_double]
+        for f in ("ref_job_assemble", "ref_job_setup"):
+            getattr(L, f).argtypes = [vp]
+        L.ref_job_iterate.argtypes = [vp, C.c_int]
+        L.ref_job_flux.argtypes = [vp, vp]
+        L.ref_job_result.argtypes = [vp, vp, _dp, C.POINTER(C.c_double)]
+        L.ref_job_free.argtypes = [vp]
+        self.L, self.p = L, p
+        self._bc = np.asarray(p.bc_type, np.int32)
+        self._bv = np.asarray(p.bc_value, np.float64)
+        self.h = L.ref_job_new(p.nx, p.ny, p.nz, p.hx, p.hy, p.hz, p.visc, p.KX, p.KY,
+                               p.KZ, self._bc, self._bv, eps)
+
+    def assemble(self):
+        self.L.ref_job_assemble(self.h)
+
+    def setup(self):
+        self.L.ref_job_setup(self.h)
+
+    def iterate(self, k=-1):
+        """Up to k CG iterations (k < 0: to convergence); True once converged."""
+        return bool(self.L.ref_job_iterate(self.h, k))
+
+    def flux(self, v=None):
+        self.L.ref_job_flux(self.h, None if v is None else _ptr(v))
+
+    def result(self, want_p=True):
+        x = np.zeros(self.p.n) if want_p else None
+        times = np.zeros(5)
+        rr = C.c_double()
+        it = self.L.ref_job_result(self.h, None if x is None else _ptr(x), times,
+                                   C.byref(rr))
+        return x, it, rr.value, times
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ref_job_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
 
 # ---- the coupled conduit model (karst.c, main.c:383-557) ----------------------
 

@@ -340,6 +340,167 @@ int ref_solve_all(int nx, int ny, int nz, double hx, double hy, double hz,
     return iter_amg;
 }
 
+/* ---- the same path in steps (the timed reference arm) -------------------
+ * ref_solve_all's work split so that a caller can time it in parts: the
+ * assembly with the CSR packing, the AMG setup with the CG start, CG
+ * iterations in chunks, the fluxes.  The CG is the loop of compute() mode
+ * 2 above (pcg.h:33-76 with the true-residual test), so a job's result is
+ * ref_solve_all's.  One job per process (the reference's globals). */
+struct RefJob {
+    int nx, ny, nz, bc[6];
+    double hx, hy, hz, visc, eps, val6[6];
+    const double *KX, *KY, *KZ;
+    ELE *pm;
+    IND *ic;
+    double *b, *p;
+    vector<int> cnt, col, nod;
+    vector<double> ele, bv, x, r, s, w;
+    amg_solver<int, double> *amg;
+    linear_operator<int, double> *lin;
+    communicator<int, double> *com;
+    vector_product<int, double> *sca;
+    vector<double> alpha, beta, sigma, sigma_last, tau;
+    int loop, done;
+    double rel, t_asm, t_setup, t_solve, t_flux;
+};
+
+void *ref_job_new(int nx, int ny, int nz, double hx, double hy, double hz, double visc,
+                  const double *KX, const double *KY, const double *KZ, const int *bc,
+                  const double *val6, double eps)
+{
+    RefJob *j = new RefJob();
+    j->nx = nx; j->ny = ny; j->nz = nz; j->hx = hx; j->hy = hy; j->hz = hz;
+    j->visc = visc; j->eps = eps;
+    for (int f = 0; f < 6; f++) { j->bc[f] = bc[f]; j->val6[f] = val6[f]; }
+    j->KX = KX; j->KY = KY; j->KZ = KZ;
+    return j;
+}
+
+/* assembly + RHS (permeabilidade_arestas, source_term) and solve_linsys's
+ * CSR packing (captured by compute() mode 0) */
+int ref_job_assemble(void *job)
+{
+    RefJob *j = (RefJob *)job;
+    double t0 = now();
+    const long n = (long)j->nx * j->ny * j->nz;
+    j->pm = (ELE *)calloc(n + 1, sizeof(ELE));
+    j->ic = (IND *)malloc((n + 1) * sizeof(IND));
+    j->b = create_vector((int)n);
+    j->p = create_vector((int)n);
+    ref_assemble(j->nx, j->ny, j->nz, j->hx, j->hy, j->hz, j->visc, j->KX, j->KY, j->KZ,
+                 j->bc, j->val6, j->pm, j->ic, j->b);
+    g_mode = 0;
+    solve_linsys(j->pm, j->ic, j->b, j->p, N);
+    g_mode = 1;
+    j->cnt.swap(g_cnt);
+    j->col.swap(g_col);
+    j->ele.swap(g_ele);
+    j->t_asm = now() - t0;
+    return 0;
+}
+
+/* amg_solver (compute.cpp:35-38) and the CG start (pcg.h:33-52) */
+int ref_job_setup(void *job)
+{
+    RefJob *j = (RefJob *)job;
+    double t0 = now();
+    const int n = (int)j->cnt.size();
+    j->nod.resize(n);
+    for (int i = 0; i < n; i++) j->nod[i] = i;
+    j->bv.assign(j->b, j->b + n);
+    j->x.assign(n, 0.0);
+    j->com = new communicator<int, double>(j->nod);
+    j->lin = new linear_operator<int, double>(j->cnt, j->col, j->ele);
+    j->sca = new vector_product<int, double>(*j->com);
+    j->amg = new amg_solver<int, double>(j->nod, j->cnt, j->col, j->ele, 16, 1, 0.0, 1.0, true);
+    double t1 = now();
+    j->alpha.assign(1, 1.0); j->beta.assign(1, 0.0); j->sigma.assign(1, 0.0);
+    j->sigma_last.assign(1, 0.0); j->tau.assign(1, 0.0);
+    j->r = j->bv;
+    j->s = j->x;
+    j->w.assign(n, 0.0);
+    (*j->lin)(j->s, j->w);
+    sub_scale(j->r, j->w, j->alpha);
+    (*j->amg)(j->r, j->w);
+    (*j->sca)(j->w, j->r, j->sigma);
+    if (j->sigma[0] < 0.0) j->sigma[0] = fabs(j->sigma[0]);
+    scale_add(j->s, j->w, j->beta);
+    j->sigma_last[0] = j->sigma[0];
+    j->loop = 0;
+    j->rel = true_relres(*j->lin, j->bv, j->x);
+    j->done = !(j->rel > j->eps);
+    j->t_setup = t1 - t0;
+    j->t_solve = now() - t1;
+    return 0;
+}
+
+/* up to k CG iterations (k < 0: to convergence); returns 1 once converged */
+int ref_job_iterate(void *job, int k)
+{
+    RefJob *j = (RefJob *)job;
+    double t0 = now();
+    for (int it = 0; !j->done && (k < 0 || it < k); it++) {
+        if (!(++j->loop < 10000)) { j->done = 1; break; }
+        (*j->lin)(j->s, j->w);
+        (*j->sca)(j->s, j->w, j->tau);
+        if (j->tau[0] < 0.0) j->tau[0] = fabs(j->tau[0]);
+        j->alpha[0] = j->sigma[0] / j->tau[0];
+        add_scale(j->x, j->s, j->alpha);
+        sub_scale(j->r, j->w, j->alpha);
+        (*j->amg)(j->r, j->w);
+        (*j->sca)(j->w, j->r, j->sigma);
+        if (j->sigma[0] < 0.0) j->sigma[0] = fabs(j->sigma[0]);
+        j->beta[0] = j->sigma[0] / j->sigma_last[0];
+        scale_add(j->s, j->w, j->beta);
+        j->sigma_last[0] = j->sigma[0];
+        j->rel = true_relres(*j->lin, j->bv, j->x);
+        if (!(j->rel > j->eps)) j->done = 1;
+    }
+    j->t_solve += now() - t0;
+    return j->done;
+}
+
+/* fluxos + divvel_pontual of the job's pressure into v (n ELE, may be NULL:
+ * then the job keeps its own) */
+int ref_job_flux(void *job, ELE *v_out)
+{
+    RefJob *j = (RefJob *)job;
+    double t0 = now();
+    const int n = (int)j->x.size();
+    for (int i = 0; i < n; i++) j->p[i] = j->x[i];
+    ELE *v = v_out ? v_out : (ELE *)calloc(n + 1, sizeof(ELE));
+    set_grid(j->nx, j->ny, j->nz, j->hx, j->hy, j->hz, j->bc, j->visc);
+    Bound *Bd = make_bound(j->val6);
+    fluxos(j->p, j->pm, v, Bd, h, N);
+    free_bound(Bd);
+    if (!v_out) free(v);
+    j->t_flux = now() - t0;
+    return 0;
+}
+
+/* p_out (n), times [assemble, setup, solve, flux, total]; returns the
+ * iteration count (compute() mode 2's) */
+int ref_job_result(void *job, double *p_out, double *times, double *relres)
+{
+    RefJob *j = (RefJob *)job;
+    if (p_out) for (size_t i = 0; i < j->x.size(); i++) p_out[i] = j->x[i];
+    if (times) {
+        times[0] = j->t_asm; times[1] = j->t_setup; times[2] = j->t_solve;
+        times[3] = j->t_flux;
+        times[4] = j->t_asm + j->t_setup + j->t_solve + j->t_flux;
+    }
+    if (relres) *relres = j->rel;
+    return j->loop;
+}
+
+void ref_job_free(void *job)
+{
+    RefJob *j = (RefJob *)job;
+    delete j->amg; delete j->lin; delete j->sca; delete j->com;
+    free(j->pm); free(j->ic); free(j->b); free(j->p);
+    delete j;
+}
+
 }  // extern "C"
 
 /* ---- the coupled conduit model ------------------------------------------ */

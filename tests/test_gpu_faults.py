@@ -100,21 +100,21 @@ def test_nan_in_right_hand_side_or_guess_gives_breakdown(where, precision):
     s = gpu.Solver(tol=1e-10, precision=precision)
     s.assemble(prob)
     s.setup()
+    _, _, b = Port().assemble(prob)   # the assembled right-hand side
     x = np.zeros(prob.n)
     if where == "x0":
         x[100] = np.nan
         with pytest.raises(gpu.HmfemError) as e:
             s.solve(x=x)
     else:
-        port = Port()
-        _, _, bb = port.assemble(prob)
-        bb = bb.copy()
+        bb = b.copy()
         bb[100] = np.nan
         with pytest.raises(gpu.HmfemError) as e:
-            s.solve(b=bb, x=x)
+            s.solve(b=bb, x=x)   # replaces the solver's right-hand side
     assert e.value.code == gpu.E_BREAKDOWN
+    assert "breakdown" in str(e.value)
     # the hierarchy is intact: the next solve converges
-    x, st = s.solve(x=np.zeros(prob.n))
+    x, st = s.solve(b=b, x=np.zeros(prob.n))
     assert st["status"] == gpu.OK and st["relres"] <= 1e-10
     s.close()
 
