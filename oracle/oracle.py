@@ -300,6 +300,7 @@ class RefJob:
         for f in ("ref_job_assemble", "ref_job_setup"):
             getattr(L, f).argtypes = [vp]
         L.ref_job_iterate.argtypes = [vp, C.c_int]
+        L.ref_job_set_eps.argtypes = [vp, C.c_double]
         L.ref_job_flux.argtypes = [vp, vp]
         L.ref_job_result.argtypes = [vp, vp, _dp, C.POINTER(C.c_double)]
         L.ref_job_free.argtypes = [vp]
@@ -318,6 +319,10 @@ class RefJob:
     def iterate(self, k=-1):
         """Up to k CG iterations (k < 0: to convergence); True once converged."""
         return bool(self.L.ref_job_iterate(self.h, k))
+
+    def set_eps(self, eps):
+        """A new tolerance; iterate() continues the same CG to it."""
+        self.L.ref_job_set_eps(self.h, eps)
 
     def flux(self, v=None):
         self.L.ref_job_flux(self.h, None if v is None else _ptr(v))

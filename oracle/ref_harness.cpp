@@ -460,6 +460,14 @@ int ref_job_iterate(void *job, int k)
     return j->done;
 }
 
+/* a new stopping tolerance: iterate() then continues the same CG to it */
+void ref_job_set_eps(void *job, double eps)
+{
+    RefJob *j = (RefJob *)job;
+    j->eps = eps;
+    j->done = !(j->rel > eps);
+}
+
 /* fluxos + divvel_pontual of the job's pressure into v (n ELE, may be NULL:
  * then the job keeps its own) */
 int ref_job_flux(void *job, ELE *v_out)
