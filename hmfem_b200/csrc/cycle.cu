@@ -8,8 +8,6 @@
 // captured iteration can be replayed past convergence at no cost.
 #include <cstdlib>
 
-#include <cooperative_groups.h>
-
 #include "cycle.cuh"
 
 namespace hm {
@@ -94,25 +92,18 @@ __device__ __forceinline__ T row_acc_r(T t, const int *__restrict__ scol,
     else return row_acc<T, SUB>(t, scol, sval, o, wd, x);
 }
 
-// Vector loads of the row functions below: plain, or through L2 only
-// (ld.global.cg) where other CTAs of the same launch wrote the vector (the
-// tail kernel).  The arithmetic does not depend on the choice.
+// Vector loads of the row functions below (a load policy, so a caller can
+// route them differently without touching the arithmetic).
 struct PlainLd {
     template <class T> __device__ __forceinline__ T operator()(const T *p, long i) const
     {
         return p[i];
     }
 };
-struct CgLd {
-    template <class T> __device__ __forceinline__ T operator()(const T *p, long i) const
-    {
-        return __ldcg(p + i);
-    }
-};
 
 // ---- smoother / transfer row functions ---------------------------------
 // One row (one coarse row for the restriction) of each Chebyshev-level
-// kernel; the kernels below and the coarse-tail kernel run the same code.
+// kernel (the kernels below run these over their grid-stride rows).
 
 template <class T, class M, class LD>
 __device__ __forceinline__ void pre_row(long r, const long long *__restrict__ sptr,
@@ -579,126 +570,6 @@ k_dense_solve(int n, const double *__restrict__ Minv, const T *__restrict__ f,
     }
 }
 
-// ---- the coarse tail of the V-cycle in one launch ------------------------
-//
-// Below some level every Chebyshev kernel of the V-cycle runs on a few
-// thousand rows, and a launch costs more than its work.  The tail kernel
-// runs the whole V-cycle from such a level down -- pre-smoothing, residual,
-// restriction on each level, the coarse solve, then prolongation and
-// post-smoothing back up -- in one launch of one thread-block cluster, with
-// a cluster barrier between phases instead of a kernel boundary.  Each phase
-// is the row function of the corresponding kernel above, over the same rows,
-// so the result is bit-identical to the per-level launches.  Vectors written
-// inside the launch are read through L2 (CgLd); the cluster barrier orders
-// them (release / acquire at cluster scope).
-
-constexpr int kTailThreads = 1024;   // per CTA
-constexpr int kTailCtas = 8;         // one cluster (the portable maximum)
-constexpr int kTailMaxLevels = 12;
-constexpr long kTailRows = 16384;    // rows of the first level the tail may start at
-
-template <class T, class M> struct TailLevel {
-    int n, nc;             // rows; rows of the next level
-    int kind;              // 0 Chebyshev, 1 dense inverse, 2 diagonal solve
-    const long long *sptr;
-    const int *scol;
-    const M *sval;
-    T *f, *ua, *ub, *dx, *rs;
-    const T *dv, *dt;      // smoother (l1) and true diagonal inverses
-    const int *prow, *pcol, *rrow, *rcol;
-    Seed<T> seed_next;     // the next level's seed, written by the restriction
-    const double *dense;   // kind 1: the explicit inverse
-};
-
-template <class T, class M> struct TailArgs {
-    int nl, K;
-    T ith, c1[10], c2[10];
-    TailLevel<T, M> lv[kTailMaxLevels];
-};
-
-template <class T, class M>
-__global__ void __launch_bounds__(kTailThreads, 1)
-k_tail(const __grid_constant__ TailArgs<T, M> a, const Ctl *ctl)
-{
-    PDL_ENTRY();
-    // ctl->done is stable once the previous kernel completed, so every
-    // thread of the cluster takes the same branch
-    if (finished(ctl)) return;
-    namespace cg = cooperative_groups;
-    cg::cluster_group cl = cg::this_cluster();
-    const long tid = (long)cl.block_rank() * blockDim.x + threadIdx.x;
-    const long nth = (long)cl.num_blocks() * blockDim.x;
-    const CgLd ld{};
-    const int K = a.K;
-    int l = 0;
-    // ---- down: pre-smoothing, residual, restriction
-    for (; l < a.nl && a.lv[l].kind == 0; l++) {
-        const TailLevel<T, M> &L = a.lv[l];
-        T *dbuf[2] = {L.ub, L.dx};
-        for (int k = 1; k < K; k++) {
-            for (long i = tid; i < L.n; i += nth) {
-                if (k == 1)
-                    cheb_step_row<T, M, 0>(i, L.sptr, L.scol, L.sval, L.f, L.dv, a.c1[k],
-                                           a.c2[k], dbuf[(k - 1) & 1], dbuf[k & 1], L.rs,
-                                           L.ua, (int)(k == K - 1), ld);
-                else
-                    cheb_step_row<T, M, 2>(i, L.sptr, L.scol, L.sval, L.f, L.dv, a.c1[k],
-                                           a.c2[k], dbuf[(k - 1) & 1], dbuf[k & 1], L.rs,
-                                           L.ua, (int)(k == K - 1), ld);
-            }
-            cl.sync();
-        }
-        for (long i = tid; i < L.n; i += nth)
-            pre_row<T>(i, L.sptr, L.scol, L.sval, L.f, L.ua, L.prow, L.rs, ld);
-        cl.sync();
-        for (long e = tid; e < L.nc; e += nth)
-            restrict_row<T>(e, L.rrow, L.rcol, L.rs, a.lv[l + 1].f, L.seed_next, ld);
-        cl.sync();
-    }
-    // ---- the coarse solve
-    {
-        const TailLevel<T, M> &L = a.lv[l];
-        if (L.kind == 1) {
-            const int lane = threadIdx.x & 31;
-            for (long i = tid >> 5; i < L.n; i += nth >> 5) {
-                const double *row = L.dense + i * (long)L.n;
-                double acc = 0.0;
-                for (int j = lane; j < L.n; j += 32) acc += row[j] * (double)ld(L.f, j);
-                acc = warp_sum(acc);
-                if (lane == 0) L.ua[i] = (T)acc;
-            }
-        } else {
-            using A = Ar<T>;
-            for (long i = tid; i < L.n; i += nth) L.ua[i] = A::mul(L.dt[i], ld(L.f, i));
-        }
-        cl.sync();
-    }
-    // ---- up: prolongation, post-smoothing
-    for (l = l - 1; l >= 0; l--) {
-        const TailLevel<T, M> &L = a.lv[l];
-        for (long i = tid; i < L.n; i += nth)
-            prolong_row<T>(i, L.prow, L.pcol, a.lv[l + 1].ua, L.ua, ld);
-        cl.sync();
-        T *dbuf[2] = {L.ub, L.dx};
-        for (long i = tid; i < L.n; i += nth)
-            cheb0_row<T>(i, L.sptr, L.scol, L.sval, L.f, L.dv, a.ith, L.ua, L.rs, dbuf[0], ld);
-        cl.sync();
-        for (int k = 1; k < K; k++) {
-            for (long i = tid; i < L.n; i += nth) {
-                if (k == 1)
-                    cheb_step_row<T, M, 1>(i, L.sptr, L.scol, L.sval, L.f, L.dv, a.c1[k],
-                                           a.c2[k], dbuf[(k - 1) & 1], dbuf[k & 1], L.rs,
-                                           L.ua, (int)(k == K - 1), ld);
-                else
-                    cheb_step_row<T, M, 2>(i, L.sptr, L.scol, L.sval, L.f, L.dv, a.c1[k],
-                                           a.c2[k], dbuf[(k - 1) & 1], dbuf[k & 1], L.rs,
-                                           L.ua, (int)(k == K - 1), ld);
-            }
-            if (k < K - 1 || l > 0) cl.sync();
-        }
-    }
-}
-
 // ---- CG kernels ---------------------------------------------------------
 
 // r = b - A x; rr = (r,r); bb = (b,b)
@@ -962,121 +833,6 @@ static void with_vals(Solver &s, const Sell &S, int l, F fn)
     } else fn(S.val32);
 }
 
-// ---- the coarse tail (k_tail) -------------------------------------------
-
-int g_tail = [] {
-    const char *e = getenv("HMFEM_TAIL");   // 0: per-level launches throughout
-    return e ? atoi(e) : 1;
-}();
-
-// level l's SELL values in the storage with_vals picks, if that is M
-template <class T, class M>
-static const M *vals_as(Solver &s, int l)
-{
-    const Sell &S = s.lv[l].S;
-    const void *v;
-    if constexpr (std::is_same<T, double>::value) v = S.val;
-    else if (s.use_bf16(l)) v = S.pk ? (const void *)S.pk : (const void *)S.val16;
-    else v = S.val32;
-    bool same;
-    if constexpr (std::is_same<T, double>::value) same = std::is_same<M, double>::value;
-    else if (s.use_bf16(l))
-        same = S.pk ? std::is_same<M, Pk16>::value : std::is_same<M, __nv_bfloat16>::value;
-    else same = std::is_same<M, float>::value;
-    return same ? (const M *)v : nullptr;
-}
-
-// The tail's arguments from level l down, or false when the levels do not
-// qualify: Chebyshev levels on SELL in one storage type, ending in the
-// dense or diagonal coarse solve, the first of at most kTailRows rows.
-template <class T, class M>
-static bool tail_args(Solver &s, int l, TailArgs<T, M> &a)
-{
-    const int last = s.nlevels - 1;
-    if (l < 1 || l >= last || l == s.direct_level || s.lv[l].A.n > kTailRows) return false;
-    const int K = s.opt.cheb_degree;
-    if (K < 1 || K > 9) return false;
-    const ChebCoef cc = cheb_coef(K);
-    memset(&a, 0, sizeof(a));
-    a.K = K;
-    a.ith = (T)cc.ith;
-    for (int k = 0; k < 10; k++) {
-        a.c1[k] = (T)cc.c1[k];
-        a.c2[k] = (T)cc.c2[k];
-    }
-    int q = 0;
-    for (int m = l;; m++, q++) {
-        if (q >= kTailMaxLevels) return false;
-        Level &L = s.lv[m];
-        TailLevel<T, M> &d = a.lv[q];
-        d.n = L.A.n;
-        d.f = s.vec_f<T>(m);
-        d.ua = s.vec_ua<T>(m);
-        d.dt = s.vec_dtrue<T>(m);
-        if (m == s.direct_level) {
-            d.kind = 1;
-            d.dense = s.dense_L;
-            break;
-        }
-        if (m == last) {
-            d.kind = 2;
-            break;
-        }
-        if (!L.cheb || L.gs || s.use_g7(m) || s.use_g19(m) || !L.S.sptr || !L.R.rowptr ||
-            !L.P.rowptr)
-            return false;
-        d.kind = 0;
-        d.nc = L.nc;
-        d.sptr = L.S.sptr;
-        d.scol = L.S.col;
-        d.sval = vals_as<T, M>(s, m);
-        if (!d.sval) return false;
-        d.ub = s.vec_ub<T>(m);
-        d.dx = vec_dx<T>(s, m);
-        d.rs = s.vec_rs<T>(m);
-        d.dv = s.vec_dinv<T>(m);
-        d.prow = L.P.rowptr;
-        d.pcol = L.P.col;
-        d.rrow = L.R.rowptr;
-        d.rcol = L.R.col;
-        d.seed_next = seed_of<T>(s, m + 1);
-    }
-    a.nl = q + 1;
-    return true;
-}
-
-template <class T, class M>
-static bool launch_tail(Solver &s, int l, cudaStream_t st, const Ctl *ctl)
-{
-    TailArgs<T, M> a;
-    if (!tail_args<T, M>(s, l, a)) return false;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(kTailCtas);
-    cfg.blockDim = dim3(kTailThreads);
-    cfg.stream = st;
-    cudaLaunchAttribute at[2];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = kTailCtas;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[1].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = g_pdl ? 2 : 1;
-    KRec rec{(const void *)k_tail<T, M>, l, nullptr, nullptr};
-    if (t_kprof) {
-        cudaEventCreate(&rec.e0);
-        cudaEventCreate(&rec.e1);
-        cudaEventRecord(rec.e0, st);
-    }
-    cudaLaunchKernelEx(&cfg, k_tail<T, M>, a, ctl);  // error: cudaGetLastError
-    if (t_kprof) {
-        cudaEventRecord(rec.e1, st);
-        t_kprof->push_back(rec);
-    }
-    return true;
-}
-
 // One V-cycle from level l: f[l] holds the right-hand side, the result is
 // left in cycle_out(l).
 template <class T>
@@ -1113,19 +869,6 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
     if (!seeded && seed_of<T>(s, l).u) {
         launch_pdl(k_seed<T>, nb(n), 256, st, n, f, seed_of<T>(s, l));
         HM_LAUNCHED();
-    }
-    // small Chebyshev levels down to the coarse solve: one launch
-    if (g_tail && !dot && l >= 1 && n <= kTailRows && L.cheb) {
-        bool done = false;
-        with_vals<T>(s, L.S, l, [&](auto vals) {
-            using M = typename std::remove_const<
-                typename std::remove_pointer<decltype(vals)>::type>::type;
-            done = launch_tail<T, M>(s, l, st, ctl);
-        });
-        if (done) {
-            HM_LAUNCHED();
-            return HMFEM_OK;
-        }
     }
     const bool g7 = s.use_g7(l), g19 = s.use_g19(l);
     const bool bf16 = !std::is_same<T, double>::value && s.use_bf16(l);
