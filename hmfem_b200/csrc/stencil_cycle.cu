@@ -97,16 +97,38 @@ template <class V> struct G19v {
 // chunks (five in FP64, ten in FP32: two rounds of gathers) so the gathers
 // overlap without holding all 19 in registers; the summation order is
 // unchanged.
+// BF16 coefficients of level 1 are stored four per 8-byte word: in slice t
+// (rows 32t..32t+31), word j of row 32t + l holds coefficients 4j..4j+3 at
+// ((5t + j) * 32 + l) (coefficient 19 is a zero pad), so a row's 19
+// coefficients are five 8-byte loads, all issued before the gathers.
+constexpr int kG19Words = 5;
+__host__ __device__ __forceinline__ long long g19q_at(long long r, int q)
+{
+    return (((r >> 5) * kG19Words + (q >> 2)) * 32 + (r & 31)) * 4 + (q & 3);
+}
+__host__ __device__ __forceinline__ long long g19q_len(long long n)
+{
+    return ((n + 31) >> 5) * (long long)kG19Words * 32 * 4;
+}
+
 template <class T, bool SUB, class V, class X>
 __device__ __forceinline__ T g19_row(T t, const G19v<V> &g, int c, X x)
 {
     using A = Ar<T>;
     constexpr int CH = sizeof(T) == 8 ? 5 : 10;
+    constexpr bool Q4 = std::is_same<V, __nv_bfloat16>::value;
     const unsigned cu = (unsigned)c;
     const unsigned row = (unsigned)__umul64hi(cu, g.mhx);
     const unsigned k = (unsigned)__umul64hi(row, g.mny), j = row - k * (unsigned)g.ny;
     const bool odd = ((j + k) & 1) != 0;
     const int last = g.n - 1;
+    uint2 wq[kG19Words];
+    if constexpr (Q4) {
+        const uint2 *w = reinterpret_cast<const uint2 *>(g.v) +
+                         (long long)(cu >> 5) * (kG19Words * 32) + (cu & 31);
+#pragma unroll
+        for (int jw = 0; jw < kG19Words; jw++) wq[jw] = __ldg(w + jw * 32);
+    }
 #pragma unroll
     for (int q0 = 0; q0 < kQ19; q0 += CH) {
         T a[CH], xv[CH];
@@ -114,7 +136,13 @@ __device__ __forceinline__ T g19_row(T t, const G19v<V> &g, int c, X x)
         for (int d = 0; d < CH; d++) {
             const int q = q0 + d;
             if (q < kQ19) {
-                a[d] = (T)ld(g.v, slice_at(c, q, kQ19));
+                if constexpr (Q4) {
+                    // BF16 -> FP32 exactly (the bits of the upper half)
+                    const unsigned wv = (q & 2) ? wq[q >> 2].y : wq[q >> 2].x;
+                    a[d] = (T)__uint_as_float((q & 1) ? (wv & 0xffff0000u) : (wv << 16));
+                } else {
+                    a[d] = (T)ld(g.v, slice_at(c, q, kQ19));
+                }
                 int e = c + (odd ? g.dq[1][q] : g.dq[0][q]);
                 e = e < 0 ? 0 : (e > last ? last : e);
                 xv[d] = x(e);
@@ -571,6 +599,19 @@ __global__ void k_g19_cast(const double *__restrict__ v, long m, D *out)
     GRID_STRIDE(t, m) cvt(v[t], out + t);
 }
 
+// the BF16 copy in the four-per-word layout (g19q_at); rows past n and the
+// pad coefficient are zero
+__global__ void k_g19_cast16(const double *__restrict__ v, long n, __nv_bfloat16 *out)
+{
+    const long m = g19q_len(n);
+    GRID_STRIDE(t, m) {
+        const long r = ((t >> 2) / (kG19Words * 32)) * 32 + ((t >> 2) & 31);
+        const int q = (int)((((t >> 2) >> 5) % kG19Words) * 4 + (t & 3));
+        out[t] = (r < n && q < kQ19) ? __float2bfloat16((float)v[slice_at(r, q, kQ19)])
+                                     : __float2bfloat16(0.0f);
+    }
+}
+
 int nb(long n)
 {
     long b = ceil_div(n, 256);
@@ -670,9 +711,10 @@ int g19_lowp(Grid19 &g, int n, bool f32, bool bf16, cudaStream_t st)
         HM_LAUNCHED();
     }
     if (bf16 && !g.v16) {
-        g.v16 = (__nv_bfloat16 *)dalloc(sizeof(__nv_bfloat16) * m);
+        const long m16 = (long)g19q_len(n);
+        g.v16 = (__nv_bfloat16 *)dalloc(sizeof(__nv_bfloat16) * m16);
         if (!g.v16) return HMFEM_E_CUDA;
-        k_g19_cast<__nv_bfloat16><<<nb(m), 256, 0, st>>>(g.v, m, g.v16);
+        k_g19_cast16<<<nb(m16), 256, 0, st>>>(g.v, n, g.v16);
         HM_LAUNCHED();
     }
     return HMFEM_OK;
