@@ -642,13 +642,30 @@ k_update(int n, double *__restrict__ x, double *__restrict__ r,
     if (finished(ctl)) return;
     const double al = ctl->alpha;
     double rr = 0.0;
-    GRID_STRIDE(i, n) {
-        x[i] = dadd(x[i], dmul(s[i], al));
-        double ri = dsub(r[i], dmul(v[i], al));
-        r[i] = ri;
-        sd.put(i, ri);
-        dm.put(i, ri);
-        rr += ri * ri;
+    // two cells per thread with 16-byte loads and stores (more bytes in
+    // flight per load); the same operations per cell
+    auto cell = [&](long i, double xi, double si, double ri, double vi, double &xo,
+                    double &ro) {
+        xo = dadd(xi, dmul(si, al));
+        ro = dsub(ri, dmul(vi, al));
+        sd.put(i, ro);
+        dm.put(i, ro);
+        rr += ro * ro;
+    };
+    GRID_STRIDE(h, (long)n >> 1) {
+        const double2 xv = reinterpret_cast<const double2 *>(x)[h];
+        const double2 sv = reinterpret_cast<const double2 *>(s)[h];
+        const double2 rv = reinterpret_cast<const double2 *>(r)[h];
+        const double2 vv = reinterpret_cast<const double2 *>(v)[h];
+        double2 xo, ro;
+        cell(2 * h, xv.x, sv.x, rv.x, vv.x, xo.x, ro.x);
+        cell(2 * h + 1, xv.y, sv.y, rv.y, vv.y, xo.y, ro.y);
+        reinterpret_cast<double2 *>(x)[h] = xo;
+        reinterpret_cast<double2 *>(r)[h] = ro;
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const long i = n - 1;
+        cell(i, x[i], s[i], r[i], v[i], x[i], r[i]);
     }
     grid_reduce_sum(rr, part, &ctl->tickets[RED_RR], [&](double t) {
         ctl->rr = t;
@@ -667,10 +684,24 @@ k_sdir(int n, double *__restrict__ s, const T *__restrict__ z, Ctl *ctl)
     PDL_ENTRY();
     if (finished(ctl)) return;
     const double be = ctl->beta;
+    // two cells per thread, 16-byte accesses to s (same operations per cell)
+    using Z2 = typename std::conditional<std::is_same<T, double>::value, double2, float2>::type;
     if (be == 0.0) {
-        GRID_STRIDE(i, n) s[i] = (double)z[i];
+        GRID_STRIDE(h, (long)n >> 1) {
+            const Z2 zv = reinterpret_cast<const Z2 *>(z)[h];
+            reinterpret_cast<double2 *>(s)[h] = make_double2((double)zv.x, (double)zv.y);
+        }
     } else {
-        GRID_STRIDE(i, n) s[i] = dadd(dmul(s[i], be), (double)z[i]);
+        GRID_STRIDE(h, (long)n >> 1) {
+            const Z2 zv = reinterpret_cast<const Z2 *>(z)[h];
+            const double2 sv = reinterpret_cast<const double2 *>(s)[h];
+            reinterpret_cast<double2 *>(s)[h] = make_double2(
+                dadd(dmul(sv.x, be), (double)zv.x), dadd(dmul(sv.y, be), (double)zv.y));
+        }
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const long i = n - 1;
+        s[i] = be == 0.0 ? (double)z[i] : dadd(dmul(s[i], be), (double)z[i]);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->sigma_last = ctl->sigma;
 }
@@ -697,21 +728,8 @@ k_finish_z(int n, const T *__restrict__ src, const double *__restrict__ r,
     double *p2 = part + kRedBlocks;
     if (flexible && !first)
         grid_reduce_sum(d2, p2, &ctl->tickets[RED_A], [&](double t) { ctl->rz_old = t; });
-    grid_reduce_sum(d1, part, &ctl->tickets[RED_SIGMA], [&](double s) {
-        if (!(s == s) || isinf(s)) { ctl->status = HMFEM_E_BREAKDOWN; ctl->done = 1; }
-        if (!flexible && s < 0.0) s = fabs(s);   // pcg.h:47, 68
-        if (first) {
-            ctl->sigma_first = s == 0.0 ? 1.0 : fabs(s);
-            ctl->sigma_last = s;
-            ctl->beta = 0.0;
-        } else if (flexible) {
-            ctl->beta = -ctl->rz_old / ctl->tau;
-        } else {
-            ctl->beta = s / ctl->sigma_last;
-        }
-        ctl->sigma = s;
-        if (ctl->stop_rule == 1 && fabs(s) / ctl->sigma_first <= ctl->tol2) ctl->done = 1;
-    });
+    grid_reduce_sum(d1, part, &ctl->tickets[RED_SIGMA],
+                    [&](double s) { zdots_finish(ctl, s, first, flexible); });
 }
 
 __global__ void k_demote(int n, const double *__restrict__ r, float *__restrict__ f,
@@ -862,6 +880,15 @@ static int cycle_t(Solver &s, int l, cudaStream_t st, bool dot, bool seeded)
         HM_CHECK((g7_sred<T>(L, f, d0, s.vec_f<T>(1), seed_of<T>(s, 1), ctl, st)));
         HM_CHECK(cycle_t<T>(s, 1, st, false, true));
         t_klevel = l;
+        if constexpr (std::is_same<T, float>::value) {
+            if (s.fuse_zdots) {
+                bool fused = false;
+                HM_CHECK((g7_sprol_zd<T>(L, f, d0, cycle_out<T>(s, 1), ub, s.r, s.v, s.ctl,
+                                         s.part, s.first_sigma, &fused, st)));
+                s.zdots_done = fused;
+                return HMFEM_OK;
+            }
+        }
         HM_CHECK((g7_sprol<T>(L, f, d0, cycle_out<T>(s, 1), ub, ctl, st)));
         return HMFEM_OK;
     }
@@ -1081,12 +1108,20 @@ int cg_precondition(Solver &s, cudaStream_t st)
         }
         return HMFEM_OK;
     }
-    // f32 and its seed were written by the kernel that produced r
-    HM_CHECK(cycle_fp32(s, 0, st, false, true));
+    // f32 and its seed were written by the kernel that produced r; the
+    // level-0 prolongation of the exact reduction forms the dots of z
+    // itself where it can (fuse_zdots), else k_finish_z does
+    s.fuse_zdots = true;
+    s.zdots_done = false;
+    const int rc = cycle_fp32(s, 0, st, false, true);
+    s.fuse_zdots = false;
+    HM_CHECK(rc);
     t_klevel = -1;
-    launch_pdl(k_finish_z<float>, nb(n), 256, st, n, cg_z32(s), s.r, s.v,
-               (double *)nullptr, s.ctl, s.part, s.first_sigma, 1);
-    HM_LAUNCHED();
+    if (!s.zdots_done) {
+        launch_pdl(k_finish_z<float>, nb(n), 256, st, n, cg_z32(s), s.r, s.v,
+                   (double *)nullptr, s.ctl, s.part, s.first_sigma, 1);
+        HM_LAUNCHED();
+    }
     return HMFEM_OK;
 }
 

@@ -133,6 +133,27 @@ __device__ __forceinline__ void sigma_finish(Ctl *ctl, double s, int first)
     if (ctl->stop_rule == 1 && s / ctl->sigma_first <= ctl->tol2) ctl->done = 1;
 }
 
+// sigma = (z, r) of the CG's preconditioned residual z (and, flexible,
+// rz = (z, A s_old)): breakdown test, beta, the reference stop rule; run by
+// the last block of the reduction (k_finish_z, and the level-0
+// prolongation that forms z when it does the dots itself).
+__device__ __forceinline__ void zdots_finish(Ctl *ctl, double s, int first, int flexible)
+{
+    if (!(s == s) || isinf(s)) { ctl->status = HMFEM_E_BREAKDOWN; ctl->done = 1; }
+    if (!flexible && s < 0.0) s = fabs(s);   // pcg.h:47, 68
+    if (first) {
+        ctl->sigma_first = s == 0.0 ? 1.0 : fabs(s);
+        ctl->sigma_last = s;
+        ctl->beta = 0.0;
+    } else if (flexible) {
+        ctl->beta = -ctl->rz_old / ctl->tau;
+    } else {
+        ctl->beta = s / ctl->sigma_last;
+    }
+    ctl->sigma = s;
+    if (ctl->stop_rule == 1 && fabs(s) / ctl->sigma_first <= ctl->tol2) ctl->done = 1;
+}
+
 // alpha = sigma / (s, A s) after the CG's SpMV (pcg.h:59-63)
 __device__ __forceinline__ void tau_finish(Ctl *ctl, double t)
 {

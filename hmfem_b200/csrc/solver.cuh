@@ -38,6 +38,10 @@ struct Solver {
 
     // CG state
     double *x = nullptr, *r = nullptr, *s = nullptr, *v = nullptr, *z = nullptr;
+    // set while the CG applies the FP32 V-cycle: the level-0 prolongation
+    // of the exact reduction then also forms (z, r), (z, v) and beta
+    bool fuse_zdots = false;
+    bool zdots_done = false;
     Ctl *ctl = nullptr;
     Ctl ctl_init{};  // host copy of the control block a solve starts from
     Ctl *ctl_host = nullptr;  // pinned, 2 slots
@@ -117,6 +121,12 @@ int g7_sred(const Level &L, const T *f, const T *dinv, T *fc, Seed<T> sd, const 
 template <class T>
 int g7_sprol(const Level &L, const T *f, const T *dinv, const T *uc, T *z, const Ctl *ctl,
              cudaStream_t st);
+// g7_sprol that, where it runs as one thread per C/F pair (nx even), also
+// forms the CG's (z, r), (z, v) and beta (*fused = true)
+template <class T>
+int g7_sprol_zd(const Level &L, const T *f, const T *dinv, const T *uc, T *z,
+                const double *r, const double *v, Ctl *ctl, double *part, int first,
+                bool *fused, cudaStream_t st);
 template <class T, class V, bool DOT>
 int g7_post(const Level &L, const T *f, const T *dinv, T w, const T *u, T *uo, Ctl *ctl,
              double *part, int first, cudaStream_t st);

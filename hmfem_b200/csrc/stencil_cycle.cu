@@ -398,6 +398,46 @@ k_g7_sprol2(G7v<V> g, const T *__restrict__ f, const T *__restrict__ dinv,
     }
 }
 
+// k_g7_sprol2 that also forms the CG's dots of the z it writes: sigma =
+// (z, r) and, after the first application, (z, v) with v = A s_old; the
+// last block derives beta (zdots_finish, flexible CG) -- the work of
+// k_finish_z, without reading z again.
+template <class T, class V>
+__global__ void __launch_bounds__(256)
+k_g7_sprol2_zd(G7v<V> g, const T *__restrict__ f, const T *__restrict__ dinv,
+               const T *__restrict__ uc, T *__restrict__ z, const double *__restrict__ r,
+               const double *__restrict__ v, Ctl *ctl, double *part, int first)
+{
+    PDL_ENTRY();
+    if (finished(ctl)) return;
+    const long npair = (long)g.nx * g.ny * g.nz / 2;
+    double d1 = 0.0, d2 = 0.0;
+    GRID_STRIDE(t, npair) {
+        const long s0 = 2 * t;
+        int i0, j, k;
+        cell_ijk((unsigned)s0, g.nx, g.ny, i0, j, k);
+        const bool c_first = ((j + k) & 1) == 0;
+        const long sc = c_first ? s0 : s0 + 1, sf = c_first ? s0 + 1 : s0;
+        const int fi = c_first ? i0 + 1 : i0;
+        const T zc = uc[sc >> 1];
+        const T zf = g7_fsolve<T>(g, sf, fi, j, k, f, dinv, uc, [](long q) { return q >> 1; });
+        z[sc] = zc;
+        z[sf] = zf;
+        const double z0 = (double)(c_first ? zc : zf), z1 = (double)(c_first ? zf : zc);
+        d1 += z0 * r[s0];
+        d1 += z1 * r[s0 + 1];
+        if (!first) {
+            d2 += z0 * v[s0];
+            d2 += z1 * v[s0 + 1];
+        }
+    }
+    double *p2 = part + kRedBlocks;
+    if (!first)
+        grid_reduce_sum(d2, p2, &ctl->tickets[RED_A], [&](double t) { ctl->rz_old = t; });
+    grid_reduce_sum(d1, part, &ctl->tickets[RED_SIGMA],
+                    [&](double s) { zdots_finish(ctl, s, first, 1); });
+}
+
 // any nx: a thread per cell, coarse ids from cid
 template <class T, class V>
 __global__ void __launch_bounds__(256)
@@ -817,6 +857,25 @@ int g7_spmv_dot(const Level &L, const double *x, double *y, Ctl *ctl, double *pa
     HM_LAUNCHED();
     return HMFEM_OK;
 }
+
+template <class T>
+int g7_sprol_zd(const Level &L, const T *f, const T *dinv, const T *uc, T *z,
+                const double *r, const double *v, Ctl *ctl, double *part, int first,
+                bool *fused, cudaStream_t st)
+{
+    *fused = false;
+    if (L.g7.nx % 2 != 0) return g7_sprol<T>(L, f, dinv, uc, z, ctl, st);
+    const G7v<T> gv = g7v<T>(L.g7);
+    const long npair = (long)L.A.n / 2;
+    const int nblk = occ_blocks((const void *)k_g7_sprol2_zd<T, T>, npair, 256, kRedBlocks);
+    launch_pdl(k_g7_sprol2_zd<T, T>, nblk, 256, st, gv, f, dinv, uc, z, r, v, ctl, part, first);
+    HM_LAUNCHED();
+    *fused = true;
+    return HMFEM_OK;
+}
+template int g7_sprol_zd<float>(const Level &, const float *, const float *, const float *,
+                                float *, const double *, const double *, Ctl *, double *, int,
+                                bool *, cudaStream_t);
 
 int g7_resid(const Level &L, const double *b, const double *x, double *r, Ctl *ctl,
              double *part, int init, Seed<double> sd, Demote dm, cudaStream_t st)
