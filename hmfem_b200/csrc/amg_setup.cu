@@ -29,7 +29,7 @@ namespace hm {
 
 namespace {
 
-constexpr int kMisTile = 256;
+constexpr int kMisTile = 1024;
 constexpr long long kMaxPolls = 1ll << 22;
 
 // The poll limit of the split's bounded wait: kMaxPolls, or lower when the
@@ -43,32 +43,53 @@ long long split_poll_limit()
     return v < 0 ? 0 : (v < kMaxPolls ? v : kMaxPolls);
 }
 
+// The greedy split in natural order (node_selection, amg.h:1-226 with
+// eps = 0): row v is C when every lower neighbour is F, F as soon as one is
+// C -- the lexicographically first maximal independent set, so any order of
+// evaluation that respects these dependencies gives the reference's split.
+// Tiles of kMisTile rows are handed out in start order (ticket); a row
+// waits (bounded) only on lower rows, i.e. on its own tile or on tiles that
+// started earlier, so every wait ends.  Decisions inside the tile are
+// exchanged through shared memory (most dependencies are short-range), and
+// written to global memory for the tiles after it.
 __global__ void __launch_bounds__(kMisTile)
 k_lfmis(const int *__restrict__ rowptr, const int *__restrict__ col, int n,
         signed char *sel, unsigned *ticket, int *err, long long max_polls)
 {
     __shared__ int s_tile;
+    __shared__ signed char s_sel[kMisTile];
     if (threadIdx.x == 0) s_tile = (int)atomicAdd(ticket, 1u);
+    s_sel[threadIdx.x] = 0;
     __syncthreads();
-    long v = (long)s_tile * kMisTile + threadIdx.x;
+    const long base = (long)s_tile * kMisTile;
+    const long v = base + threadIdx.x;
     if (v >= n) return;
     volatile signed char *vs = sel;
+    volatile signed char *ss = s_sel;
     volatile int *verr = err;
     const int a = rowptr[v], e = rowptr[v + 1];
     long long polls = 0;
     for (;;) {
-        bool anyC = false, allF = true;
+        bool anyC = false, allF = true, far = false;
         for (int k = a; k < e; k++) {
             int u = col[k];
             if (u >= v) continue;
-            signed char t = vs[u];
+            const bool in_tile = u >= base;
+            signed char t = in_tile ? ss[u - base] : vs[u];
             if (t == 1) { anyC = true; break; }
-            if (t == 0) allF = false;
+            if (t == 0) {
+                allF = false;
+                far |= !in_tile;
+            }
         }
-        if (anyC) { vs[v] = 2; return; }
-        if (allF) { vs[v] = 1; return; }
+        if (anyC || allF) {
+            const signed char d = anyC ? 2 : 1;
+            ss[threadIdx.x] = d;
+            vs[v] = d;
+            return;
+        }
         if (++polls > max_polls || *verr) { atomicExch(err, 1); return; }
-        if (polls > 32) __nanosleep(64);
+        if (far && polls > 32) __nanosleep(64);   // waiting on an earlier tile
     }
 }
 
