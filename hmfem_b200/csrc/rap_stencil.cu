@@ -43,6 +43,36 @@ __device__ __forceinline__ double aval(const int *__restrict__ rowptr,
     return val[rowptr[s] + __popc(pm & ((1u << dir) - 1))];
 }
 
+// The same entries from the level-0 stencil form (Grid7, stencil_cycle.cu):
+// a_cc and the +x, +y, +z couplings of each cell slice-interleaved; the -x
+// coupling of s is the +x coupling of s - 1 and so on.  Setup extracts that
+// form from the CSR values and checks the matrix bitwise symmetric, so every
+// entry is the CSR value bit for bit -- without the row-pointer look-up in
+// front of each load.
+struct CsrA {
+    const int *__restrict__ rowptr;
+    const double *__restrict__ val;
+    __device__ __forceinline__ double operator()(const SG &, long s, unsigned pm, int dir) const
+    {
+        return aval(rowptr, val, s, pm, dir);
+    }
+};
+struct G7A {
+    const double *__restrict__ cf;
+    __device__ __forceinline__ double operator()(const SG &g, long s, unsigned, int dir) const
+    {
+        switch (dir) {
+        case DC: return cf[slice_at(s, 0, 4)];
+        case DR: return cf[slice_at(s, 1, 4)];
+        case DL: return cf[slice_at(s - 1, 1, 4)];
+        case DU: return cf[slice_at(s, 2, 4)];
+        case DD: return cf[slice_at(s - g.nx, 2, 4)];
+        case DT: return cf[slice_at(s, 3, 4)];
+        default: return cf[slice_at(s - g.nxy, 3, 4)];
+        }
+    }
+};
+
 // The 19 coarse offsets of a level-1 row, by slot: 0, +-2e_x, +-2e_y,
 // +-2e_z, then the 12 offsets +-e_a +- e_b.
 __host__ __device__ constexpr int OX(int t)
@@ -166,9 +196,9 @@ __host__ __device__ constexpr int DZ(int d) { return d == DB ? -1 : d == DT ? 1 
 // Slots are numbered as in OX/OY/OZ; every index below is a compile-time
 // constant once the direction loops are unrolled, so acc stays in
 // registers.
+template <class AV>
 __global__ void __launch_bounds__(128)
-k_sg_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
-          const double *__restrict__ val, const double *__restrict__ pw,
+k_sg_fill(SG g, const SGT tb, AV aval, const double *__restrict__ pw,
           const int *__restrict__ cid, const int *__restrict__ crow, int *ccol,
           double *cval, double *g19v, long nc)
 {
@@ -188,7 +218,7 @@ k_sg_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
         for (int aa = 0; aa < 7; aa++) {
             const int e = adir[aa];
             if (!(pmc & (1u << e))) continue;
-            const double a_ce = aval(rowptr, val, s, pmc, e);
+            const double a_ce = aval(g, s, pmc, e);
             if (e == DC) {
                 SG_ADD(0, a_ce);
                 continue;
@@ -225,13 +255,13 @@ k_sg_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
             const long f = s + DX(d) + (long)DY(d) * g.nx + (long)DZ(d) * g.nxy;
             const unsigned pmf = present(g, i + DX(d), j + DY(d), k + DZ(d));
             const double wf = pw[f];
-            const double dg = dmul(aval(rowptr, val, f, pmf, DC), wf);
+            const double dg = dmul(aval(g, f, pmf, DC), wf);
 #pragma unroll
             for (int b2 = 0; b2 < 7; b2++) {
                 if (b2 == DC || !(pmf & (1u << b2))) continue;
                 const int sl = slot_of(DX(d) + DX(b2), DY(d) + DY(b2), DZ(d) + DZ(b2));
                 if (sl < 0) continue;
-                SG_ADD(sl, dmul(dadd(aval(rowptr, val, f, pmf, b2), dg), wf));
+                SG_ADD(sl, dmul(dadd(aval(g, f, pmf, b2), dg), wf));
             }
         }
         // ---- emit in coarse-id order (ascending fine index)
@@ -258,10 +288,11 @@ k_sg_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
 // contraction: diagonal a_cc, minus (a_cf a_cf) / a_ff for each neighbour
 // f of c in row order d,l,r,u,t,b; slot q: minus the sum, in that order of
 // f and then of f's row order, of (a_cf a_fq) / a_ff over the F cells f
-// adjacent to both c and q.
+// adjacent to both c and q.  AV reads level 0's entries (CsrA, or G7A
+// from the stencil form: the same values).
+template <class AV>
 __global__ void __launch_bounds__(128)
-k_schur_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
-             const double *__restrict__ val, const int *__restrict__ cid,
+k_schur_fill(SG g, const SGT tb, AV aval, const int *__restrict__ cid,
              const int *__restrict__ crow, int *ccol, double *cval, double *g19v)
 {
     const long n = (long)((g.nx + 1) >> 1) * g.ny * g.nz;
@@ -274,23 +305,23 @@ k_schur_fill(SG g, const SGT tb, const int *__restrict__ rowptr,
         double out[19];
         unsigned hv = 0;
         double *acc = out;
-        double dsum = aval(rowptr, val, s, pmc, DC);
+        double dsum = aval(g, s, pmc, DC);
         const int adir[6] = {DD, DL, DR, DU, DT, DB};
 #pragma unroll
         for (int aa = 0; aa < 6; aa++) {
             const int e = adir[aa];
             if (!(pmc & (1u << e))) continue;
-            const double a_ce = aval(rowptr, val, s, pmc, e);
+            const double a_ce = aval(g, s, pmc, e);
             const long f = s + DX(e) + (long)DY(e) * g.nx + (long)DZ(e) * g.nxy;
             const unsigned pmf = present(g, i + DX(e), j + DY(e), k + DZ(e));
-            const double a_ff = aval(rowptr, val, f, pmf, DC);
+            const double a_ff = aval(g, f, pmf, DC);
             dsum = dsub(dsum, dmul(a_ce, a_ce) / a_ff);
 #pragma unroll
             for (int b2 = 0; b2 < 7; b2++) {
                 if (b2 == DC || !(pmf & (1u << b2))) continue;
                 const int sl = slot_of(DX(e) + DX(b2), DY(e) + DY(b2), DZ(e) + DZ(b2));
                 if (sl <= 0) continue;  // back to c (its diagonal is above)
-                SG_ADD(sl, dmul(a_ce, aval(rowptr, val, f, pmf, b2)) / a_ff);
+                SG_ADD(sl, dmul(a_ce, aval(g, f, pmf, b2)) / a_ff);
             }
         }
         out[0] = dsum;
@@ -504,13 +535,23 @@ int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,
     out.col = (int *)dalloc(sizeof(int) * (out.nnz > 0 ? out.nnz : 1));
     out.val = (double *)dalloc(sizeof(double) * (out.nnz > 0 ? out.nnz : 1));
     if (!out.col || !out.val) return HMFEM_E_CUDA;
-    if (schur)
-        k_schur_fill<<<nbk(n / 2), 128, 0, st>>>(g, slot_table(g), L.A.rowptr, L.A.val,
+    if (schur && L.g7.cf)
+        k_schur_fill<<<nbk(n / 2), 128, 0, st>>>(g, slot_table(g), G7A{L.g7.cf}, L.cid,
+                                                 out.rowptr, out.col, out.val, g19v);
+    else if (schur)
+        k_schur_fill<<<nbk(n / 2), 128, 0, st>>>(g, slot_table(g), CsrA{L.A.rowptr, L.A.val},
                                                  L.cid, out.rowptr, out.col, out.val, g19v);
     else
-        k_sg_fill<<<nbk(n / 2), 128, 0, st>>>(g, slot_table(g), L.A.rowptr, L.A.val, L.pw,
-                                              L.cid, out.rowptr, out.col, out.val, g19v,
-                                              (long)L.nc);
+    {
+        if (L.g7.cf)
+            k_sg_fill<<<nbk(n / 2), 128, 0, st>>>(g, slot_table(g), G7A{L.g7.cf}, L.pw, L.cid,
+                                                  out.rowptr, out.col, out.val, g19v,
+                                                  (long)L.nc);
+        else
+            k_sg_fill<<<nbk(n / 2), 128, 0, st>>>(g, slot_table(g), CsrA{L.A.rowptr, L.A.val},
+                                                  L.pw, L.cid, out.rowptr, out.col, out.val,
+                                                  g19v, (long)L.nc);
+    }
     HM_LAUNCHED();
     return HMFEM_OK;
 }

@@ -317,6 +317,11 @@ int setup(Solver &s)
     // with the last synchronisation of the setup); the Galerkin levels below
     // an SPD level 0 are SPD
     HM_CUDA(cudaMemsetAsync(s.dwork + 8, 0, sizeof(int), st));
+    // the stencil form of an assembled level 0 first: the exact reduction's
+    // Galerkin level reads its coefficients from it
+    const bool low = s.opt.precision == 1;
+    if (s.have_grid && s.opt.generic_setup == 0)
+        HM_CHECK(g7_build(s.lv[0], s.nx, s.ny, s.nz, low, st, s.dwork));
     for (;;) {
         Level &L = s.lv[l];
         HM_ALLOC(L.dinv, double, L.A.n);
@@ -337,10 +342,6 @@ int setup(Solver &s)
     }
     s.nlevels = l + 1;
     HM_PHASE("setup: hierarchy", st);
-    // structured forms of the two finest levels of an assembled grid
-    const bool low = s.opt.precision == 1;
-    if (s.have_grid && s.opt.generic_setup == 0)
-        HM_CHECK(g7_build(s.lv[0], s.nx, s.ny, s.nz, low, st, s.dwork));
     if (s.schur0_built && !s.use_g7(0)) {
         // the reduction needs the stencil form of level 0 (a bitwise
         // symmetric 7-point matrix, which hmfem_assemble always produces)
