@@ -205,6 +205,18 @@ class Solver:
         except Exception:
             pass
 
+    def _after_torch(self, *arrays):
+        """Orders the solver's stream after torch's current stream when a
+        CUDA tensor is passed (the solver works on its own non-blocking
+        stream; a tensor just written on torch's stream must be complete
+        before the solver reads it).  An event wait, no host synchronisation."""
+        if not any(getattr(a, "is_cuda", False) for a in arrays):
+            return
+        import torch
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream())
+        torch.cuda.ExternalStream(self.stream).wait_event(ev)
+
     def set_stream(self, stream_handle):
         _check(self.L.hmfem_set_stream(self.h, C.c_void_p(stream_handle)))
 
@@ -229,12 +241,14 @@ class Solver:
             arr = (C.c_void_p * 6)(*[_ptr(f)[0] for f in face_vals])
             fv = arr
         self._keep = [KX, KY, KZ, face_vals]
+        self._after_torch(KX, KY, KZ, *(face_vals or ()))
         _check(self.L.hmfem_assemble(self.h, prob.nx, prob.ny, prob.nz, prob.hx,
                                      prob.hy, prob.hz, prob.visc, px, py, pz,
                                      bc, bv, fv, mem))
         self.n = prob.n
 
     def set_matrix(self, cnt, col, ele, b=None):
+        self._after_torch(cnt, col, ele, b)
         pc, mem = _ptr(cnt)
         _check(self.L.hmfem_set_matrix(self.h, len(cnt), len(col), pc,
                                        _ptr(col)[0], _ptr(ele)[0], _ptr(b)[0],
@@ -242,6 +256,7 @@ class Solver:
         self.n = len(cnt)
 
     def set_stencil(self, nx, ny, nz, perm, indcol, b=None):
+        self._after_torch(perm, indcol, b)
         pp, mem = _ptr(perm)
         _check(self.L.hmfem_set_stencil(self.h, nx, ny, nz, pp, _ptr(indcol)[0],
                                         _ptr(b)[0], mem))
@@ -254,6 +269,7 @@ class Solver:
         """Solves in place into x (initial guess in); returns Stats dict."""
         if x is None:
             x = np.zeros(self.n)
+        self._after_torch(b, x)
         pb, _ = _ptr(b)
         px, mem = _ptr(x)
         st = Stats()
@@ -264,6 +280,7 @@ class Solver:
     def fluxes(self, p, v=None):
         if v is None:
             v = np.zeros((self.n, 7))
+        self._after_torch(p, v)
         pp, mem = _ptr(p)
         dmin, dmax = C.c_double(), C.c_double()
         _check(self.L.hmfem_fluxes(self.h, pp, _ptr(v)[0], mem, C.byref(dmin),
@@ -316,12 +333,14 @@ class Solver:
 
     def vcycle(self, f):
         u = np.zeros(len(f)) if isinstance(f, np.ndarray) else f.clone()
+        self._after_torch(f, u)
         pf, mem = _ptr(f)
         _check(self.L.hmfem_vcycle(self.h, pf, _ptr(u)[0], mem))
         return u
 
     def spmv(self, level, x):
         y = np.zeros(len(x)) if isinstance(x, np.ndarray) else x.clone()
+        self._after_torch(x, y)
         px, mem = _ptr(x)
         _check(self.L.hmfem_spmv(self.h, level, px, _ptr(y)[0], mem))
         return y
