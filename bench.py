@@ -421,8 +421,12 @@ def run_ours(args):
     e2e = {"value": world * n * args.steps / e2e_s, "unit": "cells/s",
            "h2d_bytes_per_step": nk * n * 8 + n * 8, "d2h_bytes_per_step": n * 8}
 
+    batched = None if args.no_batch else run_batch(args, world)
+
     # the chosen and plain pressures and fluxes against the reference's
-    # own FP64 solution of the same problem
+    # own FP64 solution of the same problem (waits for its process; the
+    # host-side baselines below run after it, so they do not share cores
+    # with it)
     oracle_error, cpu_full = None, None
     if ref_full is not None:
         cpu_full, ref_p, ref_v = finish_reference_full(ref_full)
@@ -435,10 +439,14 @@ def run_ours(args):
                 oracle_error[name]["relres"] = r["relres"]
             oracle_error["oracle"] = cpu_full.get("oracle")
             del ref_p, ref_v
+    if batched is not None and rank == 0 and world == 1 and not args.no_cpu_baseline:
+        batched["cpu_reference"] = batch_cpu_baseline(args.tol)
+        rate = batched["cpu_reference"].get("processes", {}).get("instances_per_s")
+        if rate:
+            batched["speedup_vs_reference_processes"] = batched["instances_per_s"] / rate
     config1 = None if args.no_config1 else run_config1(args, dev)
     config4 = None if (args.no_guess or model is None) else run_config4(args, dev, model)
 
-    batched = None if args.no_batch else run_batch(args, world)
     coupled = None if args.no_coupled else run_coupled(args, world, rank)
     output = None
     if not args.no_output and rank == 0:
@@ -524,28 +532,81 @@ def run_batch(args, world, n_inst=96):
     from hmfem_b200 import batch as hb
     from hmfem_b200.problem import config_problem
     probs = [config_problem(3, realisation=r) for r in range(n_inst)]
-    opts = dict(schur0=1)   # the level-0 reduction, as the chosen 256^3 variant
-    workers, tune = hb.tune_workers(probs[:16], precision=1, tol=args.tol, options=opts)
+    # the level-0 reduction and BF16 levels, as the chosen 256^3 variant
+    opts = dict(schur0=1, bf16_from=1)
+    driver, workers, tune = hb.tune(probs[:16], precision=1, tol=args.tol, options=opts)
+    run = hb.DRIVERS[driver]
     # warm-up: one untimed pass over the whole batch, so the device memory
     # pool has grown to the batch's working set before the timed pass
-    hb.solve_batch(probs, 1, args.tol, workers=workers, options=opts)
+    run(probs, 1, args.tol, workers=workers, options=opts)
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()
-    res = hb.solve_batch(probs, 1, args.tol, workers=workers, options=opts)
+    res = run(probs, 1, args.tol, workers=workers, options=opts)
     torch.cuda.synchronize()
     wall = max_over_ranks(time.perf_counter() - t0, world)
     secs = np.sort([r[2] for r in res])
     return {"workload": f"config3: {n_inst} uneven instances, n ~ U{{24..96}}^3",
             "cells": int(sum(p.n for p in probs)),
             "instances_per_s": world * n_inst / wall,
-            "wall_s": wall, "workers": workers,
+            "wall_s": wall, "driver": driver, "workers": workers,
             "p50_ms": 1e3 * float(np.percentile(secs, 50)),
             "p99_ms": 1e3 * float(np.percentile(secs, 99)),
             "iterations_mean": float(np.mean([r[1]["iterations"] for r in res])),
+            "iterations_min_max": [int(min(r[1]["iterations"] for r in res)),
+                                   int(max(r[1]["iterations"] for r in res))],
             "max_relres": float(max(r[1]["relres"] for r in res)),
-            "timing": "host wall clock around the batch (host K in, pressure out)",
+            "timing": "host wall clock around the batch (host K in, pressure out); per "
+                      "instance: its assembly + setup + the solve it waited for",
             "tuning": tune}
+
+
+def _ref_instance(args_tuple):
+    """One config-3 instance through the reference's own path (oracle/_ref):
+    assembly + CSR + AMG setup + PCG to the tolerance; its seconds."""
+    r, tol = args_tuple
+    from hmfem_b200.problem import config_problem
+    from oracle.oracle import Ref
+    p = config_problem(3, realisation=r)
+    with _QuietStdout():
+        job = Ref().job(p, eps=tol)
+        t0 = time.perf_counter()
+        job.assemble()
+        job.setup()
+        job.iterate(-1)
+        dt = time.perf_counter() - t0
+        _, it, rel, _ = job.result(want_p=False)
+        job.close()
+    return dt, it, rel
+
+
+def batch_cpu_baseline(tol, n_inst=96, sample=8):
+    """Config 3 on the host with the reference's own code: the first
+    `sample` instances one after another on one core (instances/s, p50/p99
+    of their times), and all n_inst instances on independent processes, one
+    per core (instances/s, core count stated)."""
+    import multiprocessing as mp
+    try:
+        t0 = time.perf_counter()
+        seq = [_ref_instance((r, tol)) for r in range(sample)]
+        t_seq = time.perf_counter() - t0
+        cores = max(1, min(os.cpu_count() or 1, 16))
+        with mp.get_context("spawn").Pool(cores) as pool:
+            pool.map(_ref_instance, [(r, tol) for r in range(cores)])   # warm-up
+            t0 = time.perf_counter()
+            allr = pool.map(_ref_instance, [(r, tol) for r in range(n_inst)])
+            t_par = time.perf_counter() - t0
+    except Exception as e:  # reference build missing
+        return {"unavailable": str(e)}
+    d = np.sort([x[0] for x in seq])
+    return {"kind": "reference",
+            "one_core": {"instances_per_s": sample / t_seq, "cores": 1,
+                         "sample": f"instances 0-{sample - 1} one after another",
+                         "p50_ms": 1e3 * float(np.percentile(d, 50)),
+                         "p99_ms": 1e3 * float(np.percentile(d, 99))},
+            "processes": {"instances_per_s": n_inst / t_par, "cores": cores,
+                          "sample": f"all {n_inst} instances, one process per core",
+                          "max_relres": float(max(x[2] for x in allr))}}
 
 
 class _QuietStdout:

@@ -13,6 +13,7 @@
 namespace hm {
 
 thread_local std::vector<KRec> *t_kprof = nullptr;
+thread_local int t_nopdl = 0;
 thread_local int t_klevel = -1;
 
 int g_pdl = [] {

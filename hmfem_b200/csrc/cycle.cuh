@@ -42,6 +42,9 @@ __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.lau
     } while (0)
 
 extern int g_pdl;  // 0: plain stream order (HMFEM_PDL=0)
+// set while capturing into a conditional node's body (plain stream order
+// there: such bodies hold kernel nodes without programmatic edges)
+extern thread_local int t_nopdl;
 
 // Per-launch timing of the solve phase (hmfem_profile_iteration): while
 // t_kprof is set on a host thread, launch_pdl brackets each of its launches
@@ -73,7 +76,7 @@ inline void launch_pdl(void (*kernel)(KArgs...), int grid, int block, cudaStream
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = g_pdl ? 1 : 0;
+    cfg.numAttrs = (g_pdl && !t_nopdl) ? 1 : 0;
     cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);  // error: cudaGetLastError
     if (t_kprof) {
         cudaEventRecord(rec.e1, st);

@@ -7,6 +7,8 @@
 
 #include <cxxabi.h>
 
+#include <algorithm>
+
 #include "solver.cuh"
 #include "cycle.cuh"
 
@@ -461,6 +463,9 @@ static int ctl_reset(Solver &s, cudaStream_t st)
     return HMFEM_OK;
 }
 
+static int finish_solve(Solver &s, double *x, int mem, cudaStream_t st, cudaEvent_t e0,
+                        cudaEvent_t e1, hmfem_stats *out);
+
 int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out)
 {
     if (!s.setup_done) HM_CHECK(setup(s));
@@ -507,6 +512,17 @@ int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out)
     }
     HM_CUDA(cudaStreamSynchronize(st));
     HM_PHASE("solve: iterations", st);
+    cudaEventDestroy(ev[0]); cudaEventDestroy(ev[1]);
+    return finish_solve(s, x, mem, st, e0, e1, out);
+}
+
+// The end of a solve: the final true residual, x back to the caller, the
+// stats (and a message when the device reported a failure).  e0 marks the
+// start of the solve on st; both events are destroyed here.
+static int finish_solve(Solver &s, double *x, int mem, cudaStream_t st, cudaEvent_t e0,
+                        cudaEvent_t e1, hmfem_stats *out)
+{
+    const int n = s.lv[0].A.n;
     HM_CHECK(cg_final_residual(s, st));
     HM_CUDA(cudaEventRecord(e1, st));
     Ctl ch;
@@ -516,7 +532,6 @@ int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out)
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0); cudaEventDestroy(e1);
-    cudaEventDestroy(ev[0]); cudaEventDestroy(ev[1]);
     s.last.iterations = ch.iters;
     s.last.levels = s.nlevels;
     s.last.status = ch.done ? ch.status : HMFEM_E_NOTCONV;
@@ -541,6 +556,135 @@ int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out)
     }
     if (out) *out = s.last;
     return s.last.status;
+}
+
+// ---- many solvers solved together -----------------------------------------
+//
+// Every member is set up on its own.  Then ONE CUDA graph solves them all,
+// launched once: for each member a conditional WHILE node whose body is one
+// CG iteration of that member (its V-cycle included) followed by a kernel
+// that keeps the loop going while the member's control block is not done;
+// done is set by the member's own kernels (converged, breakdown, or the
+// iteration cap), so every member iterates exactly as long as it needs and
+// its result is the one a solve on its own gives.  The WHILE nodes are
+// independent, so the members' loops run side by side on the GPU.
+
+__global__ void k_while_next(cudaGraphConditionalHandle h, const Ctl *ctl)
+{
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, *(volatile const int *)&ctl->done ? 0u : 1u);
+}
+
+int batch_solve(Solver *const *ss, int m, double *const *x, int mem, hmfem_stats *out)
+{
+    if (m <= 0) return HMFEM_OK;
+    cudaStream_t ms;
+    HM_CUDA(cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking));
+    std::vector<cudaEvent_t> ev(m), ev0(m);
+    int rc = HMFEM_OK;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<cudaStream_t> cs(m, nullptr);
+    auto fail = [&](int r) { if (rc == HMFEM_OK) rc = r; };
+    // ---- every member: x, control block, the CG start on its own stream
+    for (int i = 0; i < m && rc == HMFEM_OK; i++) {
+        Solver &s = *ss[i];
+        set_alloc_context(s.st, s.cache);
+        if (!s.setup_done) { fail(setup(s)); if (rc) break; }
+        const int n = s.lv[0].A.n;
+        if (x && x[i]) { fail(upload(s.x, (const double *)x[i], n, mem, s.st)); }
+        else if (cudaMemsetAsync(s.x, 0, sizeof(double) * n, s.st) != cudaSuccess) fail(HMFEM_E_CUDA);
+        if (rc) break;
+        fail(ctl_reset(s, s.st));
+        if (cudaEventCreate(&ev0[i]) != cudaSuccess) fail(HMFEM_E_CUDA);
+        if (rc) break;
+        cudaEventRecord(ev0[i], s.st);
+        s.ctl_active = true;
+        fail(cg_init(s, s.st));
+        s.ctl_active = false;
+        if (cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) fail(HMFEM_E_CUDA);
+        if (rc) break;
+        cudaEventRecord(ev[i], s.st);
+        if (cudaStreamWaitEvent(ms, ev[i], 0) != cudaSuccess) fail(HMFEM_E_CUDA);
+    }
+    // ---- one graph: a WHILE node per member
+    std::vector<unsigned long long> body_kernels(m, 0);
+    if (rc == HMFEM_OK && cudaGraphCreate(&graph, 0) != cudaSuccess) fail(HMFEM_E_CUDA);
+    for (int i = 0; i < m && rc == HMFEM_OK; i++) {
+        Solver &s = *ss[i];
+        cudaGraphConditionalHandle h;
+        if (cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) !=
+            cudaSuccess) {
+            fail(HMFEM_E_CUDA);
+            break;
+        }
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphAddNode(&node, graph, nullptr, 0, &np) != cudaSuccess) {
+            fail(HMFEM_E_CUDA);
+            break;
+        }
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        if (cudaStreamCreateWithFlags(&cs[i], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamBeginCaptureToGraph(cs[i], body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            fail(HMFEM_E_CUDA);
+            break;
+        }
+        const unsigned long long before = t_nlaunch;
+        t_nopdl = 1;
+        s.ctl_active = true;
+        fail(cg_iteration(s, cs[i]));
+        s.ctl_active = false;
+        t_nopdl = 0;
+        k_while_next<<<1, 32, 0, cs[i]>>>(h, s.ctl);
+        HM_COUNT();
+        body_kernels[i] = t_nlaunch - before;
+        g_nlaunch -= body_kernels[i];  // counted per iteration below
+        cudaGraph_t captured = nullptr;
+        if (cudaStreamEndCapture(cs[i], &captured) != cudaSuccess) fail(HMFEM_E_CUDA);
+    }
+    if (rc == HMFEM_OK && cudaGraphInstantiate(&gexec, graph, 0) != cudaSuccess)
+        fail(HMFEM_E_CUDA);
+    // ---- one launch solves every member
+    if (rc == HMFEM_OK) {
+        if (cudaGraphLaunch(gexec, ms) != cudaSuccess) fail(HMFEM_E_CUDA);
+        if (cudaStreamSynchronize(ms) != cudaSuccess) fail(HMFEM_E_CUDA);
+    }
+    // ---- every member: final residual, x, stats
+    int worst = HMFEM_OK;
+    if (rc == HMFEM_OK) {
+        for (int i = 0; i < m; i++) {
+            Solver &s = *ss[i];
+            set_alloc_context(s.st, s.cache);
+            cudaEvent_t e1;
+            cudaEventCreate(&e1);
+            // the member's stream after the whole replay
+            cudaEvent_t after;
+            cudaEventCreateWithFlags(&after, cudaEventDisableTiming);
+            cudaEventRecord(after, ms);
+            cudaStreamWaitEvent(s.st, after, 0);
+            cudaEventDestroy(after);
+            const int r = finish_solve(s, x ? x[i] : nullptr, mem, s.st, ev0[i], e1,
+                                       out ? out + i : nullptr);
+            ev0[i] = nullptr;
+            g_nlaunch += (unsigned long long)(s.last.iterations + 1) * body_kernels[i];
+            if (r != HMFEM_OK && worst == HMFEM_OK) worst = r;
+        }
+    }
+    for (int i = 0; i < m; i++) {
+        if (ev[i]) cudaEventDestroy(ev[i]);
+        if (ev0[i]) cudaEventDestroy(ev0[i]);
+        if (cs[i]) cudaStreamDestroy(cs[i]);
+    }
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamSynchronize(ms);
+    cudaStreamDestroy(ms);
+    return rc != HMFEM_OK ? rc : worst;
 }
 
 // `iters` CG iterations from x = 0, launched without the graph, each
@@ -1192,6 +1336,24 @@ int hmfem_last_stats(hmfem_solver *h, hmfem_stats *st)
     if (!h || !st) return HMFEM_E_ARG;
     *st = h->s.last;
     return HMFEM_OK;
+}
+
+int hmfem_batch_solve(hmfem_solver *const *solvers, int m, double *const *x, int mem,
+                      hmfem_stats *st)
+{
+    if (m < 0 || (m > 0 && !solvers)) return HMFEM_E_ARG;
+    std::vector<Solver *> ss(m);
+    for (int i = 0; i < m; i++) {
+        if (!solvers[i] || solvers[i]->s.lv.empty()) return HMFEM_E_ARG;
+        for (int j = 0; j < i; j++)
+            if (solvers[j] == solvers[i]) {
+                hm::set_last_error("hmfem_batch_solve: a solver appears twice", __FILE__, __LINE__);
+                return HMFEM_E_ARG;
+            }
+        HM_CHECK(refuse_bad_matrix(solvers[i]->s));
+        ss[i] = &solvers[i]->s;
+    }
+    return hm::batch_solve(ss.data(), m, x, mem, st);
 }
 
 int hmfem_profile_iteration(hmfem_solver *h, int iters, hmfem_kernel_time *out, int cap,

@@ -146,6 +146,7 @@ int g19_spmv(const Level &L, const double *x, double *y, cudaStream_t st);
 int setup(Solver &s);
 int solve(Solver &s, const double *b, double *x, int mem, hmfem_stats *out);
 int profile_iteration(Solver &s, int iters, hmfem_kernel_time *out, int cap, int *count);
+int batch_solve(Solver *const *ss, int m, double *const *x, int mem, hmfem_stats *out);
 // Rebuilds level 0 of the last hmfem_assemble grid (same K, faces and
 // boundary types) with the karst / well exchange terms: KI, WI in the
 // diagonal, WI*pw in the right-hand side (device arrays, nullable).  The

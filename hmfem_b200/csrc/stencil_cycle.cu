@@ -102,10 +102,6 @@ template <class V> struct G19v {
 // ((5t + j) * 32 + l) (coefficient 19 is a zero pad), so a row's 19
 // coefficients are five 8-byte loads, all issued before the gathers.
 constexpr int kG19Words = 5;
-__host__ __device__ __forceinline__ long long g19q_at(long long r, int q)
-{
-    return (((r >> 5) * kG19Words + (q >> 2)) * 32 + (r & 31)) * 4 + (q & 3);
-}
 __host__ __device__ __forceinline__ long long g19q_len(long long n)
 {
     return ((n + 31) >> 5) * (long long)kG19Words * 32 * 4;
@@ -631,7 +627,6 @@ __global__ void k_g7_extract(int nx, int ny, int nz, const int *__restrict__ row
 }
 
 __device__ __forceinline__ void cvt(double v, float *o) { *o = (float)v; }
-__device__ __forceinline__ void cvt(double v, __nv_bfloat16 *o) { *o = __float2bfloat16((float)v); }
 
 template <class D>
 __global__ void k_g19_cast(const double *__restrict__ v, long m, D *out)

@@ -83,7 +83,7 @@ EXPORTS = [
     "hmfem_solve", "hmfem_fluxes", "hmfem_num_levels", "hmfem_level_info",
     "hmfem_level_copy", "hmfem_vcycle", "hmfem_spmv", "hmfem_rhs",
     "hmfem_last_stats", "hmfem_time_kernel", "hmfem_fluxes_noalloc",
-    "hmfem_launch_count", "hmfem_profile_iteration",
+    "hmfem_launch_count", "hmfem_profile_iteration", "hmfem_batch_solve",
 ]
 
 
@@ -135,6 +135,8 @@ def lib():
         L.hmfem_launch_count.restype = C.c_ulonglong
         L.hmfem_profile_iteration.argtypes = [vp, ip, C.POINTER(KernelTime), ip,
                                               C.POINTER(ip)]
+        L.hmfem_batch_solve.argtypes = [C.POINTER(vp), ip, C.POINTER(vp), ip,
+                                        C.POINTER(Stats)]
         L.compute.argtypes = [vp] * 6
         L.solve_linsys.argtypes = [vp, vp, vp, vp, Dim]
         L.solve_linsys.restype = None
@@ -387,6 +389,28 @@ def launch_count() -> int:
 
 def iter_amg() -> int:
     return C.c_int.in_dll(lib(), "iter_amg").value
+
+
+def batch_solve(solvers, xs=None, allow_notconv=False):
+    """hmfem_batch_solve: set-up solvers solved together (one CUDA graph with
+    a branch per solver, replayed until all converged).  xs: per solver the
+    initial guess in / solution out (numpy arrays, or CUDA tensors), or None
+    (zero guesses, nothing returned).  Returns the stats dicts."""
+    L = lib()
+    m = len(solvers)
+    hs = (C.c_void_p * m)(*[s.h for s in solvers])
+    xp, mem = None, 0
+    if xs is not None:
+        ptrs = []
+        for s, x in zip(solvers, xs):
+            s._after_torch(x)
+            pa, mem = _ptr(x)
+            ptrs.append(pa)
+        xp = (C.c_void_p * m)(*ptrs)
+    st = (Stats * m)()
+    rc = L.hmfem_batch_solve(hs, m, xp, mem, st)
+    _check(rc, (OK, E_NOTCONV) if allow_notconv else (OK,))
+    return [st[i].as_dict() for i in range(m)]
 
 
 def fluxes_noalloc(prob, KX, KY, KZ, p, v, stream=None):

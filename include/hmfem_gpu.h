@@ -217,6 +217,16 @@ int hmfem_last_stats(hmfem_solver *s, hmfem_stats *st);
 int hmfem_time_kernel(hmfem_solver *s, int which, int level, int reps,
                       float *ms, double *bytes);
 
+/* Many set-up solvers solved together (batched uneven instances): one
+ * CUDA graph holds one CG iteration of every solver, each on a branch of
+ * its own, and is replayed until every solver has converged; a converged
+ * solver's kernels return at once, so each stops at its own tolerance and
+ * gives the result it gives solved alone.  x[i]: solver i's initial guess
+ * in, solution out (NULL array or entry: zero guess, nothing copied back);
+ * st[i] (nullable) its stats.  Returns the first failing status. */
+int hmfem_batch_solve(hmfem_solver *const *solvers, int m, double *const *x,
+                      int mem, hmfem_stats *st);
+
 /* Measurement: `iters` CG iterations from x = 0 launched one kernel at a
  * time (no graph), each bracketed by CUDA events on the solver stream;
  * out[0..min(count, cap)) gets, per kernel and level (-1 = the CG's
