@@ -8,17 +8,13 @@
 //
 // Forward (and, with flipped / transposed weights, the data gradient) is an
 // implicit GEMM: D[m][n] = sum_tap sum_ci A_tap[m][ci] B_tap[n][ci] with m a
-// run of 128 consecutive cells, n the output channel, A_tap the input at
-// cell m shifted by the tap.  Per tap the 128 x Cin A tile and the Cout x
-// Cin B tile are gathered by the CTA's threads into shared memory in the
-// canonical K-major layout without swizzle (8-row x 16-byte core matrices:
-// element (row r, k) at (k/8)*LBO + r*16 + (k%8)*2 bytes, LBO = rows*16,
-// SBO = 128), then one thread issues Cin/16 tcgen05.mma (M=128, N=Cout,
-// K=16) into a TMEM accumulator of Cout FP32 columns (TMEM lane = row m).
-// Two buffers alternate between taps: the MMAs of tap t run while tap t+1
-// is gathered; tcgen05.commit on a per-buffer mbarrier says when a buffer
-// may be overwritten.  The epilogue reads TMEM with tcgen05.ld (each warp
-// its 32 lanes), adds the bias, applies ReLU and stores BF16.
+// run of 128 cells, n the output channel, A_tap the input at cell m shifted
+// by the tap.  The input of a tile of cells, with its halo, is brought into
+// shared memory once per 16 input channels by TMA and every tap's A operand
+// is a shifted view of it (the layout and the roles are described at
+// k_conv3d); tcgen05.mma (M = 128, N = Cout, K = 16) accumulates in tensor
+// memory and the epilogue reads it with tcgen05.ld, adds the bias, applies
+// ReLU and stores BF16.
 //
 // Weight gradient: D[m = co][n = ci] = sum_cell dY[cell][co] X[cell+off][ci]
 // per tap, the cells being the K dimension: a CTA takes one tap and a range
@@ -28,8 +24,11 @@
 //
 // Every mbarrier wait is bounded: on a timeout the kernel flags err, waits
 // (bounded again) for its MMAs in flight, frees its TMEM and returns.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
+
+#include <mutex>
 
 #include "common.cuh"
 
@@ -156,170 +155,308 @@ __host__ __device__ constexpr int tmem_cols(int n)
 }
 
 // ---- forward / data gradient ----------------------------------------------
-
-// Taps gathered per stage (one barrier and one commit per stage) and
-// whether all 27 taps of the weights stay resident in shared memory.
-template <int CIN, int COUT>
-struct FwdSmem {
-    static constexpr int kStage = (24 * 1024) / (CIN * 256) < 1 ? 1
-                                : (24 * 1024) / (CIN * 256) > 9 ? 9
-                                : (24 * 1024) / (CIN * 256);
-    static constexpr bool kWRes = 27 * COUT * CIN * 2 <= 56 * 1024;
-    static constexpr int kATap = CIN * 256;       // 128 rows x CIN x 2 B
-    static constexpr int kBTap = COUT * CIN * 2;  // COUT rows x CIN x 2 B
-    static constexpr int kA = kStage * kATap;     // one A buffer
-    static constexpr int kB = kWRes ? 27 * kBTap : kStage * kBTap;
-    static constexpr int kBBufs = kWRes ? 1 : 2;
-    static constexpr int kBytes = 2 * kA + kBBufs * kB + 64;
+//
+// A tile is bx x by x bz output cells.  Its input with a one-cell halo,
+// (bx+2) x (by+2) x (bz+2) cells, is copied into shared memory once per
+// 16-channel chunk of the input: halo cell q = xi + W (yi + H zi) (W = bx+2,
+// H = by+2) at byte q*16 of each 8-channel slab, the chunk's two slabs SB
+// bytes apart -- the K-major no-swizzle layout with rows 16 bytes apart, so
+// any 128 consecutive halo cells form an MMA operand (LBO = SB, SBO = 128).
+// An MMA run is 128 consecutive halo positions q0 .. q0+127; the operand of
+// tap (dx, dy, dz) for the run is the same rows shifted by dx + W dy + W H dz,
+// i.e. the run's descriptor with another start address: the 27 taps read the
+// tile that was copied once.  Row mode (bx = 128): a run is one x row of the
+// tile.  Plane mode (bx = nx < 128): the runs of a z plane cover its interior
+// rows in steps of 128 positions; positions on halo columns or beyond the
+// plane are computed and dropped by the epilogue.  The copy of a tile reads
+// (bx+2)(by+2)(bz+2) / (bx by bz) times its cells from L2.
+//
+// Roles (one CTA per SM, persistent over the tiles): lane 0 of warp 4 loads
+// each halo chunk with two TMA tensor copies (box {8 channels, W, H, bz+2}
+// of the input seen as {C, nx, ny, nz}; coordinates outside the grid read
+// zeros, which is the convolution's padding) into a ring of `ns` stages;
+// lane 0 of warp 5 issues, per chunk, 27 taps x runs MMAs of M = 128,
+// N = COUT, K = 16 into the tile's accumulator (runs x COUT FP32 columns of
+// tensor memory, `nb` = 2 buffers when they fit) and commits the stage back
+// to the producer; warps 0-3 read a finished accumulator (tcgen05.ld, warp w
+// lanes 32w..32w+31), add the bias, apply ReLU, store BF16 and release the
+// buffer -- loads, MMAs and the epilogue of different tiles overlap.  The
+// weights of a chunk (two TMA copies of box {8, COUT, 27}: the two 8-channel
+// halves, each [tap][COUT][8]) stay resident with one input chunk; otherwise
+// each stage carries its chunk's weights.  No multicast.
+struct ConvPlan {
+    int bx, by, bz;          // tile (interior cells)
+    int W, H;                // halo row pitch bx+2, halo rows per plane by+2
+    int hc, hcp;             // halo cells; cells per slab with the run overrun (x8)
+    int runs, rp;            // MMA runs per tile; runs per z plane
+    int row_mode;            // 1: bx == 128, one run per x row
+    int ntx, nty, ntz;       // tiles per axis
+    int ns, nb;              // input stages, accumulator buffers
+    int wres;                // weights resident (one input chunk)
+    int tmem_cols;
+    unsigned stage_bytes, wbytes, smem_bytes;
 };
 
-// B tile of one tap into shared memory (K-major: row n = output channel)
-template <int CIN, int COUT>
-__device__ __forceinline__ void stage_weights(const __nv_bfloat16 *__restrict__ w, int tap,
-                                              unsigned char *dst, int tid)
+constexpr int kConvThreads = 192;  // warps 0-3 epilogue, 4 TMA producer, 5 MMA
+constexpr int kEpilogue = 128;
+
+__device__ __forceinline__ void mbar_init_n(uint64_t *m, unsigned count)
 {
-    constexpr int ACH = CIN / 8;
-    const uint4 *wt = (const uint4 *)(w + (long)tap * COUT * CIN);
-    for (int i = tid; i < COUT * ACH; i += 128) {
-        const int row = i / ACH, c = i % ACH;
-        *(uint4 *)(dst + c * (COUT * 16) + row * 16) = wt[row * ACH + c];
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *m)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(m)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *m, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// TMA tensor copies into this CTA's shared memory, completion on an mbarrier
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int c0, int c1,
+                                            int c2, int c3, uint64_t *m)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(m))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, int c0, int c1,
+                                            int c2, uint64_t *m)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(m))
+        : "memory");
+}
+
+// bounded wait that also leaves when another role gave up (abort flag)
+__device__ __forceinline__ bool role_wait(uint64_t *m, unsigned parity, volatile int *abort_flag,
+                                          int *err)
+{
+    for (unsigned i = 0; i < kWaitPolls; i++) {
+        if (mbar_test(m, parity)) return true;
+        if (*abort_flag) return false;
+        if (i > 64) __nanosleep(64);
     }
+    *abort_flag = 1;
+    atomicExch(err, 1);
+    return false;
+}
+
+// first halo position of run r; its plane (0..bz-1) and, in row mode, row
+__device__ __forceinline__ int run_start(const ConvPlan &p, int r, int &plane, int &row)
+{
+    if (p.row_mode) {
+        plane = r / p.by;
+        row = r - plane * p.by;
+        return 1 + p.W * (row + 1) + p.W * p.H * (plane + 1);
+    }
+    plane = r / p.rp;
+    row = -1;
+    return 1 + p.W + p.W * p.H * (plane + 1) + 128 * (r - plane * p.rp);
 }
 
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(128)
-k_conv3d(const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__ w,
+__global__ void __launch_bounds__(kConvThreads, 1)
+k_conv3d(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_w,
          const float *__restrict__ bias, __nv_bfloat16 *__restrict__ out, int nx, int ny,
-         int nz, int relu, int *err)
+         int nz, int relu, const ConvPlan p, int *err)
 {
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 256, "channel counts");
-    extern __shared__ __align__(128) unsigned char smem[];
-    using S = FwdSmem<CIN, COUT>;
-    constexpr int ST = S::kStage;
-    unsigned char *abuf = smem, *bbuf = smem + 2 * S::kA;
-    uint64_t *mbar = (uint64_t *)(smem + 2 * S::kA + S::kBBufs * S::kB);
-    uint32_t *tslot = (uint32_t *)(mbar + 2);
-    constexpr int NCOL = tmem_cols(COUT);
+    constexpr int KC = CIN / 16;
     constexpr uint32_t IDESC = idesc_bf16(128, COUT);
-    constexpr int ACH = CIN / 8;  // 16-byte chunks per row
+    constexpr int WTAP = COUT * 16;       // one tap's rows of one 8-channel half
+    constexpr int WHALF = 27 * WTAP;      // the second half follows all 27 taps of the first
+    extern __shared__ __align__(128) unsigned char smem[];
+    const unsigned SB = (unsigned)p.hcp * 16u, SA = 2u * SB;
+    unsigned char *wres = smem;                    // resident weights (p.wres)
+    unsigned char *stages = smem + p.wbytes;
+    uint64_t *bar = (uint64_t *)(stages + (size_t)p.ns * p.stage_bytes);
+    uint64_t *full = bar, *empty = bar + p.ns, *tfull = bar + 2 * p.ns, *tempty = tfull + p.nb,
+             *drain = tempty + p.nb;
+    uint32_t *tslot = (uint32_t *)(drain + 1);
+    volatile int *abort_flag = (volatile int *)(tslot + 1);
 
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const long nxy = (long)nx * ny, n = nxy * nz;
-    const long ntiles = (n + 127) / 128;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long ntiles = (long)p.ntx * p.nty * p.ntz;
+    const int WH = p.W * p.H;
     if (tid == 0) {
-        mbar_init(&mbar[0]);
-        mbar_init(&mbar[1]);
+        for (int s = 0; s < p.ns; s++) {
+            mbar_init_n(&full[s], 1);
+            mbar_init_n(&empty[s], 1);
+        }
+        for (int b = 0; b < p.nb; b++) {
+            mbar_init_n(&tfull[b], 1);
+            mbar_init_n(&tempty[b], kEpilogue);
+        }
+        mbar_init_n(drain, 1);
+        *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (S::kWRes)  // all taps' weights, once per CTA
-        for (int t = 0; t < 27; t++) stage_weights<CIN, COUT>(w, t, bbuf + t * S::kBTap, tid);
-    if (warp == 0) tmem_alloc(tslot, NCOL);
+    if (warp == 5) tmem_alloc(tslot, p.tmem_cols);
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
     const uint32_t tmem = *tslot;
-    unsigned parity[2] = {0u, 0u};
-    int pending[2] = {0, 0};
-    bool ok = true;
 
-    for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-        const long m = tile * 128 + tid;
-        const bool valid = m < n;
-        const int x = valid ? (int)(m % nx) : 0, y = valid ? (int)((m / nx) % ny) : 0,
-                  z = valid ? (int)(m / nxy) : 0;
-        int stage = 0;
-        for (int t0 = 0; t0 < 27 && ok; t0 += ST, stage++) {
-            const int b = stage & 1;
-            const int nt = 27 - t0 < ST ? 27 - t0 : ST;
-            if (pending[b]) {  // the MMAs that read buffer b are done
-                ok = mbar_wait(&mbar[b], parity[b]);
-                parity[b] ^= 1u;
-                pending[b] = 0;
-                ok = __syncthreads_and(ok);
-                if (!ok) break;
-            }
-            unsigned char *a = abuf + b * S::kA;
-            for (int j = 0; j < nt; j++) {
-                const int tap = t0 + j;
-                const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
-                const int xx = x + dx, yy = y + dy, zz = z + dz;
-                const bool in_grid = valid && xx >= 0 && xx < nx && yy >= 0 && yy < ny &&
-                                     zz >= 0 && zz < nz;
-                const uint4 *src =
-                    (const uint4 *)(in + (xx + (long)yy * nx + (long)zz * nxy) * CIN);
-#pragma unroll
-                for (int c = 0; c < ACH; c++) {
-                    const uint4 v = in_grid ? src[c] : make_uint4(0, 0, 0, 0);
-                    *(uint4 *)(a + j * S::kATap + c * 2048 + tid * 16) = v;
-                }
-                if (!S::kWRes)
-                    stage_weights<CIN, COUT>(w, tap, bbuf + b * S::kB + j * S::kBTap, tid);
-            }
-            fence_async_smem();
-            __syncthreads();
-            if (tid == 0) {
-                tc_after_sync();
-                for (int j = 0; j < nt; j++) {
-                    const int tap = t0 + j;
-                    const uint32_t sa = smem_u32(a + j * S::kATap);
-                    const uint32_t sb = smem_u32(S::kWRes ? bbuf + tap * S::kBTap
-                                                          : bbuf + b * S::kB + j * S::kBTap);
-#pragma unroll
-                    for (int kk = 0; kk < CIN / 16; kk++) {
-                        const uint64_t da = kmajor_desc(sa + kk * 2 * 2048, 2048, 128);
-                        const uint64_t db =
-                            kmajor_desc(sb + kk * 2 * (COUT * 16), COUT * 16, 128);
-                        umma_bf16(tmem, da, db, IDESC, (tap | kk) != 0);
+    if (warp == 4) {
+        // ---- producer: TMA copies of the halo chunks (and weights)
+        if (lane == 0) {
+            unsigned wkc = 0xffffffffu;  // per stage (8 bits each): chunk of its weights
+            long item = 0;
+            bool ok = true;
+            for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                const int tx = (int)(tile % p.ntx), ty = (int)((tile / p.ntx) % p.nty),
+                          tz = (int)(tile / ((long)p.ntx * p.nty));
+                const int x0 = tx * p.bx - 1, y0 = ty * p.by - 1, z0 = tz * p.bz - 1;
+                for (int kc = 0; kc < KC; kc++, item++) {
+                    const int s = (int)(item % p.ns);
+                    const unsigned use = (unsigned)(item / p.ns);
+                    if (!role_wait(&empty[s], (use & 1u) ^ 1u, abort_flag, err)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t a = smem_u32(stages + (size_t)s * p.stage_bytes);
+                    const bool need_w =
+                        p.wres ? item == 0 : ((wkc >> (8 * s)) & 0xffu) != (unsigned)kc;
+                    mbar_expect_tx(&full[s], 32u * (unsigned)p.hc + (need_w ? 2u * WHALF : 0u));
+                    tma_load_4d(a, &tm_in, 16 * kc, x0, y0, z0, &full[s]);
+                    tma_load_4d(a + SB, &tm_in, 16 * kc + 8, x0, y0, z0, &full[s]);
+                    if (need_w) {
+                        const uint32_t wb = p.wres ? smem_u32(wres) : a + SA;
+                        tma_load_3d(wb, &tm_w, 16 * kc, 0, 0, &full[s]);
+                        tma_load_3d(wb + WHALF, &tm_w, 16 * kc + 8, 0, 0, &full[s]);
+                        wkc = (wkc & ~(0xffu << (8 * s))) | ((unsigned)kc << (8 * s));
                     }
                 }
-                umma_commit(&mbar[b]);
             }
-            pending[b] = 1;
-        }
-        if (!ok) break;
-        // the last commit covers every MMA issued before it
-        for (int b = 0; b < 2; b++) {
-            if (pending[b]) {
-                ok = ok && mbar_wait(&mbar[b], parity[b]);
-                parity[b] ^= 1u;
-                pending[b] = 0;
+            // copies still in flight land before the CTA leaves: wait for the
+            // last use of every stage (already complete unless a role gave up)
+            for (int j = 0; j < p.ns && j < item; j++) {
+                const long it = item - 1 - j;
+                if (!mbar_wait(&full[it % p.ns], (unsigned)(it / p.ns) & 1u)) atomicExch(err, 1);
             }
         }
-        ok = __syncthreads_and(ok);
-        if (!ok) break;
-        tc_after_sync();
-        // epilogue: this warp's 32 TMEM lanes = rows 32 warp .. +31
+        __syncwarp();
+    } else if (warp == 5) {
+        // ---- MMA issue (one thread).  Per run the 27 taps are unrolled: the
+        // A descriptor is the run's base plus a per-tap offset held in a
+        // register, the B descriptor the stage's base plus an immediate.
+        if (lane == 0) {
+            int offs[27];
 #pragma unroll
-        for (int c0 = 0; c0 < COUT; c0 += 16) {
-            float v[16];
-            tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + c0, v);
-            if (valid) {
-                __nv_bfloat16 o[16];
+            for (int t = 0; t < 27; t++)
+                offs[t] = (t % 3 - 1) + p.W * ((t / 3) % 3 - 1) + WH * (t / 9 - 1);
+            long item = 0, jt = 0;
+            bool ok = true;
+            for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, jt++) {
+                const int b = (int)(jt % p.nb);
+                const unsigned u = (unsigned)(jt / p.nb);
+                if (!role_wait(&tempty[b], (u & 1u) ^ 1u, abort_flag, err)) break;
+                tc_after_sync();
+                const uint32_t acc0 = tmem + (uint32_t)(b * p.runs * COUT);
+                for (int kc = 0; kc < KC; kc++, item++) {
+                    const int s = (int)(item % p.ns);
+                    const unsigned use = (unsigned)(item / p.ns);
+                    if (!role_wait(&full[s], use & 1u, abort_flag, err)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_after_sync();
+                    const uint32_t a = smem_u32(stages + (size_t)s * p.stage_bytes);
+                    const uint32_t wb = p.wres ? smem_u32(wres) : a + SA;
+                    // descriptor start addresses count 16-byte units: a run's
+                    // operand row q is one unit per position
+                    const uint64_t da0 = kmajor_desc(a, SB, 128);
+                    const uint64_t db0 = kmajor_desc(wb, WHALF, 128);
+                    const uint32_t first = kc == 0 ? 0u : 1u;
+                    // run starts without divisions (the order of run_start)
+                    int plane = 0, j = 0;
+                    for (int r = 0; r < p.runs; r++) {
+                        const int q0 = p.row_mode
+                                           ? 1 + p.W * (j + 1) + WH * (plane + 1)
+                                           : 1 + p.W + WH * (plane + 1) + 128 * j;
+                        if (++j == p.rp) {
+                            j = 0;
+                            plane++;
+                        }
+                        const uint64_t dar = da0 + (uint64_t)q0;
+                        const uint32_t acc = acc0 + (uint32_t)(r * COUT);
 #pragma unroll
-                for (int i = 0; i < 16; i++) {
-                    float t = v[i] + (bias ? bias[c0 + i] : 0.f);
-                    if (relu) t = fmaxf(t, 0.f);
-                    o[i] = __float2bfloat16(t);
+                        for (int t = 0; t < 27; t++)
+                            umma_bf16(acc, dar + (uint64_t)offs[t],
+                                      db0 + (uint64_t)(t * (WTAP / 16)), IDESC,
+                                      t == 0 ? first : 1u);
+                    }
+                    umma_commit(&empty[s]);
                 }
-                uint4 *dst = (uint4 *)(out + m * COUT + c0);
-                dst[0] = *(uint4 *)&o[0];
-                dst[1] = *(uint4 *)&o[8];
+                if (ok) umma_commit(&tfull[b]);
             }
         }
-        tc_before_sync();
-        __syncthreads();
-        tc_after_sync();
+        __syncwarp();
+    } else {
+        // ---- epilogue: warp w reads TMEM lanes 32w .. 32w+31 (rows of a run)
+        const int m = 32 * warp + lane;
+        long jt = 0;
+        for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, jt++) {
+            const int b = (int)(jt % p.nb);
+            const unsigned u = (unsigned)(jt / p.nb);
+            if (!role_wait(&tfull[b], u & 1u, abort_flag, err)) break;
+            tc_after_sync();
+            const int tx = (int)(tile % p.ntx), ty = (int)((tile / p.ntx) % p.nty),
+                      tz = (int)(tile / ((long)p.ntx * p.nty));
+            const int X0 = tx * p.bx - 1, Y0 = ty * p.by - 1, Z0 = tz * p.bz - 1;
+            for (int r = 0; r < p.runs; r++) {
+                int plane, row;
+                const int q = run_start(p, r, plane, row) + m;
+                const int zi = q / WH, rem = q - zi * WH, yi = rem / p.W, xi = rem - yi * p.W;
+                const int gx = X0 + xi, gy = Y0 + yi, gz = Z0 + zi;
+                const bool v = zi == plane + 1 && yi >= 1 && yi <= p.by && xi >= 1 &&
+                               xi <= p.bx && (row < 0 || yi == row + 1) && gx < nx && gy < ny &&
+                               gz < nz;
+                const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16) +
+                                    (uint32_t)((b * p.runs + r) * COUT);
+                __nv_bfloat16 *dst = out + (gx + (long)nx * (gy + (long)ny * gz)) * COUT;
+#pragma unroll
+                for (int c0 = 0; c0 < COUT; c0 += 16) {
+                    float f[16];
+                    tmem_ld16(ta + c0, f);
+                    if (v) {
+                        __nv_bfloat16 o[16];
+#pragma unroll
+                        for (int i = 0; i < 16; i++) {
+                            float t = f[i] + (bias ? __ldg(bias + c0 + i) : 0.f);
+                            if (relu) t = fmaxf(t, 0.f);
+                            o[i] = __float2bfloat16(t);
+                        }
+                        uint4 *d4 = (uint4 *)(dst + c0);
+                        d4[0] = *(uint4 *)&o[0];
+                        d4[1] = *(uint4 *)&o[8];
+                    }
+                }
+            }
+            tc_before_sync();
+            mbar_arrive(&tempty[b]);
+        }
     }
-    if (!ok) {
-        if (tid == 0) atomicExch(err, 1);
-        // MMAs possibly in flight: wait (bounded) before freeing their TMEM
-        for (int b = 0; b < 2; b++)
-            if (pending[b]) mbar_wait(&mbar[b], parity[b]);
+    // teardown: every MMA this CTA issued has completed before TMEM is freed
+    if (warp == 5 && lane == 0) {
+        umma_commit(drain);
+        if (!mbar_wait(drain, 0)) atomicExch(err, 1);
     }
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
-    if (warp == 0) tmem_free(tmem, NCOL);
+    if (warp == 5) tmem_free(tmem, p.tmem_cols);
 }
 
 // ---- weight gradient --------------------------------------------------------
@@ -467,29 +604,142 @@ k_conv3d_wgrad(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restr
     if (warp == 0) tmem_free(tmem, NCOL);
 }
 
+// Tile choice for a forward launch: bx = 128 (row mode) when nx >= 128, else
+// the whole x extent; (by, bz) minimise an estimate of the makespan -- per
+// tile the larger of the MMA operand reads from shared memory (A 4 KB + B
+// 32 COUT B per MMA at ~128 B per clock) and the halo copy, times the tile
+// waves over the SMs -- subject to the tensor-memory columns (runs x COUT,
+// doubled when two accumulators fit in 512) and the shared memory.
+ConvPlan plan_conv(int nx, int ny, int nz, int cin, int cout, int nsm, int smem_max)
+{
+    ConvPlan best{};
+    double best_cost = 1e300;
+    const int kc = cin / 16;
+    const int bx = nx >= 128 ? 128 : nx;
+    const bool row_mode = bx == 128;
+    const int W = bx + 2;
+    const unsigned wchunk = 27u * (unsigned)cout * 32u;
+    const unsigned fixed = 256;  // barriers, TMEM slot, abort flag
+    for (int bz = 1; bz <= (nz < 16 ? nz : 16); bz++)
+        for (int by = 1; by <= (ny < 64 ? ny : 64); by++) {
+            ConvPlan p{};
+            p.bx = bx;
+            p.by = by;
+            p.bz = bz;
+            p.W = W;
+            p.H = by + 2;
+            p.hc = W * p.H * (bz + 2);
+            p.hcp = (p.hc + 128 + 7) / 8 * 8;
+            p.row_mode = row_mode;
+            p.rp = row_mode ? by : (W * (by - 1) + bx + 127) / 128;
+            p.runs = bz * p.rp;
+            if (p.runs * cout > 512) continue;
+            p.nb = 2 * p.runs * cout <= 512 ? 2 : 1;
+            p.wres = kc == 1;
+            p.wbytes = p.wres ? wchunk : 0;
+            p.stage_bytes = 32u * (unsigned)p.hcp + (p.wres ? 0 : wchunk);
+            if ((unsigned)smem_max < fixed + p.wbytes + p.stage_bytes) continue;
+            int ns = (int)(((unsigned)smem_max - fixed - p.wbytes) / p.stage_bytes);
+            p.ns = ns > 4 ? 4 : ns;
+            p.ntx = (nx + bx - 1) / bx;
+            p.nty = (ny + by - 1) / by;
+            p.ntz = (nz + bz - 1) / bz;
+            const long tiles = (long)p.ntx * p.nty * p.ntz;
+            const double mma = (double)p.runs * 27 * kc * (4096.0 + 32.0 * cout) / 128.0;
+            const double load = (double)p.hc * kc + (p.wres ? 0.0 : 27.0 * cout * kc);
+            const double tile_t = (p.ns >= 2 ? (mma > load ? mma : load) : mma + load) +
+                                  (p.nb == 2 ? 0.0 : 4.0 * p.runs * cout) + 400.0;
+            const double cost = (double)((tiles + nsm - 1) / nsm) * tile_t;
+            if (cost < best_cost) {
+                best_cost = cost;
+                best = p;
+            }
+        }
+    best.tmem_cols = 32;
+    while (best.tmem_cols < best.nb * best.runs * cout) best.tmem_cols *= 2;
+    best.smem_bytes = best.wbytes + (unsigned)best.ns * best.stage_bytes + fixed;
+    // one CTA per SM: its tensor-memory allocation may take all 512 columns
+    if (best.smem_bytes < (unsigned)smem_max / 2 + 1024) best.smem_bytes = smem_max / 2 + 1024;
+    return best;
+}
+
+// cuTensorMapEncodeTiled from the driver (no link against libcuda)
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                 const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                 const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// A BF16 tensor map without swizzle: 16-byte aligned base and strides, boxes
+// of box[] elements, zeros outside the tensor.
+int encode_bf16_map(CUtensorMap *map, const void *base, int rank, const cuuint64_t *dims,
+                    const cuuint64_t *strides, const cuuint32_t *box)
+{
+    static EncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiled)f;
+    });
+    if (!fn) {
+        set_last_error("conv3d: cuTensorMapEncodeTiled unavailable", __FILE__, __LINE__);
+        return HMFEM_E_CUDA;
+    }
+    if (((uintptr_t)base & 15u) != 0) {
+        set_last_error("conv3d: tensors must be 16-byte aligned", __FILE__, __LINE__);
+        return HMFEM_E_ARG;
+    }
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank,
+                          const_cast<void *>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_last_error("conv3d: tensor map rejected", __FILE__, __LINE__);
+        return HMFEM_E_ARG;
+    }
+    return HMFEM_OK;
+}
+
 template <int CIN, int COUT>
 int launch_fwd(const void *in, const void *w, const float *bias, void *out, int nx, int ny,
                int nz, int relu, int *err, cudaStream_t st)
 {
-    using S = FwdSmem<CIN, COUT>;
     auto k = k_conv3d<CIN, COUT>;
-    HM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kBytes));
-    HM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    const long n = (long)nx * ny * nz, ntiles = (n + 127) / 128;
-    int per_sm = 0, dev = 0, nsm = 0, smem_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    // resident CTAs: shared memory (1 KB reserved per CTA), 16 per SM at most
-    per_sm = smem_sm / (S::kBytes + 1024);
-    if (per_sm > 16) per_sm = 16;
-    // resident CTAs must also fit the SM's 512 TMEM columns
-    const int tmem_fit = 512 / tmem_cols(COUT);
-    if (per_sm > tmem_fit) per_sm = tmem_fit;
-    long grid = (long)nsm * (per_sm > 0 ? per_sm : 1);
-    if (grid > ntiles) grid = ntiles;
-    k<<<(int)grid, 128, S::kBytes, st>>>((const __nv_bfloat16 *)in, (const __nv_bfloat16 *)w,
-                                         bias, (__nv_bfloat16 *)out, nx, ny, nz, relu, err);
+    int dev = 0, nsm = 0, smem_max = 0;
+    HM_CUDA(cudaGetDevice(&dev));
+    HM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    HM_CUDA(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const ConvPlan p = plan_conv(nx, ny, nz, CIN, COUT, nsm, smem_max);
+    if (p.ns < 1) {
+        set_last_error("conv3d: no tile fits in shared memory", __FILE__, __LINE__);
+        return HMFEM_E_ARG;
+    }
+    CUtensorMap tm_in, tm_w;
+    {
+        const cuuint64_t dims[4] = {(cuuint64_t)CIN, (cuuint64_t)nx, (cuuint64_t)ny,
+                                    (cuuint64_t)nz};
+        const cuuint64_t strides[3] = {(cuuint64_t)CIN * 2, (cuuint64_t)nx * CIN * 2,
+                                       (cuuint64_t)nx * ny * CIN * 2};
+        const cuuint32_t box[4] = {8, (cuuint32_t)p.W, (cuuint32_t)p.H, (cuuint32_t)(p.bz + 2)};
+        const int rc = encode_bf16_map(&tm_in, in, 4, dims, strides, box);
+        if (rc != HMFEM_OK) return rc;
+    }
+    {
+        const cuuint64_t dims[3] = {(cuuint64_t)CIN, (cuuint64_t)COUT, 27};
+        const cuuint64_t strides[2] = {(cuuint64_t)CIN * 2, (cuuint64_t)COUT * CIN * 2};
+        const cuuint32_t box[3] = {8, (cuuint32_t)COUT, 27};
+        const int rc = encode_bf16_map(&tm_w, w, 3, dims, strides, box);
+        if (rc != HMFEM_OK) return rc;
+    }
+    HM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_bytes));
+    const long tiles = (long)p.ntx * p.nty * p.ntz;
+    const int grid = (int)(tiles < nsm ? tiles : nsm);
+    k<<<grid, kConvThreads, p.smem_bytes, st>>>(tm_in, tm_w, bias, (__nv_bfloat16 *)out, nx, ny,
+                                                nz, relu, p, err);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -541,6 +791,20 @@ int hmfem_conv3d_fwd(const void *in, const void *w, const float *bias, void *out
 #undef X
     hm::set_last_error("conv3d: unsupported channel counts", __FILE__, __LINE__);
     return HMFEM_E_ARG;
+}
+
+int hmfem_conv3d_plan(int nx, int ny, int nz, int cin, int cout, int nsm, int smem_max,
+                      int *plan)
+{
+    if (!plan || nx < 1 || ny < 1 || nz < 1 || cin < 16 || cin % 16 || cout < 16 ||
+        cout % 16 || cout > 256 || nsm < 1 || smem_max < 1024)
+        return HMFEM_E_ARG;
+    const hm::ConvPlan p = hm::plan_conv(nx, ny, nz, cin, cout, nsm, smem_max);
+    const int v[20] = {p.bx, p.by, p.bz, p.W, p.H, p.hc, p.hcp, p.runs, p.rp, p.row_mode,
+                       p.ntx, p.nty, p.ntz, p.ns, p.nb, p.wres, p.tmem_cols,
+                       (int)p.stage_bytes, (int)p.wbytes, (int)p.smem_bytes};
+    for (int i = 0; i < 20; i++) plan[i] = v[i];
+    return p.ns >= 1 ? HMFEM_OK : HMFEM_E_ARG;
 }
 
 int hmfem_conv3d_wgrad(const void *x, const void *dy, float *dw, int nx, int ny, int nz,

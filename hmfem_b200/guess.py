@@ -34,8 +34,24 @@ def _lib():
         vp, i = C.c_void_p, C.c_int
         L.hmfem_conv3d_fwd.argtypes = [vp, vp, vp, vp, i, i, i, i, i, i, vp, vp]
         L.hmfem_conv3d_wgrad.argtypes = [vp, vp, vp, i, i, i, i, i, vp, vp]
+        L.hmfem_conv3d_plan.argtypes = [i, i, i, i, i, i, i, vp]
         L._guess_bound = True
     return L
+
+
+PLAN_FIELDS = ("bx", "by", "bz", "W", "H", "hc", "hcp", "runs", "rp", "row_mode",
+               "ntx", "nty", "ntz", "ns", "nb", "wres", "tmem_cols", "stage_bytes",
+               "wbytes", "smem_bytes")
+
+
+def conv_plan(dims, cin, cout, nsm=148, smem_max=232448):
+    """The tiling `hmfem_conv3d_fwd` launches for this grid (host only)."""
+    out = (C.c_int * len(PLAN_FIELDS))()
+    rc = _lib().hmfem_conv3d_plan(dims[0], dims[1], dims[2], cin, cout, nsm, smem_max,
+                                  C.addressof(out))
+    if rc != 0:
+        raise gpu.HmfemError(rc, gpu.last_error())
+    return dict(zip(PLAN_FIELDS, list(out)))
 
 
 _ERR = {}

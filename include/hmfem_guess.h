@@ -24,6 +24,17 @@ extern "C" {
 int hmfem_conv3d_fwd(const void *in, const void *w, const float *bias, void *out, int nx,
                      int ny, int nz, int cin, int cout, int relu, int *err, void *stream);
 
+/* The tiling hmfem_conv3d_fwd launches for this grid and channel counts on
+ * a device with `nsm` SMs and `smem_max` bytes of opt-in shared memory per
+ * block; host-only (no device call).  plan[20] = {bx, by, bz, W, H, hc, hcp,
+ * runs, rp, row_mode, ntx, nty, ntz, ns, nb, wres, tmem_cols, stage_bytes,
+ * wbytes, smem_bytes}: the interior tile, the halo row pitch and rows per
+ * plane, halo cells and cells per 8-channel slab, MMA runs per tile and per
+ * z plane, row mode, tiles per axis, input stages, accumulator buffers,
+ * resident weights, tensor-memory columns and shared-memory bytes. */
+int hmfem_conv3d_plan(int nx, int ny, int nz, int cin, int cout, int nsm, int smem_max,
+                      int *plan);
+
 /* dw[27][cout][cin] += sum over cells of dy[cell][co] x[cell + tap][ci] (the
  * weight gradient), FP32, on the tensor cores. */
 int hmfem_conv3d_wgrad(const void *x, const void *dy, float *dw, int nx, int ny, int nz,

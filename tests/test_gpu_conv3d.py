@@ -15,6 +15,8 @@ import torch.nn.functional as F  # noqa: E402
 from hmfem_b200 import guess  # noqa: E402
 
 DIMS = [(9, 7, 5), (20, 16, 12)]
+# x rows of 128 cells and more (one MMA run per row, two x tiles, the second ragged)
+ROW_DIMS = [(130, 5, 3), (128, 4, 5)]
 SHAPES = [(16, 16), (16, 32), (32, 64), (64, 64), (96, 32), (48, 16), (32, 96)]
 
 
@@ -36,7 +38,7 @@ def _rel(a, b):
     return float((a - b).norm() / max(float(b.norm()), 1e-30))
 
 
-@pytest.mark.parametrize("dims", DIMS)
+@pytest.mark.parametrize("dims", DIMS + ROW_DIMS)
 @pytest.mark.parametrize("cin,cout", SHAPES)
 def test_forward_matches_conv3d(cin, cout, dims):
     g = torch.Generator().manual_seed(cin * 100 + cout)
