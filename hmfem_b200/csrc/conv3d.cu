@@ -2,15 +2,17 @@
 // 5th-generation tensor cores (tcgen05, sm_100a): BF16 operands, FP32
 // accumulation in tensor memory.  No counterpart in the reference.
 //
-// Activations are channels-last (cell s = x + nx (y + ny z), C contiguous
-// BF16 values per cell); weights are [27 taps][Cout][Cin] with tap
-// t = 9 (dz+1) + 3 (dy+1) + (dx+1); zero padding outside the grid.
+// Activations are channel-blocked: C/8 slabs, each holding the grid's cells
+// (s = x + nx (y + ny z)) with 8 consecutive BF16 channels per cell, i.e.
+// channel c of cell s at (c/8) n + s) * 8 + c % 8; weights are
+// [27 taps][Cout][Cin] with tap t = 9 (dz+1) + 3 (dy+1) + (dx+1); zero
+// padding outside the grid.
 //
 // Forward (and, with flipped / transposed weights, the data gradient) is an
 // implicit GEMM: D[m][n] = sum_tap sum_ci A_tap[m][ci] B_tap[n][ci] with m a
 // run of 128 cells, n the output channel, A_tap the input at cell m shifted
 // by the tap.  The input of a tile of cells, with its halo, is brought into
-// shared memory once per 16 input channels by TMA and every tap's A operand
+// shared memory once per 16 input channels by bulk copies and every tap's A operand
 // is a shifted view of it (the layout and the roles are described at
 // k_conv3d); tcgen05.mma (M = 128, N = Cout, K = 16) accumulates in tensor
 // memory and the epilogue reads it with tcgen05.ld, adds the bias, applies
@@ -149,6 +151,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16])
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// 16 columns of this thread's TMEM lane into registers, without waiting:
+// the registers are valid after tmem_wait_ld()
+__device__ __forceinline__ void tmem_ld16_nw(uint32_t taddr, float v[16])
+{
+    uint32_t *r = reinterpret_cast<uint32_t *>(v);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+          "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+          "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld()
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
 __host__ __device__ constexpr int tmem_cols(int n)
 {
     return n <= 32 ? 32 : n <= 64 ? 64 : n <= 128 ? 128 : 256;
@@ -171,19 +192,32 @@ __host__ __device__ constexpr int tmem_cols(int n)
 // plane are computed and dropped by the epilogue.  The copy of a tile reads
 // (bx+2)(by+2)(bz+2) / (bx by bz) times its cells from L2.
 //
-// Roles (one CTA per SM, persistent over the tiles): lane 0 of warp 4 loads
-// each halo chunk with two TMA tensor copies (box {8 channels, W, H, bz+2}
-// of the input seen as {C, nx, ny, nz}; coordinates outside the grid read
-// zeros, which is the convolution's padding) into a ring of `ns` stages;
+// Roles (one CTA per SM, persistent over the tiles): warp 4 loads each halo
+// chunk into a ring of `ns` stages with one bulk copy per halo row and slab
+// (a halo row of a slab is contiguous in the channel-blocked input); the
+// cells and rows outside the grid (the convolution's zero padding) are
+// stored by the warp itself and fenced for the tensor cores;
 // lane 0 of warp 5 issues, per chunk, 27 taps x runs MMAs of M = 128,
 // N = COUT, K = 16 into the tile's accumulator (runs x COUT FP32 columns of
 // tensor memory, `nb` = 2 buffers when they fit) and commits the stage back
 // to the producer; warps 0-3 read a finished accumulator (tcgen05.ld, warp w
 // lanes 32w..32w+31), add the bias, apply ReLU, store BF16 and release the
 // buffer -- loads, MMAs and the epilogue of different tiles overlap.  The
-// weights of a chunk (two TMA copies of box {8, COUT, 27}: the two 8-channel
-// halves, each [tap][COUT][8]) stay resident with one input chunk; otherwise
-// each stage carries its chunk's weights.  No multicast.
+// weights of a chunk come as two TMA copies of box {8, COUT, 27} (the two
+// 8-channel halves, each [tap][COUT][8]); all chunks stay resident when they
+// fit in kWResMax bytes, otherwise each stage carries its chunk's weights.
+// No multicast.
+// Grouped x taps (XG, when 3 COUT <= 256 and the tile spans the whole x
+// extent): an MMA's cost is set by its A operand (128 rows from shared
+// memory) up to N ~ 90, so the three taps dx = -1, 0, +1 of a (dy, dz) pair
+// share one A operand -- the run's rows shifted by W dy + W H dz only -- and
+// one MMA with N = 3 COUT (B = the three taps' weights, consecutive rows of
+// the weight tile) accumulates D_dx for all three: 9 MMAs per run and chunk
+// instead of 27.  The output of row m is D_-1[m-1] + D_0[m] + D_+1[m+1]: the
+// epilogue shifts by one TMEM lane (warp shuffles; shared memory across the
+// warps' lane quarters and, in plane mode, between consecutive runs of a z
+// plane).  Any other neighbour of a stored cell is a halo column, i.e. zero
+// padding, because the tile covers the whole x extent.
 struct ConvPlan {
     int bx, by, bz;          // tile (interior cells)
     int W, H;                // halo row pitch bx+2, halo rows per plane by+2
@@ -192,13 +226,48 @@ struct ConvPlan {
     int row_mode;            // 1: bx == 128, one run per x row
     int ntx, nty, ntz;       // tiles per axis
     int ns, nb;              // input stages, accumulator buffers
-    int wres;                // weights resident (one input chunk)
+    int wres;                // weights of every chunk resident
+    int xg;                  // x taps grouped: N = 3 COUT per MMA (see k_conv3d)
     int tmem_cols;
     unsigned stage_bytes, wbytes, smem_bytes;
 };
 
 constexpr int kConvThreads = 192;  // warps 0-3 epilogue, 4 TMA producer, 5 MMA
 constexpr int kEpilogue = 128;
+constexpr unsigned kWResMax = 64 * 1024;  // resident weights (all chunks) up to this size
+constexpr unsigned kBarBytes = 128;       // mbarriers (ns, nb <= 4), TMEM slot, abort flag
+
+// shared memory after the stages: barriers, then (grouped x taps) three
+// exchange buffers of 4 + 4 + 1 boundary rows of COUT floats, then the bias
+__host__ __device__ constexpr unsigned conv_tail_bytes(int cout, bool xg)
+{
+    return kBarBytes + (xg ? 3u * 9u * 4u * (unsigned)cout : 0u) + 4u * (unsigned)cout;
+}
+
+// The MMA warp runs its loop with all lanes (descriptor arithmetic stays
+// warp-uniform); one elected lane issues.  Every MMA and commit of the
+// kernel goes through the same election, so a commit tracks the MMAs it
+// follows (both are per issuing thread).
+__device__ __forceinline__ void umma_bf16_elect(uint32_t tmem, uint64_t da, uint64_t db,
+                                                uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred e, p;\n\t"
+        "elect.sync _|e, 0xffffffff;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+        "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit_elect(uint64_t *mbar)
+{
+    asm volatile(
+        "{\n\t.reg .pred e;\n\t"
+        "elect.sync _|e, 0xffffffff;\n\t"
+        "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}\n"
+        ::"r"(smem_u32(mbar))
+        : "memory");
+}
 
 __device__ __forceinline__ void mbar_init_n(uint64_t *m, unsigned count)
 {
@@ -210,24 +279,23 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *m)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(m)) : "memory");
 }
 
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *m, uint32_t bytes)
+__device__ __forceinline__ void mbar_expect_tx_only(uint64_t *m, uint32_t bytes)
 {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)),
-                 "r"(bytes)
+    asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes)
                  : "memory");
 }
 
-// TMA tensor copies into this CTA's shared memory, completion on an mbarrier
-__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int c0, int c1,
-                                            int c2, int c3, uint64_t *m)
+// bulk copy global -> this CTA's shared memory (16-byte aligned, multiple of 16)
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes,
+                                          uint64_t *m)
 {
     asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-        "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
-        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(m))
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(dst), "l"(src), "r"(bytes), "r"(smem_u32(m))
         : "memory");
 }
 
+// TMA tensor copies into this CTA's shared memory, completion on an mbarrier
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, int c0, int c1,
                                             int c2, uint64_t *m)
 {
@@ -236,6 +304,27 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
         "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
         "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(m))
         : "memory");
+}
+
+// named barrier 1 among the epilogue warps; the reduction form returns the
+// AND of every thread's predicate (all threads agree on leaving)
+__device__ __forceinline__ void epi_sync()
+{
+    asm volatile("bar.sync 1, %0;" ::"n"(kEpilogue) : "memory");
+}
+
+__device__ __forceinline__ bool epi_all(bool v)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, 1, %2, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "n"(kEpilogue)
+        : "memory");
+    return r != 0;
 }
 
 // bounded wait that also leaves when another role gave up (abort flag)
@@ -265,15 +354,17 @@ __device__ __forceinline__ int run_start(const ConvPlan &p, int r, int &plane, i
     return 1 + p.W + p.W * p.H * (plane + 1) + 128 * (r - plane * p.rp);
 }
 
-template <int CIN, int COUT>
+template <int CIN, int COUT, bool XG>
 __global__ void __launch_bounds__(kConvThreads, 1)
-k_conv3d(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_w,
+k_conv3d(const __nv_bfloat16 *__restrict__ in, const __grid_constant__ CUtensorMap tm_w,
          const float *__restrict__ bias, __nv_bfloat16 *__restrict__ out, int nx, int ny,
          int nz, int relu, const ConvPlan p, int *err)
 {
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 256, "channel counts");
+    static_assert(!XG || 3 * COUT <= 256, "grouped x taps: N = 3 COUT <= 256");
     constexpr int KC = CIN / 16;
-    constexpr uint32_t IDESC = idesc_bf16(128, COUT);
+    constexpr int NACC = XG ? 3 * COUT : COUT;  // accumulator columns per run
+    constexpr uint32_t IDESC = idesc_bf16(128, NACC);
     constexpr int WTAP = COUT * 16;       // one tap's rows of one 8-channel half
     constexpr int WHALF = 27 * WTAP;      // the second half follows all 27 taps of the first
     extern __shared__ __align__(128) unsigned char smem[];
@@ -285,6 +376,14 @@ k_conv3d(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUte
              *drain = tempty + p.nb;
     uint32_t *tslot = (uint32_t *)(drain + 1);
     volatile int *abort_flag = (volatile int *)(tslot + 1);
+    // grouped x taps: boundary rows exchanged between warps / runs, three
+    // buffers (by a running run count): lane 31's D_-1 of each warp, lane
+    // 0's D_+1 of each warp, row 0's D_+1 of the next run
+    float *xlo = (float *)(stages + (size_t)p.ns * p.stage_bytes + kBarBytes);
+    float *xhi = xlo + 3 * 4 * COUT;
+    float *xnx = xhi + 3 * 4 * COUT;
+    float *sbias = (float *)(stages + (size_t)p.ns * p.stage_bytes + kBarBytes) +
+                   (XG ? 27 * COUT : 0);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long ntiles = (long)p.ntx * p.nty * p.ntz;
@@ -303,77 +402,117 @@ k_conv3d(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUte
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 5) tmem_alloc(tslot, p.tmem_cols);
+    for (int i = tid; i < COUT; i += kConvThreads) sbias[i] = bias ? bias[i] : 0.f;
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
     const uint32_t tmem = *tslot;
 
     if (warp == 4) {
-        // ---- producer: TMA copies of the halo chunks (and weights)
-        if (lane == 0) {
-            unsigned wkc = 0xffffffffu;  // per stage (8 bits each): chunk of its weights
-            long item = 0;
-            bool ok = true;
-            for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-                const int tx = (int)(tile % p.ntx), ty = (int)((tile / p.ntx) % p.nty),
-                          tz = (int)(tile / ((long)p.ntx * p.nty));
-                const int x0 = tx * p.bx - 1, y0 = ty * p.by - 1, z0 = tz * p.bz - 1;
-                for (int kc = 0; kc < KC; kc++, item++) {
-                    const int s = (int)(item % p.ns);
-                    const unsigned use = (unsigned)(item / p.ns);
-                    if (!role_wait(&empty[s], (use & 1u) ^ 1u, abort_flag, err)) {
-                        ok = false;
-                        break;
+        // ---- producer (whole warp): bulk copies of the halo rows
+        const long n = (long)nx * ny * nz;
+        const int D = p.bz + 2, rows = p.H * D;
+        unsigned wkc = 0xffffffffu;  // per stage (8 bits each): chunk of its weights
+        long item = 0;
+        bool ok = true;
+        for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            const int tx = (int)(tile % p.ntx), ty = (int)((tile / p.ntx) % p.nty),
+                      tz = (int)(tile / ((long)p.ntx * p.nty));
+            const int x0 = tx * p.bx - 1, y0 = ty * p.by - 1, z0 = tz * p.bz - 1;
+            // the part [xa, xb) of every halo row inside the grid, and the
+            // number of halo rows (of one slab) inside it
+            const int xa = x0 < 0 ? 0 : x0, xb = x0 + p.W < nx ? x0 + p.W : nx;
+            const int ya = y0 < 0 ? 0 : y0, yb = y0 + p.H < ny ? y0 + p.H : ny;
+            const int za = z0 < 0 ? 0 : z0, zb = z0 + D < nz ? z0 + D : nz;
+            const int rows_in = (yb - ya) * (zb - za);
+            for (int kc = 0; kc < KC; kc++, item++) {
+                const int s = (int)(item % p.ns);
+                const unsigned use = (unsigned)(item / p.ns);
+                if (!__all_sync(0xffffffffu,
+                                role_wait(&empty[s], (use & 1u) ^ 1u, abort_flag, err))) {
+                    ok = false;
+                    break;
+                }
+                const uint32_t a = smem_u32(stages + (size_t)s * p.stage_bytes);
+                const bool need_w = p.wres ? item == 0
+                                           : ((wkc >> (8 * s)) & 0xffu) != (unsigned)kc;
+                if (lane == 0)
+                    mbar_expect_tx_only(&full[s], 32u * (unsigned)(rows_in * (xb - xa)) +
+                                                      (need_w ? (p.wres ? KC : 1) * 2u * WHALF
+                                                              : 0u));
+                __syncwarp();
+                const uint4 zero = make_uint4(0, 0, 0, 0);
+                for (int i = lane; i < 2 * rows; i += 32) {
+                    const int sl = i / rows, rr = i - sl * rows, zi = rr / p.H,
+                              yi = rr - zi * p.H;
+                    const int gy = y0 + yi, gz = z0 + zi;
+                    unsigned char *drow_p = stages + (size_t)s * p.stage_bytes + (size_t)sl * SB +
+                                            (size_t)(rr * p.W) * 16u;
+                    if (gy < 0 || gy >= ny || gz < 0 || gz >= nz) {
+                        for (int c = 0; c < p.W; c++) ((uint4 *)drow_p)[c] = zero;
+                        continue;
                     }
-                    const uint32_t a = smem_u32(stages + (size_t)s * p.stage_bytes);
-                    const bool need_w =
-                        p.wres ? item == 0 : ((wkc >> (8 * s)) & 0xffu) != (unsigned)kc;
-                    mbar_expect_tx(&full[s], 32u * (unsigned)p.hc + (need_w ? 2u * WHALF : 0u));
-                    tma_load_4d(a, &tm_in, 16 * kc, x0, y0, z0, &full[s]);
-                    tma_load_4d(a + SB, &tm_in, 16 * kc + 8, x0, y0, z0, &full[s]);
-                    if (need_w) {
-                        const uint32_t wb = p.wres ? smem_u32(wres) : a + SA;
-                        tma_load_3d(wb, &tm_w, 16 * kc, 0, 0, &full[s]);
-                        tma_load_3d(wb + WHALF, &tm_w, 16 * kc + 8, 0, 0, &full[s]);
-                        wkc = (wkc & ~(0xffu << (8 * s))) | ((unsigned)kc << (8 * s));
+                    const __nv_bfloat16 *src =
+                        in + ((long)(2 * kc + sl) * n + xa + (long)nx * (gy + (long)ny * gz)) * 8;
+                    bulk_load(smem_u32(drow_p) + (uint32_t)(xa - x0) * 16u, src,
+                              (uint32_t)(xb - xa) * 16u, &full[s]);
+                    for (int c = 0; c < xa - x0; c++) ((uint4 *)drow_p)[c] = zero;
+                    for (int c = xb - x0; c < p.W; c++) ((uint4 *)drow_p)[c] = zero;
+                }
+                fence_async_smem();  // the zeros, written by this warp, for the MMAs
+                if (need_w && lane == 0) {
+                    for (int c = p.wres ? 0 : kc; c < (p.wres ? KC : kc + 1); c++) {
+                        const uint32_t wb = p.wres ? smem_u32(wres) + (uint32_t)c * 2u * WHALF
+                                                   : a + SA;
+                        tma_load_3d(wb, &tm_w, 16 * c, 0, 0, &full[s]);
+                        tma_load_3d(wb + WHALF, &tm_w, 16 * c + 8, 0, 0, &full[s]);
                     }
                 }
+                if (need_w) wkc = (wkc & ~(0xffu << (8 * s))) | ((unsigned)kc << (8 * s));
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&full[s]);
             }
-            // copies still in flight land before the CTA leaves: wait for the
-            // last use of every stage (already complete unless a role gave up)
+        }
+        // copies still in flight land before the CTA leaves: wait for the
+        // last use of every stage (already complete unless a role gave up)
+        if (lane == 0)
             for (int j = 0; j < p.ns && j < item; j++) {
                 const long it = item - 1 - j;
                 if (!mbar_wait(&full[it % p.ns], (unsigned)(it / p.ns) & 1u)) atomicExch(err, 1);
             }
-        }
         __syncwarp();
     } else if (warp == 5) {
-        // ---- MMA issue (one thread).  Per run the 27 taps are unrolled: the
-        // A descriptor is the run's base plus a per-tap offset held in a
-        // register, the B descriptor the stage's base plus an immediate.
-        if (lane == 0) {
-            int offs[27];
+        // ---- MMA issue (the whole warp, one elected lane issuing).  Per run
+        // the 27 taps are unrolled: the A descriptor is the run's base plus a
+        // per-tap offset held in a register, the B descriptor the stage's
+        // base plus an immediate.
+        {
+            constexpr int NT = XG ? 9 : 27;  // MMAs per run and chunk
+            int offs[NT];
 #pragma unroll
-            for (int t = 0; t < 27; t++)
-                offs[t] = (t % 3 - 1) + p.W * ((t / 3) % 3 - 1) + WH * (t / 9 - 1);
+            for (int t = 0; t < NT; t++)
+                offs[t] = XG ? p.W * (t % 3 - 1) + WH * (t / 3 - 1)
+                             : (t % 3 - 1) + p.W * ((t / 3) % 3 - 1) + WH * (t / 9 - 1);
             long item = 0, jt = 0;
             bool ok = true;
             for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, jt++) {
                 const int b = (int)(jt % p.nb);
                 const unsigned u = (unsigned)(jt / p.nb);
-                if (!role_wait(&tempty[b], (u & 1u) ^ 1u, abort_flag, err)) break;
+                if (!__all_sync(0xffffffffu, role_wait(&tempty[b], (u & 1u) ^ 1u, abort_flag, err)))
+                    break;
                 tc_after_sync();
-                const uint32_t acc0 = tmem + (uint32_t)(b * p.runs * COUT);
+                const uint32_t acc0 = tmem + (uint32_t)(b * p.runs * NACC);
                 for (int kc = 0; kc < KC; kc++, item++) {
                     const int s = (int)(item % p.ns);
                     const unsigned use = (unsigned)(item / p.ns);
-                    if (!role_wait(&full[s], use & 1u, abort_flag, err)) {
+                    if (!__all_sync(0xffffffffu, role_wait(&full[s], use & 1u, abort_flag, err))) {
                         ok = false;
                         break;
                     }
                     tc_after_sync();
                     const uint32_t a = smem_u32(stages + (size_t)s * p.stage_bytes);
-                    const uint32_t wb = p.wres ? smem_u32(wres) : a + SA;
+                    const uint32_t wb =
+                        p.wres ? smem_u32(wres) + (uint32_t)kc * 2u * WHALF : a + SA;
                     // descriptor start addresses count 16-byte units: a run's
                     // operand row q is one unit per position
                     const uint64_t da0 = kmajor_desc(a, SB, 128);
@@ -390,32 +529,37 @@ k_conv3d(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUte
                             plane++;
                         }
                         const uint64_t dar = da0 + (uint64_t)q0;
-                        const uint32_t acc = acc0 + (uint32_t)(r * COUT);
+                        const uint32_t acc = acc0 + (uint32_t)(r * NACC);
+                        // tap t (or group g: taps 3g .. 3g+2) starts at row t (3g) x COUT
+                        // of the weight tile
 #pragma unroll
-                        for (int t = 0; t < 27; t++)
-                            umma_bf16(acc, dar + (uint64_t)offs[t],
-                                      db0 + (uint64_t)(t * (WTAP / 16)), IDESC,
-                                      t == 0 ? first : 1u);
+                        for (int t = 0; t < NT; t++)
+                            umma_bf16_elect(acc, dar + (uint64_t)offs[t],
+                                            db0 + (uint64_t)(t * (XG ? 3 : 1) * (WTAP / 16)),
+                                            IDESC, t == 0 ? first : 1u);
                     }
-                    umma_commit(&empty[s]);
+                    umma_commit_elect(&empty[s]);
                 }
-                if (ok) umma_commit(&tfull[b]);
+                if (ok) umma_commit_elect(&tfull[b]);
             }
         }
         __syncwarp();
     } else {
         // ---- epilogue: warp w reads TMEM lanes 32w .. 32w+31 (rows of a run)
         const int m = 32 * warp + lane;
-        long jt = 0;
+        const long nc = (long)nx * ny * nz;
+        long jt = 0, gr = 0;  // tiles, runs (running count: exchange buffers)
         for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, jt++) {
             const int b = (int)(jt % p.nb);
             const unsigned u = (unsigned)(jt / p.nb);
-            if (!role_wait(&tfull[b], u & 1u, abort_flag, err)) break;
+            bool okw = role_wait(&tfull[b], u & 1u, abort_flag, err);
+            if (XG) okw = epi_all(okw);  // named barriers below: leave together
+            if (!okw) break;
             tc_after_sync();
             const int tx = (int)(tile % p.ntx), ty = (int)((tile / p.ntx) % p.nty),
                       tz = (int)(tile / ((long)p.ntx * p.nty));
             const int X0 = tx * p.bx - 1, Y0 = ty * p.by - 1, Z0 = tz * p.bz - 1;
-            for (int r = 0; r < p.runs; r++) {
+            for (int r = 0; r < p.runs; r++, gr++) {
                 int plane, row;
                 const int q = run_start(p, r, plane, row) + m;
                 const int zi = q / WH, rem = q - zi * WH, yi = rem / p.W, xi = rem - yi * p.W;
@@ -424,23 +568,92 @@ k_conv3d(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUte
                                xi <= p.bx && (row < 0 || yi == row + 1) && gx < nx && gy < ny &&
                                gz < nz;
                 const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16) +
-                                    (uint32_t)((b * p.runs + r) * COUT);
-                __nv_bfloat16 *dst = out + (gx + (long)nx * (gy + (long)ny * gz)) * COUT;
+                                    (uint32_t)((b * p.runs + r) * NACC);
+                const long cell = gx + (long)nx * (gy + (long)ny * gz);
+                // runs r-1 and r+1 of the same z plane (plane mode only)
+                const bool same_prev = !p.row_mode && r > 0 && r % p.rp != 0;
+                const bool same_next = !p.row_mode && r + 1 < p.runs && (r + 1) % p.rp != 0;
+                const int xb = (int)(gr % 3), xbp = (int)((gr + 2) % 3);
 #pragma unroll
                 for (int c0 = 0; c0 < COUT; c0 += 16) {
                     float f[16];
-                    tmem_ld16(ta + c0, f);
+                    if (XG) {
+                        float dm[16], dp[16], dn1[16];
+                        tmem_ld16_nw(ta + c0, dm);              // D_-1
+                        tmem_ld16_nw(ta + COUT + c0, f);        // D_0
+                        tmem_ld16_nw(ta + 2 * COUT + c0, dp);   // D_+1
+                        if (warp == 0 && same_next)
+                            tmem_ld16_nw(ta + NACC + 2 * COUT + c0, dn1);  // next run's D_+1
+                        tmem_wait_ld();
+                        // publish the rows other warps (and the next run) need
+                        float4 *lo = (float4 *)(xlo + (xb * 4 + warp) * COUT + c0);
+                        float4 *hi = (float4 *)(xhi + (xb * 4 + warp) * COUT + c0);
+                        if (lane == 31)
+#pragma unroll
+                            for (int i = 0; i < 4; i++)
+                                lo[i] = make_float4(dm[4 * i], dm[4 * i + 1], dm[4 * i + 2],
+                                                    dm[4 * i + 3]);
+                        if (lane == 0) {
+#pragma unroll
+                            for (int i = 0; i < 4; i++)
+                                hi[i] = make_float4(dp[4 * i], dp[4 * i + 1], dp[4 * i + 2],
+                                                    dp[4 * i + 3]);
+                            if (warp == 0 && same_next) {
+                                float4 *nx4 = (float4 *)(xnx + xb * COUT + c0);
+#pragma unroll
+                                for (int i = 0; i < 4; i++)
+                                    nx4[i] = make_float4(dn1[4 * i], dn1[4 * i + 1],
+                                                         dn1[4 * i + 2], dn1[4 * i + 3]);
+                            }
+                        }
+                        epi_sync();
+                        // row m-1's D_-1 and row m+1's D_+1
+                        float up[16], dn[16];
+#pragma unroll
+                        for (int i = 0; i < 16; i++) {
+                            up[i] = __shfl_up_sync(0xffffffffu, dm[i], 1);
+                            dn[i] = __shfl_down_sync(0xffffffffu, dp[i], 1);
+                        }
+                        if (lane == 0) {
+                            const float *src = warp > 0 ? xlo + (xb * 4 + warp - 1) * COUT + c0
+                                             : same_prev ? xlo + (xbp * 4 + 3) * COUT + c0
+                                                         : nullptr;
+#pragma unroll
+                            for (int i = 0; i < 4; i++) {
+                                const float4 t4 = src ? ((const float4 *)src)[i]
+                                                      : make_float4(0.f, 0.f, 0.f, 0.f);
+                                up[4 * i] = t4.x, up[4 * i + 1] = t4.y, up[4 * i + 2] = t4.z,
+                                up[4 * i + 3] = t4.w;
+                            }
+                        }
+                        if (lane == 31) {
+                            const float *src = warp < 3 ? xhi + (xb * 4 + warp + 1) * COUT + c0
+                                             : same_next ? xnx + xb * COUT + c0
+                                                         : nullptr;
+#pragma unroll
+                            for (int i = 0; i < 4; i++) {
+                                const float4 t4 = src ? ((const float4 *)src)[i]
+                                                      : make_float4(0.f, 0.f, 0.f, 0.f);
+                                dn[4 * i] = t4.x, dn[4 * i + 1] = t4.y, dn[4 * i + 2] = t4.z,
+                                dn[4 * i + 3] = t4.w;
+                            }
+                        }
+#pragma unroll
+                        for (int i = 0; i < 16; i++) f[i] += up[i] + dn[i];
+                    } else {
+                        tmem_ld16_nw(ta + c0, f);
+                        tmem_wait_ld();
+                    }
                     if (v) {
                         __nv_bfloat16 o[16];
 #pragma unroll
                         for (int i = 0; i < 16; i++) {
-                            float t = f[i] + (bias ? __ldg(bias + c0 + i) : 0.f);
+                            float t = f[i] + sbias[c0 + i];
                             if (relu) t = fmaxf(t, 0.f);
                             o[i] = __float2bfloat16(t);
                         }
-                        uint4 *d4 = (uint4 *)(dst + c0);
-                        d4[0] = *(uint4 *)&o[0];
-                        d4[1] = *(uint4 *)&o[8];
+                        *(uint4 *)(out + ((long)(c0 / 8) * nc + cell) * 8) = *(uint4 *)&o[0];
+                        *(uint4 *)(out + ((long)(c0 / 8 + 1) * nc + cell) * 8) = *(uint4 *)&o[8];
                     }
                 }
             }
@@ -449,9 +662,10 @@ k_conv3d(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUte
         }
     }
     // teardown: every MMA this CTA issued has completed before TMEM is freed
-    if (warp == 5 && lane == 0) {
-        umma_commit(drain);
-        if (!mbar_wait(drain, 0)) atomicExch(err, 1);
+    if (warp == 5) {
+        umma_commit_elect(drain);
+        if (lane == 0 && !mbar_wait(drain, 0)) atomicExch(err, 1);
+        __syncwarp();
     }
     tc_before_sync();
     __syncthreads();
@@ -526,7 +740,8 @@ k_conv3d_wgrad(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restr
             const long cell = c0 + k;
             const bool v = cell < c_end;
             for (int co = 0; co < COUT; co += 8) {
-                uint4 q = v ? *(const uint4 *)(dy + cell * COUT + co) : make_uint4(0, 0, 0, 0);
+                uint4 q = v ? *(const uint4 *)(dy + ((long)(co / 8) * n + cell) * 8)
+                            : make_uint4(0, 0, 0, 0);
                 const __nv_bfloat16 *e = (const __nv_bfloat16 *)&q;
 #pragma unroll
                 for (int j = 0; j < 8; j++)
@@ -545,7 +760,8 @@ k_conv3d_wgrad(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restr
                 src = xx + (long)yy * nx + (long)zz * nxy;
             }
             for (int ci = 0; ci < CIN; ci += 8) {
-                uint4 q = v ? *(const uint4 *)(x + src * CIN + ci) : make_uint4(0, 0, 0, 0);
+                uint4 q = v ? *(const uint4 *)(x + ((long)(ci / 8) * n + src) * 8)
+                            : make_uint4(0, 0, 0, 0);
                 const __nv_bfloat16 *e = (const __nv_bfloat16 *)&q;
 #pragma unroll
                 for (int j = 0; j < 8; j++)
@@ -605,11 +821,15 @@ k_conv3d_wgrad(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restr
 }
 
 // Tile choice for a forward launch: bx = 128 (row mode) when nx >= 128, else
-// the whole x extent; (by, bz) minimise an estimate of the makespan -- per
-// tile the larger of the MMA operand reads from shared memory (A 4 KB + B
-// 32 COUT B per MMA at ~128 B per clock) and the halo copy, times the tile
+// the whole x extent; the form (x taps grouped or not) and (by, bz)
+// minimise an estimate of the makespan -- per tile the largest of the MMA
+// issue (~42 cycles per MMA up to N = 84, N/2 above: the A operand read),
+// the halo copy (a bulk copy per row and slab plus its bytes) and the
+// epilogue (added instead with one accumulator buffer), times the tile
 // waves over the SMs -- subject to the tensor-memory columns (runs x COUT,
-// doubled when two accumulators fit in 512) and the shared memory.
+// x3 grouped, doubled when two accumulators fit in 512) and the shared
+// memory.  Grouping pays where the MMAs dominate: many input chunks and
+// few output columns (48 -> 16 at 128^3: 255 -> 191 us).
 ConvPlan plan_conv(int nx, int ny, int nz, int cin, int cout, int nsm, int smem_max)
 {
     ConvPlan best{};
@@ -619,45 +839,58 @@ ConvPlan plan_conv(int nx, int ny, int nz, int cin, int cout, int nsm, int smem_
     const bool row_mode = bx == 128;
     const int W = bx + 2;
     const unsigned wchunk = 27u * (unsigned)cout * 32u;
-    const unsigned fixed = 256;  // barriers, TMEM slot, abort flag
-    for (int bz = 1; bz <= (nz < 16 ? nz : 16); bz++)
-        for (int by = 1; by <= (ny < 64 ? ny : 64); by++) {
-            ConvPlan p{};
-            p.bx = bx;
-            p.by = by;
-            p.bz = bz;
-            p.W = W;
-            p.H = by + 2;
-            p.hc = W * p.H * (bz + 2);
-            p.hcp = (p.hc + 128 + 7) / 8 * 8;
-            p.row_mode = row_mode;
-            p.rp = row_mode ? by : (W * (by - 1) + bx + 127) / 128;
-            p.runs = bz * p.rp;
-            if (p.runs * cout > 512) continue;
-            p.nb = 2 * p.runs * cout <= 512 ? 2 : 1;
-            p.wres = kc == 1;
-            p.wbytes = p.wres ? wchunk : 0;
-            p.stage_bytes = 32u * (unsigned)p.hcp + (p.wres ? 0 : wchunk);
-            if ((unsigned)smem_max < fixed + p.wbytes + p.stage_bytes) continue;
-            int ns = (int)(((unsigned)smem_max - fixed - p.wbytes) / p.stage_bytes);
-            p.ns = ns > 4 ? 4 : ns;
-            p.ntx = (nx + bx - 1) / bx;
-            p.nty = (ny + by - 1) / by;
-            p.ntz = (nz + bz - 1) / bz;
-            const long tiles = (long)p.ntx * p.nty * p.ntz;
-            const double mma = (double)p.runs * 27 * kc * (4096.0 + 32.0 * cout) / 128.0;
-            const double load = (double)p.hc * kc + (p.wres ? 0.0 : 27.0 * cout * kc);
-            const double tile_t = (p.ns >= 2 ? (mma > load ? mma : load) : mma + load) +
-                                  (p.nb == 2 ? 0.0 : 4.0 * p.runs * cout) + 400.0;
-            const double cost = (double)((tiles + nsm - 1) / nsm) * tile_t;
-            if (cost < best_cost) {
-                best_cost = cost;
-                best = p;
+    // grouped x taps need N = 3 COUT <= 256 and tiles spanning the x extent
+    const int xg_max = (3 * cout <= 256 && nx <= 128) ? 1 : 0;
+    for (int xg = 0; xg <= xg_max; xg++)
+        for (int bz = 1; bz <= (nz < 16 ? nz : 16); bz++)
+            for (int by = 1; by <= (ny < 64 ? ny : 64); by++) {
+                ConvPlan p{};
+                p.bx = bx;
+                p.by = by;
+                p.bz = bz;
+                p.W = W;
+                p.H = by + 2;
+                p.hc = W * p.H * (bz + 2);
+                p.hcp = (p.hc + 128 + 7) / 8 * 8;
+                p.row_mode = row_mode;
+                p.xg = xg;
+                p.rp = row_mode ? by : (W * (by - 1) + bx + 127) / 128;
+                p.runs = bz * p.rp;
+                const int nacc = (xg ? 3 : 1) * cout;
+                if (p.runs * nacc > 512) continue;
+                p.nb = 2 * p.runs * nacc <= 512 ? 2 : 1;
+                p.wres = (unsigned)kc * wchunk <= kWResMax;
+                p.wbytes = p.wres ? (unsigned)kc * wchunk : 0;
+                p.stage_bytes = 32u * (unsigned)p.hcp + (p.wres ? 0 : wchunk);
+                const unsigned fixed = conv_tail_bytes(cout, xg);
+                if ((unsigned)smem_max < fixed + p.wbytes + p.stage_bytes) continue;
+                int ns = (int)(((unsigned)smem_max - fixed - p.wbytes) / p.stage_bytes);
+                p.ns = ns > 4 ? 4 : ns;
+                p.ntx = (nx + bx - 1) / bx;
+                p.nty = (ny + by - 1) / by;
+                p.ntz = (nz + bz - 1) / bz;
+                const long tiles = (long)p.ntx * p.nty * p.ntz;
+                const double mma_c = nacc / 2.0 > 42.0 ? nacc / 2.0 : 42.0;
+                const double mma = (double)p.runs * (xg ? 9 : 27) * kc * mma_c;
+                const double load = kc * (2.0 * p.H * (bz + 2) * 30.0 + 32.0 * p.hc / 48.0) +
+                                    (p.wres ? 0.0 : 27.0 * cout * kc);
+                // epilogue per run and 16 columns (measured): ~300 cycles, ~2000
+                // grouped (three TMEM reads, the boundary exchange, a barrier)
+                const double epi = (double)p.runs * (cout / 16) * (xg ? 2000.0 : 300.0);
+                double tile_t = mma > load ? mma : load;
+                if (p.ns < 2) tile_t = mma + load;
+                tile_t = p.nb == 2 ? (tile_t > epi ? tile_t : epi) : tile_t + epi;
+                const double cost = (double)((tiles + nsm - 1) / nsm) * (tile_t + 300.0);
+                if (cost < best_cost) {
+                    best_cost = cost;
+                    best = p;
+                }
             }
-        }
+    const int nacc = (best.xg ? 3 : 1) * cout;
     best.tmem_cols = 32;
-    while (best.tmem_cols < best.nb * best.runs * cout) best.tmem_cols *= 2;
-    best.smem_bytes = best.wbytes + (unsigned)best.ns * best.stage_bytes + fixed;
+    while (best.tmem_cols < best.nb * best.runs * nacc) best.tmem_cols *= 2;
+    best.smem_bytes = best.wbytes + (unsigned)best.ns * best.stage_bytes +
+                      conv_tail_bytes(cout, best.xg);
     // one CTA per SM: its tensor-memory allocation may take all 512 columns
     if (best.smem_bytes < (unsigned)smem_max / 2 + 1024) best.smem_bytes = smem_max / 2 + 1024;
     return best;
@@ -708,26 +941,23 @@ template <int CIN, int COUT>
 int launch_fwd(const void *in, const void *w, const float *bias, void *out, int nx, int ny,
                int nz, int relu, int *err, cudaStream_t st)
 {
-    auto k = k_conv3d<CIN, COUT>;
     int dev = 0, nsm = 0, smem_max = 0;
     HM_CUDA(cudaGetDevice(&dev));
     HM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     HM_CUDA(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const ConvPlan p = plan_conv(nx, ny, nz, CIN, COUT, nsm, smem_max);
+    auto k = k_conv3d<CIN, COUT, false>;
+    if constexpr (3 * COUT <= 256)
+        if (p.xg) k = k_conv3d<CIN, COUT, true>;
     if (p.ns < 1) {
         set_last_error("conv3d: no tile fits in shared memory", __FILE__, __LINE__);
         return HMFEM_E_ARG;
     }
-    CUtensorMap tm_in, tm_w;
-    {
-        const cuuint64_t dims[4] = {(cuuint64_t)CIN, (cuuint64_t)nx, (cuuint64_t)ny,
-                                    (cuuint64_t)nz};
-        const cuuint64_t strides[3] = {(cuuint64_t)CIN * 2, (cuuint64_t)nx * CIN * 2,
-                                       (cuuint64_t)nx * ny * CIN * 2};
-        const cuuint32_t box[4] = {8, (cuuint32_t)p.W, (cuuint32_t)p.H, (cuuint32_t)(p.bz + 2)};
-        const int rc = encode_bf16_map(&tm_in, in, 4, dims, strides, box);
-        if (rc != HMFEM_OK) return rc;
+    if (((uintptr_t)in & 15u) || ((uintptr_t)out & 15u)) {
+        set_last_error("conv3d: tensors must be 16-byte aligned", __FILE__, __LINE__);
+        return HMFEM_E_ARG;
     }
+    CUtensorMap tm_w;
     {
         const cuuint64_t dims[3] = {(cuuint64_t)CIN, (cuuint64_t)COUT, 27};
         const cuuint64_t strides[2] = {(cuuint64_t)CIN * 2, (cuuint64_t)COUT * CIN * 2};
@@ -738,8 +968,8 @@ int launch_fwd(const void *in, const void *w, const float *bias, void *out, int 
     HM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem_bytes));
     const long tiles = (long)p.ntx * p.nty * p.ntz;
     const int grid = (int)(tiles < nsm ? tiles : nsm);
-    k<<<grid, kConvThreads, p.smem_bytes, st>>>(tm_in, tm_w, bias, (__nv_bfloat16 *)out, nx, ny,
-                                                nz, relu, p, err);
+    k<<<grid, kConvThreads, p.smem_bytes, st>>>((const __nv_bfloat16 *)in, tm_w, bias,
+                                                (__nv_bfloat16 *)out, nx, ny, nz, relu, p, err);
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -800,10 +1030,10 @@ int hmfem_conv3d_plan(int nx, int ny, int nz, int cin, int cout, int nsm, int sm
         cout % 16 || cout > 256 || nsm < 1 || smem_max < 1024)
         return HMFEM_E_ARG;
     const hm::ConvPlan p = hm::plan_conv(nx, ny, nz, cin, cout, nsm, smem_max);
-    const int v[20] = {p.bx, p.by, p.bz, p.W, p.H, p.hc, p.hcp, p.runs, p.rp, p.row_mode,
+    const int v[21] = {p.bx, p.by, p.bz, p.W, p.H, p.hc, p.hcp, p.runs, p.rp, p.row_mode,
                        p.ntx, p.nty, p.ntz, p.ns, p.nb, p.wres, p.tmem_cols,
-                       (int)p.stage_bytes, (int)p.wbytes, (int)p.smem_bytes};
-    for (int i = 0; i < 20; i++) plan[i] = v[i];
+                       (int)p.stage_bytes, (int)p.wbytes, (int)p.smem_bytes, p.xg};
+    for (int i = 0; i < 21; i++) plan[i] = v[i];
     return p.ns >= 1 ? HMFEM_OK : HMFEM_E_ARG;
 }
 

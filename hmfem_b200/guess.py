@@ -9,8 +9,12 @@ training driver around them: autograd bookkeeping, the 2x average pooling,
 nearest upsampling and channel concatenation (pure data movement), the 1x1
 head and the Adam update of the FP32 master weights.
 
-Activations are channels-last: a grid of n = nx*ny*nz cells is an (n, C)
-BF16 tensor, cell s = x + nx (y + ny z).
+Activations are channel-blocked: a grid of n = nx*ny*nz cells with C
+channels is a (C/8, n, 8) BF16 tensor -- slab k holds channels 8k..8k+7 of
+every cell, cell s = x + nx (y + ny z) -- so a halo row of one slab is
+contiguous for the kernels' bulk copies, channel concatenation is
+concatenation of slabs, and pooling and upsampling are views over the
+cells.
 """
 from __future__ import annotations
 
@@ -41,7 +45,7 @@ def _lib():
 
 PLAN_FIELDS = ("bx", "by", "bz", "W", "H", "hc", "hcp", "runs", "rp", "row_mode",
                "ntx", "nty", "ntz", "ns", "nb", "wres", "tmem_cols", "stage_bytes",
-               "wbytes", "smem_bytes")
+               "wbytes", "smem_bytes", "xg")
 
 
 def conv_plan(dims, cin, cout, nsm=148, smem_max=232448):
@@ -72,16 +76,29 @@ def check_errors(dev=None):
         raise RuntimeError("conv3d: a bounded tensor-core wait gave up")
 
 
+def blocked(x):
+    """(n, C) channels-last -> (C/8, n, 8) channel-blocked."""
+    n, c = x.shape
+    return x.reshape(n, c // 8, 8).permute(1, 0, 2).contiguous()
+
+
+def unblocked(x):
+    """(C/8, n, 8) channel-blocked -> (n, C) channels-last."""
+    s, n, _ = x.shape
+    return x.permute(1, 0, 2).reshape(n, 8 * s)
+
+
 def conv3d_raw(x, w, bias, dims, relu):
-    """out = relu?(conv(x, w) + bias): x (n, cin) bf16, w (27, cout, cin) bf16."""
+    """out = relu?(conv(x, w) + bias): x (cin/8, n, 8) bf16, w (27, cout, cin)
+    bf16; out (cout/8, n, 8)."""
     nx, ny, nz = dims
-    n, cin = x.shape
+    n, cin = x.shape[1], 8 * x.shape[0]
     cout = w.shape[1]
     assert (cin, cout) in _SHAPES, (cin, cout)
     assert x.dtype == torch.bfloat16 and w.dtype == torch.bfloat16
     x = x.contiguous()
     w = w.contiguous()
-    out = torch.empty(n, cout, dtype=torch.bfloat16, device=x.device)
+    out = torch.empty(cout // 8, n, 8, dtype=torch.bfloat16, device=x.device)
     st = torch.cuda.current_stream(x.device).cuda_stream
     rc = _lib().hmfem_conv3d_fwd(x.data_ptr(), w.data_ptr(),
                                  bias.data_ptr() if bias is not None else None,
@@ -93,9 +110,10 @@ def conv3d_raw(x, w, bias, dims, relu):
 
 
 def conv3d_wgrad_raw(x, dy, dims):
-    """dw (27, cout, cin) fp32 = sum over cells dy[cell][co] x[cell + tap][ci]."""
+    """dw (27, cout, cin) fp32 = sum over cells dy[cell][co] x[cell + tap][ci];
+    x (cin/8, n, 8), dy (cout/8, n, 8)."""
     nx, ny, nz = dims
-    cin, cout = x.shape[1], dy.shape[1]
+    cin, cout = 8 * x.shape[0], 8 * dy.shape[0]
     dw = torch.zeros(27, cout, cin, dtype=torch.float32, device=x.device)
     st = torch.cuda.current_stream(x.device).cuda_stream
     rc = _lib().hmfem_conv3d_wgrad(x.contiguous().data_ptr(), dy.contiguous().data_ptr(),
@@ -128,7 +146,7 @@ class Conv3x3x3(torch.autograd.Function):
             g = g * (out > 0).to(g.dtype)
         gx = conv3d_raw(g, flip_transpose(wb), None, ctx.dims, False)
         gw = conv3d_wgrad_raw(x, g, ctx.dims)
-        gb = g.float().sum(0)
+        gb = g.float().sum(1).reshape(-1)
         return gx, gw, gb, None, None
 
 
@@ -136,20 +154,20 @@ def conv(x, w, b, dims, relu=True):
     return Conv3x3x3.apply(x, w, b, dims, relu)
 
 
-# ---- grid data movement (channels-last, dims (nx, ny, nz)) -----------------
+# ---- grid data movement (channel-blocked, dims (nx, ny, nz)) ---------------
 
 def pool2(x, dims):
     nx, ny, nz = dims
-    c = x.shape[1]
-    v = x.view(nz // 2, 2, ny // 2, 2, nx // 2, 2, c).float().mean(dim=(1, 3, 5))
-    return v.reshape(-1, c).to(x.dtype), (nx // 2, ny // 2, nz // 2)
+    s = x.shape[0]
+    v = x.view(s, nz // 2, 2, ny // 2, 2, nx // 2, 2, 8).float().mean(dim=(2, 4, 6))
+    return v.reshape(s, -1, 8).to(x.dtype), (nx // 2, ny // 2, nz // 2)
 
 
 def up2(x, dims):
     nx, ny, nz = dims
-    c = x.shape[1]
-    v = x.view(nz, 1, ny, 1, nx, 1, c).expand(nz, 2, ny, 2, nx, 2, c)
-    return v.reshape(-1, c), (2 * nx, 2 * ny, 2 * nz)
+    s = x.shape[0]
+    v = x.view(s, nz, 1, ny, 1, nx, 1, 8).expand(s, nz, 2, ny, 2, nx, 2, 8)
+    return v.reshape(s, -1, 8), (2 * nx, 2 * ny, 2 * nz)
 
 
 class UNet(torch.nn.Module):
@@ -176,7 +194,7 @@ class UNet(torch.nn.Module):
         return sum(p.numel() for p in self.parameters())
 
     def forward(self, feats, dims):
-        """feats (n, IN_CH) bf16 -> (n,) fp32 pressure correction."""
+        """feats (IN_CH/8, n, 8) bf16 -> (n,) fp32 pressure correction."""
         def block(x, a, b_, d):
             x = conv(x, self.w[a], self.b[a], d)
             return conv(x, self.w[b_], self.b[b_], d)
@@ -187,26 +205,26 @@ class UNet(torch.nn.Module):
         x, d2 = pool2(e1, d1)
         x = block(x, "bna", "bnb", d2)
         x, _ = up2(x, d2)
-        x = block(torch.cat([x, e1], 1), "d1a", "d1b", d1)
+        x = block(torch.cat([x, e1], 0), "d1a", "d1b", d1)
         x, _ = up2(x, d1)
-        x = block(torch.cat([x, e0], 1), "d0a", "d0b", d0)
-        return x.float() @ self.head + self.head_b
+        x = block(torch.cat([x, e0], 0), "d0a", "d0b", d0)
+        return torch.einsum("snc,sc->n", x.float(), self.head.view(-1, 8)) + self.head_b
 
 
 # ---- inputs and targets ------------------------------------------------------
 
 def features(K, mask, dims):
-    """(n, IN_CH) bf16 from device K (n,) and conduit mask (n,):
+    """(IN_CH/8, n, 8) bf16 from device K (n,) and conduit mask (n,):
     (log10 K + 14) / 2, the mask, the Dirichlet face mask (+1 at x = 0,
     -1 at x = 1) and zero channels up to IN_CH."""
     nx = dims[0]
     n = K.numel()
-    f = torch.zeros(n, IN_CH, dtype=torch.float32, device=K.device)
-    f[:, 0] = (torch.log10(K) + 14.0) / 2.0
+    f = torch.zeros(IN_CH // 8, n, 8, dtype=torch.float32, device=K.device)
+    f[0, :, 0] = (torch.log10(K) + 14.0) / 2.0
     if mask is not None:
-        f[:, 1] = mask.float()
+        f[0, :, 1] = mask.float()
     i = torch.arange(n, device=K.device) % nx
-    f[:, 2] = (i == 0).float() - (i == nx - 1).float()
+    f[0, :, 2] = (i == 0).float() - (i == nx - 1).float()
     return f.to(torch.bfloat16)
 
 

@@ -74,7 +74,7 @@ def make_dataset(seeds, size, device="cuda"):
         prob, K, mask = sample(sd, size, device)
         p, _ = solve(s, prob, K)
         dims = (size, size, size)
-        f3 = guess.features(K, mask, dims)[:, :3].contiguous()
+        f3 = guess.features(K, mask, dims)[0, :, :3].contiguous()
         target = (p - guess.linear_profile(dims, device)).float()
         pnorm = float(p.norm())
         data.append((f3, target, pnorm))
@@ -83,8 +83,8 @@ def make_dataset(seeds, size, device="cuda"):
 
 
 def _feats(f3):
-    f = torch.zeros(f3.shape[0], guess.IN_CH, dtype=torch.bfloat16, device=f3.device)
-    f[:, :3] = f3
+    f = torch.zeros(guess.IN_CH // 8, f3.shape[0], 8, dtype=torch.bfloat16, device=f3.device)
+    f[0, :, :3] = f3
     return f
 
 

@@ -3,8 +3,10 @@
  * guess).  No counterpart in the reference: the reference always starts its
  * CG from the previous pressure or zero.
  *
- * Tensors are device pointers.  Activations are channels-last BF16: cell
- * s = x + nx (y + ny z) holds C consecutive values.  3x3x3 weights are BF16
+ * Tensors are device pointers, 16-byte aligned.  Activations are
+ * channel-blocked BF16: C/8 slabs of the n = nx ny nz cells (s = x + nx (y +
+ * ny z)), 8 consecutive channels per cell -- channel c of cell s at
+ * ((c/8) n + s) * 8 + c % 8.  3x3x3 weights are BF16
  * [27][Cout][Cin] with tap t = 9 (dz+1) + 3 (dy+1) + (dx+1) (cross-
  * correlation, zero padding).  Supported (Cin, Cout): (16,16) (16,32)
  * (32,16) (32,32) (32,64) (64,32) (64,64) (96,32) (32,96) (48,16) (16,48).
@@ -26,12 +28,13 @@ int hmfem_conv3d_fwd(const void *in, const void *w, const float *bias, void *out
 
 /* The tiling hmfem_conv3d_fwd launches for this grid and channel counts on
  * a device with `nsm` SMs and `smem_max` bytes of opt-in shared memory per
- * block; host-only (no device call).  plan[20] = {bx, by, bz, W, H, hc, hcp,
+ * block; host-only (no device call).  plan[21] = {bx, by, bz, W, H, hc, hcp,
  * runs, rp, row_mode, ntx, nty, ntz, ns, nb, wres, tmem_cols, stage_bytes,
- * wbytes, smem_bytes}: the interior tile, the halo row pitch and rows per
- * plane, halo cells and cells per 8-channel slab, MMA runs per tile and per
- * z plane, row mode, tiles per axis, input stages, accumulator buffers,
- * resident weights, tensor-memory columns and shared-memory bytes. */
+ * wbytes, smem_bytes, xg}: the interior tile, the halo row pitch and rows
+ * per plane, halo cells and cells per 8-channel slab, MMA runs per tile and
+ * per z plane, row mode, tiles per axis, input stages, accumulator buffers,
+ * resident weights, tensor-memory columns, shared-memory bytes and whether
+ * the three x taps of each (dy, dz) share one MMA (N = 3 Cout). */
 int hmfem_conv3d_plan(int nx, int ny, int nz, int cin, int cout, int nsm, int smem_max,
                       int *plan);
 

@@ -1,11 +1,14 @@
 """The forward convolution's tiling, checked on the CPU: `hmfem_conv3d_plan`
 returns the plan `hmfem_conv3d_fwd` launches, and a numpy emulation of the
 kernel's addressing -- halo tile per 16-channel chunk, MMA runs of 128
-consecutive halo positions shifted per tap, the epilogue's validity test --
-must reproduce a direct 3x3x3 convolution, write every output cell exactly
-once, keep every operand row inside its stage (rows past the halo are NaN
-here, so a valid output that read one would show it), and fit the tensor
-memory, the shared memory and the descriptors' 14-bit fields."""
+consecutive halo positions shifted per tap (or, with grouped x taps, per
+(dy, dz) pair with the three dx products combined one row apart, boundary
+rows exchanged between consecutive runs of a z plane and zero otherwise),
+the epilogue's validity test -- must reproduce a direct 3x3x3 convolution,
+write every output cell exactly once, keep every operand row inside its
+stage (rows past the halo are NaN here, so a valid output that read one
+would show it), and fit the tensor memory, the shared memory and the
+descriptors' 14-bit fields."""
 import numpy as np
 import pytest
 
@@ -17,11 +20,17 @@ NSM = 148
 
 def _check_limits(p, cin, cout):
     assert p["ns"] >= 1 and p["nb"] in (1, 2)
-    assert p["nb"] * p["runs"] * cout <= p["tmem_cols"] <= 512
+    nacc = (3 if p["xg"] else 1) * cout
+    assert p["nb"] * p["runs"] * nacc <= p["tmem_cols"] <= 512
+    if p["xg"]:
+        assert 3 * cout <= 256 and p["ntx"] == 1          # the tile spans the x extent
     assert p["hcp"] % 8 == 0 and p["hcp"] >= p["hc"] + 128
     assert p["stage_bytes"] == 32 * p["hcp"] + (0 if p["wres"] else 27 * cout * 32)
-    assert p["wres"] == (cin == 16)
-    used = p["wbytes"] + p["ns"] * p["stage_bytes"] + 8 * (2 * p["ns"] + 2 * p["nb"] + 1) + 8
+    wall = 27 * cout * cin * 2                      # all chunks' weights
+    assert p["wres"] == (wall <= 64 * 1024)
+    assert p["wbytes"] == (wall if p["wres"] else 0)
+    assert 8 * (2 * p["ns"] + 2 * p["nb"] + 1) + 8 <= 128    # barriers, slot, flag
+    used = p["wbytes"] + p["ns"] * p["stage_bytes"] + 128 + (108 * cout if p["xg"] else 0) + 4 * cout
     assert used <= p["smem_bytes"] <= SMEM_MAX
     assert p["smem_bytes"] > SMEM_MAX // 2          # one CTA per SM
     assert p["smem_bytes"] < (1 << 18)              # 14-bit descriptor addresses
@@ -68,12 +77,32 @@ def emulate(x, w, dims, p):
                 g = (gx >= 0) & (gx < nx) & (gy >= 0) & (gy < ny) & (gz >= 0) & (gz < nz)
                 halo[:p["hc"]] = 0.0
                 halo[hq[g]] = grid[gz[g], gy[g], gx[g]]
-                for q0, plane, row in _run_starts(p):
-                    acc = np.zeros((128, cout))
-                    for t in range(27):
-                        lo = q0 + offs[t]
-                        assert 0 <= lo and lo + 128 <= p["hcp"]
-                        acc += halo[lo:lo + 128] @ w[t].T
+                starts = _run_starts(p)
+                if p["xg"]:
+                    D = []
+                    for q0, _, _ in starts:
+                        d = np.zeros((128, 3, cout))
+                        for g in range(9):
+                            lo = q0 + W * (g % 3 - 1) + W * H * (g // 3 - 1)
+                            assert 0 <= lo and lo + 128 <= p["hcp"]
+                            for dx in range(3):
+                                d[:, dx] += halo[lo:lo + 128] @ w[3 * g + dx].T
+                        D.append(d)
+                for r, (q0, plane, row) in enumerate(starts):
+                    if p["xg"]:
+                        rp = p["rp"]
+                        same_prev = not p["row_mode"] and r > 0 and r % rp != 0
+                        same_next = not p["row_mode"] and r + 1 < p["runs"] and (r + 1) % rp != 0
+                        prev = D[r - 1][127, 0] if same_prev else np.zeros(cout)
+                        nxt = D[r + 1][0, 2] if same_next else np.zeros(cout)
+                        acc = (np.vstack([prev[None], D[r][:127, 0]]) + D[r][:, 1]
+                               + np.vstack([D[r][1:, 2], nxt[None]]))
+                    else:
+                        acc = np.zeros((128, cout))
+                        for t in range(27):
+                            lo = q0 + offs[t]
+                            assert 0 <= lo and lo + 128 <= p["hcp"]
+                            acc += halo[lo:lo + 128] @ w[t].T
                     pos = q0 + q
                     zi, rem = divmod(pos, W * H)
                     yi, xi = divmod(rem, W)
@@ -103,7 +132,8 @@ def direct(x, w, dims):
 @pytest.mark.parametrize("dims,cin,cout", [
     ((9, 7, 5), 16, 16), ((20, 16, 12), 32, 64), ((11, 6, 7), 96, 32),
     ((20, 16, 12), 48, 16), ((8, 12, 8), 32, 96), ((130, 5, 3), 16, 16),
-    ((128, 9, 4), 16, 32), ((257, 3, 2), 48, 16), ((64, 10, 3), 16, 32)])
+    ((128, 9, 4), 16, 32), ((257, 3, 2), 48, 16), ((64, 10, 3), 16, 32),
+    ((128, 7, 3), 48, 16), ((40, 9, 5), 16, 48), ((33, 20, 6), 32, 64)])
 def test_emulated_tiling_matches_direct_convolution(dims, cin, cout):
     p = guess.conv_plan(dims, cin, cout, NSM, SMEM_MAX)
     _check_limits(p, cin, cout)

@@ -34,6 +34,13 @@ def _w_torch(w):  # (27, cout, cin) -> (cout, cin, kz, ky, kx)
     return w.view(3, 3, 3, w.shape[1], w.shape[2]).permute(3, 4, 0, 1, 2)
 
 
+def _fwd(x, w, b, dims, relu):
+    """The kernel on channels-last (n, C) tensors (it takes channel-blocked ones)."""
+    out = guess.conv3d_raw(guess.blocked(x.cuda()), w.cuda(),
+                           None if b is None else b.cuda(), dims, relu)
+    return guess.unblocked(out).cpu().double()
+
+
 def _rel(a, b):
     return float((a - b).norm() / max(float(b.norm()), 1e-30))
 
@@ -46,11 +53,11 @@ def test_forward_matches_conv3d(cin, cout, dims):
     x = torch.randn(n, cin, generator=g).bfloat16()
     w = (torch.randn(27, cout, cin, generator=g) * 0.1).bfloat16()
     b = torch.randn(cout, generator=g)
-    ours = guess.conv3d_raw(x.cuda(), w.cuda(), b.cuda(), dims, False).cpu().double()
+    ours = _fwd(x, w, b, dims, False)
     ref = _from_ncdhw(F.conv3d(_to_ncdhw(x.double(), dims), _w_torch(w.double()),
                                b.double(), padding=1))
     assert _rel(ours, ref) < 6e-3   # BF16 output rounding
-    relu = guess.conv3d_raw(x.cuda(), w.cuda(), b.cuda(), dims, True).cpu().double()
+    relu = _fwd(x, w, b, dims, True)
     assert _rel(relu, ref.clamp(min=0)) < 6e-3
     guess.check_errors()
 
@@ -62,7 +69,8 @@ def test_weight_gradient_matches_conv3d(cin, cout, dims):
     n = dims[0] * dims[1] * dims[2]
     x = torch.randn(n, cin, generator=g).bfloat16()
     dy = torch.randn(n, cout, generator=g).bfloat16()
-    ours = guess.conv3d_wgrad_raw(x.cuda(), dy.cuda(), dims).cpu().double()
+    ours = guess.conv3d_wgrad_raw(guess.blocked(x.cuda()), guess.blocked(dy.cuda()),
+                                  dims).cpu().double()
     ref = torch.nn.grad.conv3d_weight(_to_ncdhw(x.double(), dims), (cout, cin, 3, 3, 3),
                                       _to_ncdhw(dy.double(), dims), padding=1)
     ref = ref.permute(2, 3, 4, 0, 1).reshape(27, cout, cin)
@@ -77,8 +85,7 @@ def test_data_gradient_is_flipped_forward(cin, cout):
     n = dims[0] * dims[1] * dims[2]
     w = (torch.randn(27, cout, cin, generator=g) * 0.1).bfloat16()
     dy = torch.randn(n, cout, generator=g).bfloat16()
-    ours = guess.conv3d_raw(dy.cuda(), guess.flip_transpose(w.cuda()), None, dims,
-                            False).cpu().double()
+    ours = _fwd(dy, guess.flip_transpose(w), None, dims, False)
     ref = torch.nn.grad.conv3d_input((1, cin, dims[2], dims[1], dims[0]), _w_torch(w.double()),
                                      _to_ncdhw(dy.double(), dims), padding=1)
     assert _rel(ours, _from_ncdhw(ref)) < 6e-3

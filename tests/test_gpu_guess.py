@@ -30,7 +30,7 @@ def test_unet_matches_float64_network_and_gradients():
     for p in ref_model.parameters():
         p.data = p.data.bfloat16().double()
     ref = _ref_forward_with_grad(ref_model, feats.double(), dims)
-    out = model(feats.cuda(), dims)
+    out = model(guess.blocked(feats.cuda()), dims)   # the network takes channel-blocked input
     rel = float((out.detach().cpu().double() - ref.detach()).norm() / ref.detach().norm())
     assert rel < 5e-2  # BF16 activations between layers
     # gradients of a loss: tensor-core backward vs float64 autograd
