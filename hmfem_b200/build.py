@@ -19,7 +19,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=default", "--expt-relaxed-constexpr",
          "--extended-lambda"]
 SOURCES = ["assemble.cu", "sparse.cu", "amg_setup.cu", "rap_stencil.cu", "rap19.cu", "stencil_cycle.cu", "smoother_setup.cu", "cycle.cu", "solver.cu",
-           "device_abi.cu", "noalloc.cu", "conv3d.cu", "karst.cu", "textio.cu", "permio.cu"]
+           "device_abi.cu", "noalloc.cu", "conv3d.cu", "guess_ops.cu", "karst.cu", "textio.cu", "permio.cu"]
 
 
 def _deps():

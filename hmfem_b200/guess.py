@@ -4,10 +4,12 @@ to a pressure guess for the CG.  No counterpart in the reference.
 
 Every 3x3x3 convolution -- forward, data gradient and weight gradient --
 runs on this library's tcgen05 tensor-core kernels (`hmfem_conv3d_fwd`,
-`hmfem_conv3d_wgrad`: BF16 operands, FP32 accumulation).  PyTorch is the
-training driver around them: autograd bookkeeping, the 2x average pooling,
-nearest upsampling and channel concatenation (pure data movement), the 1x1
-head and the Adam update of the FP32 master weights.
+`hmfem_conv3d_wgrad`: BF16 operands, FP32 accumulation), and so do the
+features, the 2x average pooling and the nearest upsampling fused with the
+skip concatenation (`hmfem_guess_*`, one HBM pass each) and, at inference,
+the 1x1 head fused with the linear profile.  PyTorch is the training driver
+around them: autograd bookkeeping, the head while training and the Adam
+update of the FP32 master weights.
 
 Activations are channel-blocked: a grid of n = nx*ny*nz cells with C
 channels is a (C/8, n, 8) BF16 tensor -- slab k holds channels 8k..8k+7 of
@@ -39,6 +41,11 @@ def _lib():
         L.hmfem_conv3d_fwd.argtypes = [vp, vp, vp, vp, i, i, i, i, i, i, vp, vp]
         L.hmfem_conv3d_wgrad.argtypes = [vp, vp, vp, i, i, i, i, i, vp, vp]
         L.hmfem_conv3d_plan.argtypes = [i, i, i, i, i, i, i, vp]
+        L.hmfem_guess_features.argtypes = [vp, vp, i, i, i, vp, vp]
+        L.hmfem_guess_pool2.argtypes = [vp, i, i, i, i, vp, vp]
+        L.hmfem_guess_up2_cat.argtypes = [vp, i, vp, i, i, i, i, vp, vp]
+        L.hmfem_guess_up2_grad.argtypes = [vp, i, i, i, i, vp, vp]
+        L.hmfem_guess_head_profile.argtypes = [vp, i, vp, vp, i, i, i, vp, vp]
         L._guess_bound = True
     return L
 
@@ -156,18 +163,71 @@ def conv(x, w, b, dims, relu=True):
 
 # ---- grid data movement (channel-blocked, dims (nx, ny, nz)) ---------------
 
+def _stream(t):
+    return torch.cuda.current_stream(t.device).cuda_stream
+
+
+def _rc(rc):
+    if rc != 0:
+        raise gpu.HmfemError(rc, gpu.last_error())
+
+
+class _Pool2(torch.autograd.Function):
+    """2x2x2 average pooling; the gradient spreads 1/8 to each fine cell."""
+
+    @staticmethod
+    def forward(ctx, x, dims):
+        nx, ny, nz = dims
+        x = x.contiguous()
+        out = torch.empty(x.shape[0], x.shape[1] // 8, 8, dtype=x.dtype, device=x.device)
+        _rc(_lib().hmfem_guess_pool2(x.data_ptr(), x.shape[0], nx, ny, nz, out.data_ptr(),
+                                     _stream(x)))
+        ctx.dims = dims
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        nx, ny, nz = ctx.dims
+        g = g.contiguous()
+        out = torch.empty(g.shape[0], 8 * g.shape[1], 8, dtype=g.dtype, device=g.device)
+        _rc(_lib().hmfem_guess_up2_cat(g.data_ptr(), g.shape[0], None, 0, nx, ny, nz,
+                                       out.data_ptr(), _stream(g)))
+        return out * 0.125, None
+
+
+class _Up2Cat(torch.autograd.Function):
+    """[nearest-upsampled coarse | skip] on the fine grid; the coarse
+    gradient sums the 8 fine cells', the skip's is its slabs."""
+
+    @staticmethod
+    def forward(ctx, coarse, skip, dims):
+        nx, ny, nz = dims
+        coarse, skip = coarse.contiguous(), skip.contiguous()
+        sa, sb = coarse.shape[0], skip.shape[0]
+        out = torch.empty(sa + sb, skip.shape[1], 8, dtype=skip.dtype, device=skip.device)
+        _rc(_lib().hmfem_guess_up2_cat(coarse.data_ptr(), sa, skip.data_ptr(), sb, nx, ny, nz,
+                                       out.data_ptr(), _stream(skip)))
+        ctx.dims, ctx.sa = dims, sa
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        nx, ny, nz = ctx.dims
+        g = g.contiguous()
+        ga = torch.empty(ctx.sa, g.shape[1] // 8, 8, dtype=g.dtype, device=g.device)
+        _rc(_lib().hmfem_guess_up2_grad(g.data_ptr(), ctx.sa, nx, ny, nz, ga.data_ptr(),
+                                        _stream(g)))
+        return ga, g[ctx.sa:], None
+
+
 def pool2(x, dims):
     nx, ny, nz = dims
-    s = x.shape[0]
-    v = x.view(s, nz // 2, 2, ny // 2, 2, nx // 2, 2, 8).float().mean(dim=(2, 4, 6))
-    return v.reshape(s, -1, 8).to(x.dtype), (nx // 2, ny // 2, nz // 2)
+    return _Pool2.apply(x, dims), (nx // 2, ny // 2, nz // 2)
 
 
-def up2(x, dims):
-    nx, ny, nz = dims
-    s = x.shape[0]
-    v = x.view(s, nz, 1, ny, 1, nx, 1, 8).expand(s, nz, 2, ny, 2, nx, 2, 8)
-    return v.reshape(s, -1, 8), (2 * nx, 2 * ny, 2 * nz)
+def up2_cat(coarse, skip, dims):
+    """Upsample `coarse` to the fine grid `dims` and append `skip`'s slabs."""
+    return _Up2Cat.apply(coarse, skip, dims)
 
 
 class UNet(torch.nn.Module):
@@ -193,8 +253,8 @@ class UNet(torch.nn.Module):
     def n_params(self):
         return sum(p.numel() for p in self.parameters())
 
-    def forward(self, feats, dims):
-        """feats (IN_CH/8, n, 8) bf16 -> (n,) fp32 pressure correction."""
+    def trunk(self, feats, dims):
+        """feats (IN_CH/8, n, 8) bf16 -> the last activation (2, n, 8) bf16."""
         def block(x, a, b_, d):
             x = conv(x, self.w[a], self.b[a], d)
             return conv(x, self.w[b_], self.b[b_], d)
@@ -204,10 +264,12 @@ class UNet(torch.nn.Module):
         e1 = block(x, "e1a", "e1b", d1)
         x, d2 = pool2(e1, d1)
         x = block(x, "bna", "bnb", d2)
-        x, _ = up2(x, d2)
-        x = block(torch.cat([x, e1], 0), "d1a", "d1b", d1)
-        x, _ = up2(x, d1)
-        x = block(torch.cat([x, e0], 0), "d0a", "d0b", d0)
+        x = block(up2_cat(x, e1, d1), "d1a", "d1b", d1)
+        return block(up2_cat(x, e0, d0), "d0a", "d0b", d0)
+
+    def forward(self, feats, dims):
+        """feats (IN_CH/8, n, 8) bf16 -> (n,) fp32 pressure correction."""
+        x = self.trunk(feats, dims)
         return torch.einsum("snc,sc->n", x.float(), self.head.view(-1, 8)) + self.head_b
 
 
@@ -217,15 +279,13 @@ def features(K, mask, dims):
     """(IN_CH/8, n, 8) bf16 from device K (n,) and conduit mask (n,):
     (log10 K + 14) / 2, the mask, the Dirichlet face mask (+1 at x = 0,
     -1 at x = 1) and zero channels up to IN_CH."""
-    nx = dims[0]
-    n = K.numel()
-    f = torch.zeros(IN_CH // 8, n, 8, dtype=torch.float32, device=K.device)
-    f[0, :, 0] = (torch.log10(K) + 14.0) / 2.0
-    if mask is not None:
-        f[0, :, 1] = mask.float()
-    i = torch.arange(n, device=K.device) % nx
-    f[0, :, 2] = (i == 0).float() - (i == nx - 1).float()
-    return f.to(torch.bfloat16)
+    nx, ny, nz = dims
+    K = K.to(torch.float64).contiguous()
+    m = None if mask is None else mask.to(torch.uint8).contiguous()
+    f = torch.empty(IN_CH // 8, K.numel(), 8, dtype=torch.bfloat16, device=K.device)
+    _rc(_lib().hmfem_guess_features(K.data_ptr(), None if m is None else m.data_ptr(),
+                                    nx, ny, nz, f.data_ptr(), _stream(K)))
+    return f
 
 
 def linear_profile(dims, device="cuda"):
@@ -236,10 +296,17 @@ def linear_profile(dims, device="cuda"):
 
 
 def predict(model, K, mask, dims):
-    """FP64 pressure guess on the device."""
+    """FP64 pressure guess on the device: the trunk, then the 1x1 head and
+    the linear profile in one kernel."""
+    nx, ny, nz = dims
     with torch.no_grad():
-        corr = model(features(K, mask, dims), dims)
-    return linear_profile(dims, K.device) + corr.double()
+        x = model.trunk(features(K, mask, dims), dims).contiguous()
+        p = torch.empty(K.numel(), dtype=torch.float64, device=K.device)
+        w = model.head.detach().float().contiguous()
+        b = model.head_b.detach().float().contiguous()
+        _rc(_lib().hmfem_guess_head_profile(x.data_ptr(), x.shape[0], w.data_ptr(),
+                                            b.data_ptr(), nx, ny, nz, p.data_ptr(), _stream(x)))
+    return p
 
 
 def save(model, path):

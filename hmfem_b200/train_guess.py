@@ -8,8 +8,14 @@ Gaussian field of correlation length 8 cells (seeded white noise, FFT
 filtered on the GPU), 0-6 random-walk conduits at K = 1e-10, Dirichlet 1/0
 on the x faces, no flow elsewhere; seeds 0..train-1 train, the next `eval`
 seeds evaluate.  Targets are this solver's FP64 pressures (relres 1e-8);
-the net learns the correction to the linear profile 1 - (i + 1/2)/nx with a
-relative-L2 pressure loss.  Evaluation solves every held-out grid to
+the net learns the correction to the linear profile 1 - (i + 1/2)/nx.  The
+loss (--loss) measures the guess's error e = p_guess - p the way the CG
+sees it, relative to the linear profile's error e_lin:
+  energy    e^T A e / e_lin^T A e_lin   (A-norm; gradient 2 A e)
+  residual  |A e|^2 / |A e_lin|^2       (the initial residual; 2 A A e)
+  l2        |e| / |p|                   (plain pressure error)
+with A this sample's TPFA matrix (FP64 SpMV of the solver) and the head's
+output in FP32.  Evaluation solves every held-out grid to
 ||b - A x|| / ||b|| <= 1e-10 from the zero guess and from the net's guess
 (inference included in the timed path) and prints one JSON line.
 """
@@ -18,6 +24,7 @@ from __future__ import annotations
 import argparse
 import json
 import math
+import os
 import time
 
 import numpy as np
@@ -25,6 +32,9 @@ import torch
 
 from . import gpu, guess
 from .problem import Problem, random_walk_conduit
+
+# the shipped model: A-norm loss, seeds 0-2047 at 128^3, 4 epochs
+MODEL_PATH = os.path.join(os.path.dirname(__file__), "models", "unet_config4.npz")
 
 
 def gaussian_field_gpu(gen, n, corr, device="cuda"):
@@ -67,19 +77,55 @@ def solve(solver, prob, K, x=None):
     return x, st
 
 
+class Sample:
+    """One training grid: input features, K (FP32; the matrix is assembled
+    again from it for the A-norm and residual losses), the target correction
+    p - p_lin (FP64) and the loss normalisers."""
+
+    def __init__(self, f3, K32, target, pnorm, e_energy, e_resid):
+        self.f3, self.K32, self.target = f3, K32, target
+        self.pnorm, self.e_energy, self.e_resid = pnorm, e_energy, e_resid
+
+
 def make_dataset(seeds, size, device="cuda"):
     s = gpu.Solver(precision=1, tol=1e-8)
     data = []
+    dims = (size, size, size)
     for sd in seeds:
         prob, K, mask = sample(sd, size, device)
         p, _ = solve(s, prob, K)
-        dims = (size, size, size)
         f3 = guess.features(K, mask, dims)[0, :, :3].contiguous()
-        target = (p - guess.linear_profile(dims, device)).float()
-        pnorm = float(p.norm())
-        data.append((f3, target, pnorm))
+        target = p - guess.linear_profile(dims, device)        # -e_lin
+        K32 = K.float()
+        s.assemble(prob, KX=K32.double(), KY=K32.double(), KZ=K32.double())
+        At = s.spmv(0, target)
+        data.append(Sample(f3, K32, target, float(p.norm()), float(target @ At),
+                           float(At @ At)))
     s.close()
     return data
+
+
+class GuessLoss(torch.autograd.Function):
+    """energy: e^T A e / E0 (d/de = 2 A e / E0); residual: |A e|^2 / R0
+    (d/de = 2 A A e / R0); e = corr - target in FP64."""
+
+    @staticmethod
+    def forward(ctx, corr, target, solver, norm, kind):
+        e = corr.double() - target
+        Ae = solver.spmv(0, e)
+        if kind == "energy":
+            ctx.save_for_backward(Ae)
+            val = (e @ Ae) / norm
+        else:
+            ctx.save_for_backward(solver.spmv(0, Ae))
+            val = (Ae @ Ae) / norm
+        ctx.norm = norm
+        return val.float()
+
+    @staticmethod
+    def backward(ctx, g):
+        (v,) = ctx.saved_tensors
+        return (2.0 * g.double() * v / ctx.norm).float(), None, None, None, None
 
 
 def _feats(f3):
@@ -88,8 +134,10 @@ def _feats(f3):
     return f
 
 
-def train(model, data, size, epochs, lr=1e-3, log_every=0):
+def train(model, data, size, epochs, lr=1e-3, log_every=0, loss_kind="l2"):
     dims = (size, size, size)
+    solver = gpu.Solver(precision=1) if loss_kind != "l2" else None
+    prob = sample_problem(size)
     opt = torch.optim.Adam(model.parameters(), lr=lr)
     steps = epochs * len(data)
     sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, T_max=max(1, steps))
@@ -98,9 +146,15 @@ def train(model, data, size, epochs, lr=1e-3, log_every=0):
     k = 0
     for ep in range(epochs):
         for i in order.permutation(len(data)):
-            f3, target, pnorm = data[i]
-            pred = model(_feats(f3), dims)
-            loss = (pred - target).norm() / pnorm
+            d = data[i]
+            pred = model(_feats(d.f3), dims)
+            if loss_kind == "l2":
+                loss = (pred.double() - d.target).norm() / d.pnorm
+            else:
+                K = d.K32.double()
+                solver.assemble(prob, KX=K, KY=K, KZ=K)
+                norm = d.e_energy if loss_kind == "energy" else d.e_resid
+                loss = GuessLoss.apply(pred, d.target, solver, norm, loss_kind)
             opt.zero_grad(set_to_none=True)
             loss.backward()
             torch.nn.utils.clip_grad_norm_(model.parameters(), 1.0)
@@ -110,7 +164,15 @@ def train(model, data, size, epochs, lr=1e-3, log_every=0):
             if log_every and k % log_every == 0:
                 hist.append((k, float(loss.detach())))
     guess.check_errors()
+    if solver is not None:
+        solver.close()
     return hist
+
+
+def sample_problem(size):
+    """The Problem (dims, spacing, boundary conditions) of a training grid."""
+    dummy = np.zeros(1)
+    return Problem(size, size, size, 1.0 / size, 1.0 / size, 1.0 / size, dummy, dummy, dummy)
 
 
 def evaluate(model, seeds, size, device="cuda", tol=1e-10):
@@ -126,16 +188,25 @@ def evaluate(model, seeds, size, device="cuda", tol=1e-10):
         t_zero = time.perf_counter() - t0
         t0 = time.perf_counter()
         xg = guess.predict(model, K, mask, dims)
-        e_guess = float((xg - x0).norm() / x0.norm())
-        x1, st1 = solve(s, prob, K, xg)
+        x1, st1 = solve(s, prob, K, xg.clone())   # the solve overwrites its guess
         torch.cuda.synchronize()
         t_net = time.perf_counter() - t0
+        e_guess = float((xg - x0).norm() / x0.norm())
         xl = guess.linear_profile(dims, device)
         e_lin = float((xl - x0).norm() / x0.norm())
+        # the guesses' errors as the CG sees them, relative to the profile's
+        # (A of this grid is assembled: the last solve)
+        en, rn = [], []
+        for xx in (xg, xl):
+            e = xx - x0
+            Ae = s.spmv(0, e)
+            en.append(float(e @ Ae))
+            rn.append(float(Ae.norm()))
         xl, stl = solve(s, prob, K, xl)
         rows.append(dict(seed=sd, it_zero=st0["iterations"], it_net=st1["iterations"],
                          it_linear=stl["iterations"], t_zero=t_zero, t_net=t_net,
                          err_guess=e_guess, err_linear=e_lin,
+                         energy_ratio=en[0] / en[1], resid_ratio=rn[0] / rn[1],
                          relres_net=st1["relres"], diff=float((x1 - x0).norm() / x0.norm())))
     s.close()
     return rows
@@ -164,6 +235,7 @@ def main():
     ap.add_argument("--epochs", type=int, default=4)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default="unet_guess.npz")
+    ap.add_argument("--loss", default="energy", choices=("energy", "residual", "l2"))
     ap.add_argument("--infer-only", action="store_true",
                     help="time one inference at --size (no training) and exit")
     args = ap.parse_args()
@@ -176,7 +248,8 @@ def main():
     t_data = time.perf_counter() - t0
     model = guess.UNet().cuda()
     t0 = time.perf_counter()
-    hist = train(model, data, args.size, args.epochs, args.lr, log_every=256)
+    hist = train(model, data, args.size, args.epochs, args.lr, log_every=256,
+                 loss_kind=args.loss)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     del data
@@ -192,6 +265,8 @@ def main():
         "iterations_linear_guess": mean("it_linear"),
         "time_zero_guess_ms": 1e3 * mean("t_zero"), "time_net_guess_ms": 1e3 * mean("t_net"),
         "guess_rel_error": mean("err_guess"), "linear_rel_error": mean("err_linear"),
+        "loss": args.loss, "guess_energy_vs_linear": mean("energy_ratio"),
+        "guess_residual_vs_linear": mean("resid_ratio"),
         "max_relres_net": max(r["relres_net"] for r in rows),
         "max_pressure_diff_vs_zero_guess": max(r["diff"] for r in rows),
         "out": args.out}), flush=True)

@@ -43,6 +43,31 @@ int hmfem_conv3d_plan(int nx, int ny, int nz, int cin, int cout, int nsm, int sm
 int hmfem_conv3d_wgrad(const void *x, const void *dy, float *dw, int nx, int ny, int nz,
                        int cin, int cout, int *err, void *stream);
 
+/* The data movement around the convolutions (one HBM pass each; even grid
+ * dimensions where a 2x level is involved).  Features: out[2][n][8] =
+ * ((log10 K + 14)/2, conduit mask (NULL: 0), Dirichlet face mask +1 at x = 0
+ * and -1 at x = nx-1, zeros) from device K (FP64) and mask (uint8). */
+int hmfem_guess_features(const double *K, const unsigned char *mask, int nx, int ny, int nz,
+                         void *out, void *stream);
+
+/* 2x2x2 average pooling of `slabs` slabs of the fine grid nx x ny x nz. */
+int hmfem_guess_pool2(const void *x, int slabs, int nx, int ny, int nz, void *out, void *stream);
+
+/* out = [nearest-upsampled coarse (slabs_a slabs of the nx/2 x ny/2 x nz/2
+ * grid) | skip (slabs_b slabs of the nx x ny x nz grid)]. */
+int hmfem_guess_up2_cat(const void *coarse, int slabs_a, const void *skip, int slabs_b, int nx,
+                        int ny, int nz, void *out, void *stream);
+
+/* The gradient of the upsampling: out (slabs_a slabs of the coarse grid) =
+ * the sum of the gradients of each coarse cell's 8 fine cells. */
+int hmfem_guess_up2_grad(const void *g, int slabs_a, int nx, int ny, int nz, void *out,
+                         void *stream);
+
+/* p[s] = 1 - (x + 1/2)/nx + sum_c x[c] w[c] + b[0] (FP32 head, FP64 out):
+ * the guess from the last activation (8 * slabs head weights). */
+int hmfem_guess_head_profile(const void *x, int slabs, const float *w, const float *b, int nx,
+                             int ny, int nz, double *p, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
