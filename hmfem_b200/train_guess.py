@@ -3,11 +3,12 @@
     python -m hmfem_b200.train_guess --size 128 --train 2048 --eval 256 \\
         --epochs 4 --out unet_guess.npz
 
-Data (config 4 distribution): log10 K = -14 + 1.5 g with g a unit-variance
-Gaussian field of correlation length 8 cells (seeded white noise, FFT
-filtered on the GPU), 0-6 random-walk conduits at K = 1e-10, Dirichlet 1/0
-on the x faces, no flow elsewhere; seeds 0..train-1 train, the next `eval`
-seeds evaluate.  Targets are this solver's FP64 pressures (relres 1e-8);
+Data: log10 K = -14 + 1.5 g with g a unit-variance Gaussian field of
+correlation length 8 cells (seeded white noise, FFT filtered on the GPU)
+and random-walk conduits, Dirichlet 1/0 on the x faces, no flow elsewhere
+(--dist): config4 = 0-6 conduits at K = 1e-10, config2 = 0-8 at 1e-9 (the
+256^3 headline problem's kind), mixed = the two alternately by seed parity;
+seeds 0..train-1 train, the next `eval` seeds (config-4 kind) evaluate.  Targets are this solver's FP64 pressures (relres 1e-8);
 the net learns the correction to the linear profile 1 - (i + 1/2)/nx.  The
 loss (--loss) measures the guess's error e = p_guess - p the way the CG
 sees it, relative to the linear profile's error e_lin:
@@ -51,15 +52,25 @@ def gaussian_field_gpu(gen, n, corr, device="cuda"):
     return (g / g.std()).reshape(-1)
 
 
-def sample(seed, size, device="cuda"):
+DISTS = {"config4": (7, 1e-10), "config2": (9, 1e-9)}  # (conduits < n, K of a conduit)
+
+
+def dist_of(seed, dist):
+    """The distribution of a seed: `dist`, or for "mixed" config4 on even
+    seeds and config2 on odd ones."""
+    return ("config2" if seed % 2 else "config4") if dist == "mixed" else dist
+
+
+def sample(seed, size, device="cuda", dist="config4"):
     """(Problem without host K, device K, device conduit mask) of one seed."""
+    n_max, k_conduit = DISTS[dist_of(seed, dist)]
     rng = np.random.default_rng(1400 + seed)
     gen = torch.Generator(device=device).manual_seed(77_000 + seed)
     K = 10.0 ** (-14.0 + 1.5 * gaussian_field_gpu(gen, size, 8.0, device))
     mask = torch.zeros(size ** 3, dtype=torch.uint8, device=device)
-    for _ in range(int(rng.integers(0, 7))):
+    for _ in range(int(rng.integers(0, n_max))):
         c = torch.as_tensor(random_walk_conduit(rng, size, size, size), device=device)
-        K[c] = 1e-10
+        K[c] = k_conduit
         mask[c] = 1
     dummy = np.zeros(1)
     p = Problem(size, size, size, 1.0 / size, 1.0 / size, 1.0 / size, dummy, dummy, dummy)
@@ -87,12 +98,12 @@ class Sample:
         self.pnorm, self.e_energy, self.e_resid = pnorm, e_energy, e_resid
 
 
-def make_dataset(seeds, size, device="cuda"):
+def make_dataset(seeds, size, device="cuda", dist="config4"):
     s = gpu.Solver(precision=1, tol=1e-8)
     data = []
     dims = (size, size, size)
     for sd in seeds:
-        prob, K, mask = sample(sd, size, device)
+        prob, K, mask = sample(sd, size, device, dist)
         p, _ = solve(s, prob, K)
         f3 = guess.features(K, mask, dims)[0, :, :3].contiguous()
         target = p - guess.linear_profile(dims, device)        # -e_lin
@@ -236,6 +247,7 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default="unet_guess.npz")
     ap.add_argument("--loss", default="energy", choices=("energy", "residual", "l2"))
+    ap.add_argument("--dist", default="config4", choices=("config4", "config2", "mixed"))
     ap.add_argument("--infer-only", action="store_true",
                     help="time one inference at --size (no training) and exit")
     args = ap.parse_args()
@@ -244,7 +256,7 @@ def main():
         return
     torch.manual_seed(0)
     t0 = time.perf_counter()
-    data = make_dataset(range(args.train), args.size)
+    data = make_dataset(range(args.train), args.size, dist=args.dist)
     t_data = time.perf_counter() - t0
     model = guess.UNet().cuda()
     t0 = time.perf_counter()
@@ -265,7 +277,7 @@ def main():
         "iterations_linear_guess": mean("it_linear"),
         "time_zero_guess_ms": 1e3 * mean("t_zero"), "time_net_guess_ms": 1e3 * mean("t_net"),
         "guess_rel_error": mean("err_guess"), "linear_rel_error": mean("err_linear"),
-        "loss": args.loss, "guess_energy_vs_linear": mean("energy_ratio"),
+        "loss": args.loss, "dist": args.dist, "guess_energy_vs_linear": mean("energy_ratio"),
         "guess_residual_vs_linear": mean("resid_ratio"),
         "max_relres_net": max(r["relres_net"] for r in rows),
         "max_pressure_diff_vs_zero_guess": max(r["diff"] for r in rows),
