@@ -187,7 +187,7 @@ __host__ __device__ constexpr int tmem_cols(int n)
 // tap (dx, dy, dz) for the run is the same rows shifted by dx + W dy + W H dz,
 // i.e. the run's descriptor with another start address: the 27 taps read the
 // tile that was copied once.  Row mode (bx = 128): a run is one x row of the
-// tile.  Plane mode (bx = nx < 128): the runs of a z plane cover its interior
+// tile.  Plane mode (bx = nx, any width): the runs of a z plane cover its interior
 // rows in steps of 128 positions; positions on halo columns or beyond the
 // plane are computed and dropped by the epilogue.  The copy of a tile reads
 // (bx+2)(by+2)(bz+2) / (bx by bz) times its cells from L2.
@@ -236,6 +236,7 @@ constexpr int kConvThreads = 192;  // warps 0-3 epilogue, 4 TMA producer, 5 MMA
 constexpr int kEpilogue = 128;
 constexpr unsigned kWResMax = 64 * 1024;  // resident weights (all chunks) up to this size
 constexpr unsigned kBarBytes = 128;       // mbarriers (ns, nb <= 4), TMEM slot, abort flag
+constexpr int kMaxPlaneX = 1024;          // widest grid a plane-mode tile spans
 
 // shared memory after the stages: barriers, then (grouped x taps) three
 // exchange buffers of 4 + 4 + 1 boundary rows of COUT floats, then the bias
@@ -820,8 +821,8 @@ k_conv3d_wgrad(const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restr
     if (warp == 0) tmem_free(tmem, NCOL);
 }
 
-// Tile choice for a forward launch: bx = 128 (row mode) when nx >= 128, else
-// the whole x extent; the form (x taps grouped or not) and (by, bz)
+// Tile choice for a forward launch: row mode (bx = 128) or plane mode (bx =
+// nx, the whole x extent); the mode, the form (x taps grouped or not) and (by, bz)
 // minimise an estimate of the makespan -- per tile the largest of the MMA
 // issue (~42 cycles per MMA up to N = 84, N/2 above: the A operand read),
 // the halo copy (a bulk copy per row and slab plus its bytes) and the
@@ -835,15 +836,20 @@ ConvPlan plan_conv(int nx, int ny, int nz, int cin, int cout, int nsm, int smem_
     ConvPlan best{};
     double best_cost = 1e300;
     const int kc = cin / 16;
-    const int bx = nx >= 128 ? 128 : nx;
-    const bool row_mode = bx == 128;
-    const int W = bx + 2;
     const unsigned wchunk = 27u * (unsigned)cout * 32u;
-    // grouped x taps need N = 3 COUT <= 256 and tiles spanning the x extent
-    const int xg_max = (3 * cout <= 256 && nx <= 128) ? 1 : 0;
-    for (int xg = 0; xg <= xg_max; xg++)
+    // row mode (bx = 128, x tiles) when nx >= 128; plane mode (bx = nx, the
+    // whole x extent) for any width up to kMaxPlaneX
+    for (int pm = 0; pm < 2; pm++)
+    for (int xg = 0; xg < 2; xg++)
         for (int bz = 1; bz <= (nz < 16 ? nz : 16); bz++)
             for (int by = 1; by <= (ny < 64 ? ny : 64); by++) {
+                const bool row_mode = pm == 0;
+                if (row_mode ? nx < 128 : nx > kMaxPlaneX) continue;
+                const int bx = row_mode ? 128 : nx;
+                const int W = bx + 2;
+                // grouped x taps need N = 3 COUT <= 256 and tiles spanning
+                // the x extent (their x neighbours outside the tile are zero)
+                if (xg && (3 * cout > 256 || (row_mode && nx != 128))) continue;
                 ConvPlan p{};
                 p.bx = bx;
                 p.by = by;

@@ -38,6 +38,7 @@ def _check_limits(p, cin, cout):
     if p["row_mode"]:
         assert p["bx"] == 128 and p["rp"] == p["by"]
     else:
+        assert p["ntx"] == 1   # plane mode spans the x extent
         assert p["rp"] == -(-(p["W"] * (p["by"] - 1) + p["bx"]) // 128)
     assert p["runs"] == p["bz"] * p["rp"]
 
@@ -133,11 +134,12 @@ def direct(x, w, dims):
     ((9, 7, 5), 16, 16), ((20, 16, 12), 32, 64), ((11, 6, 7), 96, 32),
     ((20, 16, 12), 48, 16), ((8, 12, 8), 32, 96), ((130, 5, 3), 16, 16),
     ((128, 9, 4), 16, 32), ((257, 3, 2), 48, 16), ((64, 10, 3), 16, 32),
-    ((128, 7, 3), 48, 16), ((40, 9, 5), 16, 48), ((33, 20, 6), 32, 64)])
+    ((128, 7, 3), 48, 16), ((40, 9, 5), 16, 48), ((33, 20, 6), 32, 64),
+    ((256, 3, 2), 48, 16), ((200, 4, 3), 16, 16)])
 def test_emulated_tiling_matches_direct_convolution(dims, cin, cout):
     p = guess.conv_plan(dims, cin, cout, NSM, SMEM_MAX)
     _check_limits(p, cin, cout)
-    assert p["row_mode"] == (dims[0] >= 128)
+    assert p["row_mode"] == 0 or dims[0] >= 128
     rng = np.random.default_rng(dims[0] + cin)
     n = dims[0] * dims[1] * dims[2]
     x = rng.standard_normal((n, cin))

@@ -15,8 +15,9 @@ import torch.nn.functional as F  # noqa: E402
 from hmfem_b200 import guess  # noqa: E402
 
 DIMS = [(9, 7, 5), (20, 16, 12)]
-# x rows of 128 cells and more (one MMA run per row, two x tiles, the second ragged)
-ROW_DIMS = [(130, 5, 3), (128, 4, 5)]
+# x rows of 128 cells and more: row mode (one MMA run per x row, x tiles,
+# the last ragged) or plane mode over the whole x extent, as the planner picks
+ROW_DIMS = [(130, 5, 3), (128, 4, 5), (256, 3, 2)]
 SHAPES = [(16, 16), (16, 32), (32, 64), (64, 64), (96, 32), (48, 16), (32, 96)]
 
 
@@ -89,3 +90,22 @@ def test_data_gradient_is_flipped_forward(cin, cout):
     ref = torch.nn.grad.conv3d_input((1, cin, dims[2], dims[1], dims[0]), _w_torch(w.double()),
                                      _to_ncdhw(dy.double(), dims), padding=1)
     assert _rel(ours, _from_ncdhw(ref)) < 6e-3
+
+
+@pytest.mark.parametrize("cin,cout", [(48, 16), (32, 16)])
+def test_wide_plane_grouped_forward(cin, cout):
+    """A 256-wide grid the planner tiles in plane mode with grouped x taps
+    (the form 48 -> 16 takes at 256^3): against torch's conv3d."""
+    dims = (256, 6, 16)
+    p = guess.conv_plan(dims, cin, cout)
+    assert p["row_mode"] == 0 and p["xg"] == 1 and p["bx"] == 256
+    g = torch.Generator().manual_seed(cin + 7)
+    n = dims[0] * dims[1] * dims[2]
+    x = torch.randn(n, cin, generator=g).bfloat16()
+    w = (torch.randn(27, cout, cin, generator=g) * 0.1).bfloat16()
+    b = torch.randn(cout, generator=g)
+    ours = _fwd(x, w, b, dims, False)
+    ref = _from_ncdhw(F.conv3d(_to_ncdhw(x.double(), dims), _w_torch(w.double()),
+                               b.double(), padding=1))
+    assert _rel(ours, ref) < 6e-3
+    guess.check_errors()
