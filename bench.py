@@ -318,27 +318,14 @@ def run_ours(args):
         mask = torch.as_tensor(prob.conduit_mask, device=dev)
         dims = (prob.nx, prob.ny, prob.nz)
 
-    # the guess depends on K only, not on the hierarchy: its inference runs
-    # on a side stream while the AMG setup runs on the solver's stream, which
-    # waits for it before the solve starts from the guess
-    side = torch.cuda.Stream(device=dev)
-
     def step(s, x, stream=None, learned=False):
+        if learned:  # inference beside the setup (guess.solve_from_guess)
+            _, st = guess.solve_from_guess(s, prob, model, K, mask=mask, x=x)
+            return st
         s.assemble(prob, KX=K, KY=K, KZ=K)
-        if learned:
-            side.wait_stream(stream)
-            with torch.cuda.stream(side):
-                xg = guess.predict(model, K, mask, dims)
-                done = torch.cuda.Event()
-                done.record(side)
         s.setup()
         with torch.cuda.stream(stream):  # the solver's stream: ordered
-            if learned:
-                stream.wait_event(done)
-                xg.record_stream(stream)
-                x.copy_(xg)
-            else:
-                x.zero_()
+            x.zero_()
         _, st = s.solve(x=x)
         return st
 
@@ -438,18 +425,7 @@ def run_ours(args):
         with torch.cuda.stream(e2e_stream):
             Kd.copy_(k_pin)
             md.copy_(m_pin)
-        s_e2e.assemble(prob, KX=Kd, KY=Kd, KZ=Kd)
-        side.wait_stream(e2e_stream)
-        with torch.cuda.stream(side):          # inference beside the setup
-            xg = guess.predict(model, Kd, md, dims)
-            done = torch.cuda.Event()
-            done.record(side)
-        s_e2e.setup()
-        with torch.cuda.stream(e2e_stream):
-            e2e_stream.wait_event(done)
-            xg.record_stream(e2e_stream)
-            xd.copy_(xg)
-        s_e2e.solve(x=xd)
+        guess.solve_from_guess(s_e2e, prob, model, Kd, mask=md, x=xd)
         with torch.cuda.stream(e2e_stream):
             x_pin.copy_(xd)
         e2e_stream.synchronize()

@@ -309,6 +309,44 @@ def predict(model, K, mask, dims):
     return p
 
 
+_SIDE = {}
+
+
+def solve_from_guess(solver, prob, model, KX, KY=None, KZ=None, mask=None, x=None):
+    """Assembly, AMG setup and the solve started from the learned guess.
+
+    The guess depends on K alone, not on the hierarchy, so its inference
+    runs on a side stream while the setup runs on the solver's stream, which
+    waits for it before the solve.  K arrays and the conduit mask are CUDA
+    tensors (the features use KX); x, a CUDA FP64 tensor (allocated when
+    None), receives the pressure.  Every solve still runs to the solver's
+    tolerance.  Returns (x, stats)."""
+    KY = KX if KY is None else KY
+    KZ = KX if KZ is None else KZ
+    dims = (prob.nx, prob.ny, prob.nz)
+    stream = torch.cuda.ExternalStream(solver.stream)
+    dev = KX.device
+    if dev not in _SIDE:
+        _SIDE[dev] = torch.cuda.Stream(device=dev)
+    side = _SIDE[dev]
+    if x is None:
+        x = torch.empty(prob.n, dtype=torch.float64, device=dev)
+    solver.assemble(prob, KX=KX, KY=KY, KZ=KZ)
+    side.wait_stream(stream)
+    with torch.cuda.stream(side):
+        xg = predict(model, KX, mask, dims)
+        done = torch.cuda.Event()
+        done.record(side)
+    solver.setup()
+    with torch.cuda.stream(stream):
+        stream.wait_event(done)
+        xg.record_stream(stream)
+        x.copy_(xg)
+    del xg
+    _, st = solver.solve(x=x)
+    return x, st
+
+
 def save(model, path):
     np.savez(path, **{k: v.detach().cpu().float().numpy() for k, v in model.state_dict().items()})
 

@@ -13,7 +13,7 @@ if not torch.cuda.is_available():  # pragma: no cover
 
 import torch.nn.functional as F  # noqa: E402
 
-from hmfem_b200 import guess, train_guess  # noqa: E402
+from hmfem_b200 import gpu, guess, train_guess  # noqa: E402
 
 
 def test_unet_matches_float64_network_and_gradients():
@@ -170,3 +170,20 @@ def test_data_movement_kernels_match_torch():
         corr = model(guess.features(K, mask, dims), dims)
     assert torch.allclose(p, guess.linear_profile(dims) + corr.double(), rtol=0, atol=1e-5)
     guess.check_errors()
+
+
+def test_solve_from_guess_equals_the_sequential_solve():
+    """The overlapped call (inference beside the setup) starts the CG from
+    the same guess as predict-then-solve: the same iterations and pressure."""
+    size = 32
+    model = guess.UNet(seed=5).cuda()
+    prob, K, mask = train_guess.sample(7, size)
+    s = gpu.Solver(precision=1, tol=1e-10)
+    x1, st1 = guess.solve_from_guess(s, prob, model, K, mask=mask)
+    s.assemble(prob, KX=K, KY=K, KZ=K)
+    s.setup()
+    x2 = guess.predict(model, K, mask, (size, size, size))
+    _, st2 = s.solve(x=x2)
+    assert st1["iterations"] == st2["iterations"] and st1["relres"] <= 1e-10
+    assert torch.equal(x1, x2)
+    s.close()
