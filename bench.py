@@ -70,8 +70,9 @@ def parse():
                     help="skip the 128^3 plain-vs-chosen comparison (config 1)")
     ap.add_argument("--profile-step", type=int, default=-1, metavar="PRECISION",
                     help="run one untimed step (assembly + setup + solve) of "
-                         "the plain (0) or chosen (1) variant and exit: the "
-                         "command the ncu summaries under profiles/ profile")
+                         "the plain FP64 (0), the FP32 zero-guess (1) or the "
+                         "FP32 learned-guess (2) variant and exit: the command "
+                         "the ncu summaries under profiles/ profile")
     return ap.parse_args()
 
 
@@ -1184,15 +1185,21 @@ def profile_step(args):
     from hmfem_b200.problem import config_problem
     prob = config_problem(2, size=args.size)
     K = torch.tensor(prob.KX, device="cuda")
-    # the options of the bench's variants: plain FP64, or the chosen FP32
-    # V-cycle with levels >= 1 stored in BF16
-    s = gpu.Solver(precision=args.profile_step, tol=args.tol,
-                   bf16_from=1 if args.profile_step == 1 else -1, check_every=2,
-                   schur0=1 if args.profile_step == 1 else 0)
+    # the options of the bench's variants: plain FP64, or the FP32 V-cycle
+    # with levels >= 1 stored in BF16 (from the zero or the learned guess)
+    fp32 = args.profile_step >= 1
+    s = gpu.Solver(precision=1 if fp32 else 0, tol=args.tol,
+                   bf16_from=1 if fp32 else -1, check_every=2, schur0=1 if fp32 else 0)
     x = torch.zeros(prob.n, dtype=torch.float64, device="cuda")
-    s.assemble(prob, KX=K, KY=K, KZ=K)
-    s.setup()
-    _, st = s.solve(x=x)
+    if args.profile_step == 2:
+        from hmfem_b200 import guess
+        model = guess.load(os.path.join(ROOT, "hmfem_b200", "models", "unet_config4.npz"))
+        mask = torch.as_tensor(prob.conduit_mask, device="cuda")
+        _, st = guess.solve_from_guess(s, prob, model, K, mask=mask, x=x)
+    else:
+        s.assemble(prob, KX=K, KY=K, KZ=K)
+        s.setup()
+        _, st = s.solve(x=x)
     torch.cuda.synchronize()
     print(json.dumps({"profile_step": args.profile_step, "size": args.size,
                       "iterations": st["iterations"], "relres": st["relres"],
