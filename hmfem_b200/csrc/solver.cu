@@ -10,8 +10,6 @@
 #include <algorithm>
 
 #include "solver.cuh"
-#include <cooperative_groups.h>
-
 #include "cycle.cuh"
 
 namespace hm {
@@ -85,131 +83,10 @@ __global__ void k_gj_step(int n, int k, const double *__restrict__ src, double *
     }
 }
 
-// The whole Gauss-Jordan inverse in one launch: a cluster of C CTAs, CTA c
-// holding rows [c R, c R + R) of the matrix in its shared memory.  Step k
-// reads the pivot row k that its owner published (after step k-1) into a
-// double-buffered slot, through distributed shared memory; every CTA updates
-// its own rows in place with k_gj_step's arithmetic (column k saved first);
-// the owner of row k+1 publishes it; one cluster barrier per step.  All CTAs
-// run the same steps and barriers (a non-positive pivot only sets err).
-constexpr int kGjThreads = 512;
-
-__global__ void __launch_bounds__(kGjThreads)
-k_gj_cluster(int n, int rows_per, const int *__restrict__ rowptr, const int *__restrict__ col,
-             const double *__restrict__ val, double *__restrict__ out, int *err)
-{
-    namespace cg = cooperative_groups;
-    extern __shared__ double gj_sm[];
-    cg::cluster_group cl = cg::this_cluster();
-    const int rank = (int)cl.block_rank();
-    const int r0 = rank * rows_per, r1 = r0 + rows_per < n ? r0 + rows_per : n;
-    const int nr = r1 > r0 ? r1 - r0 : 0;
-    double *M = gj_sm;                            // nr x n, own rows
-    double *pub = M + (size_t)rows_per * n;       // 2 x n, published pivot rows
-    double *prow = pub + 2 * (size_t)n;           // n, this step's pivot row
-    double *colk = prow + n;                      // rows_per, column k of own rows
-    const int tid = threadIdx.x;
-    for (long e = tid; e < (long)nr * n; e += kGjThreads) M[e] = 0.0;
-    __syncthreads();
-    for (int i = r0 + tid; i < r1; i += kGjThreads)
-        for (int q = rowptr[i]; q < rowptr[i + 1]; q++) M[(size_t)(i - r0) * n + col[q]] += val[q];
-    __syncthreads();
-    if (r0 == 0 && nr > 0)
-        for (int j = tid; j < n; j += kGjThreads) pub[j] = M[j];
-    cl.sync();
-    for (int k = 0; k < n; k++) {
-        const double *src = cl.map_shared_rank(pub + (size_t)(k & 1) * n, k / rows_per);
-        for (int j = tid; j < n; j += kGjThreads) prow[j] = src[j];
-        for (int i = tid; i < nr; i += kGjThreads) colk[i] = M[(size_t)i * n + k];
-        __syncthreads();
-        const double p = prow[k];
-        const double pinv = 1.0 / (p > 0.0 ? p : 1.0);
-        if (rank == 0 && tid == 0 && !(p > 0.0)) *err = 1;
-        // a warp per row, lanes over the columns
-        for (int il = tid >> 5; il < nr; il += kGjThreads / 32) {
-            const double cik = colk[il];
-            double *mi = M + (size_t)il * n;
-            const bool pivot_row = r0 + il == k;
-            for (int j = tid & 31; j < n; j += 32) {
-                double v;
-                if (pivot_row) v = j == k ? pinv : prow[j] * pinv;
-                else if (j == k) v = cik * -pinv;
-                else v = mi[j] - cik * (prow[j] * pinv);
-                mi[j] = v;
-            }
-        }
-        __syncthreads();
-        const int k1 = k + 1;
-        if (k1 < n && k1 >= r0 && k1 < r1)
-            for (int j = tid; j < n; j += kGjThreads)
-                pub[(size_t)(k1 & 1) * n + j] = M[(size_t)(k1 - r0) * n + j];
-        cl.sync();
-    }
-    for (long e = tid; e < (long)nr * n; e += kGjThreads) out[(size_t)r0 * n + e] = M[e];
-}
-
-// Shared memory of k_gj_cluster for rows_per rows of an n x n matrix.
-static size_t gj_smem(int n, int rows_per)
-{
-    return sizeof(double) * ((size_t)rows_per * n + 3 * (size_t)n + rows_per);
-}
-
-// One launch over the smallest cluster (1..16 CTAs) whose row bands fit in
-// shared memory; false when no cluster fits or the launch is refused.
-static bool dense_factor_cluster(const Csr &A, double *Lf, int *err, cudaStream_t st)
-{
-    const int n = A.n;
-    int dev = 0, smax = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
-        return false;
-    for (int c = 1; c <= 16; c *= 2) {
-        const int rows_per = (int)ceil_div(n, c);
-        const size_t sm = gj_smem(n, rows_per);
-        if (sm > (size_t)smax) continue;
-        if (cudaFuncSetAttribute(k_gj_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sm) != cudaSuccess ||
-            (c > 8 && cudaFuncSetAttribute(k_gj_cluster,
-                                           cudaFuncAttributeNonPortableClusterSizeAllowed,
-                                           1) != cudaSuccess)) {
-            cudaGetLastError();
-            return false;
-        }
-        cudaLaunchConfig_t cfg = {};
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = (unsigned)c;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.gridDim = dim3((unsigned)c);
-        cfg.blockDim = dim3(kGjThreads);
-        cfg.dynamicSmemBytes = sm;
-        cfg.stream = st;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        int clusters = 0;  // can such a cluster be resident at all?
-        if (cudaOccupancyMaxActiveClusters(&clusters, (void *)k_gj_cluster, &cfg) != cudaSuccess ||
-            clusters < 1) {
-            cudaGetLastError();
-            continue;
-        }
-        if (cudaLaunchKernelEx(&cfg, k_gj_cluster, n, rows_per, (const int *)A.rowptr,
-                               (const int *)A.col, (const double *)A.val, Lf, err) !=
-            cudaSuccess) {
-            cudaGetLastError();
-            return false;
-        }
-        HM_COUNT();
-        return true;
-    }
-    return false;
-}
-
 int dense_factor(const Csr &A, double *Lf, int *err, cudaStream_t st)
 {
     const int n = A.n;
     if (n <= 0) return HMFEM_OK;
-    if (dense_factor_cluster(A, Lf, err, st)) return HMFEM_OK;
     double *tmp = (double *)dalloc(sizeof(double) * (size_t)n * n);
     if (!tmp) return HMFEM_E_CUDA;
     const int th = n < 128 ? 32 * (int)ceil_div(n, 32) : 128;
