@@ -27,12 +27,9 @@
 
 namespace hm {
 
-namespace {
-
-constexpr int kMisTile = 1024;
 constexpr long long kMaxPolls = 1ll << 22;
 
-// The poll limit of the split's bounded wait: kMaxPolls, or lower when the
+// The poll limit of the splits' bounded waits: kMaxPolls, or lower when the
 // environment sets HMFEM_TEST_POLL_LIMIT (a test makes the wait run out and
 // checks that the call returns HMFEM_E_TIMEOUT and the next one succeeds).
 long long split_poll_limit()
@@ -42,6 +39,10 @@ long long split_poll_limit()
     long long v = atoll(e);
     return v < 0 ? 0 : (v < kMaxPolls ? v : kMaxPolls);
 }
+
+namespace {
+
+constexpr int kMisTile = 1024;
 
 // The greedy split in natural order (node_selection, amg.h:1-226 with
 // eps = 0): row v is C when every lower neighbour is F, F as soon as one is
@@ -660,17 +661,30 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
     const int n = L.A.n;
     // ---- C/F split ----------------------------------------------------
     HM_CUDA(cudaMemsetAsync(dwork, 0, 4 * sizeof(int), st));
+    int *wave = nullptr, *wave_err = nullptr;  // the level-1 split's work and error word
     if (L.sel_split) {  // formed on the side stream while the level above coarsened
         HM_CUDA(cudaStreamWaitEvent(st, L.sel_ready, 0));
         cudaEventDestroy(L.sel_ready);
         L.sel_ready = nullptr;
+        wave = L.split_work;
+        wave_err = L.split_err;
+        L.split_work = L.split_err = nullptr;
     } else {
         L.sel = (signed char *)dalloc(n > 0 ? n : 1);
         HM_CUDA(cudaMemsetAsync(L.sel, 0, n > 0 ? n : 1, st));
         if (grid3) {
             HM_CHECK(stencil_parity_split(grid3[0], grid3[1], grid3[2], L.sel, st));
         } else if (L.g19.nx > 0) {
-            HM_CHECK(stencil19_split(L.g19.nx, L.g19.ny, L.g19.nz, L.sel, st));
+            const long wi = stencil19_split_work_ints(L.g19.nx, L.g19.ny, L.g19.nz);
+            wave = (int *)dalloc(sizeof(int) * wi);
+            if (!wave) return HMFEM_E_CUDA;
+            wave_err = wave + wi - 1;
+            const int rc = stencil19_split(L.g19.nx, L.g19.ny, L.g19.nz, L.sel, wave, st);
+            if (rc != HMFEM_OK) {
+                cudaStreamSynchronize(st);
+                dfree(wave);
+                return rc;
+            }
         } else if (n > 0) {
             k_lfmis<<<(int)ceil_div(n, kMisTile), kMisTile, 0, st>>>(
                 L.A.rowptr, L.A.col, n, L.sel, (unsigned *)(dwork + 2), dwork,
@@ -678,11 +692,14 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
             HM_LAUNCHED();
         }
     }
-    int herr = 0;
-    HM_CUDA(cudaMemcpyAsync(&herr, dwork, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int herr[2] = {0, 0};
+    HM_CUDA(cudaMemcpyAsync(&herr[0], dwork, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (wave_err)
+        HM_CUDA(cudaMemcpyAsync(&herr[1], wave_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     HM_CUDA(cudaStreamSynchronize(st));
+    dfree(wave);
     HM_PHASE("  C/F split", st);
-    if (herr) {
+    if (herr[0] || herr[1]) {
         set_last_error("C/F split wavefront gave up waiting", __FILE__, __LINE__);
         return HMFEM_E_TIMEOUT;
     }
@@ -698,14 +715,17 @@ int amg_coarsen(Level &L, Level &C, cudaStream_t st, int *dwork,
     // stream, overlapping the rest of this level's coarsening
     if (grid3 && g19_applies(grid3[0], grid3[1], grid3[2]) && nc > 0) {
         C.sel = (signed char *)dalloc(nc);
-        if (!C.sel) return HMFEM_E_CUDA;
+        const long wi = stencil19_split_work_ints(grid3[0], grid3[1], grid3[2]);
+        C.split_work = (int *)dalloc(sizeof(int) * wi);
+        if (!C.sel || !C.split_work) return HMFEM_E_CUDA;
+        C.split_err = C.split_work + wi - 1;
         cudaEvent_t allocated;
         HM_CUDA(cudaEventCreateWithFlags(&allocated, cudaEventDisableTiming));
         HM_CUDA(cudaEventRecord(allocated, st));
         cudaStream_t side = side_stream();
         HM_CUDA(cudaStreamWaitEvent(side, allocated, 0));
         cudaEventDestroy(allocated);
-        HM_CHECK(stencil19_split(grid3[0], grid3[1], grid3[2], C.sel, side));
+        HM_CHECK(stencil19_split(grid3[0], grid3[1], grid3[2], C.sel, C.split_work, side));
         HM_CUDA(cudaEventCreateWithFlags(&C.sel_ready, cudaEventDisableTiming));
         HM_CUDA(cudaEventRecord(C.sel_ready, side));
         C.sel_split = true;

@@ -88,6 +88,8 @@ struct Level {
     signed char *sel = nullptr;  // 1 = C, 2 = F
     bool sel_split = false;           // sel formed early on a side stream,
     cudaEvent_t sel_ready = nullptr;  // complete once this event is
+    int *split_work = nullptr;        // that split's flags, ticket, error word
+    int *split_err = nullptr;         // (freed once the split is consumed)
     int *cid = nullptr;          // coarse id of C rows (prefix count)
     int nc = 0;
     Csr P;                    // P rows: coarse ids in the fine row's order
@@ -176,8 +178,13 @@ int stencil_parity_split(int nx, int ny, int nz, signed char *sel, cudaStream_t 
 // set to P's nnz)
 int stencil_parity_R(int nx, int ny, int nz, const int *cid, int nc, Csr &R, cudaStream_t st);
 // level 1 of a parity split (nx even, nx, ny >= 4): its greedy C/F split
-// from the 19-offset structure, one launch per x-row wavefront
-int stencil19_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st);
+// from the 19-offset structure, the x-row wavefront in one launch; work
+// holds stencil19_split_work_ints(nx, ny, nz) ints (8-byte aligned), the
+// last one the error word (1 when a bounded wait gave up)
+long stencil19_split_work_ints(int nx, int ny, int nz);
+int stencil19_split(int nx, int ny, int nz, signed char *sel, int *work, cudaStream_t st);
+// the poll limit of the splits' bounded waits (HMFEM_TEST_POLL_LIMIT lowers it)
+long long split_poll_limit();
 // schur: the exact red-black reduction's level 1 instead of the Galerkin
 // product with the averaging interpolation (same rows and columns)
 int stencil_galerkin(int nx, int ny, int nz, const Level &L, Csr &out,

@@ -403,113 +403,161 @@ int nbk(long n)
 // (0,-2,0), (-1,-1,0), (1,-1,0) -- in the x-rows (j,k-2), (j-1,k-1),
 // (j,k-1), (j+1,k-1), (j-2,k), (j-1,k) -- and (-2,0,0), the previous cell of
 // the same x-row.  So an x-row depends only on rows with a smaller
-// t = j + 2k, and the rows of one t are independent: one launch per t,
-// one warp per row.  Inside a row, with "blocked" = some lower neighbour in
+// t = j + 2k.  Inside a row, with "blocked" = some lower neighbour in
 // another row is C, the row recurrence C_b = !blocked_b && !C_{b-1} makes
 // every run of unblocked cells alternate C, F, C, ... from its first cell
 // (or from the carried state of the previous 32-cell chunk).
-__global__ void __launch_bounds__(128)
-k_mis19_front(SG g, int t, int kmin, int rows, signed char *sel)
+//
+// One launch for the whole wavefront: warps take x-rows from a ticket in
+// (t, k) order and resolve them 32 cells (one chunk) at a time.  A row
+// publishes each chunk as one 64-bit word, its C bits in the low half and a
+// valid bit above them (an aligned 64-bit store is seen whole or not at
+// all), so a reader needs no flag, fence or second load: lanes 0-17 poll
+// the words c-1, c, c+1 of the six rows below (bounded waits) and every
+// lane picks its neighbours' bits from them.  Those rows have smaller t,
+// so earlier tickets, held by warps that are already running: every wait
+// ends.  Chunk c of a row waits only for chunk c+1 of the rows before it,
+// so consecutive rows of the wavefront overlap chunk by chunk.
+
+constexpr int kWaveThreads = 128;
+// 256 warps cover the wavefront's width at 256^3 (alone: 1.3 ms for its 766
+// diagonals) and leave most SMs to the level-0 kernels it runs beside; one
+// CTA on every SM slowed those 1.4x (setup 24.4 against 23.5 ms at 256^3)
+constexpr int kWaveBlocks = 64;
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
 {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (w >= rows) return;  // whole warps leave together
-    const int k = kmin + w, j = t - 2 * k;
-    const int p = (j + k) & 1, m = (g.nx - p + 1) >> 1;
-    const long rowbase = (long)j * g.nx + (long)k * g.nxy;
-    bool prev_c = false;
-    for (int b0 = 0; b0 < m; b0 += 32) {
-        const int b = b0 + lane;
-        const bool valid = b < m;
-        const int i = p + 2 * b;
-        const long s = rowbase + i;
-        bool blocked = !valid;
-        if (valid) {
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const int a = i + q19x(q), bb = j + q19y(q), c = k + q19z(q);
-                if (a >= 0 && a < g.nx && bb >= 0 && bb < g.ny && c >= 0 && c < g.nz &&
-                    sel[(s + q19x(q) + q19y(q) * (long)g.nx + q19z(q) * g.nxy) >> 1] == 1)
-                    blocked = true;
-            }
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// x-rows (j, k) of an ny x nz plane with j + 2k < t
+__host__ __device__ __forceinline__ long long rows_before(long long t, int ny, int nz)
+{
+    if (t <= 0) return 0;
+    long long kf = t >= ny ? (t - ny) / 2 + 1 : 0;  // rows with t - 2k >= ny: all ny
+    long long kp = (t + 1) / 2;                     // rows with t - 2k > 0
+    if (kf > nz) kf = nz;
+    if (kp > nz) kp = nz;
+    return (long long)ny * kf + (kp - kf) * t - (kp - kf) * (kf + kp - 1);
+}
+
+// words: [ny * nz rows][W chunks] (W = chunks of nx / 2 cells), zero on entry
+__global__ void __launch_bounds__(kWaveThreads)
+k_mis19_wave(SG g, signed char *sel, unsigned long long *words, int W, unsigned *ticket,
+             int *err, long long max_polls)
+{
+    const unsigned full = 0xffffffffu;
+    const unsigned long long valid = 1ull << 32;
+    const int lane = threadIdx.x & 31;
+    const unsigned rows = (unsigned)g.ny * (unsigned)g.nz;
+    const long long tmax = (g.ny - 1) + 2LL * (g.nz - 1);
+    const int m = g.nx >> 1;  // cells of every x-row of level 1 (nx even)
+    volatile int *verr = err;
+    // lane L < 18 watches word c + (L % 3) - 1 of row L / 3: (j,k-2),
+    // (j-1,k-1), (j,k-1), (j+1,k-1), (j-2,k), (j-1,k)
+    const int ri = lane / 3, wo = lane % 3 - 1;
+    const int dj = ri == 1 || ri == 5 ? -1 : ri == 3 ? 1 : ri == 4 ? -2 : 0;
+    const int dk = ri == 0 ? -2 : ri <= 3 ? -1 : 0;
+    for (;;) {
+        unsigned tk = 0;
+        if (lane == 0) tk = atomicAdd(ticket, 1u);
+        tk = __shfl_sync(full, tk, 0);
+        if (tk >= rows) return;
+        long long lo = 0, hi = tmax;  // the largest t with rows_before(t) <= tk
+        while (lo < hi) {
+            const long long mid = (lo + hi + 1) >> 1;
+            if (rows_before(mid, g.ny, g.nz) <= (long long)tk) lo = mid;
+            else hi = mid - 1;
         }
-        const unsigned B = __ballot_sync(0xffffffffu, blocked);
-        const unsigned lower = B & ((1u << lane) - 1u);
-        bool is_c;
-        if (lower) is_c = !blocked && (((lane - (31 - __clz(lower)) - 1) & 1) == 0);
-        else is_c = !blocked && ((lane & 1) == (prev_c ? 1 : 0));
-        if (valid) sel[s >> 1] = is_c ? 1 : 2;
-        prev_c = __shfl_sync(0xffffffffu, is_c, 31);
+        const int t = (int)lo;
+        const int kmin = t > g.ny - 1 ? (t - g.ny + 2) / 2 : 0;
+        const int k = kmin + (int)((long long)tk - rows_before(t, g.ny, g.nz));
+        const int j = t - 2 * k;
+        const int p = (j + k) & 1;
+        // the x-neighbours -1 / +1 of cell b sit at bit b + dm / b + dp of
+        // the rows of the other parity
+        const int dm = p == 0 ? -1 : 0, dp = p == 0 ? 0 : 1;
+        const int jj = j + dj, kk = k + dk;
+        const bool row_in = lane < 18 && jj >= 0 && jj < g.ny && kk >= 0 && kk < g.nz;
+        const unsigned long long *nrow = words + (row_in ? ((long)jj + (long)g.ny * kk) * W : 0);
+        unsigned long long *own = words + ((long)j + (long)g.ny * k) * W;
+        const long rowbase = (long)j * g.nx + (long)k * g.nxy;
+        bool prev_c = false;
+        for (int c = 0; c < W; c++) {
+            const int w = c + wo;
+            const bool need = row_in && w >= 0 && w < W;
+            unsigned long long v = 0;
+            long long polls = 0;
+            for (;;) {
+                if (need && !(v & valid)) v = ld_relaxed_u64(nrow + w);
+                if (__all_sync(full, !need || (v & valid))) break;
+                if (__any_sync(full, ++polls > max_polls || *verr != 0)) {
+                    if (lane == 0) atomicExch(err, 1);
+                    return;  // the whole warp: the rest of its row stays unpublished
+                }
+                __nanosleep(polls > 8 ? 128 : 16);
+            }
+            unsigned x[18];
+#pragma unroll
+            for (int q = 0; q < 18; q++) x[q] = __shfl_sync(full, (unsigned)v, q);
+            auto bit = [&](int r, int d) -> bool {
+                const int pos = lane + d;
+                return pos < 0 ? (x[3 * r] >> 31) & 1u
+                     : pos > 31 ? x[3 * r + 2] & 1u : (x[3 * r + 1] >> pos) & 1u;
+            };
+            const int b = 32 * c + lane;
+            const bool blocked = b >= m || bit(0, 0) || bit(1, 0) || bit(2, dm) || bit(2, dp) ||
+                                 bit(3, 0) || bit(4, 0) || bit(5, dm) || bit(5, dp);
+            const unsigned B = __ballot_sync(full, blocked);
+            const unsigned lower = B & ((1u << lane) - 1u);
+            bool is_c;
+            if (lower) is_c = !blocked && (((lane - (31 - __clz(lower)) - 1) & 1) == 0);
+            else is_c = !blocked && ((lane & 1) == (prev_c ? 1 : 0));
+            const unsigned cm = __ballot_sync(full, is_c);
+            if (lane == 0) st_relaxed_u64(own + c, valid | cm);
+            if (b < m) sel[(rowbase + p + 2 * b) >> 1] = is_c ? 1 : 2;
+            prev_c = (cm >> 31) & 1u;
+        }
     }
 }
 
 }  // namespace
 
-static int mis19_enqueue(const SG &g, signed char *sel, cudaStream_t st)
+// work: the rows' chunk words (two ints each), then the ticket and the
+// error word
+static long wave_chunks(int nx) { return ((long)(nx >> 1) + 31) >> 5; }
+
+long stencil19_split_work_ints(int nx, int ny, int nz)
 {
-    const int tmax = (g.ny - 1) + 2 * (g.nz - 1);
-    for (int t = 0; t <= tmax; t++) {
-        const int kmin = t - (g.ny - 1) > 0 ? (t - (g.ny - 1) + 1) / 2 : 0;
-        const int kmax = t / 2 < g.nz - 1 ? t / 2 : g.nz - 1;
-        const int rows = kmax - kmin + 1;
-        if (rows <= 0) continue;
-        k_mis19_front<<<(rows + 3) / 4, 128, 0, st>>>(g, t, kmin, rows, sel);
-        HM_LAUNCHED();
-    }
-    return HMFEM_OK;
+    return 2 * (long)ny * nz * wave_chunks(nx) + 2;
 }
 
-// The wavefront is a few hundred dependent launches; a grid shape seen
-// twice on this host thread (a solver set up again, the same shape of
-// another realisation) has them recorded in a CUDA graph and replayed.
-// The graph holds the sel address, so it is kept per (shape, sel).
-struct Mis19Graph {
-    int nx = 0, ny = 0, nz = 0;
-    signed char *sel = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    unsigned long long kernels = 0;
-};
-static thread_local Mis19Graph t_mis_graph;
-static thread_local int t_mis_seen[3] = {0, 0, 0};
-
-int stencil19_split(int nx, int ny, int nz, signed char *sel, cudaStream_t st)
+int stencil19_split(int nx, int ny, int nz, signed char *sel, int *work, cudaStream_t st)
 {
     SG g{nx, ny, nz, (long)nx * ny};
-    Mis19Graph &G = t_mis_graph;
-    if (G.exec && G.nx == nx && G.ny == ny && G.nz == nz && G.sel == sel) {
-        HM_CUDA(cudaGraphLaunch(G.exec, st));
-        g_nlaunch += G.kernels;
-        return HMFEM_OK;
+    const long rows = (long)ny * nz;
+    if (rows <= 0 || nx < 2) return HMFEM_OK;
+    if (rows > 0x7fffffffL || (nx & 1)) {
+        set_last_error("level-1 split: needs an even nx and fewer than 2^31 x-rows",
+                       __FILE__, __LINE__);
+        return HMFEM_E_CAPACITY;
     }
-    const bool seen = t_mis_seen[0] == nx && t_mis_seen[1] == ny && t_mis_seen[2] == nz;
-    t_mis_seen[0] = nx; t_mis_seen[1] = ny; t_mis_seen[2] = nz;
-    if (!seen) return mis19_enqueue(g, sel, st);
-    // record it on a private stream, then replay on st
-    cudaStream_t cs;
-    HM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-    HM_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    const unsigned long long before = t_nlaunch;
-    int rc = mis19_enqueue(g, sel, cs);
-    const unsigned long long k = t_nlaunch - before;
-    g_nlaunch -= k;  // counted when replayed
-    cudaGraph_t graph = nullptr;
-    cudaError_t e = cudaStreamEndCapture(cs, &graph);
-    cudaStreamDestroy(cs);
-    if (rc != HMFEM_OK || e != cudaSuccess) {
-        if (graph) cudaGraphDestroy(graph);
-        cudaGetLastError();
-        return rc != HMFEM_OK ? rc : mis19_enqueue(g, sel, st);
-    }
-    cudaGraphExec_t ex = nullptr;
-    e = cudaGraphInstantiate(&ex, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return mis19_enqueue(g, sel, st);
-    }
-    if (G.exec) cudaGraphExecDestroy(G.exec);
-    G.nx = nx; G.ny = ny; G.nz = nz; G.sel = sel; G.exec = ex; G.kernels = k;
-    HM_CUDA(cudaGraphLaunch(ex, st));
-    g_nlaunch += k;
+    const long wi = stencil19_split_work_ints(nx, ny, nz);
+    HM_CUDA(cudaMemsetAsync(work, 0, sizeof(int) * wi, st));
+    const long warps = kWaveThreads / 32;
+    long blocks = (rows + warps - 1) / warps;
+    if (blocks > kWaveBlocks) blocks = kWaveBlocks;
+    k_mis19_wave<<<(int)blocks, kWaveThreads, 0, st>>>(
+        g, sel, (unsigned long long *)work, (int)wave_chunks(nx), (unsigned *)(work + wi - 2),
+        work + wi - 1, split_poll_limit());
+    HM_LAUNCHED();
     return HMFEM_OK;
 }
 

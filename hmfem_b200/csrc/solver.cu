@@ -49,10 +49,20 @@ int launch_smoother_diag(const Csr &A, int kind, double *dsm, float *dsm32,
 
 // Explicit FP64 inverse of a small SPD level by Gauss-Jordan elimination
 // (SPD, so no pivoting): the coarse solve then is a single dense mat-vec.
-// One launch per pivot k over the whole matrix, reading one buffer and
-// writing the other (every element reads the old pivot row and column, so
-// no ordering inside a step is needed); err = 1 on a non-positive pivot.
+// Step k maps row i != k to r_i - r_ik (r_k / p) (column k: -r_ik / p) and
+// row k to r_k / p (column k: 1 / p), p = r_kk; err = 1 on a non-positive
+// pivot.
+//
+// kGjBlock steps per launch, reading one buffer and writing the other.
+// Every CTA first takes the block's pivot rows through the block's steps in
+// shared memory -- each becomes its normalised form r_k / p at its own step
+// -- then each warp applies the steps in turn to its rows, one at a time in
+// shared memory, from those normalised rows.  Entry by entry the operations and
+// operands are those of the one-step-per-launch form; 272 launches become
+// 17 at the coarse size of a 256^3 grid.
 constexpr int kDenseMax = 512;
+constexpr int kGjBlock = 16;
+constexpr int kGjThreads = 256;
 
 __global__ void k_dense_load(int n, const int *__restrict__ rowptr,
                              const int *__restrict__ col, const double *__restrict__ val,
@@ -65,21 +75,53 @@ __global__ void k_dense_load(int n, const int *__restrict__ rowptr,
         for (int k = rowptr[i]; k < rowptr[i + 1]; k++) M[(long)i * n + col[k]] += val[k];
 }
 
-__global__ void k_gj_step(int n, int k, const double *__restrict__ src, double *__restrict__ dst,
-                          int *err)
+__global__ void __launch_bounds__(kGjThreads)
+k_gj_block(int n, int k0, int nb, const double *__restrict__ src, double *__restrict__ dst,
+           int *err)
 {
-    const int i = blockIdx.y;
-    const double p = src[(long)k * n + k];
-    const double pinv = 1.0 / (p > 0.0 ? p : 1.0);
-    if (i == 0 && threadIdx.x == 0 && !(p > 0.0)) *err = 1;
-    const double *rk = src + (long)k * n, *ri = src + (long)i * n;
-    const double cik = ri[k];
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        double v;
-        if (i == k) v = j == k ? pinv : rk[j] * pinv;
-        else if (j == k) v = cik * -pinv;
-        else v = ri[j] - cik * (rk[j] * pinv);
-        dst[(long)i * n + j] = v;
+    // [kGjBlock][n] the pivot rows, then their normalised forms; then one
+    // row of n per warp
+    extern __shared__ double panel[];
+    __shared__ double c_sh[kGjBlock];
+    for (int e = threadIdx.x; e < nb * n; e += blockDim.x)
+        panel[e] = src[(long)k0 * n + e];
+    __syncthreads();
+    for (int s = 0; s < nb; s++) {
+        const int k = k0 + s;
+        double *rk = panel + (long)s * n;
+        const double p = rk[k];
+        const double pinv = 1.0 / (p > 0.0 ? p : 1.0);
+        if (blockIdx.x == 0 && threadIdx.x == 0 && !(p > 0.0)) *err = 1;
+        if (threadIdx.x > s && threadIdx.x < nb) c_sh[threadIdx.x] = panel[(long)threadIdx.x * n + k];
+        __syncthreads();
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const double nj = j == k ? pinv : rk[j] * pinv;
+            for (int t = s + 1; t < nb; t++) {
+                double *rt = panel + (long)t * n;
+                const double c = c_sh[t];
+                rt[j] = j == k ? c * -pinv : rt[j] - c * nj;
+            }
+            rk[j] = nj;
+        }
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    double *row = panel + (long)kGjBlock * n + (long)(threadIdx.x >> 5) * n;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        for (int j = lane; j < n; j += 32) row[j] = src[(long)i * n + j];
+        __syncwarp();
+        for (int s = 0; s < nb; s++) {
+            const int k = k0 + s;
+            const double *nk = panel + (long)s * n;
+            const double c = row[k], pinv = nk[k];
+            __syncwarp();
+            for (int j = lane; j < n; j += 32)
+                row[j] = i == k ? nk[j] : j == k ? c * -pinv : row[j] - c * nk[j];
+            __syncwarp();
+        }
+        for (int j = lane; j < n; j += 32) dst[(long)i * n + j] = row[j];
+        __syncwarp();
     }
 }
 
@@ -87,15 +129,25 @@ int dense_factor(const Csr &A, double *Lf, int *err, cudaStream_t st)
 {
     const int n = A.n;
     if (n <= 0) return HMFEM_OK;
+    if (n > kDenseMax) {
+        set_last_error("dense coarse solve: level too large", __FILE__, __LINE__);
+        return HMFEM_E_ARG;
+    }
     double *tmp = (double *)dalloc(sizeof(double) * (size_t)n * n);
     if (!tmp) return HMFEM_E_CUDA;
+    const int launches = (int)ceil_div(n, kGjBlock);
+    // after the last launch the inverse must land in Lf: start in the other buffer
+    double *a = (launches & 1) ? tmp : Lf, *b = (launches & 1) ? Lf : tmp;
     const int th = n < 128 ? 32 * (int)ceil_div(n, 32) : 128;
-    // after n steps the inverse must land in Lf: start in the other buffer
-    double *a = (n & 1) ? tmp : Lf, *b = (n & 1) ? Lf : tmp;
     k_dense_load<<<dim3(1, n), th, 0, st>>>(n, A.rowptr, A.col, A.val, a);
     HM_LAUNCHED();
-    for (int k = 0; k < n; k++) {
-        k_gj_step<<<dim3(1, n), th, 0, st>>>(n, k, a, b, err);
+    const size_t smem = sizeof(double) * (size_t)(kGjBlock + kGjThreads / 32) * n;
+    HM_CUDA(cudaFuncSetAttribute(k_gj_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(double) * (kGjBlock + kGjThreads / 32) * kDenseMax)));
+    const int blocks = (int)ceil_div((long)n * 32, kGjThreads);
+    for (int k0 = 0; k0 < n; k0 += kGjBlock) {
+        const int nb = n - k0 < kGjBlock ? n - k0 : kGjBlock;
+        k_gj_block<<<blocks, kGjThreads, smem, st>>>(n, k0, nb, a, b, err);
         HM_LAUNCHED();
         double *t = a; a = b; b = t;
     }
@@ -133,6 +185,7 @@ static void free_level_setup(Level &L, bool keep_matrix)
         cudaEventDestroy(L.sel_ready);
         L.sel_ready = nullptr;
     }
+    dfree(L.split_work);
     if (!keep_matrix) free_csr(L.A);
     free_sell(L.S);
     dfree(L.dinv); dfree(L.dinv32); dfree(L.dsm); dfree(L.dsm32);
@@ -398,6 +451,7 @@ int setup(Solver &s)
                 } else {
                     s.direct_level = k;
                 }
+                HM_PHASE("setup: coarse inverse", st);
                 break;
             }
         }

@@ -75,17 +75,21 @@ def test_levels_below_the_schur_level_bit_exact(name, port):
     s.close()
 
 
-def test_exact_when_level1_is_solved_exactly(port):
-    """8^3 with the dense direct solve from 300 rows down: level 1 (256
-    rows) is solved exactly, so one cycle is A^-1 (to the cycle's rounding)
-    and the flexible CG needs two steps."""
-    p = make_problem(8, 8, 8, log10k=(-14.0, 1.0, 1.0), seed=2)
+@pytest.mark.parametrize("dims", [(8, 8, 8), (10, 9, 7), (6, 5, 3), (10, 10, 10)],
+                         ids=lambda d: "x".join(map(str, d)))
+def test_exact_when_level1_is_solved_exactly(dims, port):
+    """The dense direct solve below level 0's size (at most 512 rows):
+    level 1 (n/2 rows: 256, 315, 45 and 500 -- whole and ragged blocks of
+    the Gauss-Jordan steps, up to the dense limit) is solved exactly, so one
+    cycle is A^-1 (to the cycle's rounding) and the flexible CG needs two
+    steps."""
+    p = make_problem(*dims, log10k=(-14.0, 1.0, 1.0), seed=2)
     perm, ind, b = port.assemble(p)
     cnt, col, ele = port.pack(perm, ind)
     ptr = np.zeros(p.n + 1, np.int64)
     ptr[1:] = np.cumsum(cnt)
     A = sp.csr_matrix((ele, col, ptr), shape=(p.n, p.n)).toarray()
-    s = _solver(tol=1e-10, coarse_direct=300)
+    s = _solver(tol=1e-10, coarse_direct=min(512, p.n - 1))
     s.assemble(p)
     s.setup()
     f = np.random.default_rng(0).standard_normal(p.n)
