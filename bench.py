@@ -37,7 +37,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes (read + write) per cell of one k_g7_spmv_dot launch, from an
+# DRAM bytes (read + write) per cell of one k_g7_spmv_dot2 launch, from an
 # ncu --set full capture of the same kernel on config 2 at 192^3 (7.08M
 # cells, 328 MB): the launch is linear in cells, so bench scales it.
 SPMV_TRAFFIC_B_PER_CELL = 46.4
@@ -129,6 +129,7 @@ def kernel_bytes(name, level, info, precision):
     n0 = info[0][0]
     table = {
         "k_g7_spmv_dot": 48 * n0,                       # 4 coefficients + s + v
+        "k_g7_spmv_dot2": 48 * n0,                      # the same on x-adjacent cell pairs
         "k_update": 48 * n0 + (4 if precision == 1 else 16) * n0,  # x, r, s, v + FP32 r / FP64 seed
         "k_g7_resid": (56 + (4 if precision == 1 else 16)) * n0,   # runs on check iterations
         "k_finish_z": (T + 16) * n0,                    # z, r, v
@@ -502,8 +503,9 @@ def run_ours(args):
             "speedup_chosen_vs_plain": ch["value"] / results["plain_fp64"]["value"],
             "e2e": e2e,
             "roofline": {"bound": "hbm",
-                         "kernel": "k_g7_spmv_dot (L0 SpMV FP64 of the CG, 7-point form; "
-                                   "algorithmic bytes 48 per cell)",
+                         "kernel": "k_g7_spmv_dot2 (L0 SpMV FP64 of the CG, 7-point form, "
+                                   "two x-adjacent cells per thread; algorithmic bytes 48 "
+                                   "per cell)",
                          "achieved": round(achieved, 1), "peak": peak,
                          "peak_source": peak_src, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),

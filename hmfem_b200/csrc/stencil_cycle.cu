@@ -494,6 +494,81 @@ k_g7_spmv_dot(G7v<double> g, int n, const double *__restrict__ x, double *__rest
     grid_reduce_sum(d, part, &ctl->tickets[RED_TAU], [&](double t) { tau_finish(ctl, t); });
 }
 
+// The same SpMV for nx even, two x-adjacent cells (s, s + 1; s even) per
+// thread with 16-byte loads: the pair's x values, those one row and one
+// plane away and the pair's coefficients arrive in 10 loads of 16 bytes and
+// 3 of 8 instead of 28 of 8 (more bytes in flight per thread).  Each cell's
+// sum keeps the terms, operations and order of g7_row (d,l,c,r,u,t,b from
+// 0.0), so y is bit-identical; tau's partial sums group differently.
+// DOT = false: y = A x alone (the inspection SpMV).
+__device__ __forceinline__ double2 ld2(const double *p)
+{
+    return *reinterpret_cast<const double2 *>(p);
+}
+
+template <bool DOT>
+__global__ void __launch_bounds__(256)
+k_g7_spmv_dot2(G7v<double> g, int n, const double *__restrict__ x, double *__restrict__ y,
+               Ctl *ctl, double *part)
+{
+    PDL_ENTRY();
+    if (finished(ctl)) return;
+    using A = Ar<double>;
+    const long nx = g.nx, nxy = (long)g.nx * g.ny;
+    const double2 z2 = make_double2(0.0, 0.0);
+    double d = 0.0;
+    GRID_STRIDE(h, (long)n >> 1) {
+        const long s = 2 * h;
+        int i, j, k;
+        cell_ijk((unsigned)s, g.nx, g.ny, i, j, k);  // i even, s + 1 = (i + 1, j, k)
+        const bool hd = j > 0, hu = j < g.ny - 1, ht = k < g.nz - 1, hb = k > 0;
+        const bool hl = i > 0, hr = i + 2 < g.nx;    // -x of s, +x of s + 1
+        const double2 xd = hd ? ld2(x + s - nx) : z2;
+        const double xl = hl ? x[s - 1] : 0.0;
+        const double2 xc = ld2(x + s);
+        const double xr = hr ? x[s + 2] : 0.0;
+        const double2 xu = hu ? ld2(x + s + nx) : z2;
+        const double2 xt = ht ? ld2(x + s + nxy) : z2;
+        const double2 xb = hb ? ld2(x + s - nxy) : z2;
+        const double2 ad = hd ? ld2(g.cf + slice_at(s - nx, 2, 4)) : z2;
+        const double al = hl ? g.cf[slice_at(s - 1, 1, 4)] : 0.0;
+        const double2 ac = ld2(g.cf + slice_at(s, 0, 4));
+        const double2 ar = ld2(g.cf + slice_at(s, 1, 4));  // s -> s + 1, s + 1 -> s + 2
+        const double2 au = hu ? ld2(g.cf + slice_at(s, 2, 4)) : z2;
+        const double2 at = ht ? ld2(g.cf + slice_at(s, 3, 4)) : z2;
+        const double2 ab = hb ? ld2(g.cf + slice_at(s - nxy, 3, 4)) : z2;
+        double t0 = 0.0, t1 = 0.0;
+        auto acc = [&](double &t, double a, double xv) { t = A::add(t, A::mul(a, xv)); };
+        if (hd) acc(t0, ad.x, xd.x);
+        if (hl) acc(t0, al, xl);
+        acc(t0, ac.x, xc.x);
+        acc(t0, ar.x, xc.y);
+        if (hu) acc(t0, au.x, xu.x);
+        if (ht) acc(t0, at.x, xt.x);
+        if (hb) acc(t0, ab.x, xb.x);
+        if (hd) acc(t1, ad.y, xd.y);
+        acc(t1, ar.x, xc.x);  // -x of s + 1: the +x coupling of s
+        acc(t1, ac.y, xc.y);
+        if (hr) acc(t1, ar.y, xr);
+        if (hu) acc(t1, au.y, xu.y);
+        if (ht) acc(t1, at.y, xt.y);
+        if (hb) acc(t1, ab.y, xb.y);
+        *reinterpret_cast<double2 *>(y + s) = make_double2(t0, t1);
+        if (DOT) {
+            d += xc.x * t0;
+            d += xc.y * t1;
+        }
+    }
+    if (DOT)
+        grid_reduce_sum(d, part, &ctl->tickets[RED_TAU], [&](double t) { tau_finish(ctl, t); });
+}
+
+// the pair form applies: nx even, every array 16-byte aligned
+bool g7_pairs(const G7v<double> &g, const double *x, const double *y)
+{
+    return g.nx % 2 == 0 && (((uintptr_t)x | (uintptr_t)y | (uintptr_t)g.cf) & 15) == 0;
+}
+
 // plain y = A x (inspection)
 __global__ void __launch_bounds__(256)
 k_g7_spmv(G7v<double> g, int n, const double *__restrict__ x, double *__restrict__ y)
@@ -847,8 +922,15 @@ int g7_spmv_dot(const Level &L, const double *x, double *y, Ctl *ctl, double *pa
                  cudaStream_t st)
 {
     const int n = L.A.n;
-    const int nblk = occ_blocks((const void *)k_g7_spmv_dot, n, 256, kRedBlocks);
-    launch_pdl(k_g7_spmv_dot, nblk, 256, st, g7v<double>(L.g7), n, x, y, ctl, part);
+    const auto gv = g7v<double>(L.g7);
+    if (g7_pairs(gv, x, y)) {
+        const int nblk =
+            occ_blocks((const void *)k_g7_spmv_dot2<true>, (long)n / 2, 256, kRedBlocks);
+        launch_pdl(k_g7_spmv_dot2<true>, nblk, 256, st, gv, n, x, y, ctl, part);
+    } else {
+        const int nblk = occ_blocks((const void *)k_g7_spmv_dot, n, 256, kRedBlocks);
+        launch_pdl(k_g7_spmv_dot, nblk, 256, st, gv, n, x, y, ctl, part);
+    }
     HM_LAUNCHED();
     return HMFEM_OK;
 }
@@ -886,8 +968,16 @@ int g7_resid(const Level &L, const double *b, const double *x, double *r, Ctl *c
 int g7_spmv(const Level &L, const double *x, double *y, cudaStream_t st)
 {
     const int n = L.A.n;
-    const int nblk = occ_blocks((const void *)k_g7_spmv, n, 256, kRedBlocks);
-    launch_pdl(k_g7_spmv, nblk, 256, st, g7v<double>(L.g7), n, x, y);
+    const auto gv = g7v<double>(L.g7);
+    if (g7_pairs(gv, x, y)) {  // the CG's kernel without its dot
+        const int nblk =
+            occ_blocks((const void *)k_g7_spmv_dot2<false>, (long)n / 2, 256, kRedBlocks);
+        launch_pdl(k_g7_spmv_dot2<false>, nblk, 256, st, gv, n, x, y, (Ctl *)nullptr,
+                   (double *)nullptr);
+    } else {
+        const int nblk = occ_blocks((const void *)k_g7_spmv, n, 256, kRedBlocks);
+        launch_pdl(k_g7_spmv, nblk, 256, st, gv, n, x, y);
+    }
     HM_LAUNCHED();
     return HMFEM_OK;
 }
