@@ -136,6 +136,7 @@ def kernel_bytes(name, level, info, precision):
         "k_sdir": (T + 16) * n0,                        # z, s in/out
         "k_g7_sred": (T + 3 * vb + T // 2 + T) * n,     # f, couplings, F-half D^-1, fc + seed
         "k_g7_sprol2": (3 * vb + T + T // 2 + T) * n,   # couplings, F-half f/D^-1, uc, z
+        "k_g7_sprol2_zd": (3 * vb + T + T // 2 + T + 16) * n,  # the same + the CG's r, v for the dots
         "k_g7_pre": (4 * vb + 3 * T) * n,
         "k_g7_post": (4 * vb + 4 * T) * n,
         "k_g7_restrict": T * n + 3 * T * nc,

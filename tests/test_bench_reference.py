@@ -75,3 +75,16 @@ def test_reference_arm_prints_one_line_on_the_bench_configuration():
     assert d["config"]["workload"] == "config2 16^3 lognormal+8 conduits"
     assert d["value"] > 0 and d["cpu_baseline"]["max_relres"] <= 1e-10
     assert d["e2e"]["value"] == d["value"]
+
+
+def test_kernel_byte_models_of_the_level0_kernels():
+    """The bench's algorithmic bytes of the CG's pair SpMV and of the
+    level-0 prolongation that also forms the CG's dots, from their
+    demangled names."""
+    import bench
+    n0 = 1000
+    info = [(n0, 7 * n0, 0), (n0 // 2, 19 * n0 // 2, n0)]
+    assert bench.kernel_bytes("void (anonymous namespace)::k_g7_spmv_dot2<true>(...)", -1,
+                              info, 1) == 48 * n0
+    assert bench.kernel_bytes("void (anonymous namespace)::k_g7_sprol2_zd<float, float>(...)",
+                              0, info, 1) == 38 * n0
